@@ -1,0 +1,203 @@
+"""B200-native face-detection cascade (Compact CNN Cascade, arXiv:1508.01292).
+
+`FaceDetector` mirrors the reference's public class CompactCNNLib::FaceDetector
+(src/CNNObjectDetector/CompactCNNLibAPI_v2.h:35-190): the same method names, parameter fields and
+return conventions (Init/Detect/Clear return 0 or the face count, -1 on error). Every call goes
+through the C ABI in include/ccnn.h to hand-written sm_100a kernels; nothing runs on the CPU.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import CCNNError, Face, Image, Params
+
+__all__ = ["FaceDetector", "Param", "synth_frame", "CCNNError", "default_params"]
+
+Pipeline = {"CPU": 0, "GPU": 1, "GPU_CPU": 2}
+DetectMode = {"disable": 0, "sync": 1, "async": 2}
+DetectPrecision = {"def": 0, "low": 1, "normal": 2, "high": 3, "ultra": 4}
+
+
+def default_params():
+    """FaceDetector::Param defaults (CompactCNNLibAPI_v2.h:97-161)."""
+    p = Params()
+    _capi.lib().ccnn_default_params(ctypes.byref(p))
+    return p
+
+
+Param = default_params
+
+
+def _as_image(img):
+    a = np.ascontiguousarray(img) if not img.flags["C_CONTIGUOUS"] else img
+    if a.dtype != np.uint8 or a.ndim not in (2, 3):
+        raise ValueError("image must be a uint8 HxW or HxWxC array")
+    ch = 1 if a.ndim == 2 else a.shape[2]
+    im = Image(a.shape[1], a.shape[0], ch, a.ctypes.data, a.strides[0])
+    return im, a
+
+
+class FaceDetector:
+    """CompactCNNLib::FaceDetector over the B200 path; one handle per instance (no global singleton)."""
+
+    def __init__(self):
+        self._h = None
+        self._param = None
+        self._models = [None, None, None]
+
+    # ---- lifecycle ----
+    def Init(self, param=None, models=None):
+        """FaceDetector::Init (CompactCNNLibAPI_v2.cpp:373-407). Returns 0 or -1."""
+        if self._h is not None:
+            self.Clear()
+        self._param = param if param is not None else default_params()
+        if models is not None:
+            self._models = list(models)
+        arr = (ctypes.c_char_p * 3)(*[(m.encode() if m else None) for m in self._models])
+        h = ctypes.c_void_p()
+        st = _capi.lib().ccnn_create(ctypes.byref(self._param), arr, ctypes.byref(h))
+        if st != _capi.OK:
+            self.last_status = st
+            return -1
+        self._h = h
+        return 0
+
+    def Clear(self):
+        if self._h is None:
+            return -1
+        _capi.lib().ccnn_destroy(self._h)
+        self._h = None
+        return 0
+
+    def isEmpty(self):
+        return self._h is None
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass
+
+    # ---- detection ----
+    def Detect(self, img, capacity=4096):
+        """FaceDetector::Detect: returns a list of (x, y, width, height, score); raises on error."""
+        if self._h is None:
+            raise CCNNError(_capi.ERR_INVALID_ARG, "Detect (detector not initialised)")
+        im, _keep = _as_image(img)
+        faces = (Face * capacity)()
+        n = ctypes.c_int(0)
+        st = _capi.lib().ccnn_detect(self._h, ctypes.byref(im), faces, capacity, ctypes.byref(n))
+        _capi.check(st, "ccnn_detect")
+        return [(f.x, f.y, f.width, f.height, f.score) for f in faces[: min(n.value, capacity)]]
+
+    def DetectBatch(self, imgs, capacity=4096):
+        """Several frames of one size through the pipelined batch entry point."""
+        if not imgs:
+            return []
+        keep = []
+        arr = (Image * len(imgs))()
+        for i, img in enumerate(imgs):
+            im, a = _as_image(img)
+            arr[i] = im
+            keep.append(a)
+        faces = (Face * (capacity * len(imgs)))()
+        ns = (ctypes.c_int * len(imgs))()
+        st = _capi.lib().ccnn_detect_batch(self._h, arr, len(imgs), faces, capacity, ns)
+        _capi.check(st, "ccnn_detect_batch")
+        out = []
+        for i in range(len(imgs)):
+            fs = faces[i * capacity: i * capacity + min(ns[i], capacity)]
+            out.append([(f.x, f.y, f.width, f.height, f.score) for f in fs])
+        return out
+
+    # ---- parameters ----
+    def getParam(self):
+        p = Params()
+        _capi.check(_capi.lib().ccnn_get_params(self._h, ctypes.byref(p)), "ccnn_get_params")
+        return p
+
+    def setParam(self, param):
+        _capi.check(_capi.lib().ccnn_set_params(self._h, ctypes.byref(param)), "ccnn_set_params")
+
+    def getMaxImageSize(self):
+        p = self.getParam()
+        return (p.max_image_width, p.max_image_height)
+
+    def setMaxImageSize(self, size):
+        _capi.check(_capi.lib().ccnn_set_max_image_size(self._h, int(size[0]), int(size[1])), "ccnn_set_max_image_size")
+
+    def getMinObjectHeight(self):
+        return self.getParam().min_face_height
+
+    def setMinObjectHeight(self, v):
+        _capi.check(_capi.lib().ccnn_set_min_object_height(self._h, int(v)), "ccnn_set_min_object_height")
+
+    def getMaxObjectHeight(self):
+        return self.getParam().max_face_height
+
+    def setMaxObjectHeight(self, v):
+        _capi.check(_capi.lib().ccnn_set_max_object_height(self._h, int(v)), "ccnn_set_max_object_height")
+
+    def getNumThreads(self):
+        return self.getParam().num_threads
+
+    def setNumThreads(self, v):
+        _capi.check(_capi.lib().ccnn_set_num_threads(self._h, int(v)), "ccnn_set_num_threads")
+
+    def getGrayImage32F(self):
+        """The fp32 gray image of the last frame, copied to a numpy array."""
+        w, h = ctypes.c_int(), ctypes.c_int()
+        p = self.getParam()
+        out = np.empty(p.max_image_width * p.max_image_height, np.float32)
+        _capi.check(_capi.lib().ccnn_get_gray_host(self._h, out.ctypes.data, out.size, ctypes.byref(w), ctypes.byref(h)),
+                    "ccnn_get_gray_host")
+        return out[: w.value * h.value].reshape(h.value, w.value)
+
+    @staticmethod
+    def CNTKDump2Binary(binary_file, cntk_model_dump):
+        """The offline CNTK-dump converter is not part of the detection path."""
+        raise NotImplementedError("model conversion (cnn_models_converter.cpp) is offline tooling outside this path")
+
+    # ---- inspection (include/ccnn_inspect.h) ----
+    def levels(self):
+        L = _capi.lib()
+        buf = (_capi.LevelInfo * 512)()
+        n = ctypes.c_int()
+        _capi.check(L.ccnn_inspect_levels(self._h, buf, 512, ctypes.byref(n)), "ccnn_inspect_levels")
+        return [(b.width, b.height, b.scale, b.resp_width, b.resp_height) for b in buf[: n.value]]
+
+    def response_map(self, level):
+        info = self.levels()[level]
+        out = np.empty(info[3] * info[4], np.float32)
+        _capi.check(_capi.lib().ccnn_inspect_response(self._h, level, out.ctypes.data, out.size), "ccnn_inspect_response")
+        return out.reshape(info[4], info[3])
+
+    def candidates(self):
+        L = _capi.lib()
+        n = ctypes.c_int()
+        _capi.check(L.ccnn_inspect_candidates(self._h, None, 0, ctypes.byref(n)), "ccnn_inspect_candidates")
+        buf = (_capi.CandidateInfo * max(1, n.value))()
+        _capi.check(L.ccnn_inspect_candidates(self._h, buf, n.value, ctypes.byref(n)), "ccnn_inspect_candidates")
+        return [(c.level, c.x, c.y, c.score, c.accepted, c.check_score, c.knn) for c in buf[: n.value]]
+
+    def raw_detections(self):
+        L = _capi.lib()
+        n = ctypes.c_int()
+        _capi.check(L.ccnn_inspect_raw_detections(self._h, None, 0, ctypes.byref(n)), "ccnn_inspect_raw_detections")
+        buf = (_capi.Detection * max(1, n.value))()
+        _capi.check(L.ccnn_inspect_raw_detections(self._h, buf, n.value, ctypes.byref(n)), "ccnn_inspect_raw_detections")
+        return [(d.x, d.y, d.width, d.height, d.score, d.scale, d.knn, d.num_detect) for d in buf[: n.value]]
+
+
+def synth_frame(width, height, seed, n_faces, min_face, max_face, channels=3):
+    """Seeded synthetic frame (uint8 HxWxC, BGR order for 3 channels) and its face patches."""
+    S = _capi.synth()
+    shape = (height, width) if channels == 1 else (height, width, channels)
+    img = np.empty(shape, np.uint8)
+    faces = (_capi.SynthFace * max(1, n_faces))()
+    st = S.ccnn_synth_frame(img.ctypes.data, width, height, channels, width * channels, seed, n_faces, min_face, max_face,
+                            faces)
+    if st < 0:
+        raise ValueError(f"ccnn_synth_frame failed ({st})")
+    return img, [(f.cx, f.cy, f.w, f.h, f.angle_deg, f.contrast) for f in faces[:n_faces]]

@@ -1,0 +1,212 @@
+// extern "C" boundary: include/ccnn.h and include/ccnn_inspect.h.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "detector.h"
+#include "replay.cuh"
+
+namespace ccnn {
+const char* last_error_cstr();
+}
+
+struct ccnn_detector {
+    ccnn::Detector det;
+};
+
+using ccnn::set_error;
+
+extern "C" {
+
+CCNN_API const char* ccnn_version(void) { return "compactcnncascade_b200 0.1 (sm_100a)"; }
+
+CCNN_API const char* ccnn_last_error(void) { return ccnn::last_error_cstr(); }
+
+CCNN_API void ccnn_default_params(ccnn_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->max_image_width = 1920;
+    p->max_image_height = 1080;
+    p->min_face_height = 80;
+    p->max_face_height = 0;
+    p->scale_factor = 1.15f;
+    p->min_neighbors = 2;
+    p->detect_precision = CCNN_PRECISION_HIGH;
+    p->treshold[0] = -1.5f;
+    p->treshold[1] = -1.25f;
+    p->treshold[2] = -1.0f;
+    p->drop_detect = 1;
+    p->equalize = 1;
+    p->reflection = 1;
+    p->pipeline = CCNN_PIPELINE_GPU;
+    p->detect_mode = CCNN_DETECT_ASYNC;
+    p->num_threads = 2;
+    p->index_output[0] = 1;
+    p->index_output[1] = 0;
+    p->index_output[2] = 0;
+    p->device_info = 1;
+    p->cuda_device_id = 0;
+    p->cl_platform_id = -1;
+    p->cl_device_id = -1;
+    p->facial_analysis = 0;
+}
+
+CCNN_API ccnn_status ccnn_create(const ccnn_params* params, const char* const* model_paths, ccnn_handle* out) {
+    if (!params || !out) {
+        set_error("null argument");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    ccnn_detector* h = new (std::nothrow) ccnn_detector();
+    if (!h) {
+        set_error("out of host memory");
+        return CCNN_ERR_OOM;
+    }
+    ccnn_status st = h->det.create(*params, model_paths);
+    if (st != CCNN_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return CCNN_OK;
+}
+
+CCNN_API ccnn_status ccnn_destroy(ccnn_handle h) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    delete h;
+    return CCNN_OK;
+}
+
+CCNN_API ccnn_status ccnn_detect(ccnn_handle h, const ccnn_image* img, ccnn_face* faces, int capacity, int* n_faces) {
+    if (!h || !img) {
+        set_error("null argument");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    return h->det.detect(*img, false, nullptr, faces, capacity, n_faces);
+}
+
+CCNN_API ccnn_status ccnn_detect_device(ccnn_handle h, const ccnn_image* img, void* stream, ccnn_face* faces, int capacity, int* n_faces) {
+    if (!h || !img) {
+        set_error("null argument");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    return h->det.detect(*img, true, (cudaStream_t)stream, faces, capacity, n_faces);
+}
+
+CCNN_API ccnn_status ccnn_detect_batch(ccnn_handle h, const ccnn_image* imgs, int n_images, ccnn_face* faces, int capacity_per_image,
+                                       int* n_faces) {
+    if (!h) {
+        set_error("null argument");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    return h->det.detect_batch(imgs, n_images, faces, capacity_per_image, n_faces);
+}
+
+CCNN_API ccnn_status ccnn_get_gray_device(ccnn_handle h, const float** data, int* cols, int* rows, size_t* step) {
+    if (!h || !data || !cols || !rows || !step) return CCNN_ERR_INVALID_ARG;
+    return h->det.get_gray_device(data, cols, rows, step);
+}
+
+CCNN_API ccnn_status ccnn_get_gray_host(ccnn_handle h, float* out, int capacity, int* cols, int* rows) {
+    if (!h || !out || !cols || !rows) return CCNN_ERR_INVALID_ARG;
+    return h->det.get_gray_host(out, capacity, cols, rows);
+}
+
+CCNN_API ccnn_status ccnn_get_params(ccnn_handle h, ccnn_params* out) {
+    if (!h || !out) return CCNN_ERR_INVALID_ARG;
+    return h->det.get_params(out);
+}
+CCNN_API ccnn_status ccnn_set_params(ccnn_handle h, const ccnn_params* p) {
+    if (!h || !p) return CCNN_ERR_INVALID_ARG;
+    return h->det.set_params(*p);
+}
+CCNN_API ccnn_status ccnn_set_max_image_size(ccnn_handle h, int width, int height) {
+    if (!h || width <= 0 || height <= 0) return CCNN_ERR_INVALID_ARG;
+    return h->det.set_max_image_size(width, height);
+}
+CCNN_API ccnn_status ccnn_set_min_object_height(ccnn_handle h, int v) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    return h->det.set_min_object_height(v);
+}
+CCNN_API ccnn_status ccnn_set_max_object_height(ccnn_handle h, int v) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    return h->det.set_max_object_height(v);
+}
+CCNN_API ccnn_status ccnn_set_num_threads(ccnn_handle h, int v) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    return h->det.set_num_threads(v);
+}
+
+// ---- inspection ----
+
+CCNN_API ccnn_status ccnn_gray_u8_to_f32(const unsigned char* d_src, int cols, int rows, int channels, size_t src_step, float* d_dst,
+                                         size_t dst_step, void* stream) {
+    if (!d_src || !d_dst || cols <= 0 || rows <= 0 || (dst_step % 64) != 0) {
+        set_error("invalid arguments (dst_step must be a multiple of 64 bytes)");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaError_t e = ccnn::launch_gray(d_src, (int)src_step, cols, rows, channels, d_dst, (int)(dst_step / sizeof(float)), (cudaStream_t)stream);
+    if (e == cudaErrorInvalidValue) {
+        set_error("unsupported channel count");
+        return CCNN_ERR_UNSUPPORTED;
+    }
+    if (e == cudaErrorMisalignedAddress) {
+        set_error("buffers must be 64-byte aligned with a source step that is a multiple of 64");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    ccnn_status st = ccnn::cuda_status(e, "gray kernel");
+    if (st != CCNN_OK) return st;
+    return ccnn::cuda_status(cudaStreamSynchronize((cudaStream_t)stream), "gray kernel");
+}
+
+CCNN_API ccnn_status ccnn_resize_f32(const float* d_src, int src_cols, int src_rows, size_t src_step, float* d_dst, int dst_cols,
+                                     int dst_rows, size_t dst_step, int type, void* stream) {
+    if (!d_src || !d_dst || src_cols < 2 || src_rows < 2 || dst_cols <= 0 || dst_rows <= 0 || (src_step % 4) || (dst_step % 4)) {
+        set_error("invalid arguments");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaError_t e = ccnn::launch_resize_f32(d_src, (int)(src_step / 4), src_cols, src_rows, d_dst, (int)(dst_step / 4), dst_cols, dst_rows,
+                                            type, (cudaStream_t)stream);
+    ccnn_status st = ccnn::cuda_status(e, "resize kernel");
+    if (st != CCNN_OK) return st;
+    return ccnn::cuda_status(cudaStreamSynchronize((cudaStream_t)stream), "resize kernel");
+}
+
+CCNN_API ccnn_status ccnn_stage1_forward(ccnn_handle h, const float* d_img, int cols, int rows, size_t step, float* d_resp, int resp_cap,
+                                         int* resp_cols, int* resp_rows, void* stream) {
+    if (!h || !d_img || !d_resp || !resp_cols || !resp_rows) return CCNN_ERR_INVALID_ARG;
+    return h->det.stage1_forward(d_img, cols, rows, step, d_resp, resp_cap, resp_cols, resp_rows, (cudaStream_t)stream);
+}
+
+CCNN_API ccnn_status ccnn_inspect_levels(ccnn_handle h, ccnn_level_info* out, int capacity, int* n_levels) {
+    if (!h || !n_levels || (capacity > 0 && !out)) return CCNN_ERR_INVALID_ARG;
+    return h->det.inspect_levels(out, capacity, n_levels);
+}
+CCNN_API ccnn_status ccnn_inspect_response(ccnn_handle h, int level, float* out, int capacity) {
+    if (!h || !out) return CCNN_ERR_INVALID_ARG;
+    return h->det.inspect_response(level, out, capacity);
+}
+CCNN_API ccnn_status ccnn_inspect_candidates(ccnn_handle h, ccnn_candidate* out, int capacity, int* n) {
+    if (!h || !n || (capacity > 0 && !out)) return CCNN_ERR_INVALID_ARG;
+    return h->det.inspect_candidates(out, capacity, n);
+}
+CCNN_API ccnn_status ccnn_inspect_raw_detections(ccnn_handle h, ccnn_detection* out, int capacity, int* n) {
+    if (!h || !n || (capacity > 0 && !out)) return CCNN_ERR_INVALID_ARG;
+    return h->det.inspect_raw(out, capacity, n);
+}
+
+CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm) {
+    if (n < 0 || (n > 0 && (!scales || !perm))) return CCNN_ERR_INVALID_ARG;
+    std::vector<ccnn::Det> v(n);
+    for (int i = 0; i < n; ++i) {
+        v[i] = ccnn::make_det(i, 0, 1, 1, 0.f, scales[i], 0);
+    }
+    if (n > 16) ccnn::introsort_scale_desc(v.data(), n);  // n <= 16: insertion sort of a sorted list
+    else ccnn::insertion_sort(v.data(), 0, n);
+    for (int i = 0; i < n; ++i) perm[i] = v[i].x;
+    return CCNN_OK;
+}
+
+}  // extern "C"

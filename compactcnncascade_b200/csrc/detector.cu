@@ -1,0 +1,818 @@
+// Host runtime of the B200 detection path.
+//
+// Mirrors the reference's CNNDetector lifecycle (src/CNNObjectDetector/cnn_detector_v3.cpp):
+// Init (:907-985) with the precision rules (:922-963) and InitScales (:289-346); Detect
+// (:2483-2813) with its re-initialisation rules (frame larger than max_image_size :2499-2513,
+// multi-channel frame while gray_image_only :2531-2546) and the level-count state num_scales
+// that RunCPUDetect lowers when a level is smaller than the stage-2/3 window (:2083-2088).
+// The parameters are FaceDetector::Param converted as paramConverter does
+// (CompactCNNLibAPI_v2.cpp:280-329).
+//
+// Per frame the device runs: gray conversion -> stage-1 front (all levels) -> stage-1 back (all
+// levels) -> candidate count -> candidate write -> stage-2/3 windows -> replay/sort/merge, plus
+// the download of the face count and the first faces. The chain is captured once per
+// (slot, pyramid plan) as a CUDA graph and replayed; only the frame upload is issued per call.
+#include "detector.h"
+#include "model.h"
+
+#include <algorithm>
+#include <cstring>
+
+namespace ccnn {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error_cstr() { return g_last_error.c_str(); }
+
+ccnn_status cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CCNN_OK;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return CCNN_ERR_OOM;
+    return CCNN_ERR_CUDA;
+}
+
+#define CCNN_CUDA(call)                                         \
+    do {                                                        \
+        ccnn_status _s = cuda_status((call), #call);            \
+        if (_s != CCNN_OK) return _s;                           \
+    } while (0)
+
+namespace {
+constexpr int kChunk = 2048;  // candidate-scan chunk (response pixels per block)
+inline long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+// Size * float with truncation (type.h:200-203)
+inline void size_scale(int w, int h, float s, int* ow, int* oh) {
+    *ow = (int)((float)w * s);
+    *oh = (int)((float)h * s);
+}
+}  // namespace
+
+Detector::~Detector() { clear(); }
+
+void Detector::free_slot(Slot& s) {
+    if (s.exec) cudaGraphExecDestroy(s.exec);
+    cudaFree(s.d_in);
+    cudaFree(s.d_gray);
+    cudaFree(s.d_s1);
+    cudaFree(s.d_resp);
+    cudaFree(s.d_counts);
+    cudaFree(s.d_cands);
+    cudaFree(s.d_ncand);
+    cudaFree(s.d_results);
+    cudaFree(s.D);
+    cudaFree(s.R);
+    cudaFree(s.M);
+    cudaFree(s.F);
+    cudaFree(s.first_dec);
+    cudaFree(s.survivors);
+    cudaFree(s.checked);
+    cudaFree(s.d_nraw);
+    cudaFree(s.d_faces);
+    cudaFree(s.d_nfaces);
+    cudaFreeHost(s.h_nfaces);
+    cudaFreeHost(s.h_faces);
+    if (s.done) cudaEventDestroy(s.done);
+    if (s.st) cudaStreamDestroy(s.st);
+    s = Slot();
+}
+
+void Detector::clear() {
+    if (!inited_) return;
+    cudaSetDevice(device_);
+    for (auto& s : slots_) {
+        if (s.st) cudaStreamSynchronize(s.st);
+        free_slot(s);
+    }
+    for (auto& kv : plans_) {
+        cudaFree(kv.second->d_levels);
+        cudaFree(kv.second->d_chunks);
+    }
+    plans_.clear();
+    scales_.clear();
+    inited_ = false;
+}
+
+ccnn_status Detector::apply_precision() {
+    // paramConverter (CompactCNNLibAPI_v2.cpp:300-326) then Init's precision rules (:922-963)
+    type_check_ = 1;
+    min_num_detect_ = 1;
+    drop_detect_ = api_.drop_detect != 0;
+    equalize_ = api_.equalize != 0;
+    reflection_ = api_.reflection != 0;
+    adapt_min_neighbors_ = false;
+    double_check_ = true;
+    detect_enabled_ = api_.detect_mode != CCNN_DETECT_DISABLE;
+    merger_detect_ = detect_enabled_;
+    if (api_.detect_precision == CCNN_PRECISION_DEF) {
+        gray_image_only_ = true;
+        type_check_ = 1;
+        equalize_ = true;
+        reflection_ = true;
+        adapt_min_neighbors_ = true;
+        double_check_ = true;
+        drop_detect_ = false;
+        min_num_detect_ = 1;
+        merger_detect_ = true;
+    }
+    switch (api_.detect_precision) {
+        case CCNN_PRECISION_LOW: type_check_ = 0; drop_detect_ = false; break;
+        case CCNN_PRECISION_NORMAL: type_check_ = 1; break;
+        case CCNN_PRECISION_HIGH: type_check_ = 2; break;
+        case CCNN_PRECISION_ULTRA: type_check_ = 2; min_num_detect_ = 2; break;
+        default: break;
+    }
+    if (!detect_enabled_) drop_detect_ = false;
+    return CCNN_OK;
+}
+
+ccnn_status Detector::create(const ccnn_params& p, const char* const* model_paths) {
+    api_ = p;
+    if (p.facial_analysis) {
+        set_error("facial_analysis is not supported by this detector");
+        return CCNN_ERR_UNSUPPORTED;
+    }
+    for (int i = 0; i < 3; ++i) {
+        const char* mp = model_paths ? model_paths[i] : nullptr;
+        static const char* kNames[3] = {"cnn4face1_cntk.bin", "cnn4face2_cntk.bin", "cnn4face3_cntk.bin"};
+        model_paths_[i] = (mp && mp[0]) ? std::string(mp) : bundled_model_dir() + "/" + kNames[i];
+    }
+    gray_image_only_ = true;
+    max_w_ = p.max_image_width;
+    max_h_ = p.max_image_height;
+    return init();
+}
+
+ccnn_status Detector::init() {
+    apply_precision();
+    device_ = api_.cuda_device_id;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        set_error("no CUDA device available (this detector has no CPU path)");
+        return CCNN_ERR_CUDA;
+    }
+    if (device_ < 0 || device_ >= ndev) {
+        set_error("cuda_device_id out of range");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    CCNN_CUDA(cudaSetDevice(device_));
+    if (max_w_ <= 0 || max_h_ <= 0) {
+        set_error("max_image_size must be positive");
+        return CCNN_ERR_INVALID_ARG;
+    }
+
+    // models (InitCNN / InitCNNCheck)
+    RawModel m[3];
+    std::string err;
+    for (int i = 0; i < 3; ++i)
+        if (!load_model_file(model_paths_[i], &m[i], &err)) {
+            set_error(err);
+            return CCNN_ERR_MODEL;
+        }
+    if (!wn_) wn_.reset(new WindowNets());
+    if (!pack_model(m[0], api_.index_output[0], &w1_, &err) || !pack_model(m[1], api_.index_output[1], &wn_->s2, &err) ||
+        !pack_model(m[2], api_.index_output[2], &wn_->s3, &err)) {
+        set_error(err);
+        return CCNN_ERR_MODEL;
+    }
+    pat_w_ = m[0].min_w;
+    pat_h_ = m[0].min_h;
+    if (pat_w_ != kPatW || pat_h_ != kPatH || m[1].min_w != 36 || m[1].min_h != 40 || m[2].min_w != 36 || m[2].min_h != 40) {
+        set_error("model window sizes differ from the cascade prototype (23x27 / 36x40)");
+        return CCNN_ERR_MODEL;
+    }
+    if (detect_enabled_) {
+        ext_w_ = 36 + kExtOff;
+        ext_h_ = 40 + kExtOff;
+    } else {
+        ext_w_ = pat_w_;
+        ext_h_ = pat_h_;
+    }
+
+    // InitScales (cnn_detector_v3.cpp:289-346)
+    scales_.clear();
+    input_downscale_ = false;
+    input_scale_ = 0.f;
+    float max_scale = 1.f;
+    if (api_.min_face_height > 0) {
+        max_scale = (float)pat_h_ / (float)api_.min_face_height;
+        max_scale = 3.f > max_scale ? max_scale : 3.f;
+        if (gray_image_only_ && max_scale < 0.8f) {
+            input_downscale_ = true;
+            input_scale_ = max_scale;
+            max_scale = 1.f;
+        }
+    }
+    float min_scale = api_.max_face_height > 0 ? (float)pat_h_ / (float)api_.max_face_height : (float)pat_h_ / (float)max_h_;
+    min_scale = max_scale > min_scale ? min_scale : max_scale;
+    if (api_.scale_factor < 1.f) api_.scale_factor = 1.1f;
+    float scale = max_scale;
+    if (api_.scale_factor != 1.f) {
+        while (scale > min_scale) {
+            scales_.push_back(scale);
+            scale /= api_.scale_factor;
+        }
+    } else {
+        scales_.push_back(scale);
+    }
+    if (scales_.empty()) {
+        set_error("invalid configuration: empty scale list");
+        return CCNN_ERR_CONFIG;
+    }
+    num_scales_ = (int)scales_.size();
+
+    cfg_.thr1 = api_.treshold[0];
+    cfg_.thr2 = api_.treshold[1];
+    cfg_.thr3 = api_.treshold[2];
+    cfg_.type_check = type_check_;
+    cfg_.min_neighbors = api_.min_neighbors;
+    cfg_.adapt_min_neighbors = adapt_min_neighbors_;
+    cfg_.double_check = double_check_;
+    cfg_.drop_detect = drop_detect_;
+    cfg_.equalize = equalize_;
+    cfg_.reflection = reflection_;
+    cfg_.detect_enabled = detect_enabled_;
+    cfg_.merger_detect = merger_detect_;
+    cfg_.min_num_detect = min_num_detect_;
+    cfg_.rescale_output = input_downscale_ ? 1 : 0;
+    cfg_.rescale = (float)api_.min_face_height / (float)pat_h_;
+
+    // capacities from the largest plans this configuration can produce
+    s1_cap_ = resp_cap_ = 0;
+    chunk_cap_ = 0;
+    for (int ch : {1, 3}) {
+        Plan tmp;
+        ccnn_status st = build_plan(max_w_, max_h_, ch, (int)scales_.size(), &tmp);
+        if (st != CCNN_OK) return st;
+        s1_cap_ = std::max(s1_cap_, tmp.s1_floats);
+        resp_cap_ = std::max(resp_cap_, tmp.resp_floats);
+        chunk_cap_ = std::max(chunk_cap_, (int)tmp.chunks.size());
+    }
+    cand_cap_ = std::max(1LL, resp_cap_);
+    chunk_cap_ = std::max(chunk_cap_, 1);
+    cudaDeviceProp prop;
+    CCNN_CUDA(cudaGetDeviceProperties(&prop, device_));
+    // persistent stage-2/3 grid: 6 resident 256-thread CTAs per SM (shared memory bound)
+    window_grid_ = prop.multiProcessorCount * 6;
+
+    inited_ = true;
+    for (auto& s : slots_) {
+        ccnn_status st = alloc_slot(s);
+        if (st != CCNN_OK) {
+            clear();
+            return st;
+        }
+    }
+    return CCNN_OK;
+}
+
+ccnn_status Detector::alloc_slot(Slot& s) {
+    CCNN_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+    CCNN_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+    s.in_pitch = (size_t)round_up((long long)max_w_ * 4, 64);
+    CCNN_CUDA(cudaMalloc(&s.d_in, s.in_pitch * max_h_));
+    s.gray_pitch = (int)round_up(max_w_, 16);
+    CCNN_CUDA(cudaMalloc(&s.d_gray, sizeof(float) * (size_t)s.gray_pitch * max_h_));
+    CCNN_CUDA(cudaMalloc(&s.d_s1, sizeof(float) * std::max(1LL, s1_cap_)));
+    CCNN_CUDA(cudaMalloc(&s.d_resp, sizeof(float) * std::max(1LL, resp_cap_)));
+    CCNN_CUDA(cudaMalloc(&s.d_counts, sizeof(int) * chunk_cap_));
+    CCNN_CUDA(cudaMalloc(&s.d_cands, sizeof(Candidate) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.d_ncand, sizeof(int)));
+    CCNN_CUDA(cudaMalloc(&s.d_results, sizeof(CandResult) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.D, sizeof(Det) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.R, sizeof(Det) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.M, sizeof(Det) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.F, sizeof(Det) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.first_dec, sizeof(int) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.survivors, sizeof(int) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.checked, cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.d_nraw, sizeof(int)));
+    CCNN_CUDA(cudaMalloc(&s.d_faces, sizeof(FaceOut) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.d_nfaces, sizeof(int)));
+    CCNN_CUDA(cudaMallocHost(&s.h_nfaces, sizeof(int)));
+    CCNN_CUDA(cudaMallocHost(&s.h_faces, sizeof(FaceOut) * kHostFaces));
+    CCNN_CUDA(cudaMemsetAsync(s.d_ncand, 0, sizeof(int), s.st));
+    CCNN_CUDA(cudaMemsetAsync(s.d_nraw, 0, sizeof(int), s.st));
+    CCNN_CUDA(cudaMemsetAsync(s.d_nfaces, 0, sizeof(int), s.st));
+    return CCNN_OK;
+}
+
+ccnn_status Detector::build_plan(int w, int h, int ch, int num_scales, Plan* p) {
+    p->in_w = w;
+    p->in_h = h;
+    p->ch = ch;
+    p->downscale = input_downscale_ && ch == 1;
+    if (p->downscale)
+        size_scale(w, h, input_scale_, &p->gw, &p->gh);
+    else {
+        p->gw = w;
+        p->gh = h;
+    }
+    p->levels.clear();
+    p->chunks.clear();
+    long long s1 = 0, resp = 0;
+    int k1 = 0, k2 = 0;
+    int n = 0;
+    for (int scl = 0; scl < num_scales && scl < (int)scales_.size(); ++scl) {
+        LevelDesc L{};
+        size_scale(p->gw, p->gh, scales_[scl], &L.w, &L.h);
+        if (L.w < ext_w_ || L.h < ext_h_) break;  // this and every smaller level are skipped
+        L.mode = (L.w == p->gw && L.h == p->gh) ? 0 : (scales_[scl] > 0.7f ? 1 : 2);
+        L.sclx = ((uint32_t)p->gw << 12) / (uint32_t)L.w + 1u;
+        L.scly = ((uint32_t)p->gh << 12) / (uint32_t)L.h + 1u;
+        L.scale = scales_[scl];
+        L.inv_scale = 1.f / scales_[scl];
+        L.p1w = (L.w - 3) >> 1;
+        L.p1h = (L.h - 3) >> 1;
+        L.p2w = (L.p1w - 2) >> 1;
+        L.p2h = (L.p1h - 2) >> 1;
+        L.ow = L.p2w - 3;
+        L.oh = L.p2h - 4;
+        L.s1_pitch = (int)round_up(L.p1w, 32);
+        L.s1_plane = (long long)L.s1_pitch * L.p1h;
+        L.s1_off = s1;
+        s1 += 4 * L.s1_plane;
+        L.resp_off = resp;
+        resp += (long long)L.ow * L.oh;
+        L.k1_tiles_x = (L.p1w + kK1TileX - 1) / kK1TileX;
+        L.k1_base = k1;
+        k1 += L.k1_tiles_x * ((L.p1h + kK1TileY - 1) / kK1TileY);
+        L.k2_tiles_x = (L.ow + kK2TileX - 1) / kK2TileX;
+        L.k2_base = k2;
+        k2 += L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY);
+        p->levels.push_back(L);
+        ++n;
+    }
+    p->n_levels = n;
+    for (int scl = n - 1; scl >= 0; --scl) {
+        LevelDesc& L = p->levels[scl];
+        L.order = n - 1 - scl;
+        const int total = L.ow * L.oh;
+        for (int s = 0; s < total; s += kChunk) p->chunks.push_back(make_int4(scl, s, std::min(kChunk, total - s), 0));
+    }
+    p->k1_tiles = k1;
+    p->k2_tiles = k2;
+    p->s1_floats = s1;
+    p->resp_floats = resp;
+    return CCNN_OK;
+}
+
+// Resolves the pyramid plan of a frame and advances num_scales as RunCPUDetect does.
+ccnn_status Detector::plan_for(int w, int h, int ch, const Plan** out) {
+    const bool downscale = input_downscale_ && ch == 1;
+    auto key = std::make_tuple(w, h, downscale ? 1 : 3, num_scales_);
+    auto it = plans_.find(key);
+    if (it == plans_.end()) {
+        std::unique_ptr<Plan> p(new Plan());
+        ccnn_status st = build_plan(w, h, ch, num_scales_, p.get());
+        if (st != CCNN_OK) return st;
+        if (p->s1_floats > s1_cap_ || p->resp_floats > resp_cap_ || (long long)p->chunks.size() > chunk_cap_) {
+            set_error("internal: pyramid plan exceeds the allocated buffers");
+            return CCNN_ERR_CUDA;
+        }
+        if (p->n_levels > 0) {
+            CCNN_CUDA(cudaMalloc(&p->d_levels, sizeof(LevelDesc) * p->n_levels));
+            CCNN_CUDA(cudaMemcpy(p->d_levels, p->levels.data(), sizeof(LevelDesc) * p->n_levels, cudaMemcpyHostToDevice));
+        }
+        if (!p->chunks.empty()) {
+            CCNN_CUDA(cudaMalloc(&p->d_chunks, sizeof(int4) * p->chunks.size()));
+            CCNN_CUDA(cudaMemcpy(p->d_chunks, p->chunks.data(), sizeof(int4) * p->chunks.size(), cudaMemcpyHostToDevice));
+        }
+        it = plans_.emplace(key, std::move(p)).first;
+    }
+    const Plan* p = it->second.get();
+    // a level too small for the stage-2/3 window lowers num_scales for later frames (:2086)
+    if (p->n_levels < num_scales_) num_scales_ = p->n_levels;
+    *out = p;
+    return CCNN_OK;
+}
+
+ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
+    cudaError_t e;
+    if (p.downscale)
+        e = launch_gray_u8_resized(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, s.d_gray, s.gray_pitch, p.gw, p.gh, s.st);
+    else
+        e = launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st);
+    CCNN_CUDA(e);
+    CCNN_CUDA(launch_stage1(w1_, p.d_levels, p.n_levels, p.k1_tiles, p.k2_tiles, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_s1, s.d_resp, s.st));
+    CCNN_CUDA(launch_candidates(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
+                                (int)cand_cap_, s.st));
+    if (detect_enabled_)
+        CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_results, cfg_,
+                                window_grid_, s.st));
+    ReplayArgs a;
+    a.cands = s.d_cands;
+    a.n_cand = s.d_ncand;
+    a.results = s.d_results;
+    a.levels = p.d_levels;
+    a.cfg = cfg_;
+    a.D = s.D;
+    a.R = s.R;
+    a.M = s.M;
+    a.F = s.F;
+    a.first_dec = s.first_dec;
+    a.survivors = s.survivors;
+    a.checked = s.checked;
+    a.n_raw = s.d_nraw;
+    a.faces = s.d_faces;
+    a.face_cap = (int)cand_cap_;
+    a.n_faces = s.d_nfaces;
+    CCNN_CUDA(launch_replay(a, s.st));
+    CCNN_CUDA(cudaMemcpyAsync(s.h_nfaces, s.d_nfaces, sizeof(int), cudaMemcpyDeviceToHost, s.st));
+    CCNN_CUDA(cudaMemcpyAsync(s.h_faces, s.d_faces, sizeof(FaceOut) * kHostFaces, cudaMemcpyDeviceToHost, s.st));
+    return CCNN_OK;
+}
+
+ccnn_status Detector::enqueue(Slot& s, const Plan& p, const ccnn_image& img, bool device_input, cudaStream_t) {
+    const size_t row = (size_t)img.cols * img.channels;
+    CCNN_CUDA(cudaMemcpy2DAsync(s.d_in, s.in_pitch, img.data, img.step, row, img.rows,
+                                device_input ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s.st));
+    if (s.exec_plan != &p) {
+        if (s.exec) {
+            cudaGraphExecDestroy(s.exec);
+            s.exec = nullptr;
+        }
+        cudaGraph_t g;
+        CCNN_CUDA(cudaStreamBeginCapture(s.st, cudaStreamCaptureModeThreadLocal));
+        ccnn_status st = enqueue_kernels(s, p);
+        cudaError_t ce = cudaStreamEndCapture(s.st, &g);
+        if (st != CCNN_OK) return st;
+        CCNN_CUDA(ce);
+        ce = cudaGraphInstantiate(&s.exec, g, 0);
+        cudaGraphDestroy(g);
+        CCNN_CUDA(ce);
+        s.exec_plan = &p;
+    }
+    CCNN_CUDA(cudaGraphLaunch(s.exec, s.st));
+    CCNN_CUDA(cudaEventRecord(s.done, s.st));
+    s.last_plan = &p;
+    return CCNN_OK;
+}
+
+ccnn_status Detector::collect(Slot& s, ccnn_face* faces, int cap, int* n) {
+    CCNN_CUDA(cudaEventSynchronize(s.done));
+    CCNN_CUDA(cudaGetLastError());
+    const int nf = *s.h_nfaces;
+    *n = nf;
+    const int take = std::min(nf, cap);
+    std::vector<FaceOut> extra;
+    if (take > kHostFaces) {
+        extra.resize(take);
+        CCNN_CUDA(cudaMemcpy(extra.data(), s.d_faces, sizeof(FaceOut) * take, cudaMemcpyDeviceToHost));
+    }
+    const FaceOut* src = take > kHostFaces ? extra.data() : s.h_faces;
+    for (int i = 0; i < take; ++i) {
+        faces[i].x = src[i].x;
+        faces[i].y = src[i].y;
+        faces[i].width = src[i].w;
+        faces[i].height = src[i].h;
+        faces[i].score = src[i].score;
+        faces[i].gender = faces[i].smile = faces[i].glasses = -1;
+    }
+    return nf > cap ? CCNN_TRUNCATED : CCNN_OK;
+}
+
+// Frame admission: the reference's size and channel rules, then the frame's plan.
+ccnn_status Detector::prepare_frame(const ccnn_image& img, const Plan** plan, bool* empty) {
+    *empty = false;
+    if (img.cols <= 0 || img.rows <= 0 || !img.data || img.step < (size_t)img.cols * img.channels) {
+        set_error("invalid image");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    if (img.channels != 1 && img.channels != 3 && img.channels != 4) {
+        set_error("this type of image is not supported (1, 3 or 4 channels)");
+        return CCNN_ERR_UNSUPPORTED;
+    }
+    if (!inited_) {
+        ccnn_status st = init();
+        if (st != CCNN_OK) return st;
+    }
+    if (img.cols < ext_w_ || img.rows < ext_h_) {
+        *empty = true;
+        return CCNN_OK;
+    }
+    if (img.cols > max_w_ || img.rows > max_h_) {
+        clear();
+        max_w_ = img.cols;
+        max_h_ = img.rows;
+        if (gray_image_only_ && img.channels != 1) gray_image_only_ = false;
+        ccnn_status st = init();
+        if (st != CCNN_OK) return st;
+    } else if (img.cols != max_w_ || img.rows != max_h_) {
+        num_scales_ = (int)scales_.size();
+    }
+    if (gray_image_only_ && input_downscale_ && img.channels != 1) {
+        gray_image_only_ = false;
+        clear();
+        ccnn_status st = init();
+        if (st != CCNN_OK) return st;
+        if (gray_image_only_ && input_downscale_) {
+            // precision `def` forces gray_image_only back on in Init; the reference then recurses
+            // without end (cnn_detector_v3.cpp:2540-2545 with :924-926)
+            set_error("precision 'def' with a colour frame needs min_face_height < 34 (the reference recurses forever)");
+            return CCNN_ERR_CONFIG;
+        }
+    }
+    return plan_for(img.cols, img.rows, img.channels, plan);
+}
+
+ccnn_status Detector::detect(const ccnn_image& img, bool device_input, cudaStream_t user_stream, ccnn_face* faces, int cap, int* n) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!n || (cap > 0 && !faces) || cap < 0) {
+        set_error("invalid output arguments");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(device_);
+    const Plan* p = nullptr;
+    bool empty = false;
+    ccnn_status st = prepare_frame(img, &p, &empty);
+    if (st != CCNN_OK) return st;
+    if (empty) {
+        *n = 0;
+        return CCNN_OK;
+    }
+    Slot& s = slots_[0];
+    if (user_stream) {
+        // order the frame after the caller's pending work on its stream
+        cudaEvent_t ev;
+        CCNN_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaEventRecord(ev, user_stream);
+        cudaStreamWaitEvent(s.st, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    st = enqueue(s, *p, img, device_input, user_stream);
+    if (st != CCNN_OK) return st;
+    return collect(s, faces, cap, n);
+}
+
+ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, ccnn_face* faces, int cap_per, int* n_faces) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (n_img < 0 || (n_img > 0 && (!imgs || !n_faces)) || cap_per < 0 || (cap_per > 0 && n_img > 0 && !faces)) {
+        set_error("invalid arguments");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(device_);
+    int pending[kSlots];
+    for (int k = 0; k < kSlots; ++k) pending[k] = -1;
+    ccnn_status worst = CCNN_OK;
+    for (int i = 0; i < n_img; ++i) {
+        const int k = i % kSlots;
+        Slot& s = slots_[k];
+        if (pending[k] >= 0) {
+            ccnn_status st = collect(s, faces + (size_t)pending[k] * cap_per, cap_per, &n_faces[pending[k]]);
+            if (st < 0) return st;
+            if (st == CCNN_TRUNCATED) worst = CCNN_TRUNCATED;
+            pending[k] = -1;
+        }
+        const Plan* p = nullptr;
+        bool empty = false;
+        // frame admission may re-initialise (and so free the slots): drain in-flight frames first
+        if (!inited_ || imgs[i].cols > max_w_ || imgs[i].rows > max_h_ || (gray_image_only_ && input_downscale_ && imgs[i].channels != 1)) {
+            for (int q = 0; q < kSlots; ++q)
+                if (pending[q] >= 0) {
+                    ccnn_status st = collect(slots_[q], faces + (size_t)pending[q] * cap_per, cap_per, &n_faces[pending[q]]);
+                    if (st < 0) return st;
+                    if (st == CCNN_TRUNCATED) worst = CCNN_TRUNCATED;
+                    pending[q] = -1;
+                }
+        }
+        ccnn_status st = prepare_frame(imgs[i], &p, &empty);
+        if (st != CCNN_OK) return st;
+        if (empty) {
+            n_faces[i] = 0;
+            continue;
+        }
+        st = enqueue(slots_[k], *p, imgs[i], false, nullptr);
+        if (st != CCNN_OK) return st;
+        pending[k] = i;
+    }
+    for (int k = 0; k < kSlots; ++k)
+        if (pending[k] >= 0) {
+            ccnn_status st = collect(slots_[k], faces + (size_t)pending[k] * cap_per, cap_per, &n_faces[pending[k]]);
+            if (st < 0) return st;
+            if (st == CCNN_TRUNCATED) worst = CCNN_TRUNCATED;
+        }
+    return worst;
+}
+
+ccnn_status Detector::get_gray_device(const float** data, int* cols, int* rows, size_t* step) {
+    std::lock_guard<std::mutex> lk(mu_);
+    Slot& s = slots_[0];
+    if (!inited_ || !s.last_plan) {
+        set_error("no frame has been processed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    *data = s.d_gray;
+    *cols = s.last_plan->gw;
+    *rows = s.last_plan->gh;
+    *step = sizeof(float) * (size_t)s.gray_pitch;
+    return CCNN_OK;
+}
+
+ccnn_status Detector::get_gray_host(float* out, int cap, int* cols, int* rows) {
+    std::lock_guard<std::mutex> lk(mu_);
+    Slot& s = slots_[0];
+    if (!inited_ || !s.last_plan) {
+        set_error("no frame has been processed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    const Plan& p = *s.last_plan;
+    *cols = p.gw;
+    *rows = p.gh;
+    if ((long long)p.gw * p.gh > cap) {
+        set_error("output capacity too small");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    CCNN_CUDA(cudaMemcpy2D(out, sizeof(float) * p.gw, s.d_gray, sizeof(float) * s.gray_pitch, sizeof(float) * p.gw, p.gh,
+                           cudaMemcpyDeviceToHost));
+    return CCNN_OK;
+}
+
+ccnn_status Detector::get_params(ccnn_params* out) {
+    std::lock_guard<std::mutex> lk(mu_);
+    *out = api_;
+    out->max_image_width = max_w_;
+    out->max_image_height = max_h_;
+    return CCNN_OK;
+}
+
+ccnn_status Detector::set_params(const ccnn_params& p) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (p.facial_analysis) {
+        set_error("facial_analysis is not supported by this detector");
+        return CCNN_ERR_UNSUPPORTED;
+    }
+    clear();
+    api_ = p;
+    max_w_ = p.max_image_width;
+    max_h_ = p.max_image_height;
+    gray_image_only_ = true;
+    return CCNN_OK;  // the next frame re-initialises (Detect :2485-2492)
+}
+
+ccnn_status Detector::set_max_image_size(int w, int h) {
+    std::lock_guard<std::mutex> lk(mu_);
+    clear();
+    max_w_ = w;
+    max_h_ = h;
+    return CCNN_OK;
+}
+
+ccnn_status Detector::set_min_object_height(int v) {
+    std::lock_guard<std::mutex> lk(mu_);
+    clear();
+    api_.min_face_height = v;
+    return CCNN_OK;
+}
+
+ccnn_status Detector::set_max_object_height(int v) {
+    std::lock_guard<std::mutex> lk(mu_);
+    clear();
+    api_.max_face_height = v;
+    return CCNN_OK;
+}
+
+ccnn_status Detector::set_num_threads(int v) {
+    std::lock_guard<std::mutex> lk(mu_);
+    api_.num_threads = v;  // the cascade's parallelism is on the device; kept for getParam
+    return CCNN_OK;
+}
+
+ccnn_status Detector::stage1_forward(const float* d_img, int w, int h, size_t step, float* d_resp, int cap, int* rw, int* rh,
+                                     cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!inited_) {
+        ccnn_status s = init();
+        if (s != CCNN_OK) return s;
+    }
+    if (w < pat_w_ || h < pat_h_ || (step % sizeof(float)) != 0) {
+        set_error("image smaller than the stage-1 window or misaligned step");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(device_);
+    LevelDesc L{};
+    L.w = w;
+    L.h = h;
+    L.mode = 0;
+    L.scale = 1.f;
+    L.inv_scale = 1.f;
+    L.p1w = (w - 3) >> 1;
+    L.p1h = (h - 3) >> 1;
+    L.p2w = (L.p1w - 2) >> 1;
+    L.p2h = (L.p1h - 2) >> 1;
+    L.ow = L.p2w - 3;
+    L.oh = L.p2h - 4;
+    L.s1_pitch = (int)round_up(L.p1w, 32);
+    L.s1_plane = (long long)L.s1_pitch * L.p1h;
+    L.k1_tiles_x = (L.p1w + kK1TileX - 1) / kK1TileX;
+    L.k2_tiles_x = (L.ow + kK2TileX - 1) / kK2TileX;
+    const int k1 = L.k1_tiles_x * ((L.p1h + kK1TileY - 1) / kK1TileY);
+    const int k2 = L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY);
+    *rw = L.ow;
+    *rh = L.oh;
+    if ((long long)L.ow * L.oh > cap) {
+        set_error("response capacity too small");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    LevelDesc* d_l = nullptr;
+    float* d_s1 = nullptr;
+    CCNN_CUDA(cudaMallocAsync(&d_l, sizeof(LevelDesc), st));
+    CCNN_CUDA(cudaMallocAsync(&d_s1, sizeof(float) * 4 * L.s1_plane, st));
+    CCNN_CUDA(cudaMemcpyAsync(d_l, &L, sizeof(LevelDesc), cudaMemcpyHostToDevice, st));
+    CCNN_CUDA(launch_stage1(w1_, d_l, 1, k1, k2, d_img, (int)(step / sizeof(float)), w, h, d_s1, d_resp, st));
+    CCNN_CUDA(cudaFreeAsync(d_s1, st));
+    CCNN_CUDA(cudaFreeAsync(d_l, st));
+    CCNN_CUDA(cudaStreamSynchronize(st));
+    return CCNN_OK;
+}
+
+ccnn_status Detector::inspect_levels(ccnn_level_info* out, int cap, int* n) {
+    std::lock_guard<std::mutex> lk(mu_);
+    const Plan* p = slots_[0].last_plan;
+    if (!inited_ || !p) {
+        set_error("no frame has been processed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    *n = p->n_levels;
+    for (int i = 0; i < p->n_levels && i < cap; ++i) {
+        const LevelDesc& L = p->levels[i];
+        out[i].width = L.w;
+        out[i].height = L.h;
+        out[i].scale = L.scale;
+        out[i].resp_width = L.ow;
+        out[i].resp_height = L.oh;
+    }
+    return CCNN_OK;
+}
+
+ccnn_status Detector::inspect_response(int level, float* out, int cap) {
+    std::lock_guard<std::mutex> lk(mu_);
+    const Plan* p = slots_[0].last_plan;
+    if (!inited_ || !p || level < 0 || level >= p->n_levels) {
+        set_error("no such level");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    const LevelDesc& L = p->levels[level];
+    if ((long long)L.ow * L.oh > cap) {
+        set_error("output capacity too small");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    CCNN_CUDA(cudaMemcpy(out, slots_[0].d_resp + L.resp_off, sizeof(float) * L.ow * L.oh, cudaMemcpyDeviceToHost));
+    return CCNN_OK;
+}
+
+ccnn_status Detector::inspect_candidates(ccnn_candidate* out, int cap, int* n) {
+    std::lock_guard<std::mutex> lk(mu_);
+    Slot& s = slots_[0];
+    if (!inited_ || !s.last_plan) {
+        set_error("no frame has been processed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    int nc = 0;
+    CCNN_CUDA(cudaMemcpy(&nc, s.d_ncand, sizeof(int), cudaMemcpyDeviceToHost));
+    *n = nc;
+    const int take = std::min(nc, cap);
+    std::vector<Candidate> c(take);
+    std::vector<CandResult> r(take);
+    if (take > 0) {
+        CCNN_CUDA(cudaMemcpy(c.data(), s.d_cands, sizeof(Candidate) * take, cudaMemcpyDeviceToHost));
+        if (detect_enabled_) CCNN_CUDA(cudaMemcpy(r.data(), s.d_results, sizeof(CandResult) * take, cudaMemcpyDeviceToHost));
+    }
+    for (int i = 0; i < take; ++i) {
+        out[i].level = c[i].level;
+        out[i].x = c[i].px;
+        out[i].y = c[i].py;
+        out[i].score = c[i].score;
+        out[i].accepted = detect_enabled_ ? r[i].accepted : 0;
+        out[i].check_score = detect_enabled_ ? r[i].score : 0.f;
+        out[i].knn = detect_enabled_ ? r[i].knn : 0;
+    }
+    return CCNN_OK;
+}
+
+ccnn_status Detector::inspect_raw(ccnn_detection* out, int cap, int* n) {
+    std::lock_guard<std::mutex> lk(mu_);
+    Slot& s = slots_[0];
+    if (!inited_ || !s.last_plan) {
+        set_error("no frame has been processed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    int nr = 0;
+    CCNN_CUDA(cudaMemcpy(&nr, s.d_nraw, sizeof(int), cudaMemcpyDeviceToHost));
+    *n = nr;
+    const int take = std::min(nr, cap);
+    std::vector<Det> d(take);
+    if (take > 0) CCNN_CUDA(cudaMemcpy(d.data(), s.D, sizeof(Det) * take, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < take; ++i) {
+        out[i].x = d[i].x;
+        out[i].y = d[i].y;
+        out[i].width = d[i].w;
+        out[i].height = d[i].h;
+        out[i].score = d[i].score;
+        out[i].scale = d[i].scale;
+        out[i].knn = d[i].knn;
+        out[i].num_detect = d[i].num_detect;
+    }
+    return CCNN_OK;
+}
+
+}  // namespace ccnn

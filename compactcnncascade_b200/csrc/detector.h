@@ -1,0 +1,137 @@
+// Host runtime of the detection path: configuration, pyramid planning, device buffers,
+// CUDA-graph capture of the per-frame kernel chain, result download.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/ccnn.h"
+#include "../../include/ccnn_inspect.h"
+#include "kernels.h"
+
+namespace ccnn {
+
+// One pyramid plan: everything that depends on the frame size and the level count in force.
+struct Plan {
+    int in_w = 0, in_h = 0, ch = 0;  // input frame
+    int gw = 0, gh = 0;              // gray image (after the optional 8-bit downscale)
+    bool downscale = false;
+    int n_levels = 0;                // processed levels scl = 0 .. n_levels-1
+    std::vector<LevelDesc> levels;
+    std::vector<int4> chunks;        // candidate-scan chunks in visiting order
+    int k1_tiles = 0, k2_tiles = 0;
+    long long s1_floats = 0, resp_floats = 0;
+    LevelDesc* d_levels = nullptr;
+    int4* d_chunks = nullptr;
+};
+
+// Device buffers and stream of one in-flight frame.
+struct Slot {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    uint8_t* d_in = nullptr;
+    size_t in_pitch = 0;
+    float* d_gray = nullptr;
+    int gray_pitch = 0;  // floats
+    float* d_s1 = nullptr;
+    float* d_resp = nullptr;
+    int* d_counts = nullptr;
+    Candidate* d_cands = nullptr;
+    int* d_ncand = nullptr;
+    CandResult* d_results = nullptr;
+    Det *D = nullptr, *R = nullptr, *M = nullptr, *F = nullptr;
+    int* first_dec = nullptr;
+    int* survivors = nullptr;
+    uint8_t* checked = nullptr;
+    int* d_nraw = nullptr;
+    FaceOut* d_faces = nullptr;
+    int* d_nfaces = nullptr;
+    int* h_nfaces = nullptr;   // pinned
+    FaceOut* h_faces = nullptr;  // pinned, kHostFaces entries
+    cudaGraphExec_t exec = nullptr;
+    const Plan* exec_plan = nullptr;
+    const Plan* last_plan = nullptr;  // plan of the last frame run on this slot
+};
+
+class Detector {
+   public:
+    static constexpr int kSlots = 2;
+    static constexpr int kHostFaces = 1024;
+
+    Detector() = default;
+    ~Detector();
+
+    ccnn_status create(const ccnn_params& p, const char* const* model_paths);
+    ccnn_status detect(const ccnn_image& img, bool device_input, cudaStream_t user_stream, ccnn_face* faces, int cap, int* n);
+    ccnn_status detect_batch(const ccnn_image* imgs, int n_img, ccnn_face* faces, int cap_per, int* n_faces);
+
+    ccnn_status get_gray_device(const float** data, int* cols, int* rows, size_t* step);
+    ccnn_status get_gray_host(float* out, int cap, int* cols, int* rows);
+    ccnn_status get_params(ccnn_params* out);
+    ccnn_status set_params(const ccnn_params& p);
+    ccnn_status set_max_image_size(int w, int h);
+    ccnn_status set_min_object_height(int v);
+    ccnn_status set_max_object_height(int v);
+    ccnn_status set_num_threads(int v);
+
+    ccnn_status stage1_forward(const float* d_img, int w, int h, size_t step, float* d_resp, int cap, int* rw, int* rh, cudaStream_t st);
+    ccnn_status inspect_levels(ccnn_level_info* out, int cap, int* n);
+    ccnn_status inspect_response(int level, float* out, int cap);
+    ccnn_status inspect_candidates(ccnn_candidate* out, int cap, int* n);
+    ccnn_status inspect_raw(ccnn_detection* out, int cap, int* n);
+
+   private:
+    // configuration (FaceDetector::Param + the AdvancedParam the API derives from it)
+    ccnn_params api_{};
+    int device_ = 0;
+    bool gray_image_only_ = true;
+    int type_check_ = 2, min_num_detect_ = 1;
+    bool adapt_min_neighbors_ = false, drop_detect_ = true, detect_enabled_ = true, merger_detect_ = true;
+    bool equalize_ = true, reflection_ = true, double_check_ = true;
+
+    // models
+    std::string model_paths_[3];
+    Stage1W w1_{};
+    std::unique_ptr<WindowNets> wn_;
+    int pat_w_ = kPatW, pat_h_ = kPatH;     // stage-1 window
+    int ext_w_ = kWinW, ext_h_ = kWinH;     // smallest level processed
+
+    // initialised state (CNNDetector::Init)
+    bool inited_ = false;
+    int max_w_ = 0, max_h_ = 0;
+    std::vector<float> scales_;
+    bool input_downscale_ = false;
+    float input_scale_ = 0.f;
+    int num_scales_ = 0;
+
+    CascadeConfig cfg_{};
+    Slot slots_[kSlots];
+    long long cand_cap_ = 0, s1_cap_ = 0, resp_cap_ = 0;
+    int chunk_cap_ = 0;
+    int window_grid_ = 0;
+    std::map<std::tuple<int, int, int, int>, std::unique_ptr<Plan>> plans_;
+    std::mutex mu_;
+
+    ccnn_status init();
+    void clear();
+    ccnn_status alloc_slot(Slot& s);
+    void free_slot(Slot& s);
+    ccnn_status plan_for(int w, int h, int ch, const Plan** out);
+    ccnn_status build_plan(int w, int h, int ch, int num_scales, Plan* p);
+    ccnn_status enqueue(Slot& s, const Plan& p, const ccnn_image& img, bool device_input, cudaStream_t copy_stream);
+    ccnn_status enqueue_kernels(Slot& s, const Plan& p);
+    ccnn_status prepare_frame(const ccnn_image& img, const Plan** plan, bool* empty);
+    ccnn_status collect(Slot& s, ccnn_face* faces, int cap, int* n);
+    ccnn_status apply_precision();
+};
+
+void set_error(const std::string& msg);
+ccnn_status cuda_status(cudaError_t e, const char* what);
+
+}  // namespace ccnn

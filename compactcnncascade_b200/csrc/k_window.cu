@@ -1,0 +1,328 @@
+// Stage-2/3 window CNNs on the compacted stage-1 candidates.
+//
+// Reference: CNNDetector::CPUCheckDetect (src/CNNObjectDetector/cnn_detector_v3.cpp:1485-1818):
+//   crop  x = int((px-6)/s), y = int((py-5)/s), w = int(36/s), h = int(38/s)  (:1492-1495)
+//   retry window (mod 1) shrunk by 15 % (:1535-1542), clamped to the frame (:1553-1556)
+//   nearest-neighbour resize to 49 x 51 (:1565), byte rounding uchar(v + 0.5) (image_proc.cpp:365),
+//   histogram equalisation (image_proc.cpp:720-799),
+//   stage 2 on columns 2..48 (UCharToFloat offset 2, image_proc.cpp:417-427),
+//   stage 3 on the mirror of columns 0..46 (UCharToFloat_inv, image_proc.cpp:478-490),
+//   4x4 response maps counted against treshold_2 / treshold_3 with the type_check early exits
+//   (:1655-1706) and the accept rule (:1709-1725); score s0 + k1*max(-1.7159, m1) + k2*max(-1.7159, m2).
+//
+// Every candidate is evaluated (first window, and the retry window when the first is rejected);
+// whether the reference would have reached it (drop_detect) is decided later by the replay
+// kernel, so the result is the same while all candidates run in parallel.
+//
+// One CTA (256 threads) per candidate, persistent over the candidate list. The networks run
+// entirely in shared memory: L1 (6 maps, 44x48 -> pooled 22x24), neighbour sums, L2 (12 maps,
+// 20x22 -> pooled 10x11), sums, L3 (24 maps, 7w x 8h -> 4x4), hidden layer and output neuron.
+#include "kernels.h"
+#include "resample.cuh"
+
+namespace ccnn {
+
+constexpr int kWT = 256;
+constexpr int kP1W = 22, kP1H = 24;   // pooled L1 of a 47x51 window
+constexpr int kP2W = 10, kP2H = 11;   // pooled L2
+constexpr int kOutN = 16;             // 4x4 response map
+
+struct WindowSmem {
+    uint8_t crop[kCropH][kCropW + 3];
+    int hist[256];
+    int lut[256];
+    float s1[6][kP1H][kP1W + 1];
+    float p2[12][kP2H][kP2W + 1];
+    float s2[12][kP2H][kP2W + 1];
+    float a3[24][kOutN];
+    float hbuf[84][kOutN];
+    float out[kOutN];
+    int geo[4];
+};
+
+// mode: 0 = stage-2 view (columns 2..48), 1 = mirrored (46 - x), 2 = plain (columns 0..46)
+__device__ __forceinline__ float win_in(const WindowSmem& S, int mode, int x, int y) {
+    int c = mode == 0 ? x + kXOff : (mode == 1 ? (kWinW - 1) - x : x);
+    return (float)S.crop[y][c];
+}
+
+template <class NW>
+__device__ void window_net(const NW& W, WindowSmem& S, int mode) {
+    // L1: conv 4x4 + folded BN/LReLU + 2x2 max, then neighbour sums (add / add2)
+    for (int p = threadIdx.x; p < kP1W * kP1H; p += kWT) {
+        const int x = p % kP1W, y = p / kP1W;
+        float win[5][5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r)
+#pragma unroll
+            for (int c = 0; c < 5; ++c) win[r][c] = win_in(S, mode, 2 * x + c, 2 * y + r);
+        float P[NW::kM1];
+#pragma unroll
+        for (int m = 0; m < NW::kM1; ++m) {
+            float cv[4];
+#pragma unroll
+            for (int d = 0; d < 4; ++d) {
+                const int dy = d >> 1, dx = d & 1;
+                float acc = fmul(win[dy][dx], W.k1[m][0]);
+#pragma unroll
+                for (int k = 1; k < 16; ++k) acc = fadd(acc, fmul(win[dy + (k >> 2)][dx + (k & 3)], W.k1[m][k]));
+                cv[d] = lrelu_bn(acc, W.b1[m], W.w1a[m], W.w1b[m], W.bn1[m]);
+            }
+            P[m] = fmaxf(fmaxf(cv[0], cv[1]), fmaxf(cv[2], cv[3]));
+        }
+        S.s1[0][y][x] = fadd(P[0], P[1]);
+#pragma unroll
+        for (int k = 1; k < NW::kM1 - 1; ++k) S.s1[k][y][x] = fadd(fadd(P[k - 1], P[k]), P[k + 1]);
+        S.s1[NW::kM1 - 1][y][x] = fadd(P[NW::kM1 - 2], P[NW::kM1 - 1]);
+    }
+    __syncthreads();
+    // L2: map pair (2i, 2i+1) convolves sum map i; 3x3 + BN/LReLU + 2x2 max
+    for (int it = threadIdx.x; it < kP2W * kP2H * NW::kM1; it += kWT) {
+        const int i = it / (kP2W * kP2H);
+        const int p = it - i * (kP2W * kP2H);
+        const int x = p % kP2W, y = p / kP2W;
+        float q[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) q[r][c] = S.s1[i][2 * y + r][2 * x + c];
+#pragma unroll
+        for (int hm = 0; hm < 2; ++hm) {
+            const int m = 2 * i + hm;
+            float cv[4];
+#pragma unroll
+            for (int d = 0; d < 4; ++d) {
+                const int dy = d >> 1, dx = d & 1;
+                float acc = fmul(q[dy][dx], W.k2[m][0]);
+#pragma unroll
+                for (int k = 1; k < 9; ++k) acc = fadd(acc, fmul(q[dy + k / 3][dx + k % 3], W.k2[m][k]));
+                cv[d] = lrelu_bn(acc, W.b2[m], W.w2a[m], W.w2b[m], W.bn2[m]);
+            }
+            S.p2[m][y][x] = fmaxf(fmaxf(cv[0], cv[1]), fmaxf(cv[2], cv[3]));
+        }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < kP2W * kP2H; p += kWT) {
+        const int x = p % kP2W, y = p / kP2W;
+        constexpr int M = NW::kM2;
+        S.s2[0][y][x] = fadd(S.p2[0][y][x], S.p2[1][y][x]);
+        for (int k = 1; k < M - 1; ++k) S.s2[k][y][x] = fadd(fadd(S.p2[k - 1][y][x], S.p2[k][y][x]), S.p2[k + 1][y][x]);
+        S.s2[M - 1][y][x] = fadd(S.p2[M - 2][y][x], S.p2[M - 1][y][x]);
+    }
+    __syncthreads();
+    // L3: 7w x 8h conv summed in one left-to-right chain (conv_8x7), BN/LReLU, no pooling
+    for (int it = threadIdx.x; it < NW::kM3 * kOutN; it += kWT) {
+        const int m = it / kOutN, o = it - m * kOutN;
+        const int ox = o & 3, oy = o >> 2;
+        const int i = m >> 1;
+        float acc = fmul(S.s2[i][oy][ox], W.k3[m][0]);
+#pragma unroll
+        for (int k = 1; k < NW::kK3W * NW::kK3H; ++k)
+            acc = fadd(acc, fmul(S.s2[i][oy + k / NW::kK3W][ox + k % NW::kK3W], W.k3[m][k]));
+        S.a3[m][o] = lrelu_bn(acc, W.b3[m], W.w3a[m], W.w3b[m], W.bn3[m]);
+    }
+    __syncthreads();
+    // hidden neurons n = HS*i + t read L3 maps i .. i+CONN-1
+    for (int it = threadIdx.x; it < NW::kHL * kOutN; it += kWT) {
+        const int n = it / kOutN, o = it - n * kOutN;
+        const int i = n / NW::kHS, t = n - i * NW::kHS;
+        float s = W.hb[n];
+#pragma unroll
+        for (int j = 0; j < NW::kConn; ++j) s = fadd(s, fmul(S.a3[i + j][o], W.hw[n][j]));
+        s = fmul(s, W.htw[i]);
+        s = tanh_rational(s);
+        s = fadd(fmul(0.5f, s), 0.5f);
+        S.hbuf[n][o] = fadd(fmul(W.hbnw[t], s), W.hbnb[t]);
+    }
+    __syncthreads();
+    if (threadIdx.x < kOutN) {
+        const int o = threadIdx.x;
+        float acc = fmul(S.hbuf[0][o], W.ow[0]);
+        for (int n = 1; n < NW::kHL; ++n) acc = fadd(fmul(S.hbuf[n][o], W.ow[n]), acc);
+        float c = fmul(fadd(acc, W.ob), W.otw);
+        c = tanh_rational(c);
+        S.out[o] = (W.af == 0.f) ? fadd(fmul(0.5f, c), 0.5f) : fmul(W.af, c);
+    }
+    __syncthreads();
+}
+
+struct WinArgs {
+    const float* gray;
+    int gpitch, gw, gh;
+    const Candidate* cands;
+    const int* n_cand;
+    const LevelDesc* levels;
+    CandResult* results;
+    CascadeConfig cfg;
+};
+
+// crop + byte rounding + (optional) equalisation of one window into S.crop
+__device__ void prepare_window(const WinArgs& a, WindowSmem& S, const Candidate& cd, float inv_scale, int mod) {
+    if (threadIdx.x == 0) {
+        int x = (int)((float)(cd.px - (kExtOff + kXOff) / 2) * inv_scale);
+        int y = (int)((float)(cd.py - kExtOff / 2) * inv_scale);
+        int width = (int)((float)(kPatW + kExtOff + kXOff) * inv_scale);
+        int height = (int)((float)(kPatH + kExtOff) * inv_scale);
+        if (mod == 1) {
+            const float k = 0.15f;
+            x = (int)(fadd((float)x, fdiv(fmul((float)width, k), 2.f)));
+            width = (int)(fsub((float)width, fmul((float)width, k)));
+            y = (int)(fadd((float)y, fdiv(fmul((float)height, k), 2.f)));
+            height = (int)(fsub((float)height, fmul((float)height, k)));
+        }
+        const int rx = min(max(x, 0), a.gw);
+        const int ry = min(max(y, 0), a.gh);
+        const int rcols = min(max(x + width, 0), a.gw) - rx;
+        const int rrows = min(max(y + height, 0), a.gh) - ry;
+        S.geo[0] = rx;
+        S.geo[1] = ry;
+        S.geo[2] = rcols;
+        S.geo[3] = rrows;
+    }
+    if (threadIdx.x < 256) S.hist[threadIdx.x] = 0;
+    __syncthreads();
+    const int rx = S.geo[0], ry = S.geo[1], rcols = S.geo[2], rrows = S.geo[3];
+    const bool copy = (rcols == kCropW && rrows == kCropH);  // FastImageResize copies equal sizes
+    const uint32_t sclx = fp_step(max(rcols, 1), kCropW), scly = fp_step(max(rrows, 1), kCropH);
+    for (int p = threadIdx.x; p < kCropW * kCropH; p += kWT) {
+        const int ix = p % kCropW, iy = p / kCropW;
+        int sx, sy;
+        if (copy) {
+            sx = ix;
+            sy = iy;
+        } else {
+            sx = (int)sample_col(ix, sclx, rcols).idx;
+            sy = (int)sample_row(iy, scly, rrows).idx;
+        }
+        // memory guard only: valid candidates always sample inside the frame
+        const int gx = min(max(rx + sx, 0), a.gw - 1), gy = min(max(ry + sy, 0), a.gh - 1);
+        const float v = a.gray[(size_t)gy * a.gpitch + gx];
+        const uint8_t u = (uint8_t)__float2int_rz(fadd(v, 0.5f));
+        S.crop[iy][ix] = u;
+        if (a.cfg.equalize) atomicAdd(&S.hist[u], 1);
+    }
+    __syncthreads();
+    if (!a.cfg.equalize) return;
+    // cumulative histogram (256 bins, one per thread): shuffle scan + warp totals
+    {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        int v = S.hist[threadIdx.x];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y2 = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y2;
+        }
+        __shared__ int wsum[8];
+        if (lane == 31) wsum[wid] = v;
+        __syncthreads();
+        int add = 0;
+        for (int w = 0; w < wid; ++w) add += wsum[w];
+        S.lut[threadIdx.x] = v + add;  // cf_hist
+        __syncthreads();
+    }
+    const float bmin = (float)S.lut[0], bmax = (float)S.lut[255];
+    if (bmin == bmax) return;  // the reference leaves the window unchanged
+    const float delt = fdiv(255.f, fsub(bmax, bmin));
+    const int lv = (int)fadd(fmul(fsub((float)S.lut[threadIdx.x], bmin), delt), 0.5f);
+    __syncthreads();
+    S.lut[threadIdx.x] = lv;
+    __syncthreads();
+    for (int p = threadIdx.x; p < kCropW * kCropH; p += kWT) {
+        const int ix = p % kCropW, iy = p / kCropW;
+        S.crop[iy][ix] = (uint8_t)S.lut[S.crop[iy][ix]];
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kWT) window_kernel(const __grid_constant__ WindowNets N, const WinArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WindowSmem& S = *reinterpret_cast<WindowSmem*>(smem_raw);
+    __shared__ float s_max[2];
+    __shared__ int s_knn[2];
+    const int n = *a.n_cand;
+    const CascadeConfig& C = a.cfg;
+    for (int ci = blockIdx.x; ci < n; ci += gridDim.x) {
+        const Candidate cd = a.cands[ci];
+        const LevelDesc& L = a.levels[cd.level];
+        const float scale = L.scale, inv_scale = L.inv_scale;
+        const int mn = (C.adapt_min_neighbors && scale > 0.7f && C.min_neighbors > 1) ? C.min_neighbors - 1 : C.min_neighbors;
+        CandResult res;
+        res.accepted = 0;
+        res.score = 0.f;
+        res.knn = 0;
+        res.pad = 0;
+        const int n_mod = C.double_check ? 2 : 1;
+        for (int mod = 0; mod < n_mod; ++mod) {
+            prepare_window(a, S, cd, inv_scale, mod);
+            float max1 = -10.f, max2 = -10.f;
+            int k1 = 0, k2 = 0;
+            for (int icx = 0; icx < 2; ++icx) {
+                if (icx == 0)
+                    window_net(N.s2, S, 0);
+                else
+                    window_net(N.s3, S, C.reflection ? 1 : 2);
+                if (threadIdx.x == 0) {
+                    float mx = -10.f;
+                    int kc = 0;
+                    const float thr = icx == 0 ? C.thr2 : C.thr3;
+                    for (int o = 0; o < kOutN; ++o) {
+                        const float d = S.out[o];
+                        mx = (mx < d) ? d : mx;
+                        if (d > thr) kc++;
+                    }
+                    s_max[icx] = mx;
+                    s_knn[icx] = kc;
+                }
+                __syncthreads();
+                if (icx == 0) {
+                    max1 = s_max[0];
+                    k1 = s_knn[0];
+                } else {
+                    max2 = s_max[1];
+                    k2 = s_knn[1];
+                }
+                __syncthreads();
+                if (C.type_check == 0 && k1 >= mn) break;
+                if (C.type_check > 0 && k1 <= 0) break;
+                if (C.type_check == 2 && k1 < mn) break;
+            }
+            bool flag = false;
+            switch (C.type_check) {
+                case 0: flag = (k1 >= mn || k2 >= mn); break;
+                case 1: flag = (k1 >= mn && k2 > 0) || (k1 > 0 && k2 >= mn); break;
+                case 2: flag = (k1 >= mn && k2 >= mn); break;
+            }
+            if (flag) {
+                const float m1 = (-1.7159f < max1) ? max1 : -1.7159f;
+                const float m2 = (-1.7159f < max2) ? max2 : -1.7159f;
+                res.accepted = mod + 1;
+                res.score = fadd(fadd(cd.score, fmul((float)k1, m1)), fmul((float)k2, m2));
+                res.knn = min(k1, k2);
+                break;
+            }
+        }
+        if (threadIdx.x == 0) a.results[ci] = res;
+        __syncthreads();
+    }
+}
+
+int window_smem_bytes() { return (int)sizeof(WindowSmem); }
+
+cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
+                          const LevelDesc* levels, CandResult* results, const CascadeConfig& cfg, int grid, cudaStream_t st) {
+    static_assert(sizeof(WindowSmem) + 64 <= 48 * 1024, "window kernel shared memory must stay under the default 48 KB");
+    WinArgs a;
+    a.gray = gray;
+    a.gpitch = gpitch;
+    a.gw = gw;
+    a.gh = gh;
+    a.cands = cands;
+    a.n_cand = n_cand;
+    a.levels = levels;
+    a.results = results;
+    a.cfg = cfg;
+    window_kernel<<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
+    return cudaGetLastError();
+}
+
+}  // namespace ccnn

@@ -1,0 +1,51 @@
+// Launch wrappers of the detection kernels (host-callable, defined in k_*.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ccnn_common.cuh"
+
+namespace ccnn {
+
+struct FaceOut {
+    int x, y, w, h;
+    float score;
+};
+
+struct ReplayArgs {
+    const Candidate* cands;
+    const int* n_cand;
+    const CandResult* results;
+    const LevelDesc* levels;
+    CascadeConfig cfg;
+    // scratch, each sized for the candidate capacity
+    Det* D;          // detections in the reference's cpu_detect_rect order
+    Det* R;          // reversed + sorted copy
+    Det* M;          // first clustering pass
+    Det* F;          // second clustering pass
+    int* first_dec;  // per candidate: first decisive earlier box (scan test)
+    int* survivors;  // per level: candidates surviving the scan
+    uint8_t* checked;
+    // outputs
+    int* n_raw;
+    FaceOut* faces;
+    int face_cap;
+    int* n_faces;
+};
+
+cudaError_t launch_gray(const uint8_t* src, int spitch, int w, int h, int ch, float* dst, int dpitch, cudaStream_t st);
+cudaError_t launch_gray_u8_resized(const uint8_t* src, int spitch, int sw, int sh, float* dst, int dpitch, int dw, int dh,
+                                   cudaStream_t st);
+cudaError_t launch_resize_f32(const float* src, int spitch, int sw, int sh, float* dst, int dpitch, int dw, int dh, int type,
+                              cudaStream_t st);
+cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, int k2_tiles, const float* gray,
+                          int gpitch, int gw, int gh, float* s1, float* resp, cudaStream_t st);
+cudaError_t launch_candidates(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
+                              Candidate* out, int* n_out, int cap, cudaStream_t st);
+cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
+                          const LevelDesc* levels, CandResult* results, const CascadeConfig& cfg, int grid, cudaStream_t st);
+int window_smem_bytes();
+cudaError_t launch_replay(const ReplayArgs& a, cudaStream_t st);
+
+}  // namespace ccnn

@@ -1,0 +1,228 @@
+// Box geometry, the reference's sort order and its box clustering, usable on host and device.
+//
+// Rect semantics follow src/CNNObjectDetector/type.h:239-328 (Rect, overlap, intersects,
+// operator*). The sort reproduces the permutation of the reference's
+//   std::sort(v.begin(), v.end(), [](Detection& a, Detection& b){ return b.scale < a.scale; })
+// (cnn_detector_v3.cpp:2750). std::sort is not stable, so equal-scale detections come out in
+// the order of libstdc++'s introsort (GCC 13): depth limit 2*floor(log2 n), 16-element
+// threshold, median-of-three pivot moved to the front, unguarded Hoare partition, heapsort
+// fallback, final (unguarded) insertion sort. The same steps are written out here so the GPU
+// yields the identical order; tests compare the permutation with std::sort on the host.
+#pragma once
+
+#include "ccnn_common.cuh"
+
+#if defined(__CUDACC__)
+#define CCNN_HD __host__ __device__ __forceinline__
+#else
+#define CCNN_HD inline
+#endif
+
+namespace ccnn {
+
+CCNN_HD Det make_det(int x, int y, int w, int h, float score, float scale, int knn) {
+    Det d;
+    d.x = x;
+    d.y = y;
+    d.w = w;
+    d.h = h;
+    d.x2 = x + w;
+    d.y2 = y + h;
+    d.score = score;
+    d.scale = scale;
+    d.knn = knn;
+    d.num_detect = 0;
+    return d;
+}
+
+CCNN_HD int imin(int a, int b) { return a > b ? b : a; }
+CCNN_HD int imax(int a, int b) { return a < b ? b : a; }
+
+// Rect::overlap (type.h:284-305): intersection over the bounding-box "union"
+CCNN_HD float rect_overlap(const Det& a, const Det& b) {
+    if (a.x > b.x2 || b.x > a.x2 || a.y > b.y2 || b.y > a.y2) return 0.f;
+    const int X0 = imin(a.x, b.x), X1 = imax(a.x, b.x), X2 = imin(a.x2, b.x2), X3 = imax(a.x2, b.x2);
+    const int Y0 = imin(a.y, b.y), Y1 = imax(a.y, b.y), Y2 = imin(a.y2, b.y2), Y3 = imax(a.y2, b.y2);
+    const float su = (float)((X3 - X0) * (Y3 - Y0));
+    const float si = (float)((X2 - X1) * (Y2 - Y1));
+    return si / su;
+}
+
+// Rect::intersects (type.h:269-283)
+CCNN_HD int rect_intersects(const Det& a, const Det& b) {
+    if (a.x > b.x2 || b.x > a.x2 || a.y > b.y2 || b.y > a.y2) return 0;
+    const int X1 = imax(a.x, b.x), X2 = imin(a.x2, b.x2);
+    const int Y1 = imax(a.y, b.y), Y2 = imin(a.y2, b.y2);
+    return (X2 - X1) * (Y2 - Y1);
+}
+
+// Rect::operator*(0.7f) (type.h:320-327)
+CCNN_HD Det rect_shrink(const Det& r, float s) {
+    s = 1.f - s;
+    const int sx = (int)((float)r.w * s);
+    const int sy = (int)((float)r.h * s);
+    return make_det(r.x + (sx >> 1), r.y + (sy >> 1), r.w - sx, r.h - sy, 0.f, 0.f, 0);
+}
+
+// DropDetection's test of one earlier detection (cnn_detector_v3.cpp:1820-1840):
+// 0 = not decisive, 1 = overlap > 0.5 (a copy is appended, candidate dropped), 2 = dropped
+CCNN_HD int drop_test(const Det& nr, const Det& exp_r, const Det& e) {
+    const float ov = rect_overlap(nr, e);
+    if (ov == 0.f) return 0;
+    if (ov > 0.5f) return 1;
+    if (rect_intersects(e, exp_r) == exp_r.w * exp_r.h) return 2;
+    return 0;
+}
+
+// ---- libstdc++ introsort order for comp(a, b) = b.scale < a.scale ----
+
+CCNN_HD bool comp_scale_desc(const Det& a, const Det& b) { return b.scale < a.scale; }
+
+CCNN_HD void swap_det(Det* a, Det* b) {
+    Det t = *a;
+    *a = *b;
+    *b = t;
+}
+
+CCNN_HD void push_heap_det(Det* first, int hole, int top, Det value) {
+    int parent = (hole - 1) / 2;
+    while (hole > top && comp_scale_desc(first[parent], value)) {
+        first[hole] = first[parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    first[hole] = value;
+}
+
+CCNN_HD void adjust_heap_det(Det* first, int hole, int len, Det value) {
+    const int top = hole;
+    int child = hole;
+    while (child < (len - 1) / 2) {
+        child = 2 * (child + 1);
+        if (comp_scale_desc(first[child], first[child - 1])) child--;
+        first[hole] = first[child];
+        hole = child;
+    }
+    if ((len & 1) == 0 && child == (len - 2) / 2) {
+        child = 2 * (child + 1);
+        first[hole] = first[child - 1];
+        hole = child - 1;
+    }
+    push_heap_det(first, hole, top, value);
+}
+
+CCNN_HD void heap_sort_det(Det* first, int len) {
+    if (len >= 2) {  // make_heap
+        int parent = (len - 2) / 2;
+        while (true) {
+            Det v = first[parent];
+            adjust_heap_det(first, parent, len, v);
+            if (parent == 0) break;
+            parent--;
+        }
+    }
+    // (heap_select over an empty tail is a no-op) sort_heap:
+    int last = len;
+    while (last > 1) {
+        --last;
+        Det v = first[last];
+        first[last] = first[0];
+        adjust_heap_det(first, 0, last, v);
+    }
+}
+
+CCNN_HD void median_to_first(Det* result, Det* a, Det* b, Det* c) {
+    if (comp_scale_desc(*a, *b)) {
+        if (comp_scale_desc(*b, *c)) swap_det(result, b);
+        else if (comp_scale_desc(*a, *c)) swap_det(result, c);
+        else swap_det(result, a);
+    } else if (comp_scale_desc(*a, *c)) swap_det(result, a);
+    else if (comp_scale_desc(*b, *c)) swap_det(result, c);
+    else swap_det(result, b);
+}
+
+CCNN_HD int unguarded_partition(Det* v, int first, int last, int pivot) {
+    while (true) {
+        while (comp_scale_desc(v[first], v[pivot])) ++first;
+        --last;
+        while (comp_scale_desc(v[pivot], v[last])) --last;
+        if (!(first < last)) return first;
+        swap_det(&v[first], &v[last]);
+        ++first;
+    }
+}
+
+CCNN_HD void unguarded_linear_insert(Det* v, int last) {
+    Det val = v[last];
+    int next = last - 1;
+    while (comp_scale_desc(val, v[next])) {
+        v[last] = v[next];
+        last = next;
+        --next;
+    }
+    v[last] = val;
+}
+
+CCNN_HD void insertion_sort(Det* v, int first, int last) {
+    if (first == last) return;
+    for (int i = first + 1; i != last; ++i) {
+        if (comp_scale_desc(v[i], v[first])) {
+            Det val = v[i];
+            for (int k = i; k > first; --k) v[k] = v[k - 1];
+            v[first] = val;
+        } else {
+            unguarded_linear_insert(v, i);
+        }
+    }
+}
+
+CCNN_HD int floor_log2(int n) {
+    int r = 0;
+    while (n > 1) {
+        n >>= 1;
+        ++r;
+    }
+    return r;
+}
+
+// iterative form of the introsort loop: the recursion is on the right part, the loop on the left
+CCNN_HD void introsort_scale_desc(Det* v, int n) {
+    if (n <= 1) return;
+    const int kThreshold = 16;
+    // explicit stack of (first, last, depth) for the recursive calls
+    int st_first[64], st_last[64], st_depth[64];
+    int sp = 0;
+    st_first[sp] = 0;
+    st_last[sp] = n;
+    st_depth[sp] = 2 * floor_log2(n);
+    sp++;
+    while (sp > 0) {
+        sp--;
+        int first = st_first[sp], last = st_last[sp], depth = st_depth[sp];
+        while (last - first > kThreshold) {
+            if (depth == 0) {
+                heap_sort_det(v + first, last - first);
+                break;
+            }
+            --depth;
+            const int mid = first + (last - first) / 2;
+            median_to_first(&v[first], &v[first + 1], &v[mid], &v[last - 1]);
+            const int cut = unguarded_partition(v, first + 1, last, first);
+            // the reference recurses into [cut, last) before continuing with [first, cut);
+            // both halves are disjoint, so finishing the left first gives the same result
+            st_first[sp] = cut;
+            st_last[sp] = last;
+            st_depth[sp] = depth;
+            sp++;
+            last = cut;
+        }
+    }
+    if (n > kThreshold) {
+        insertion_sort(v, 0, kThreshold);
+        for (int i = kThreshold; i < n; ++i) unguarded_linear_insert(v, i);
+    } else {
+        insertion_sort(v, 0, n);
+    }
+}
+
+}  // namespace ccnn

@@ -1,0 +1,69 @@
+/* compactcnncascade_b200 — inspection entry points of the detection path.
+ *
+ * These expose the path's internal steps so that each can be checked against the reference's
+ * own objects on the same inputs: the gray converter (ImageConverter::Img8uToImg32fGRAY,
+ * src/CNNObjectDetector/image_proc.cpp:299-317), the pyramid resizer
+ * (ImageResizer::FastImageResize, image_resize.cpp:564-584), the stage-1 net
+ * (ConvNeuralNetwork::Forward, cnn_simd_cntk.cpp:964-995), the per-level response maps and
+ * candidate scan (CNNDetector::RunCheckDetect, cnn_detector_v3.cpp:1842-2011) and the raw
+ * detection list before clustering (cpu_detect_rect, cnn_detector_v3.cpp:2745-2750).
+ * They are not needed to run the detector.
+ */
+#ifndef CCNN_INSPECT_H
+#define CCNN_INSPECT_H
+
+#include "ccnn.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int width, height;           /* level image size */
+    float scale;
+    int resp_width, resp_height; /* stage-1 response map size */
+} ccnn_level_info;
+
+typedef struct {
+    int level;                   /* level index (0 = largest scale) */
+    int x, y;                    /* point in level pixels (4 x response index) */
+    float score;                 /* stage-1 response */
+    int accepted;                /* stage-2/3 verdict: 0 no, 1 first window, 2 shrunken retry window */
+    float check_score;           /* score of an accepted window */
+    int knn;
+} ccnn_candidate;
+
+typedef struct {
+    int x, y, width, height;
+    float score, scale;
+    int knn, num_detect;
+} ccnn_detection;
+
+/* fp32 gray from 8-bit gray/BGR/BGRA; both pointers device memory, steps in bytes. The source
+ * step must be a multiple of 64 and both pointers 64-byte aligned. */
+CCNN_API ccnn_status ccnn_gray_u8_to_f32(const unsigned char* d_src, int cols, int rows, int channels, size_t src_step, float* d_dst,
+                                         size_t dst_step, void* stream);
+
+/* fp32 resize; type 0 = nearest neighbour, 1 = bilinear (ImgResize enum). Device pointers. */
+CCNN_API ccnn_status ccnn_resize_f32(const float* d_src, int src_cols, int src_rows, size_t src_step, float* d_dst, int dst_cols,
+                                     int dst_rows, size_t dst_step, int type, void* stream);
+
+/* Stage-1 net of the handle on one fp32 device image (treated as a single pyramid level at
+ * scale 1). The response map (dense, resp_cols floats per row) goes to d_resp. */
+CCNN_API ccnn_status ccnn_stage1_forward(ccnn_handle h, const float* d_img, int cols, int rows, size_t step, float* d_resp, int resp_cap,
+                                         int* resp_cols, int* resp_rows, void* stream);
+
+/* Intermediates of the handle's last frame. */
+CCNN_API ccnn_status ccnn_inspect_levels(ccnn_handle h, ccnn_level_info* out, int capacity, int* n_levels);
+CCNN_API ccnn_status ccnn_inspect_response(ccnn_handle h, int level, float* out, int capacity);
+CCNN_API ccnn_status ccnn_inspect_candidates(ccnn_handle h, ccnn_candidate* out, int capacity, int* n);
+CCNN_API ccnn_status ccnn_inspect_raw_detections(ccnn_handle h, ccnn_detection* out, int capacity, int* n);
+
+/* The permutation the detector's device sort applies to detections with the given scales
+ * (perm[i] = input index placed at slot i); equals std::sort with comp(a, b) = b < a. */
+CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CCNN_INSPECT_H */

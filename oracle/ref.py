@@ -1,0 +1,161 @@
+"""Test infrastructure only: ctypes access to the reference's own CPU path.
+
+oracle/_ref/libccnn_ref.so (strict IEEE build) and libccnn_ref_fast.so (the reference's shipped
+-O2 -ffast-math flags) are compiled by oracle/Makefile from the unmodified reference sources plus
+oracle/ref_harness.cpp. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+arm may use this module; it is the checker, never the measured or shipped path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_STRICT = os.path.join(HERE, "_ref", "libccnn_ref.so")
+REF_FAST = os.path.join(HERE, "_ref", "libccnn_ref_fast.so")
+MODELS = os.path.join(HERE, "..", "compactcnncascade_b200", "models")
+
+
+class RefParams(ctypes.Structure):
+    _fields_ = [("max_image_w", ctypes.c_int), ("max_image_h", ctypes.c_int), ("min_face_height", ctypes.c_int),
+                ("max_face_height", ctypes.c_int), ("scale_factor", ctypes.c_float), ("min_neighbors", ctypes.c_int),
+                ("detect_precision", ctypes.c_int), ("treshold", ctypes.c_float * 3), ("drop_detect", ctypes.c_int),
+                ("equalize", ctypes.c_int), ("reflection", ctypes.c_int), ("detect_mode", ctypes.c_int)]
+
+
+class RefDet(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_int), ("y", ctypes.c_int), ("w", ctypes.c_int), ("h", ctypes.c_int),
+                ("score", ctypes.c_float), ("scale", ctypes.c_float), ("knn", ctypes.c_int), ("num_detect", ctypes.c_int)]
+
+
+def available(fast=False):
+    return os.path.exists(REF_FAST if fast else REF_STRICT)
+
+
+_libs = {}
+
+
+def load(fast=False):
+    path = REF_FAST if fast else REF_STRICT
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (oracle/Makefile needs the reference sources)")
+        L = ctypes.CDLL(path)
+        vp, ci, P = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER
+        L.ref_gray.argtypes = [vp, ci, ci, ci, ci, vp]
+        L.ref_resize_f32.argtypes = [vp, ci, ci, ci, vp, ci, ci, ci]
+        L.ref_resize_u8.argtypes = [vp, ci, ci, ci, vp, ci, ci, ci]
+        L.ref_equalize.argtypes = [vp, ci, ci]
+        L.ref_net_forward.argtypes = [ctypes.c_char_p, ci, vp, ci, ci, ci, vp, ci, P(ci), P(ci)]
+        L.ref_face_detect.argtypes = [P(RefParams), vp, ci, ci, ci, ci, P(RefDet), ci]
+        L.ref_api_init.argtypes = [P(RefParams)]
+        L.ref_api_detect.argtypes = [vp, ci, ci, ci, ci, P(RefDet), ci]
+        L.ref_detect_steps.argtypes = [P(RefParams), vp, ci, ci, ci, ci,
+                                       vp, P(ci), P(ci),
+                                       ci, P(ci), vp, vp, vp,
+                                       vp, ctypes.c_long,
+                                       vp, vp, vp, ctypes.c_long,
+                                       P(RefDet), ci, P(ci),
+                                       P(RefDet), ci]
+        L.ref_sort_by_scale_desc.argtypes = [vp, ci, vp]
+        L.ref_merger.argtypes = [P(RefDet), ci, ctypes.c_float, ci, P(RefDet), ci]
+        _libs[path] = L
+    return _libs[path]
+
+
+def params(min_face=40, max_face=240, scale_factor=1.15, max_w=1920, max_h=1080, precision=3, thr=(-1.5, -1.25, -1.0),
+           min_neighbors=2, drop_detect=1, equalize=1, reflection=1, detect_mode=1):
+    return RefParams(max_w, max_h, min_face, max_face, scale_factor, min_neighbors, precision,
+                     (ctypes.c_float * 3)(*thr), drop_detect, equalize, reflection, detect_mode)
+
+
+def gray(img):
+    L = load()
+    h, w = img.shape[:2]
+    ch = 1 if img.ndim == 2 else img.shape[2]
+    out = np.empty((h, w), np.float32)
+    rc = L.ref_gray(img.ctypes.data, w, h, ch, img.strides[0], out.ctypes.data)
+    assert rc == 0
+    return out
+
+
+def resize_f32(src, dw, dh, type_):
+    L = load()
+    src = np.ascontiguousarray(src, np.float32)
+    out = np.empty((dh, dw), np.float32)
+    L.ref_resize_f32(src.ctypes.data, src.shape[1], src.shape[0], src.shape[1], out.ctypes.data, dw, dh, type_)
+    return out
+
+
+def net_forward(stage, img, index_output):
+    L = load()
+    img = np.ascontiguousarray(img, np.float32)
+    out = np.empty(img.size, np.float32)
+    ow, oh = ctypes.c_int(), ctypes.c_int()
+    path = os.path.join(MODELS, f"cnn4face{stage}_cntk.bin").encode()
+    rc = L.ref_net_forward(path, index_output, img.ctypes.data, img.shape[1], img.shape[0], img.shape[1], out.ctypes.data,
+                           out.size, ctypes.byref(ow), ctypes.byref(oh))
+    if rc != 0:
+        raise RuntimeError(f"ref_net_forward failed ({rc})")
+    return out[: ow.value * oh.value].reshape(oh.value, ow.value)
+
+
+def face_detect(img, p, fast=False):
+    L = load(fast)
+    h, w = img.shape[:2]
+    ch = 1 if img.ndim == 2 else img.shape[2]
+    out = (RefDet * 65536)()
+    n = L.ref_face_detect(ctypes.byref(p), img.ctypes.data, w, h, ch, img.strides[0], out, 65536)
+    if n < 0:
+        raise RuntimeError(f"ref_face_detect failed ({n})")
+    return [(d.x, d.y, d.w, d.h, d.score) for d in out[:n]]
+
+
+def detect_steps(img, p):
+    """Replay of CNNDetector::Detect capturing gray, levels, response maps, raw and final detections."""
+    L = load()
+    h, w = img.shape[:2]
+    ch = 1 if img.ndim == 2 else img.shape[2]
+    gray_out = np.empty(h * w, np.float32)
+    gw, gh = ctypes.c_int(), ctypes.c_int()
+    cap = 512
+    nl = ctypes.c_int()
+    scales = np.empty(cap, np.float32)
+    lw = np.empty(cap, np.int32)
+    lh = np.empty(cap, np.int32)
+    lev_cap = int(w * h * 3)
+    levels = np.empty(lev_cap, np.float32)
+    rw = np.empty(cap, np.int32)
+    rh = np.empty(cap, np.int32)
+    resp = np.empty(lev_cap // 8 + 1024, np.float32)
+    raw = (RefDet * 400000)()
+    nraw = ctypes.c_int()
+    fin = (RefDet * 65536)()
+    nf = L.ref_detect_steps(ctypes.byref(p), img.ctypes.data, w, h, ch, img.strides[0],
+                            gray_out.ctypes.data, ctypes.byref(gw), ctypes.byref(gh),
+                            cap, ctypes.byref(nl), scales.ctypes.data, lw.ctypes.data, lh.ctypes.data,
+                            levels.ctypes.data, lev_cap,
+                            rw.ctypes.data, rh.ctypes.data, resp.ctypes.data, resp.size,
+                            raw, 400000, ctypes.byref(nraw), fin, 65536)
+    if nf < 0:
+        raise RuntimeError(f"ref_detect_steps failed ({nf})")
+    res = {"gray": gray_out[: gw.value * gh.value].reshape(gh.value, gw.value), "levels": [], "resp": []}
+    lo = ro = 0
+    for i in range(nl.value):
+        W, H = int(lw[i]), int(lh[i])
+        res["levels"].append((W, H, float(scales[i]), np.array(levels[lo: lo + W * H]).reshape(H, W)))
+        lo += W * H
+        RW, RH = int(rw[i]), int(rh[i])
+        res["resp"].append(np.array(resp[ro: ro + RW * RH]).reshape(RH, RW))
+        ro += RW * RH
+    res["raw"] = [(d.x, d.y, d.w, d.h, d.score, d.scale, d.knn, d.num_detect) for d in raw[: nraw.value]]
+    res["final"] = [(d.x, d.y, d.w, d.h, d.score) for d in fin[:nf]]
+    return res
+
+
+def sort_perm(keys):
+    L = load()
+    keys = np.ascontiguousarray(keys, np.float32)
+    perm = np.empty(len(keys), np.int32)
+    L.ref_sort_by_scale_desc(keys.ctypes.data, len(keys), perm.ctypes.data)
+    return perm
