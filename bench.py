@@ -1,0 +1,407 @@
+"""Throughput of the plain face-detection cascade on 1920x1080 BGR frames.
+
+A step is one pass of the detection path over a batch of B synthetic 1080p frames (seeded
+generator: 20 face patches of 30-300 px), detector settings min face 40, max face 240,
+scale factor 1.15, precision high, drop_detect/equalize/reflection on.
+
+  value  frames/s over all ranks, inputs resident in device memory when timing starts;
+         device time from CUDA events recorded by the library on its own streams
+         (ccnn_detect_device_batch), summed over the K timed steps, max over ranks.
+  e2e    the same frames through the public host-memory API (ccnn_detect_batch) from pinned
+         host buffers: upload, the cascade and the result download inside the timed region
+         (host wall clock around the synchronous calls).
+
+Multi-GPU: frames are independent, so N ranks are N replicas on disjoint frame seeds, with no
+data-path collective; value = all ranks' frames / the slowest rank's time.
+
+`--impl reference` times the reference's own CPU cascade (oracle/_ref, built from the
+unmodified sources with the reference's shipped flags) on all host cores on the same workload.
+"""
+import argparse
+import ctypes
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H = 1920, 1080
+N_FACES, MIN_PATCH, MAX_PATCH = 20, 30, 300
+MIN_FACE, MAX_FACE, SCALE_FACTOR = 40, 240, 1.15
+WORKLOAD = "plain cascade, 1920x1080 BGR synthetic frames (20 face patches 30-300 px), min face 40, max face 240, scale 1.15"
+METRIC = "1080p frames/s & p99 ms, batched+gated vs plain cascade at >=99% box recall"
+KERNELS = ["gray", "stage1_front", "stage1_back", "cand_count", "cand_write", "stage23_windows", "replay_merge"]
+
+
+def _gen_frame(seed):
+    import compactcnncascade_b200 as ccnn
+    img, _ = ccnn.synth_frame(W, H, seed, N_FACES, MIN_PATCH, MAX_PATCH)
+    return img
+
+
+def _frames(seeds, workers):
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(min(workers, len(seeds))) as pool:
+        return pool.map(_gen_frame, seeds)
+
+
+# ---------------- reference CPU path (test oracle; never the measured product) ----------------
+
+def _ref_worker(args):
+    seeds, fast = args
+    from oracle import ref
+    import compactcnncascade_b200 as ccnn
+    L = ref.load(fast=fast)
+    p = ref.params(min_face=MIN_FACE, max_face=MAX_FACE, scale_factor=SCALE_FACTOR)
+    L.ref_api_init(ctypes.byref(p))
+    out = (ref.RefDet * 65536)()
+    frames = [ccnn.synth_frame(W, H, s, N_FACES, MIN_PATCH, MAX_PATCH)[0] for s in seeds]
+    # first call re-initialises for colour input (cnn_detector_v3.cpp:2531-2546): warm-up
+    L.ref_api_detect(frames[0].ctypes.data, W, H, 3, W * 3, out, 65536)
+    t = time.perf_counter()
+    n = 0
+    for f in frames:
+        n += max(0, L.ref_api_detect(f.ctypes.data, W, H, 3, W * 3, out, 65536))
+    return time.perf_counter() - t, len(frames), n
+
+
+def reference_cpu(frames_per_worker=2, workers=None, seed0=10_000):
+    """All host cores, one reference detector per process (the reference API is a per-process
+    singleton). Returns (frames/s, workers, frames, seconds, kind)."""
+    from oracle import ref
+    fast = ref.available(fast=True)
+    kind = "reference"
+    if not ref.available(fast=fast):
+        return None
+    workers = workers or os.cpu_count() or 1
+    jobs = [([seed0 + w * frames_per_worker + i for i in range(frames_per_worker)], fast) for w in range(workers)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+        res = pool.map(_ref_worker, jobs)
+    wall = max(r[0] for r in res)
+    nfr = sum(r[1] for r in res)
+    return nfr / wall, workers, nfr, wall, kind, fast
+
+
+# ---------------- clocks ----------------
+
+class ClockSampler:
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ---------------- work accounting (per frame) ----------------
+
+def algorithmic_work(levels, gw, gh):
+    """Stage-1 FLOPs and algorithmic bytes of the two stage-1 kernels for one frame."""
+    fl_front = fl_back = 0
+    by_front = 4 * gw * gh
+    by_back = 0
+    for (w, h, _s, ow, oh) in levels:
+        w1, h1 = w - 3, h - 3
+        p1w, p1h = w1 >> 1, h1 >> 1
+        w2, h2 = p1w - 2, p1h - 2
+        fl_front += 2 * 64 * w1 * h1
+        fl_back += 2 * (72 * w2 * h2 + 580 * ow * oh)
+        by_front += 16 * p1w * p1h
+        by_back += 16 * p1w * p1h + 4 * ow * oh
+    return {"stage1_front": (fl_front, by_front), "stage1_back": (fl_back, by_back)}
+
+
+def frame_bytes(levels, w, h):
+    """Algorithmic bytes of a frame: BGR read, gray write+read, each level write+read, response maps."""
+    return 3 * w * h + 8 * w * h + sum(8 * a[0] * a[1] for a in levels) + sum(4 * a[3] * a[4] for a in levels)
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------- main ----------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=16, help="frames per step")
+    ap.add_argument("--distinct", type=int, default=24, help="distinct frames cycled (24 x 6.2 MB > L2)")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-frames", type=int, default=2, help="frames per host core for the CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--latency-frames", type=int, default=200)
+    ap.add_argument("--profile-iters", type=int, default=20)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    # frames and the CPU baseline use spawn pools, started before this process touches CUDA
+    seeds = [rank * 100_000 + i for i in range(args.distinct)]
+    frames = _frames(seeds, os.cpu_count() or 4)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = reference_cpu(frames_per_worker=args.cpu_frames)
+
+    import torch
+    import compactcnncascade_b200 as ccnn
+    from compactcnncascade_b200 import _capi
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+
+    p = ccnn.default_params()
+    p.max_image_width, p.max_image_height = W, H
+    p.min_face_height, p.max_face_height, p.scale_factor = MIN_FACE, MAX_FACE, SCALE_FACTOR
+    p.detect_mode = 1
+    p.cuda_device_id = dev
+    det = ccnn.FaceDetector()
+    if det.Init(p) != 0:
+        raise SystemExit(f"detector init failed: {_capi.last_error()}")
+    L = _capi.lib()
+
+    d_frames = [torch.from_numpy(f).to(f"cuda:{dev}") for f in frames]
+    h_frames = [torch.from_numpy(f).pin_memory() for f in frames]
+    B = args.batch
+    cap = 256
+
+    def make_batch(step, dev_side):
+        arr = (_capi.Image * B)()
+        for j in range(B):
+            k = (step * B + j) % len(frames)
+            t = d_frames[k] if dev_side else h_frames[k]
+            arr[j] = _capi.Image(W, H, 3, t.data_ptr(), W * 3)
+        return arr
+
+    faces = (_capi.Face * (B * cap))()
+    nf = (ctypes.c_int * B)()
+    gms = ctypes.c_float()
+
+    def device_step(step):
+        st = L.ccnn_detect_device_batch(det._h, make_batch(step, True), B, faces, cap, nf, ctypes.byref(gms))
+        if st < 0:
+            raise SystemExit(f"ccnn_detect_device_batch failed: {_capi.last_error()}")
+        return gms.value
+
+    def host_step(step):
+        st = L.ccnn_detect_batch(det._h, make_batch(step, False), B, faces, cap, nf)
+        if st < 0:
+            raise SystemExit(f"ccnn_detect_batch failed: {_capi.last_error()}")
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- value: device-resident inputs ----
+    for s in range(args.warmup):
+        device_step(s)
+    barrier()
+    with ClockSampler(dev) as clk:
+        t0 = time.perf_counter()
+        gpu_ms = 0.0
+        faces_total = 0
+        for s in range(args.steps):
+            gpu_ms += device_step(args.warmup + s)
+            faces_total += sum(nf[j] for j in range(B))
+        barrier()
+        wall_dev = time.perf_counter() - t0
+    clocks = clk.summary()
+    t_dev = gpu_ms / 1e3
+    if dist:
+        t = torch.tensor([t_dev, wall_dev], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev, wall_dev = float(t[0]), float(t[1])
+    frames_timed = args.steps * B * world
+    value = frames_timed / t_dev
+
+    # ---- e2e: pinned host frames through the public host API ----
+    for s in range(args.warmup):
+        host_step(s)
+    barrier()
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        host_step(args.warmup + s)
+    barrier()
+    wall_e2e = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([wall_e2e], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall_e2e = float(t[0])
+    e2e = frames_timed / wall_e2e
+
+    # ---- single-frame latency (synchronous ccnn_detect, pinned host input) ----
+    lat = []
+    one = (_capi.Face * cap)()
+    n1 = ctypes.c_int()
+    for i in range(args.latency_frames):
+        t = h_frames[i % len(frames)]
+        im = _capi.Image(W, H, 3, t.data_ptr(), W * 3)
+        t0 = time.perf_counter()
+        L.ccnn_detect(det._h, ctypes.byref(im), one, cap, ctypes.byref(n1))
+        lat.append((time.perf_counter() - t0) * 1e3)
+    lat = np.array(lat[min(5, len(lat) - 1):])
+
+    # ---- per-kernel profile of the last frame (CUDA events around each kernel) ----
+    kms = (ctypes.c_float * 7)()
+    L.ccnn_profile_last_frame(det._h, args.profile_iters, kms, 7)
+    kernel_ms = {KERNELS[i]: float(kms[i]) for i in range(7)}
+    levels = det.levels()
+    cands = det.candidates()
+    work = algorithmic_work(levels, W, H)
+    dom = max(kernel_ms, key=kernel_ms.get)
+    hbm_peak, peak_src = load_peaks()
+    sm_mhz = clocks.get("sm_max_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # nominal FMA peak, TFLOP/s
+    if dom in work:
+        fl, by = work[dom]
+    else:
+        fl, by = work["stage1_front"]
+    ms = kernel_ms[dom]
+    achieved_gbs = by / (ms * 1e-3) / 1e9
+    achieved_tf = fl / (ms * 1e-3) / 1e12
+    roofline = {
+        "kernel": dom, "bound": "hbm", "achieved": round(achieved_gbs, 2), "peak": hbm_peak, "unit": "GB/s",
+        "frac": round(achieved_gbs / hbm_peak, 4), "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
+        "traffic": None, "kernel_ms": round(ms, 4), "algorithmic_bytes_per_launch": by,
+        "fp32": {"achieved_tflops": round(achieved_tf, 3), "nominal_fma_peak_tflops": round(fp32_peak, 1),
+                 "frac": round(achieved_tf / fp32_peak, 4), "flops_per_launch": fl,
+                 "note": "compute-bound on CUDA cores; the exact reference arithmetic issues separate FMUL+FADD (no FMA), "
+                         "so the attainable ceiling is half the FMA peak"},
+        "kernel_ms_all": {k: round(v, 4) for k, v in kernel_ms.items()},
+    }
+    fb = frame_bytes(levels, W, H)
+
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "frames/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(t_dev / args.steps * 1e3, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generator; no public frames available)",
+        "config": {"workload": WORKLOAD, "frames_per_step": B, "distinct_frames": len(frames),
+                   "l2": f"inputs larger than L2: {len(frames)} distinct frames x {W * H * 3 / 1e6:.1f} MB cycled",
+                   "parallelism": f"replicas x{world}", "levels": len(levels),
+                   "stage1_candidates_last_frame": len(cands), "faces_per_frame": round(faces_total / (args.steps * B), 2)},
+        "p50_ms": round(float(np.percentile(lat, 50)), 3),
+        "p99_ms": round(float(np.percentile(lat, 99)), 3),
+        "hbm_frac_frame_bytes": round(value / world * fb / (hbm_peak * 1e9), 5),
+        "clocks": clocks,
+        "e2e": {"value": round(e2e, 2), "unit": "frames/s", "h2d_bytes_per_step": B * W * H * 3,
+                "d2h_bytes_per_step": B * (4 + 1024 * 20)},
+        "gpu_launches": len(KERNELS) * args.steps * B,
+        "roofline": roofline,
+        "wall_value": round(frames_timed / wall_dev, 2),
+    }
+    if cpu:
+        fps, workers, nfr, secs, kind, fast = cpu
+        line["cpu_baseline"] = {"value": round(fps, 3), "unit": "frames/s", "cores": workers, "kind": kind,
+                                "sample": f"{nfr} frames of the same workload, {args.cpu_frames} per core, "
+                                          f"reference plain-C++ cascade ({'-O2 -ffast-math as shipped' if fast else 'strict IEEE build'}), {secs:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    det.Clear()
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_reference(args, world, rank):
+    """The reference's own CPU cascade on all host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent at build time)"}))
+        return
+    per_step = []
+    total_frames = 0
+    workers = os.cpu_count() or 1
+    for s in range(args.warmup + args.steps):
+        fps, workers, nfr, secs, kind, fast = reference_cpu(frames_per_worker=1, seed0=20_000 + s * 1000)
+        if s >= args.warmup:
+            per_step.append(secs)
+            total_frames += nfr
+    t = sum(per_step)
+    v = total_frames / t
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "frames/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator)", "config": {"workload": WORKLOAD, "frames_per_step": workers,
+                                                               "parallelism": f"{workers} host processes"},
+            "cpu_baseline": {"value": round(v, 3), "unit": "frames/s", "cores": workers, "kind": "reference",
+                             "sample": f"{total_frames} frames, one per host core per step, reference plain-C++ cascade "
+                                       f"({'-O2 -ffast-math as shipped' if fast else 'strict IEEE build'})"},
+            "e2e": {"value": round(v, 3), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

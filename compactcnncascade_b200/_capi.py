@@ -28,7 +28,7 @@ EXPORTED = [
     "ccnn_set_max_object_height", "ccnn_set_num_threads", "ccnn_last_error", "ccnn_version",
     "ccnn_gray_u8_to_f32", "ccnn_resize_f32", "ccnn_stage1_forward", "ccnn_inspect_levels",
     "ccnn_inspect_response", "ccnn_inspect_candidates", "ccnn_inspect_raw_detections",
-    "ccnn_sort_permutation",
+    "ccnn_sort_permutation", "ccnn_detect_device_batch", "ccnn_profile_last_frame",
 ]
 
 
@@ -118,6 +118,8 @@ def lib():
         L.ccnn_inspect_candidates.argtypes = [vp, P(CandidateInfo), ci, P(ci)]
         L.ccnn_inspect_raw_detections.argtypes = [vp, P(Detection), ci, P(ci)]
         L.ccnn_sort_permutation.argtypes = [vp, ci, vp]
+        L.ccnn_detect_device_batch.argtypes = [vp, P(Image), ci, P(Face), ci, P(ci), P(ctypes.c_float)]
+        L.ccnn_profile_last_frame.argtypes = [vp, ci, P(ctypes.c_float), ci]
         _lib = L
     return _lib
 

@@ -101,7 +101,21 @@ CCNN_API ccnn_status ccnn_detect_batch(ccnn_handle h, const ccnn_image* imgs, in
         set_error("null argument");
         return CCNN_ERR_INVALID_ARG;
     }
-    return h->det.detect_batch(imgs, n_images, faces, capacity_per_image, n_faces);
+    return h->det.detect_batch(imgs, n_images, false, faces, capacity_per_image, n_faces, nullptr);
+}
+
+CCNN_API ccnn_status ccnn_detect_device_batch(ccnn_handle h, const ccnn_image* imgs, int n_images, ccnn_face* faces,
+                                              int capacity_per_image, int* n_faces, float* gpu_ms) {
+    if (!h) {
+        set_error("null argument");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    return h->det.detect_batch(imgs, n_images, true, faces, capacity_per_image, n_faces, gpu_ms);
+}
+
+CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* kernel_ms, int n_kernels) {
+    if (!h || !kernel_ms || n_kernels <= 0) return CCNN_ERR_INVALID_ARG;
+    return h->det.profile(iters, kernel_ms, n_kernels);
 }
 
 CCNN_API ccnn_status ccnn_get_gray_device(ccnn_handle h, const float** data, int* cols, int* rows, size_t* step) {

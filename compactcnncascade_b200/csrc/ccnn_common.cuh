@@ -119,6 +119,12 @@ struct CandResult {
     int pad;
 };
 
+// stage-2/3 output summary of one (candidate, window, stage) work item
+struct WinOut {
+    float max;  // largest of the 16 responses (starting from -10)
+    int knn;    // responses above the stage threshold
+};
+
 struct Det {
     int x, y, w, h, x2, y2;
     float score, scale;

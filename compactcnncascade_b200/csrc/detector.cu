@@ -59,6 +59,7 @@ void Detector::free_slot(Slot& s) {
     cudaFree(s.d_cands);
     cudaFree(s.d_ncand);
     cudaFree(s.d_results);
+    cudaFree(s.d_win);
     cudaFree(s.D);
     cudaFree(s.R);
     cudaFree(s.M);
@@ -251,8 +252,9 @@ ccnn_status Detector::init() {
     chunk_cap_ = std::max(chunk_cap_, 1);
     cudaDeviceProp prop;
     CCNN_CUDA(cudaGetDeviceProperties(&prop, device_));
-    // persistent stage-2/3 grid: 6 resident 256-thread CTAs per SM (shared memory bound)
-    window_grid_ = prop.multiProcessorCount * 6;
+    // persistent stage-2/3 grid: 4 resident 256-thread CTAs per SM (register bound)
+    window_grid_ = prop.multiProcessorCount * 4;
+    CCNN_CUDA(replay_setup());
 
     inited_ = true;
     for (auto& s : slots_) {
@@ -278,6 +280,7 @@ ccnn_status Detector::alloc_slot(Slot& s) {
     CCNN_CUDA(cudaMalloc(&s.d_cands, sizeof(Candidate) * cand_cap_));
     CCNN_CUDA(cudaMalloc(&s.d_ncand, sizeof(int)));
     CCNN_CUDA(cudaMalloc(&s.d_results, sizeof(CandResult) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.d_win, sizeof(WinOut) * 4 * cand_cap_));
     CCNN_CUDA(cudaMalloc(&s.D, sizeof(Det) * cand_cap_));
     CCNN_CUDA(cudaMalloc(&s.R, sizeof(Det) * cand_cap_));
     CCNN_CUDA(cudaMalloc(&s.M, sizeof(Det) * cand_cap_));
@@ -397,13 +400,15 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
     CCNN_CUDA(launch_candidates(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                 (int)cand_cap_, s.st));
     if (detect_enabled_)
-        CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_results, cfg_,
+        CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
                                 window_grid_, s.st));
     ReplayArgs a;
     a.cands = s.d_cands;
     a.n_cand = s.d_ncand;
+    a.win = s.d_win;
     a.results = s.d_results;
     a.levels = p.d_levels;
+    a.n_levels = p.n_levels;
     a.cfg = cfg_;
     a.D = s.D;
     a.R = s.R;
@@ -544,7 +549,8 @@ ccnn_status Detector::detect(const ccnn_image& img, bool device_input, cudaStrea
     return collect(s, faces, cap, n);
 }
 
-ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, ccnn_face* faces, int cap_per, int* n_faces) {
+ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, bool device_input, ccnn_face* faces, int cap_per, int* n_faces,
+                                   float* gpu_ms) {
     std::lock_guard<std::mutex> lk(mu_);
     if (n_img < 0 || (n_img > 0 && (!imgs || !n_faces)) || cap_per < 0 || (cap_per > 0 && n_img > 0 && !faces)) {
         set_error("invalid arguments");
@@ -554,6 +560,15 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, ccnn_face*
     int pending[kSlots];
     for (int k = 0; k < kSlots; ++k) pending[k] = -1;
     ccnn_status worst = CCNN_OK;
+    // device time of the whole batch: from an event before the first frame's upload (both
+    // slot streams wait on it) to an event after the last frame of either slot
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (gpu_ms && inited_) {
+        CCNN_CUDA(cudaEventCreate(&t0));
+        CCNN_CUDA(cudaEventCreate(&t1));
+        CCNN_CUDA(cudaEventRecord(t0, slots_[0].st));
+        for (int k = 1; k < kSlots; ++k) CCNN_CUDA(cudaStreamWaitEvent(slots_[k].st, t0, 0));
+    }
     for (int i = 0; i < n_img; ++i) {
         const int k = i % kSlots;
         Slot& s = slots_[k];
@@ -581,9 +596,15 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, ccnn_face*
             n_faces[i] = 0;
             continue;
         }
-        st = enqueue(slots_[k], *p, imgs[i], false, nullptr);
+        st = enqueue(slots_[k], *p, imgs[i], device_input, nullptr);
         if (st != CCNN_OK) return st;
         pending[k] = i;
+    }
+    if (t0) {
+        if (inited_) {
+            for (int k = 1; k < kSlots; ++k) CCNN_CUDA(cudaStreamWaitEvent(slots_[0].st, slots_[k].done, 0));
+            CCNN_CUDA(cudaEventRecord(t1, slots_[0].st));
+        }
     }
     for (int k = 0; k < kSlots; ++k)
         if (pending[k] >= 0) {
@@ -591,6 +612,13 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, ccnn_face*
             if (st < 0) return st;
             if (st == CCNN_TRUNCATED) worst = CCNN_TRUNCATED;
         }
+    if (t0) {
+        float ms = 0.f;
+        if (inited_ && cudaEventSynchronize(t1) == cudaSuccess && cudaEventElapsedTime(&ms, t0, t1) == cudaSuccess) *gpu_ms = ms;
+        else *gpu_ms = -1.f;
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+    }
     return worst;
 }
 
@@ -722,6 +750,75 @@ ccnn_status Detector::stage1_forward(const float* d_img, int w, int h, size_t st
     CCNN_CUDA(cudaFreeAsync(d_s1, st));
     CCNN_CUDA(cudaFreeAsync(d_l, st));
     CCNN_CUDA(cudaStreamSynchronize(st));
+    return CCNN_OK;
+}
+
+// Re-runs the last frame's kernel chain on slot 0 `iters` times with an event between every
+// two kernels; ms[k] gets the mean duration of kernel k: gray, stage-1 front, stage-1 back,
+// candidate count, candidate write, stage-2/3 windows, replay.
+ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
+    std::lock_guard<std::mutex> lk(mu_);
+    Slot& s = slots_[0];
+    if (!inited_ || !s.last_plan || iters <= 0) {
+        set_error("no frame has been processed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(device_);
+    const Plan& p = *s.last_plan;
+    constexpr int K = 7;
+    cudaEvent_t ev[K + 1];
+    for (auto& e : ev) CCNN_CUDA(cudaEventCreate(&e));
+    double acc[K] = {0};
+    ReplayArgs a;
+    a.cands = s.d_cands;
+    a.n_cand = s.d_ncand;
+    a.win = s.d_win;
+    a.results = s.d_results;
+    a.levels = p.d_levels;
+    a.n_levels = p.n_levels;
+    a.cfg = cfg_;
+    a.D = s.D;
+    a.R = s.R;
+    a.M = s.M;
+    a.F = s.F;
+    a.first_dec = s.first_dec;
+    a.survivors = s.survivors;
+    a.checked = s.checked;
+    a.n_raw = s.d_nraw;
+    a.faces = s.d_faces;
+    a.face_cap = (int)cand_cap_;
+    a.n_faces = s.d_nfaces;
+    for (int it = 0; it < iters; ++it) {
+        CCNN_CUDA(cudaEventRecord(ev[0], s.st));
+        if (p.downscale)
+            CCNN_CUDA(launch_gray_u8_resized(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, s.d_gray, s.gray_pitch, p.gw, p.gh, s.st));
+        else
+            CCNN_CUDA(launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st));
+        CCNN_CUDA(cudaEventRecord(ev[1], s.st));
+        CCNN_CUDA(launch_stage1_front(w1_, p.d_levels, p.n_levels, p.k1_tiles, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_s1, s.st));
+        CCNN_CUDA(cudaEventRecord(ev[2], s.st));
+        CCNN_CUDA(launch_stage1_back(w1_, p.d_levels, p.n_levels, p.k2_tiles, s.d_s1, s.d_resp, s.st));
+        CCNN_CUDA(cudaEventRecord(ev[3], s.st));
+        CCNN_CUDA(launch_cand_count(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.st));
+        CCNN_CUDA(cudaEventRecord(ev[4], s.st));
+        CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
+                                    (int)cand_cap_, s.st));
+        CCNN_CUDA(cudaEventRecord(ev[5], s.st));
+        if (detect_enabled_)
+            CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
+                                    window_grid_, s.st));
+        CCNN_CUDA(cudaEventRecord(ev[6], s.st));
+        CCNN_CUDA(launch_replay(a, s.st));
+        CCNN_CUDA(cudaEventRecord(ev[7], s.st));
+        CCNN_CUDA(cudaEventSynchronize(ev[7]));
+        for (int k = 0; k < K; ++k) {
+            float m = 0.f;
+            CCNN_CUDA(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));
+            acc[k] += m;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < n_ms && k < K; ++k) ms[k] = (float)(acc[k] / iters);
     return CCNN_OK;
 }
 

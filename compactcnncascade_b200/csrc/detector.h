@@ -45,6 +45,7 @@ struct Slot {
     Candidate* d_cands = nullptr;
     int* d_ncand = nullptr;
     CandResult* d_results = nullptr;
+    WinOut* d_win = nullptr;
     Det *D = nullptr, *R = nullptr, *M = nullptr, *F = nullptr;
     int* first_dec = nullptr;
     int* survivors = nullptr;
@@ -61,7 +62,7 @@ struct Slot {
 
 class Detector {
    public:
-    static constexpr int kSlots = 2;
+    static constexpr int kSlots = 4;
     static constexpr int kHostFaces = 1024;
 
     Detector() = default;
@@ -69,7 +70,9 @@ class Detector {
 
     ccnn_status create(const ccnn_params& p, const char* const* model_paths);
     ccnn_status detect(const ccnn_image& img, bool device_input, cudaStream_t user_stream, ccnn_face* faces, int cap, int* n);
-    ccnn_status detect_batch(const ccnn_image* imgs, int n_img, ccnn_face* faces, int cap_per, int* n_faces);
+    ccnn_status detect_batch(const ccnn_image* imgs, int n_img, bool device_input, ccnn_face* faces, int cap_per, int* n_faces,
+                             float* gpu_ms);
+    ccnn_status profile(int iters, float* ms, int n_ms);
 
     ccnn_status get_gray_device(const float** data, int* cols, int* rows, size_t* step);
     ccnn_status get_gray_host(float* out, int cap, int* cols, int* rows);

@@ -105,12 +105,24 @@ __global__ void __launch_bounds__(kChunkThreads) cand_write_kernel(const int4* _
     }
 }
 
-cudaError_t launch_candidates(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
-                              Candidate* out, int* n_out, int cap, cudaStream_t st) {
+cudaError_t launch_cand_count(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
+                              cudaStream_t st) {
+    if (n_chunks > 0) cand_count_kernel<<<n_chunks, kChunkThreads, 0, st>>>(d_chunks, d_levels, resp, thr, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
+                              const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st) {
     if (n_chunks <= 0) return cudaMemsetAsync(n_out, 0, sizeof(int), st);
-    cand_count_kernel<<<n_chunks, kChunkThreads, 0, st>>>(d_chunks, d_levels, resp, thr, counts);
     cand_write_kernel<<<n_chunks, kChunkThreads, 0, st>>>(d_chunks, n_chunks, d_levels, resp, thr, counts, out, n_out, cap);
     return cudaGetLastError();
+}
+
+cudaError_t launch_candidates(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
+                              Candidate* out, int* n_out, int cap, cudaStream_t st) {
+    cudaError_t e = launch_cand_count(d_chunks, n_chunks, d_levels, resp, thr, counts, st);
+    if (e != cudaSuccess) return e;
+    return launch_cand_write(d_chunks, n_chunks, d_levels, resp, thr, counts, out, n_out, cap, st);
 }
 
 }  // namespace ccnn

@@ -168,37 +168,123 @@ __device__ int merger_warp(const Det* in, int n, uint8_t* checked, Det* out, flo
     return nout;
 }
 
+constexpr int kMaxLevels = 1024;
+
+// stage-2/3 verdict of one candidate from its four speculative (max, count) pairs, applying the
+// reference's order: stage 2, early exits (:1698-1706), stage 3, accept rule (:1709-1725), retry
+// with the shrunken window when rejected and double_check is on (:1806-1811)
+__device__ __forceinline__ CandResult verdict(const WinOut* w, const Candidate& cd, float scale, const CascadeConfig& C) {
+    const int mn = (C.adapt_min_neighbors && scale > 0.7f && C.min_neighbors > 1) ? C.min_neighbors - 1 : C.min_neighbors;
+    CandResult r;
+    r.accepted = 0;
+    r.score = 0.f;
+    r.knn = 0;
+    r.pad = 0;
+    const int n_mod = C.double_check ? 2 : 1;
+    for (int mod = 0; mod < n_mod; ++mod) {
+        const float max1 = w[2 * mod].max;
+        const int k1 = w[2 * mod].knn;
+        const bool stop = (C.type_check == 0 && k1 >= mn) || (C.type_check > 0 && k1 <= 0) || (C.type_check == 2 && k1 < mn);
+        const float max2 = stop ? -10.f : w[2 * mod + 1].max;
+        const int k2 = stop ? 0 : w[2 * mod + 1].knn;
+        bool flag = false;
+        switch (C.type_check) {
+            case 0: flag = (k1 >= mn || k2 >= mn); break;
+            case 1: flag = (k1 >= mn && k2 > 0) || (k1 > 0 && k2 >= mn); break;
+            case 2: flag = (k1 >= mn && k2 >= mn); break;
+        }
+        if (flag) {
+            const float m1 = (-1.7159f < max1) ? max1 : -1.7159f;
+            const float m2 = (-1.7159f < max2) ? max2 : -1.7159f;
+            r.accepted = mod + 1;
+            r.score = fadd(fadd(cd.score, fmul((float)k1, m1)), fmul((float)k2, m2));
+            r.knn = imin(k1, k2);
+            return r;
+        }
+    }
+    return r;
+}
+
 __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
-    __shared__ int s_e, s_nD, s_nS;
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ int s_lvl_start[kMaxLevels + 1];
+    __shared__ int s_nD, s_nS;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const CascadeConfig& C = a.cfg;
     const int n = *a.n_cand;
-    int nD = 0;  // kept uniform in every thread through s_nD
-    int g = 0;
-    while (g < n) {
-        const int lev = a.cands[g].level;
-        if (tid == 0) s_e = n;
-        __syncthreads();
-        for (int base = g; base < n; base += kRT) {
-            const int i = base + tid;
-            if (i < n && a.cands[i].level != lev) atomicMin(&s_e, i);
-            __syncthreads();
-            if (s_e < n) break;
+    const int nl = a.n_levels;
+
+    // working set in shared memory when it fits (121 bytes per candidate), else global scratch:
+    //   region A: candidates, verdicts, scan results, survivors (40 B each); later the first merge
+    //   region B: detections in reference order; later the second merge
+    //   region C: reversed + sorted detections; region E: merge flags
+    const bool fits = (long long)n * 121 + 64 <= kReplaySmemBytes;
+    Candidate* cands;
+    CandResult* res;
+    int* first_dec;
+    int* surv;
+    Det *D, *R, *M, *F;
+    uint8_t* checked;
+    if (fits) {
+        unsigned char* p = sm;
+        cands = reinterpret_cast<Candidate*>(p);
+        res = reinterpret_cast<CandResult*>(p + 16LL * n);
+        first_dec = reinterpret_cast<int*>(p + 32LL * n);
+        surv = reinterpret_cast<int*>(p + 36LL * n);
+        M = reinterpret_cast<Det*>(p);
+        D = reinterpret_cast<Det*>(p + 40LL * n);
+        F = D;
+        R = reinterpret_cast<Det*>(p + 80LL * n);
+        checked = p + 120LL * n;
+        for (int i = tid; i < n; i += kRT) cands[i] = a.cands[i];
+    } else {
+        cands = const_cast<Candidate*>(a.cands);
+        res = a.results;
+        first_dec = a.first_dec;
+        surv = a.survivors;
+        D = a.D;
+        R = a.R;
+        M = a.M;
+        F = a.F;
+        checked = a.checked;
+    }
+    for (int l = tid; l <= nl; l += kRT) s_lvl_start[l] = 0;
+    __syncthreads();
+    // verdicts and per-level candidate counts (candidates are grouped by level, smallest first)
+    for (int i = tid; i < n; i += kRT) {
+        const Candidate cd = cands[i];
+        if (C.detect_enabled) {
+            const CandResult r = verdict(a.win + (size_t)i * 4, cd, a.levels[cd.level].scale, C);
+            res[i] = r;
+            if (fits) a.results[i] = r;  // kept for inspection
         }
-        const int e = s_e;
-        const LevelDesc L = a.levels[lev];
+        atomicAdd(&s_lvl_start[nl - 1 - cd.level + 1], 1);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int k = 1; k <= nl; ++k) s_lvl_start[k] += s_lvl_start[k - 1];
+        s_nD = 0;
+    }
+    __syncthreads();
+
+    int nD = 0;
+    for (int k = 0; k < nl; ++k) {
+        const int g = s_lvl_start[k], e = s_lvl_start[k + 1];
+        if (g == e) continue;
+        const int lev = nl - 1 - k;
+        const LevelDesc& L = a.levels[lev];
         const float scale = L.scale, inv_scale = L.inv_scale;
         const int n_prefix = nD;
 
         if (C.drop_detect) {
             // scan test against the detections of earlier levels, one warp per candidate
             for (int c = g + warp; c < e; c += kRT / 32) {
-                const Det nr = cand_rect(a.cands[c], inv_scale, scale);
+                const Det nr = cand_rect(cands[c], inv_scale, scale);
                 const Det ex = rect_shrink(nr, 0.7f);
                 int code = -1;
                 for (int base = 0; base < n_prefix; base += 32) {
-                    const int k = base + lane;
-                    const int t = k < n_prefix ? drop_test(nr, ex, a.D[k]) : 0;
+                    const int kk = base + lane;
+                    const int t = kk < n_prefix ? drop_test(nr, ex, D[kk]) : 0;
                     const unsigned m = __ballot_sync(0xffffffffu, t != 0);
                     if (m) {
                         const int f = __ffs(m) - 1;
@@ -207,23 +293,24 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                         break;
                     }
                 }
-                if (lane == 0) a.first_dec[c] = code;
+                if (lane == 0) first_dec[c] = code;
             }
             __syncthreads();
             if (warp == 0) {
                 int nS = 0;
                 for (int c = g; c < e; ++c) {
-                    const Det nr = cand_rect(a.cands[c], inv_scale, scale);
-                    int code = a.first_dec[c];
+                    const int code = first_dec[c];
                     int k0 = -1, type = 0;
+                    Det nr;
                     if (code >= 0) {
                         k0 = code >> 1;
                         type = (code & 1) + 1;
-                    } else {
+                    } else if (nD > n_prefix) {
+                        nr = cand_rect(cands[c], inv_scale, scale);
                         const Det ex = rect_shrink(nr, 0.7f);
                         for (int base = n_prefix; base < nD; base += 32) {
-                            const int k = base + lane;
-                            const int t = k < nD ? drop_test(nr, ex, a.D[k]) : 0;
+                            const int kk = base + lane;
+                            const int t = kk < nD ? drop_test(nr, ex, D[kk]) : 0;
                             const unsigned m = __ballot_sync(0xffffffffu, t != 0);
                             if (m) {
                                 const int f = __ffs(m) - 1;
@@ -236,15 +323,16 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                     if (k0 >= 0) {
                         if (type == 1) {
                             if (lane == 0) {
-                                const Det src = a.D[k0];
-                                a.D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, src.score, scale, src.knn);
+                                nr = cand_rect(cands[c], inv_scale, scale);
+                                const Det src = D[k0];
+                                D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, src.score, scale, src.knn);
                             }
                             nD++;
+                            __syncwarp();
                         }
-                        __syncwarp();
                         continue;
                     }
-                    if (lane == 0) a.survivors[nS] = c;
+                    if (lane == 0) surv[nS] = c;
                     nS++;
                 }
                 if (lane == 0) {
@@ -260,14 +348,14 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
             const int nS = C.drop_detect ? s_nS : (e - g);
             const int rect_size = nD;
             for (int si = 0; si < nS; ++si) {
-                const int c = C.drop_detect ? a.survivors[si] : g + si;
-                const Candidate cd = a.cands[c];
+                const int c = C.drop_detect ? surv[si] : g + si;
+                const Candidate cd = cands[c];
                 const Det nr = cand_rect(cd, inv_scale, scale);
-                if (C.drop_detect && C.detect_enabled) {
+                if (C.drop_detect && C.detect_enabled && nD > rect_size) {
                     int k0 = -1;
                     for (int base = rect_size; base < nD; base += 32) {
-                        const int k = base + lane;
-                        const bool hit = k < nD && rect_overlap(nr, a.D[k]) > 0.5f;
+                        const int kk = base + lane;
+                        const bool hit = kk < nD && rect_overlap(nr, D[kk]) > 0.5f;
                         const unsigned m = __ballot_sync(0xffffffffu, hit);
                         if (m) {
                             k0 = base + __ffs(m) - 1;
@@ -276,8 +364,8 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                     }
                     if (k0 >= 0) {
                         if (lane == 0) {
-                            const Det src = a.D[k0];
-                            a.D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, src.score, scale, src.knn);
+                            const Det src = D[k0];
+                            D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, src.score, scale, src.knn);
                         }
                         nD++;
                         __syncwarp();
@@ -285,12 +373,12 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                     }
                 }
                 if (!C.detect_enabled) {
-                    if (lane == 0) a.D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, cd.score, scale, 0);
+                    if (lane == 0) D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, cd.score, scale, 0);
                     nD++;
                 } else {
-                    const CandResult r = a.results[c];
+                    const CandResult r = res[c];
                     if (r.accepted) {
-                        if (lane == 0) a.D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, r.score, scale, r.knn);
+                        if (lane == 0) D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, r.score, scale, r.knn);
                         nD++;
                     }
                 }
@@ -300,50 +388,53 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
         }
         __syncthreads();
         nD = s_nD;
-        g = e;
     }
+
+    // raw list (reference order) to global memory for inspection; reversed copy for the sort
+    if (fits)
+        for (int i = tid; i < nD; i += kRT) a.D[i] = D[i];
+    for (int i = tid; i < nD; i += kRT) R[i] = D[nD - 1 - i];
+    __syncthreads();
 
     // post-processing in warp 0
     if (warp != 0) return;
     if (lane == 0) *a.n_raw = nD;
-    for (int i = lane; i < nD; i += 32) a.R[i] = a.D[nD - 1 - i];
-    __syncwarp();
-    if (nD > 16 && lane == 0) introsort_scale_desc(a.R, nD);
+    if (nD > 16 && lane == 0) introsort_scale_desc(R, nD);
     __syncwarp();
     int nF = 0;
-    const Det* fin = a.R;
+    const Det* fin = R;
     if (nD > 0) {
         if (C.merger_detect) {
-            int nM = merger_warp(a.R, nD, a.checked, a.M, 0.5f, false);
+            int nM = merger_warp(R, nD, checked, M, 0.5f, false);
             if (C.min_num_detect > 1) {
                 // stable erase of clusters with fewer than min_num_detect merges
                 int w = 0;
                 for (int base = 0; base < nM; base += 32) {
-                    const int k = base + lane;
-                    const bool keep = k < nM && a.M[k].num_detect >= C.min_num_detect;
-                    const Det v = k < nM ? a.M[k] : a.M[0];
+                    const int kk = base + lane;
+                    const bool keep = kk < nM && M[kk].num_detect >= C.min_num_detect;
+                    const Det v = kk < nM ? M[kk] : M[0];
                     const unsigned m = __ballot_sync(0xffffffffu, keep);
                     const int pos = w + __popc(m & ((1u << lane) - 1u));
                     __syncwarp();
-                    if (keep) a.M[pos] = v;
+                    if (keep) M[pos] = v;
                     __syncwarp();
                     w += __popc(m);
                 }
                 nM = w;
             }
             if (nM > 0) {
-                nF = merger_warp(a.M, nM, a.checked, a.F, 0.2f, true);
-                fin = a.F;
+                nF = merger_warp(M, nM, checked, F, 0.2f, true);
+                fin = F;
             } else {
                 nF = 0;
             }
         } else {
             nF = nD;
-            fin = a.R;
+            fin = R;
         }
     }
     for (int i = lane; i < nF && i < a.face_cap; i += 32) {
-        Det d = fin[i];
+        const Det d = fin[i];
         FaceOut f;
         if (C.rescale_output) {
             f.x = (int)((float)d.x * C.rescale);
@@ -362,8 +453,10 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
     if (lane == 0) *a.n_faces = nF;
 }
 
+cudaError_t replay_setup() { return cudaFuncSetAttribute(replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReplaySmemBytes); }
+
 cudaError_t launch_replay(const ReplayArgs& a, cudaStream_t st) {
-    replay_kernel<<<1, kRT, 0, st>>>(a);
+    replay_kernel<<<1, kRT, kReplaySmemBytes, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -196,11 +196,23 @@ __global__ void __launch_bounds__(256) stage1_back_kernel(const __grid_constant_
     if (gx < L.ow && gy < L.oh) resp[L.resp_off + (long long)gy * L.ow + gx] = r;
 }
 
-cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, int k2_tiles, const float* gray,
-                          int gpitch, int gw, int gh, float* s1, float* resp, cudaStream_t st) {
+cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, const float* gray, int gpitch,
+                                int gw, int gh, float* s1, cudaStream_t st) {
     if (k1_tiles > 0) stage1_front_kernel<<<k1_tiles, 256, 0, st>>>(W, d_levels, n_levels, gray, gpitch, gw, gh, s1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k2_tiles, const float* s1, float* resp,
+                               cudaStream_t st) {
     if (k2_tiles > 0) stage1_back_kernel<<<k2_tiles, 256, 0, st>>>(W, d_levels, n_levels, s1, resp);
     return cudaGetLastError();
+}
+
+cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, int k2_tiles, const float* gray,
+                          int gpitch, int gw, int gh, float* s1, float* resp, cudaStream_t st) {
+    cudaError_t e = launch_stage1_front(W, d_levels, n_levels, k1_tiles, gray, gpitch, gw, gh, s1, st);
+    if (e != cudaSuccess) return e;
+    return launch_stage1_back(W, d_levels, n_levels, k2_tiles, s1, resp, st);
 }
 
 }  // namespace ccnn

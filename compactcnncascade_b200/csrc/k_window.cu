@@ -10,11 +10,12 @@
 //   4x4 response maps counted against treshold_2 / treshold_3 with the type_check early exits
 //   (:1655-1706) and the accept rule (:1709-1725); score s0 + k1*max(-1.7159, m1) + k2*max(-1.7159, m2).
 //
-// Every candidate is evaluated (first window, and the retry window when the first is rejected);
-// whether the reference would have reached it (drop_detect) is decided later by the replay
-// kernel, so the result is the same while all candidates run in parallel.
+// Every candidate is evaluated speculatively: both nets on both the first and the retry window,
+// as four independent CTA work items. Which of them the reference would have reached (early
+// exits, retry, drop_detect) is decided by the replay kernel, so the verdicts are the same while
+// all items run in parallel.
 //
-// One CTA (256 threads) per candidate, persistent over the candidate list. The networks run
+// One CTA (256 threads) per work item, persistent over the item list. The networks run
 // entirely in shared memory: L1 (6 maps, 44x48 -> pooled 22x24), neighbour sums, L2 (12 maps,
 // 20x22 -> pooled 10x11), sums, L3 (24 maps, 7w x 8h -> 4x4), hidden layer and output neuron.
 #include "kernels.h"
@@ -152,7 +153,7 @@ struct WinArgs {
     const Candidate* cands;
     const int* n_cand;
     const LevelDesc* levels;
-    CandResult* results;
+    WinOut* out;
     CascadeConfig cfg;
 };
 
@@ -234,74 +235,54 @@ __device__ void prepare_window(const WinArgs& a, WindowSmem& S, const Candidate&
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kWT) window_kernel(const __grid_constant__ WindowNets N, const WinArgs a) {
+// One work item = (candidate, window): window 0 is the first crop, window 1 the shrunken retry
+// crop. Both windows of a candidate run in parallel (the retry is speculative: whether the
+// reference reaches it is decided by the replay kernel). Inside an item, stage 3 runs only when
+// stage 2 does not end the check (the reference's early exits, cnn_detector_v3.cpp:1698-1706);
+// otherwise its slot keeps (max -10, count 0), exactly what the reference leaves behind.
+__global__ void __launch_bounds__(kWT, 4) window_kernel(const __grid_constant__ WindowNets N, const WinArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WindowSmem& S = *reinterpret_cast<WindowSmem*>(smem_raw);
-    __shared__ float s_max[2];
-    __shared__ int s_knn[2];
     const int n = *a.n_cand;
     const CascadeConfig& C = a.cfg;
-    for (int ci = blockIdx.x; ci < n; ci += gridDim.x) {
+    const int per_cand = C.double_check ? 2 : 1;
+    const int total = n * per_cand;
+    for (int it = blockIdx.x; it < total; it += gridDim.x) {
+        const int ci = it / per_cand;
+        const int mod = it - ci * per_cand;
         const Candidate cd = a.cands[ci];
         const LevelDesc& L = a.levels[cd.level];
-        const float scale = L.scale, inv_scale = L.inv_scale;
-        const int mn = (C.adapt_min_neighbors && scale > 0.7f && C.min_neighbors > 1) ? C.min_neighbors - 1 : C.min_neighbors;
-        CandResult res;
-        res.accepted = 0;
-        res.score = 0.f;
-        res.knn = 0;
-        res.pad = 0;
-        const int n_mod = C.double_check ? 2 : 1;
-        for (int mod = 0; mod < n_mod; ++mod) {
-            prepare_window(a, S, cd, inv_scale, mod);
-            float max1 = -10.f, max2 = -10.f;
-            int k1 = 0, k2 = 0;
-            for (int icx = 0; icx < 2; ++icx) {
-                if (icx == 0)
-                    window_net(N.s2, S, 0);
-                else
-                    window_net(N.s3, S, C.reflection ? 1 : 2);
-                if (threadIdx.x == 0) {
-                    float mx = -10.f;
-                    int kc = 0;
-                    const float thr = icx == 0 ? C.thr2 : C.thr3;
-                    for (int o = 0; o < kOutN; ++o) {
-                        const float d = S.out[o];
-                        mx = (mx < d) ? d : mx;
-                        if (d > thr) kc++;
-                    }
-                    s_max[icx] = mx;
-                    s_knn[icx] = kc;
-                }
-                __syncthreads();
-                if (icx == 0) {
-                    max1 = s_max[0];
-                    k1 = s_knn[0];
-                } else {
-                    max2 = s_max[1];
-                    k2 = s_knn[1];
-                }
-                __syncthreads();
-                if (C.type_check == 0 && k1 >= mn) break;
-                if (C.type_check > 0 && k1 <= 0) break;
-                if (C.type_check == 2 && k1 < mn) break;
+        const int mn = (C.adapt_min_neighbors && L.scale > 0.7f && C.min_neighbors > 1) ? C.min_neighbors - 1 : C.min_neighbors;
+        prepare_window(a, S, cd, L.inv_scale, mod);
+        WinOut r[2];
+        r[1].max = -10.f;
+        r[1].knn = 0;
+        for (int stage = 0; stage < 2; ++stage) {
+            if (stage == 0)
+                window_net(N.s2, S, 0);
+            else
+                window_net(N.s3, S, C.reflection ? 1 : 2);
+            // every thread reduces the 16 responses itself (no extra barrier needed)
+            const float thr = stage == 0 ? C.thr2 : C.thr3;
+            float mx = -10.f;
+            int kc = 0;
+#pragma unroll
+            for (int o = 0; o < kOutN; ++o) {
+                const float d = S.out[o];
+                mx = (mx < d) ? d : mx;  // MAX(max_score, d) (cnn_detector_v3.cpp:1667-1683)
+                if (d > thr) kc++;
             }
-            bool flag = false;
-            switch (C.type_check) {
-                case 0: flag = (k1 >= mn || k2 >= mn); break;
-                case 1: flag = (k1 >= mn && k2 > 0) || (k1 > 0 && k2 >= mn); break;
-                case 2: flag = (k1 >= mn && k2 >= mn); break;
-            }
-            if (flag) {
-                const float m1 = (-1.7159f < max1) ? max1 : -1.7159f;
-                const float m2 = (-1.7159f < max2) ? max2 : -1.7159f;
-                res.accepted = mod + 1;
-                res.score = fadd(fadd(cd.score, fmul((float)k1, m1)), fmul((float)k2, m2));
-                res.knn = min(k1, k2);
-                break;
+            r[stage].max = mx;
+            r[stage].knn = kc;
+            if (stage == 0) {
+                const bool stop = (C.type_check == 0 && kc >= mn) || (C.type_check > 0 && kc <= 0) || (C.type_check == 2 && kc < mn);
+                if (stop) break;
             }
         }
-        if (threadIdx.x == 0) a.results[ci] = res;
+        if (threadIdx.x == 0) {
+            a.out[(size_t)ci * 4 + 2 * mod] = r[0];
+            a.out[(size_t)ci * 4 + 2 * mod + 1] = r[1];
+        }
         __syncthreads();
     }
 }
@@ -309,7 +290,7 @@ __global__ void __launch_bounds__(kWT) window_kernel(const __grid_constant__ Win
 int window_smem_bytes() { return (int)sizeof(WindowSmem); }
 
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
-                          const LevelDesc* levels, CandResult* results, const CascadeConfig& cfg, int grid, cudaStream_t st) {
+                          const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st) {
     static_assert(sizeof(WindowSmem) + 64 <= 48 * 1024, "window kernel shared memory must stay under the default 48 KB");
     WinArgs a;
     a.gray = gray;
@@ -319,7 +300,7 @@ cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, in
     a.cands = cands;
     a.n_cand = n_cand;
     a.levels = levels;
-    a.results = results;
+    a.out = out;
     a.cfg = cfg;
     window_kernel<<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
     return cudaGetLastError();

@@ -16,8 +16,10 @@ struct FaceOut {
 struct ReplayArgs {
     const Candidate* cands;
     const int* n_cand;
-    const CandResult* results;
+    const WinOut* win;     // 4 per candidate: (window 0, stage 2), (0, 3), (1, 2), (1, 3)
+    CandResult* results;   // verdict per candidate (written by the replay kernel)
     const LevelDesc* levels;
+    int n_levels;
     CascadeConfig cfg;
     // scratch, each sized for the candidate capacity
     Det* D;          // detections in the reference's cpu_detect_rect order
@@ -41,11 +43,22 @@ cudaError_t launch_resize_f32(const float* src, int spitch, int sw, int sh, floa
                               cudaStream_t st);
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, int k2_tiles, const float* gray,
                           int gpitch, int gw, int gh, float* s1, float* resp, cudaStream_t st);
+cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, const float* gray, int gpitch,
+                                int gw, int gh, float* s1, cudaStream_t st);
+cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k2_tiles, const float* s1, float* resp,
+                               cudaStream_t st);
+cudaError_t launch_cand_count(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
+                              cudaStream_t st);
+cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
+                              const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st);
 cudaError_t launch_candidates(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
                               Candidate* out, int* n_out, int cap, cudaStream_t st);
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
-                          const LevelDesc* levels, CandResult* results, const CascadeConfig& cfg, int grid, cudaStream_t st);
+                          const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st);
 int window_smem_bytes();
+// dynamic shared memory of the replay kernel (set once per device before any launch)
+constexpr int kReplaySmemBytes = 200 * 1024;
+cudaError_t replay_setup();
 cudaError_t launch_replay(const ReplayArgs& a, cudaStream_t st);
 
 }  // namespace ccnn

@@ -105,6 +105,12 @@ CCNN_API ccnn_status ccnn_detect_device(ccnn_handle h, const ccnn_image* img, vo
 CCNN_API ccnn_status ccnn_detect_batch(ccnn_handle h, const ccnn_image* imgs, int n_images, ccnn_face* faces, int capacity_per_image,
                                        int* n_faces);
 
+/* Several device frames (img[i].data are device pointers) of one size, pipelined like
+ * ccnn_detect_batch. gpu_ms (nullable) receives the device time of the whole batch, measured with
+ * CUDA events on the handle's streams from before the first frame to after the last. */
+CCNN_API ccnn_status ccnn_detect_device_batch(ccnn_handle h, const ccnn_image* imgs, int n_images, ccnn_face* faces,
+                                              int capacity_per_image, int* n_faces, float* gpu_ms);
+
 /* FaceDetector::getGrayImage32F (CompactCNNLibAPI_v2.cpp:464-505), GPU pipeline: the internal fp32
  * gray image of the last frame, as a device pointer with its size and row pitch in bytes.
  * Valid until the next call on the handle. */

@@ -59,6 +59,11 @@ CCNN_API ccnn_status ccnn_inspect_response(ccnn_handle h, int level, float* out,
 CCNN_API ccnn_status ccnn_inspect_candidates(ccnn_handle h, ccnn_candidate* out, int capacity, int* n);
 CCNN_API ccnn_status ccnn_inspect_raw_detections(ccnn_handle h, ccnn_detection* out, int capacity, int* n);
 
+/* Re-runs the handle's last frame `iters` times and writes the mean duration (ms, CUDA events)
+ * of each kernel of the chain: [0] gray, [1] stage-1 front, [2] stage-1 back, [3] candidate count,
+ * [4] candidate write, [5] stage-2/3 windows, [6] replay/sort/merge. */
+CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* kernel_ms, int n_kernels);
+
 /* The permutation the detector's device sort applies to detections with the given scales
  * (perm[i] = input index placed at slot i); equals std::sort with comp(a, b) = b < a. */
 CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm);

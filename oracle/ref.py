@@ -111,45 +111,49 @@ def face_detect(img, p, fast=False):
     return [(d.x, d.y, d.w, d.h, d.score) for d in out[:n]]
 
 
-def detect_steps(img, p):
+def detect_steps(img, p, with_levels=True):
     """Replay of CNNDetector::Detect capturing gray, levels, response maps, raw and final detections."""
     L = load()
     h, w = img.shape[:2]
     ch = 1 if img.ndim == 2 else img.shape[2]
-    gray_out = np.empty(h * w, np.float32)
-    gw, gh = ctypes.c_int(), ctypes.c_int()
-    cap = 512
-    nl = ctypes.c_int()
-    scales = np.empty(cap, np.float32)
-    lw = np.empty(cap, np.int32)
-    lh = np.empty(cap, np.int32)
-    lev_cap = int(w * h * 3)
-    levels = np.empty(lev_cap, np.float32)
-    rw = np.empty(cap, np.int32)
-    rh = np.empty(cap, np.int32)
-    resp = np.empty(lev_cap // 8 + 1024, np.float32)
-    raw = (RefDet * 400000)()
-    nraw = ctypes.c_int()
-    fin = (RefDet * 65536)()
-    nf = L.ref_detect_steps(ctypes.byref(p), img.ctypes.data, w, h, ch, img.strides[0],
-                            gray_out.ctypes.data, ctypes.byref(gw), ctypes.byref(gh),
-                            cap, ctypes.byref(nl), scales.ctypes.data, lw.ctypes.data, lh.ctypes.data,
-                            levels.ctypes.data, lev_cap,
-                            rw.ctypes.data, rh.ctypes.data, resp.ctypes.data, resp.size,
-                            raw, 400000, ctypes.byref(nraw), fin, 65536)
-    if nf < 0:
-        raise RuntimeError(f"ref_detect_steps failed ({nf})")
-    res = {"gray": gray_out[: gw.value * gh.value].reshape(gh.value, gw.value), "levels": [], "resp": []}
+    img = np.ascontiguousarray(img)
+    cap = 1024
+
+    def run(lev_cap, resp_cap):
+        r = {"gray": np.empty(h * w, np.float32), "gw": ctypes.c_int(), "gh": ctypes.c_int(), "nl": ctypes.c_int(),
+             "scales": np.empty(cap, np.float32), "lw": np.empty(cap, np.int32), "lh": np.empty(cap, np.int32),
+             "rw": np.empty(cap, np.int32), "rh": np.empty(cap, np.int32), "nraw": ctypes.c_int(),
+             "raw": (RefDet * 400000)(), "fin": (RefDet * 65536)()}
+        r["levels"] = np.empty(max(lev_cap, 1), np.float32) if lev_cap else None
+        r["resp"] = np.empty(max(resp_cap, 1), np.float32) if resp_cap else None
+        nf = L.ref_detect_steps(ctypes.byref(p), img.ctypes.data, w, h, ch, img.strides[0],
+                                r["gray"].ctypes.data, ctypes.byref(r["gw"]), ctypes.byref(r["gh"]),
+                                cap, ctypes.byref(r["nl"]), r["scales"].ctypes.data, r["lw"].ctypes.data, r["lh"].ctypes.data,
+                                r["levels"].ctypes.data if lev_cap else None, lev_cap,
+                                r["rw"].ctypes.data, r["rh"].ctypes.data, r["resp"].ctypes.data if resp_cap else None, resp_cap,
+                                r["raw"], 400000, ctypes.byref(r["nraw"]), r["fin"], 65536)
+        if nf < 0:
+            raise RuntimeError(f"ref_detect_steps failed ({nf})")
+        r["nf"] = nf
+        return r
+
+    first = run(0, 0)
+    nl = first["nl"].value
+    lev_cap = int(sum(int(first["lw"][i]) * int(first["lh"][i]) for i in range(nl))) if with_levels else 0
+    resp_cap = int(sum(int(first["rw"][i]) * int(first["rh"][i]) for i in range(nl)))
+    r = run(lev_cap, resp_cap)
+    res = {"gray": r["gray"][: r["gw"].value * r["gh"].value].reshape(r["gh"].value, r["gw"].value), "levels": [], "resp": []}
     lo = ro = 0
-    for i in range(nl.value):
-        W, H = int(lw[i]), int(lh[i])
-        res["levels"].append((W, H, float(scales[i]), np.array(levels[lo: lo + W * H]).reshape(H, W)))
+    for i in range(nl):
+        W, H = int(r["lw"][i]), int(r["lh"][i])
+        lvl = np.array(r["levels"][lo: lo + W * H]).reshape(H, W) if with_levels else None
+        res["levels"].append((W, H, float(r["scales"][i]), lvl))
         lo += W * H
-        RW, RH = int(rw[i]), int(rh[i])
-        res["resp"].append(np.array(resp[ro: ro + RW * RH]).reshape(RH, RW))
+        RW, RH = int(r["rw"][i]), int(r["rh"][i])
+        res["resp"].append(np.array(r["resp"][ro: ro + RW * RH]).reshape(RH, RW))
         ro += RW * RH
-    res["raw"] = [(d.x, d.y, d.w, d.h, d.score, d.scale, d.knn, d.num_detect) for d in raw[: nraw.value]]
-    res["final"] = [(d.x, d.y, d.w, d.h, d.score) for d in fin[:nf]]
+    res["raw"] = [(d.x, d.y, d.w, d.h, d.score, d.scale, d.knn, d.num_detect) for d in r["raw"][: r["nraw"].value]]
+    res["final"] = [(d.x, d.y, d.w, d.h, d.score) for d in r["fin"][: r["nf"]]]
     return res
 
 
