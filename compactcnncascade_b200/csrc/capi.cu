@@ -1,6 +1,7 @@
 // extern "C" boundary: include/ccnn.h and include/ccnn_inspect.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -209,6 +210,50 @@ CCNN_API ccnn_status ccnn_inspect_candidates(ccnn_handle h, ccnn_candidate* out,
 CCNN_API ccnn_status ccnn_inspect_raw_detections(ccnn_handle h, ccnn_detection* out, int capacity, int* n) {
     if (!h || !n || (capacity > 0 && !out)) return CCNN_ERR_INVALID_ARG;
     return h->det.inspect_raw(out, capacity, n);
+}
+
+CCNN_API ccnn_status ccnn_plan_levels(const ccnn_params* p, int cols, int rows, int channels, ccnn_level_info* out, int capacity,
+                                      int* n_levels) {
+    if (!p || !n_levels || cols <= 0 || rows <= 0 || (capacity > 0 && !out)) return CCNN_ERR_INVALID_ARG;
+    // a fresh handle: a frame above max_image_size raises it; a colour frame turns gray_image_only off
+    int max_h = p->max_image_height;
+    if (cols > p->max_image_width || rows > p->max_image_height) max_h = rows;  // Detect :2499-2513 takes the frame size
+    const bool detect = p->detect_mode != CCNN_DETECT_DISABLE;
+    const int ext_w = detect ? 36 + ccnn::kExtOff : ccnn::kPatW, ext_h = detect ? 40 + ccnn::kExtOff : ccnn::kPatH;
+    std::vector<float> scales;
+    bool down = false;
+    float in_scale = 0.f;
+    bool gray_only = channels == 1 || p->detect_precision == CCNN_PRECISION_DEF;
+    if (!ccnn::compute_scales(*p, gray_only, ccnn::kPatH, max_h, &scales, &down, &in_scale)) {
+        set_error("invalid configuration: empty scale list");
+        return CCNN_ERR_CONFIG;
+    }
+    int gw = cols, gh = rows;
+    if (down && channels == 1) {
+        gw = (int)((float)cols * in_scale);
+        gh = (int)((float)rows * in_scale);
+    } else if (down) {
+        set_error("precision 'def' with a colour frame needs min_face_height < 34 (the reference recurses forever)");
+        return CCNN_ERR_CONFIG;
+    }
+    int n = 0;
+    if (cols >= ext_w && rows >= ext_h) {
+        for (size_t i = 0; i < scales.size(); ++i) {
+            const int w = (int)((float)gw * scales[i]), h = (int)((float)gh * scales[i]);
+            if (w < ext_w || h < ext_h) break;
+            if (n < capacity) {
+                out[n].width = w;
+                out[n].height = h;
+                out[n].scale = scales[i];
+                const int p1w = (w - 3) >> 1, p1h = (h - 3) >> 1;
+                out[n].resp_width = ((p1w - 2) >> 1) - 3;
+                out[n].resp_height = ((p1h - 2) >> 1) - 4;
+            }
+            ++n;
+        }
+    }
+    *n_levels = n;
+    return CCNN_OK;
 }
 
 CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm) {

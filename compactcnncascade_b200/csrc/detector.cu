@@ -47,6 +47,40 @@ inline void size_scale(int w, int h, float s, int* ow, int* oh) {
 }
 }  // namespace
 
+// InitScales (cnn_detector_v3.cpp:289-346): scales from max_scale = min(3, 27 / min face) down
+// to min_scale = 27 / max face (or / max image height) by repeated division by the factor. With
+// gray-only input and max_scale < 0.8 the frame itself is shrunk by max_scale and the pyramid
+// starts at 1.
+bool compute_scales(const ccnn_params& p, bool gray_only, int pat_h, int max_h, std::vector<float>* scales, bool* downscale,
+                    float* input_scale) {
+    scales->clear();
+    *downscale = false;
+    *input_scale = 0.f;
+    float max_scale = 1.f;
+    if (p.min_face_height > 0) {
+        max_scale = (float)pat_h / (float)p.min_face_height;
+        max_scale = 3.f > max_scale ? max_scale : 3.f;
+        if (gray_only && max_scale < 0.8f) {
+            *downscale = true;
+            *input_scale = max_scale;
+            max_scale = 1.f;
+        }
+    }
+    float min_scale = p.max_face_height > 0 ? (float)pat_h / (float)p.max_face_height : (float)pat_h / (float)max_h;
+    min_scale = max_scale > min_scale ? min_scale : max_scale;
+    const float sf = p.scale_factor < 1.f ? 1.1f : p.scale_factor;
+    float scale = max_scale;
+    if (sf != 1.f) {
+        while (scale > min_scale) {
+            scales->push_back(scale);
+            scale /= sf;
+        }
+    } else {
+        scales->push_back(scale);
+    }
+    return !scales->empty();
+}
+
 Detector::~Detector() { clear(); }
 
 void Detector::free_slot(Slot& s) {
@@ -145,17 +179,6 @@ ccnn_status Detector::create(const ccnn_params& p, const char* const* model_path
 
 ccnn_status Detector::init() {
     apply_precision();
-    device_ = api_.cuda_device_id;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
-        set_error("no CUDA device available (this detector has no CPU path)");
-        return CCNN_ERR_CUDA;
-    }
-    if (device_ < 0 || device_ >= ndev) {
-        set_error("cuda_device_id out of range");
-        return CCNN_ERR_INVALID_ARG;
-    }
-    CCNN_CUDA(cudaSetDevice(device_));
     if (max_w_ <= 0 || max_h_ <= 0) {
         set_error("max_image_size must be positive");
         return CCNN_ERR_INVALID_ARG;
@@ -190,35 +213,11 @@ ccnn_status Detector::init() {
     }
 
     // InitScales (cnn_detector_v3.cpp:289-346)
-    scales_.clear();
-    input_downscale_ = false;
-    input_scale_ = 0.f;
-    float max_scale = 1.f;
-    if (api_.min_face_height > 0) {
-        max_scale = (float)pat_h_ / (float)api_.min_face_height;
-        max_scale = 3.f > max_scale ? max_scale : 3.f;
-        if (gray_image_only_ && max_scale < 0.8f) {
-            input_downscale_ = true;
-            input_scale_ = max_scale;
-            max_scale = 1.f;
-        }
-    }
-    float min_scale = api_.max_face_height > 0 ? (float)pat_h_ / (float)api_.max_face_height : (float)pat_h_ / (float)max_h_;
-    min_scale = max_scale > min_scale ? min_scale : max_scale;
-    if (api_.scale_factor < 1.f) api_.scale_factor = 1.1f;
-    float scale = max_scale;
-    if (api_.scale_factor != 1.f) {
-        while (scale > min_scale) {
-            scales_.push_back(scale);
-            scale /= api_.scale_factor;
-        }
-    } else {
-        scales_.push_back(scale);
-    }
-    if (scales_.empty()) {
+    if (!compute_scales(api_, gray_image_only_, pat_h_, max_h_, &scales_, &input_downscale_, &input_scale_)) {
         set_error("invalid configuration: empty scale list");
         return CCNN_ERR_CONFIG;
     }
+    if (api_.scale_factor < 1.f) api_.scale_factor = 1.1f;  // InitScales rewrites the parameter (:327-330)
     num_scales_ = (int)scales_.size();
 
     cfg_.thr1 = api_.treshold[0];
@@ -250,6 +249,17 @@ ccnn_status Detector::init() {
     }
     cand_cap_ = std::max(1LL, resp_cap_);
     chunk_cap_ = std::max(chunk_cap_, 1);
+    device_ = api_.cuda_device_id;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        set_error("no CUDA device available (this detector has no CPU path)");
+        return CCNN_ERR_CUDA;
+    }
+    if (device_ < 0 || device_ >= ndev) {
+        set_error("cuda_device_id out of range");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    CCNN_CUDA(cudaSetDevice(device_));
     cudaDeviceProp prop;
     CCNN_CUDA(cudaGetDeviceProperties(&prop, device_));
     // persistent stage-2/3 grid: 4 resident 256-thread CTAs per SM (register bound)

@@ -134,6 +134,8 @@ class Detector {
     ccnn_status apply_precision();
 };
 
+bool compute_scales(const ccnn_params& p, bool gray_only, int pat_h, int max_h, std::vector<float>* scales, bool* downscale,
+                    float* input_scale);
 void set_error(const std::string& msg);
 ccnn_status cuda_status(cudaError_t e, const char* what);
 

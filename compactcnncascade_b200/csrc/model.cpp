@@ -71,7 +71,11 @@ bool parse_model(const uint8_t* data, size_t n, RawModel* m, std::string* err) {
     m->hl = r.get<int32_t>();
     m->conn = r.get<int32_t>();
     m->hs = r.get<int32_t>();
-    if (!r.ok || !m->max_pool || m->kw[1] * m->kh[1] != 9) {
+    if (!r.ok) {
+        *err = "model file is truncated";
+        return false;
+    }
+    if (!m->max_pool || m->kw[1] * m->kh[1] != 9) {
         // the reference refuses the same (cnn_simd_cntk.cpp:322-329)
         *err = "this configuration of cnn models is not supported (max pooling and a 3x3 second layer required)";
         return false;

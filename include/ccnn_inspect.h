@@ -59,6 +59,12 @@ CCNN_API ccnn_status ccnn_inspect_response(ccnn_handle h, int level, float* out,
 CCNN_API ccnn_status ccnn_inspect_candidates(ccnn_handle h, ccnn_candidate* out, int capacity, int* n);
 CCNN_API ccnn_status ccnn_inspect_raw_detections(ccnn_handle h, ccnn_detection* out, int capacity, int* n);
 
+/* The pyramid a freshly created handle processes for a frame of this size and channel count
+ * (CNNDetector::InitScales, cnn_detector_v3.cpp:289-346, with the level-size rule of RunCPUDetect
+ * :2080-2088 and the re-initialisation rules of Detect :2499-2546). Host-only; needs no GPU. */
+CCNN_API ccnn_status ccnn_plan_levels(const ccnn_params* p, int cols, int rows, int channels, ccnn_level_info* out, int capacity,
+                                      int* n_levels);
+
 /* Re-runs the handle's last frame `iters` times and writes the mean duration (ms, CUDA events)
  * of each kernel of the chain: [0] gray, [1] stage-1 front, [2] stage-1 back, [3] candidate count,
  * [4] candidate write, [5] stage-2/3 windows, [6] replay/sort/merge. */
