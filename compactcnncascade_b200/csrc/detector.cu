@@ -299,7 +299,9 @@ ccnn_status Detector::alloc_slot(Slot& s) {
     CCNN_CUDA(cudaMalloc(&s.survivors, sizeof(int) * cand_cap_));
     CCNN_CUDA(cudaMalloc(&s.checked, cand_cap_));
     CCNN_CUDA(cudaMalloc(&s.d_nraw, sizeof(int)));
-    CCNN_CUDA(cudaMalloc(&s.d_faces, sizeof(FaceOut) * cand_cap_));
+    // at least kHostFaces entries: the per-frame download copies that many
+    CCNN_CUDA(cudaMalloc(&s.d_faces, sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces)));
+    CCNN_CUDA(cudaMemset(s.d_faces, 0, sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces)));
     CCNN_CUDA(cudaMalloc(&s.d_nfaces, sizeof(int)));
     CCNN_CUDA(cudaMallocHost(&s.h_nfaces, sizeof(int)));
     CCNN_CUDA(cudaMallocHost(&s.h_faces, sizeof(FaceOut) * kHostFaces));

@@ -121,9 +121,13 @@ def test_gray_device_pointer(frames):
     d.Detect(frames[0])
     ptr, w, h, step = ctypes.c_void_p(), ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
     assert _capi.lib().ccnn_get_gray_device(d._h, ctypes.byref(ptr), ctypes.byref(w), ctypes.byref(h), ctypes.byref(step)) == 0
-    host = np.empty((h.value, step.value // 4), np.float32)
-    torch.cuda.synchronize()
-    import ctypes as C
-    cudart = C.CDLL("libcudart.so") if False else None  # noqa: F841  (copy through the host entry point instead)
-    assert np.array_equal(d.getGrayImage32F(), orc.gray(frames[0]))
-    assert (w.value, h.value) == (640, 480) and step.value % 64 == 0
+    assert ptr.value and (w.value, h.value) == (640, 480) and step.value % 64 == 0
+    # read the device buffer by address
+    n = h.value * step.value // 4
+    buf = torch.empty(n, dtype=torch.float32, device="cuda")
+    cudart = ctypes.CDLL("/usr/local/cuda/lib64/libcudart.so.12")
+    cudart.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    assert cudart.cudaMemcpy(buf.data_ptr(), ptr.value, n * 4, 3) == 0  # cudaMemcpyDeviceToDevice
+    dev = buf.view(h.value, step.value // 4)[:, : w.value].cpu().numpy()
+    assert np.array_equal(dev, d.getGrayImage32F())
+    assert np.array_equal(dev, orc.gray(frames[0]))
