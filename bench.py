@@ -192,8 +192,9 @@ def main():
         run_reference(args, world, rank)
         return
 
+    from compactcnncascade_b200.replicas import rank_seeds
     # frames and the CPU baseline use spawn pools, started before this process touches CUDA
-    seeds = [rank * 100_000 + i for i in range(args.distinct)]
+    seeds = rank_seeds(rank, args.distinct)
     frames = _frames(seeds, os.cpu_count() or 4)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
