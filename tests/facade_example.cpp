@@ -30,6 +30,7 @@ int main(int argc, char** argv) {
     const int n = detector.Detect(faces, img);
     for (int i = 0; i < n; ++i) printf("%d %d %d %d %.6f\n", faces[i].x, faces[i].y, faces[i].width, faces[i].height, faces[i].score);
     FaceDetector::ImageData gray;
-    printf("gray %d %d %dx%d\n", detector.getGrayImage32F(&gray, FaceDetector::Pipeline::CPU), gray.channels, gray.cols, gray.rows);
+    const int grc = detector.getGrayImage32F(&gray, FaceDetector::Pipeline::CPU);
+    printf("gray %d %d %dx%d\n", grc, gray.channels, gray.cols, gray.rows);
     return 0;
 }
