@@ -28,7 +28,7 @@ EXPORTED = [
     "ccnn_set_max_object_height", "ccnn_set_num_threads", "ccnn_last_error", "ccnn_version",
     "ccnn_gray_u8_to_f32", "ccnn_resize_f32", "ccnn_stage1_forward", "ccnn_inspect_levels",
     "ccnn_inspect_response", "ccnn_inspect_candidates", "ccnn_inspect_raw_detections",
-    "ccnn_sort_permutation", "ccnn_detect_device_batch", "ccnn_profile_last_frame", "ccnn_plan_levels",
+    "ccnn_sort_permutation", "ccnn_detect_device_batch", "ccnn_profile_last_frame", "ccnn_plan_levels", "ccnn_stage1_forward_static",
 ]
 
 
@@ -121,6 +121,7 @@ def lib():
         L.ccnn_detect_device_batch.argtypes = [vp, P(Image), ci, P(Face), ci, P(ci), P(ctypes.c_float)]
         L.ccnn_profile_last_frame.argtypes = [vp, ci, P(ctypes.c_float), ci]
         L.ccnn_plan_levels.argtypes = [P(Params), ci, ci, ci, P(LevelInfo), ci, P(ci)]
+        L.ccnn_stage1_forward_static.argtypes = [ctypes.c_char_p, vp, ci, ci, ctypes.c_size_t, vp, ci, P(ci), P(ci), vp]
         _lib = L
     return _lib
 

@@ -53,6 +53,21 @@ CCNN_API ccnn_status ccnn_resize_f32(const float* d_src, int src_cols, int src_r
 CCNN_API ccnn_status ccnn_stage1_forward(ccnn_handle h, const float* d_img, int cols, int rows, size_t step, float* d_resp, int resp_cap,
                                          int* resp_cols, int* resp_rows, void* stream);
 
+/* Stage-1 response map of one fp32 device image, allocating no device memory. No counterpart in
+ * the reference: it serves callers that may not call cudaMalloc — plug-in hosts that budget all
+ * device memory up front and pass a component only its input and output buffers, or processes whose
+ * device memory is already held by another framework's caching allocator, where a new allocation
+ * would fail or stall the device. Instead of per-handle buffers it uses one fixed scratch array
+ * compiled into the library (9 MiB + 256 B per GPU that loads the library, held until exit):
+ * images up to 2,359,296 floats of L1 planes (about 1920x1080, 2^21 pixels) are accepted, larger
+ * ones are refused with CCNN_ERR_INVALID_ARG and a message naming the limit. model_path may be NULL
+ * for the bundled cnn4face1_cntk.bin. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call before any stream capture.
+ * All calls share the array and it keeps the last call's contents; calls that overlap on the GPU
+ * (other streams or threads) race on it. Returns after the response map is written. */
+CCNN_API ccnn_status ccnn_stage1_forward_static(const char* model_path, const float* d_img, int cols, int rows, size_t step,
+                                                float* d_resp, int resp_cap, int* resp_cols, int* resp_rows, void* stream);
+
 /* Intermediates of the handle's last frame. */
 CCNN_API ccnn_status ccnn_inspect_levels(ccnn_handle h, ccnn_level_info* out, int capacity, int* n_levels);
 CCNN_API ccnn_status ccnn_inspect_response(ccnn_handle h, int level, float* out, int capacity);
