@@ -39,6 +39,8 @@ def build(verbose=False, force=False):
     deps += [os.path.join(HERE, "..", "include", f) for f in ("ccnn.h", "ccnn_inspect.h")]
     if force or _stale(out, deps):
         tmp = out + ".tmp"
+        if os.path.exists(out):
+            os.remove(out)  # a failed build must not leave a stale library behind
         _run([NVCC] + NVCC_FLAGS + ["-o", tmp] + srcs + ["-ldl"], verbose)
         os.replace(tmp, out)
     synth = os.path.join(HERE, "libccnn_synth.so")

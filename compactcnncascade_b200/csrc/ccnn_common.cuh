@@ -19,6 +19,44 @@ __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
 
+// Packed pairs of fp32 (sm_100 f32x2 instructions): two independent IEEE round-to-nearest
+// operations per lane per instruction. Used where two outputs run the same operation chain, so
+// each element still sees exactly the reference's sequence of roundings. (Tested against the
+// scalar _rn chain bit for bit by the parity tests.)
+typedef unsigned long long f2_t;
+__device__ __forceinline__ f2_t f2_pack(float lo, float hi) {
+    f2_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float f2_lo(f2_t v) {
+    float lo;
+    asm("{ .reg .f32 t; mov.b64 {%0, t}, %1; }" : "=f"(lo) : "l"(v));
+    return lo;
+}
+__device__ __forceinline__ float f2_hi(f2_t v) {
+    float hi;
+    asm("{ .reg .f32 t; mov.b64 {t, %0}, %1; }" : "=f"(hi) : "l"(v));
+    return hi;
+}
+__device__ __forceinline__ f2_t f2_dup(float v) { return f2_pack(v, v); }
+__device__ __forceinline__ f2_t f2_ld(const float2& v) { return *reinterpret_cast<const f2_t*>(&v); }
+// Packed product. ptxas contracts a packed mul followed by a packed add into one packed FMA
+// (a single rounding), even with fmad disabled, which would break the reference's two-rounding
+// arithmetic. The product is therefore an FMA whose addend is a (-0, -0) pair the compiler cannot
+// see (it comes from the kernel's weight block at run time): fma(a, b, -0) is exactly the rounded
+// product a*b, sign of zero included, and an FMA cannot be merged with the following add.
+__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b, f2_t negzero) {
+    f2_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(negzero));
+    return r;
+}
+__device__ __forceinline__ f2_t f2_add(f2_t a, f2_t b) {
+    f2_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
 // Rational tanh approximation of the reference (cnnpp_cplusplus.cpp:662-666, 680-683):
 //   s = sgn(c) * (1 - 1 / (((1 + |c|) + c*c) + (((a*c)*c)*c)*c)),  a = 1.41645
 __device__ __forceinline__ float tanh_rational(float c) {
@@ -41,7 +79,8 @@ __device__ __forceinline__ float lrelu_bn(float x, float b, float w1, float w2, 
 
 // ---------------------------------------------------------------------------------------
 // Network weights, passed to kernels by value (__grid_constant__) so that every tap is a
-// constant-bank operand. Shapes are the CNTK prototypes of cntk/stage_{1,2,3}.cntk.
+// constant-bank operand. Shapes are the CNTK prototypes of cntk/stage_{1,2,3}.cntk. Taps are
+// stored as the (lo, hi) pairs the packed-pair kernels consume.
 // ---------------------------------------------------------------------------------------
 
 template <int M1, int M2, int M3, int K1W, int K1H, int K2W, int K2H, int K3W, int K3H, int HL, int CONN, int HS>
@@ -49,18 +88,21 @@ struct NetWeights {
     static constexpr int kM1 = M1, kM2 = M2, kM3 = M3;
     static constexpr int kK1W = K1W, kK1H = K1H, kK2W = K2W, kK2H = K2H, kK3W = K3W, kK3H = K3H;
     static constexpr int kHL = HL, kConn = CONN, kHS = HS, kGroups = HL / HS;
-    float k1[M1][K1W * K1H];
+    float2 k1d[M1][K1W * K1H];      // L1 taps duplicated (w, w): two pixels of one map per packed op
+    float2 k1p[M1 / 2][K1W * K1H];  // L1 taps of maps (2i, 2i+1), which read the same input
     float b1[M1], w1a[M1], w1b[M1], bn1[M1];
-    float k2[M2][K2W * K2H];
+    float2 k2p[M2 / 2][K2W * K2H];  // L2 taps of maps (2i, 2i+1), which read the same sum map i
     float b2[M2], w2a[M2], w2b[M2], bn2[M2];
-    float k3[M3][K3W * K3H];
+    float2 k3p[M3 / 2][K3W * K3H];  // L3 taps of maps (2i, 2i+1)
     float b3[M3], w3a[M3], w3b[M3], bn3[M3];
-    float hw[HL][CONN];  // hidden weights, neuron n = HS*i + t reads L3 maps i .. i+CONN-1
+    float2 hwp[HL / 2][CONN];       // hidden weights of neurons (2q, 2q+1); neuron n = HS*i + t reads
+                                    // L3 maps i .. i+CONN-1 (HS even, so a pair shares its group)
     float hb[HL];
     float htw[HL / HS];  // per-group tanh slope
     float hbnw[HS], hbnb[HS];
     float ow[HL];        // selected output neuron's weights, index t*(HL/HS) + i
     float ob, otw, af;   // output bias, output tanh slope, signed output scale
+    float2 negzero;      // (-0.f, -0.f): the run-time addend of f2_mul
 };
 
 // cnn4face1_cntk.bin: 23x27 window, 4/8/16 maps, 4x4 / 3x3 / 4(w)x5(h), hidden 52 = 13 x 4

@@ -19,9 +19,11 @@ __device__ __forceinline__ float gray_bgr(uint32_t b, uint32_t g, uint32_t r) {
 template <int CH>
 __global__ void __launch_bounds__(256) gray_kernel(const uint8_t* __restrict__ src, int spitch, int w, int h,
                                                    float* __restrict__ dst, int dpitch) {
-    int y = blockIdx.y;
-    int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 16;
-    if (y >= h || x0 >= w) return;
+    const int chunks = (w + 15) >> 4;  // 16-pixel chunks per row; one chunk per thread
+    const int item = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = item / chunks;
+    const int x0 = (item - y * chunks) * 16;
+    if (y >= h) return;
     const uint8_t* row = src + (size_t)y * spitch;
     float* out = dst + (size_t)y * dpitch;
     if (x0 + 16 <= w) {
@@ -52,7 +54,8 @@ cudaError_t launch_gray(const uint8_t* src, int spitch, int w, int h, int ch, fl
     if ((spitch & 63) || (dpitch & 15) || (reinterpret_cast<uintptr_t>(src) & 63) || (reinterpret_cast<uintptr_t>(dst) & 63))
         return cudaErrorMisalignedAddress;  // the staging buffers are allocated 64-byte aligned
     dim3 block(256);
-    dim3 grid((w + 16 * 256 - 1) / (16 * 256), h);
+    const long long items = (long long)h * ((w + 15) / 16);
+    dim3 grid((unsigned)((items + 255) / 256));
     switch (ch) {
         case 1: gray_kernel<1><<<grid, block, 0, st>>>(src, spitch, w, h, dst, dpitch); break;
         case 3: gray_kernel<3><<<grid, block, 0, st>>>(src, spitch, w, h, dst, dpitch); break;

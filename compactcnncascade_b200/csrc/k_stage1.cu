@@ -32,11 +32,18 @@ __device__ __forceinline__ int find_level(const LevelDesc* __restrict__ lv, int 
 
 constexpr int kInW = 2 * kK1TileX + 3;  // 67
 constexpr int kInH = 2 * kK1TileY + 3;  // 35
+constexpr int kInWh = (kInW + 1) / 2;   // 34 columns of each parity
 
-__global__ void __launch_bounds__(256) stage1_front_kernel(const __grid_constant__ Stage1W W, const LevelDesc* __restrict__ levels,
-                                                           int n_levels, const float* __restrict__ gray, int gpitch, int gw, int gh,
-                                                           float* __restrict__ s1) {
-    __shared__ float tin[kInH][kInW + 1];
+// Tile layout for the front kernel: row r of the input tile is stored next to row r+2 as a packed
+// pair (a thread computes two vertically adjacent pooled pixels, whose windows are 2 rows apart),
+// and columns are split by parity so that the stride-2 column walk of a warp is conflict-free.
+__global__ void __launch_bounds__(256, 4) stage1_front_kernel(const __grid_constant__ Stage1W W, const LevelDesc* __restrict__ levels,
+                                                              int n_levels, const float* __restrict__ gray, int gpitch, int gw, int gh,
+                                                              float* __restrict__ s1) {
+    __shared__ float2 tinp[kInH - 2][2][kInWh];
+    __shared__ float tin_tail[2][kInW];        // the last two rows have no partner below
+    __shared__ uint32_t col_idx[kInW], row_idx[kInH];
+    __shared__ float col_f[kInW], col_c[kInW], row_f[kInH], row_c[kInH];
     const int lvl = find_level(levels, n_levels, blockIdx.x, true);
     const LevelDesc L = levels[lvl];
     const int t = blockIdx.x - L.k1_base;
@@ -44,46 +51,82 @@ __global__ void __launch_bounds__(256) stage1_front_kernel(const __grid_constant
     const int py0 = (t / L.k1_tiles_x) * kK1TileY;
     const int ix0 = 2 * px0, iy0 = 2 * py0;
 
+    // per-tile sampling table: one column / row of the resampler each
+    if (L.mode != 0) {
+        if (threadIdx.x < kInW) {
+            const AxisSample sx = sample_col(ix0 + threadIdx.x, L.sclx, gw);
+            col_idx[threadIdx.x] = sx.idx;
+            col_f[threadIdx.x] = sx.f;
+            col_c[threadIdx.x] = sx.c;
+        } else if (threadIdx.x >= 128 && threadIdx.x < 128 + kInH) {
+            const int r = threadIdx.x - 128;
+            const AxisSample sy = sample_row(iy0 + r, L.scly, gh);
+            uint32_t py = sy.idx;
+            if (L.mode == 2 && py + 1 >= (uint32_t)gh) py--;  // bilinear keeps a row below
+            row_idx[r] = py;
+            row_f[r] = sy.f;
+            row_c[r] = sy.c;
+        }
+        __syncthreads();
+    }
     for (int i = threadIdx.x; i < kInH * kInW; i += blockDim.x) {
-        int r = i / kInW, c = i - r * kInW;
-        int lx = ix0 + c, ly = iy0 + r;
+        const int r = i / kInW, c = i - r * kInW;
+        const int lx = ix0 + c, ly = iy0 + r;
         float v = 0.f;
-        if (lx < L.w && ly < L.h) v = level_pixel(gray, gpitch, gw, gh, L, lx, ly);
-        tin[r][c] = v;
+        if (lx < L.w && ly < L.h) {
+            if (L.mode == 0) {
+                v = gray[(size_t)ly * gpitch + lx];
+            } else if (L.mode == 1) {
+                v = gray[(size_t)row_idx[r] * gpitch + col_idx[c]];
+            } else {
+                const float* r0 = gray + (size_t)row_idx[r] * gpitch + col_idx[c];
+                const float top = fadd(fmul(r0[0], col_c[c]), fmul(r0[1], col_f[c]));
+                const float bot = fadd(fmul(r0[gpitch], col_c[c]), fmul(r0[gpitch + 1], col_f[c]));
+                v = fadd(fmul(top, row_c[r]), fmul(bot, row_f[r]));
+            }
+        }
+        float* lo = r < kInH - 2 ? &tinp[r][c & 1][c >> 1].x : &tin_tail[r - (kInH - 2)][c];
+        *lo = v;
+        if (r >= 2) tinp[r - 2][c & 1][c >> 1].y = v;
     }
     __syncthreads();
 
     const int qx = threadIdx.x & (kK1TileX - 1);
     const int qy = (threadIdx.x >> 5) * 2;
-    float win[7][5];
+    const f2_t nz = f2_ld(W.negzero);
+    // pr[r][c] = (input row 2qy+r, row 2qy+r+2) at column 2qx+c: the windows of both pixels
+    f2_t pr[5][5];
 #pragma unroll
-    for (int r = 0; r < 7; ++r)
+    for (int r = 0; r < 5; ++r)
 #pragma unroll
-        for (int c = 0; c < 5; ++c) win[r][c] = tin[2 * qy + r][2 * qx + c];
+        for (int c = 0; c < 5; ++c) pr[r][c] = *reinterpret_cast<const f2_t*>(&tinp[2 * qy + r][c & 1][qx + (c >> 1)]);
 
+    float P[2][4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        float cv[2][4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const int dy = d >> 1, dx = d & 1;
+            f2_t acc = f2_mul(pr[dy][dx], f2_ld(W.k1d[m][0]), nz);
+#pragma unroll
+            for (int k = 1; k < 16; ++k)
+                acc = f2_add(acc, f2_mul(pr[dy + (k >> 2)][dx + (k & 3)], f2_ld(W.k1d[m][k]), nz));
+            cv[0][d] = lrelu_bn(f2_lo(acc), W.b1[m], W.w1a[m], W.w1b[m], W.bn1[m]);
+            cv[1][d] = lrelu_bn(f2_hi(acc), W.b1[m], W.w1a[m], W.w1b[m], W.bn1[m]);
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) P[q][m] = fmaxf(fmaxf(cv[q][0], cv[q][1]), fmaxf(cv[q][2], cv[q][3]));
+    }
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-        float P[4];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            float cv[4];
-#pragma unroll
-            for (int d = 0; d < 4; ++d) {
-                const int dy = d >> 1, dx = d & 1;
-                float acc = fmul(win[2 * q + dy][dx], W.k1[m][0]);
-#pragma unroll
-                for (int k = 1; k < 16; ++k) acc = fadd(acc, fmul(win[2 * q + dy + (k >> 2)][dx + (k & 3)], W.k1[m][k]));
-                cv[d] = lrelu_bn(acc, W.b1[m], W.w1a[m], W.w1b[m], W.bn1[m]);
-            }
-            P[m] = fmaxf(fmaxf(cv[0], cv[1]), fmaxf(cv[2], cv[3]));
-        }
         const int gx = px0 + qx, gy = py0 + qy + q;
         if (gx < L.p1w && gy < L.p1h) {
             float* o = s1 + L.s1_off + (long long)gy * L.s1_pitch + gx;
-            o[0] = fadd(P[0], P[1]);
-            o[L.s1_plane] = fadd(fadd(P[0], P[1]), P[2]);
-            o[2 * L.s1_plane] = fadd(fadd(P[1], P[2]), P[3]);
-            o[3 * L.s1_plane] = fadd(P[2], P[3]);
+            o[0] = fadd(P[q][0], P[q][1]);
+            o[L.s1_plane] = fadd(fadd(P[q][0], P[q][1]), P[q][2]);
+            o[2 * L.s1_plane] = fadd(fadd(P[q][1], P[q][2]), P[q][3]);
+            o[3 * L.s1_plane] = fadd(P[q][2], P[q][3]);
         }
     }
 }
@@ -92,10 +135,11 @@ constexpr int kP2TW = kK2TileX + 3;  // 19
 constexpr int kP2TH = kK2TileY + 4;  // 20
 constexpr int kS1TW = 2 * kP2TW + 2; // 40
 constexpr int kS1TH = 2 * kP2TH + 2; // 42
+constexpr int kS1TWh = kS1TW / 2 + 1; // 21 columns of each parity (+1 pad)
 
 __global__ void __launch_bounds__(256) stage1_back_kernel(const __grid_constant__ Stage1W W, const LevelDesc* __restrict__ levels,
                                                           int n_levels, const float* __restrict__ s1, float* __restrict__ resp) {
-    __shared__ float ts1[4][kS1TH][kS1TW + 1];
+    __shared__ float ts1[4][kS1TH][2 * kS1TWh];  // column c stored at (c & 1) * kS1TWh + (c >> 1)
     __shared__ float ts2[8][kP2TH][kP2TW + 1];
     const int lvl = find_level(levels, n_levels, blockIdx.x, false);
     const LevelDesc L = levels[lvl];
@@ -111,35 +155,35 @@ __global__ void __launch_bounds__(256) stage1_back_kernel(const __grid_constant_
         int x = sx0 + c, y = sy0 + r;
         float v = 0.f;
         if (x < L.p1w && y < L.p1h) v = s1[L.s1_off + m * L.s1_plane + (long long)y * L.s1_pitch + x];
-        ts1[m][r][c] = v;
+        ts1[m][r][(c & 1) * kS1TWh + (c >> 1)] = v;
     }
     __syncthreads();
 
-    // pooled L2 maps and their neighbour sums on the (19 x 20) halo tile
+    const f2_t nz = f2_ld(W.negzero);
+    // pooled L2 maps and their neighbour sums on the (19 x 20) halo tile; maps 2i and 2i+1 read the
+    // same sum map i, so they run as one packed pair
     for (int p = threadIdx.x; p < kP2TW * kP2TH; p += blockDim.x) {
         const int x = p % kP2TW, y = p / kP2TW;
         float P[8];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            float q[4][4];
+            f2_t q[4][4];
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
-                for (int c = 0; c < 4; ++c) q[r][c] = ts1[i][2 * y + r][2 * x + c];
+                for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(ts1[i][2 * y + r][(c & 1) * kS1TWh + x + (c >> 1)]);
+            float cv[2][4];
 #pragma unroll
-            for (int hm = 0; hm < 2; ++hm) {
-                const int m = 2 * i + hm;
-                float cv[4];
+            for (int d = 0; d < 4; ++d) {
+                const int dy = d >> 1, dx = d & 1;
+                f2_t acc = f2_mul(q[dy][dx], f2_ld(W.k2p[i][0]), nz);
 #pragma unroll
-                for (int d = 0; d < 4; ++d) {
-                    const int dy = d >> 1, dx = d & 1;
-                    float acc = fmul(q[dy][dx], W.k2[m][0]);
-#pragma unroll
-                    for (int k = 1; k < 9; ++k) acc = fadd(acc, fmul(q[dy + k / 3][dx + k % 3], W.k2[m][k]));
-                    cv[d] = lrelu_bn(acc, W.b2[m], W.w2a[m], W.w2b[m], W.bn2[m]);
-                }
-                P[m] = fmaxf(fmaxf(cv[0], cv[1]), fmaxf(cv[2], cv[3]));
+                for (int k = 1; k < 9; ++k) acc = f2_add(acc, f2_mul(q[dy + k / 3][dx + k % 3], f2_ld(W.k2p[i][k]), nz));
+                cv[0][d] = lrelu_bn(f2_lo(acc), W.b2[2 * i], W.w2a[2 * i], W.w2b[2 * i], W.bn2[2 * i]);
+                cv[1][d] = lrelu_bn(f2_hi(acc), W.b2[2 * i + 1], W.w2a[2 * i + 1], W.w2b[2 * i + 1], W.bn2[2 * i + 1]);
             }
+            P[2 * i] = fmaxf(fmaxf(cv[0][0], cv[0][1]), fmaxf(cv[0][2], cv[0][3]));
+            P[2 * i + 1] = fmaxf(fmaxf(cv[1][0], cv[1][1]), fmaxf(cv[1][2], cv[1][3]));
         }
         ts2[0][y][x] = fadd(P[0], P[1]);
 #pragma unroll
@@ -152,41 +196,46 @@ __global__ void __launch_bounds__(256) stage1_back_kernel(const __grid_constant_
     float A[16];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        float q[5][4];
+        f2_t q[5][4];
 #pragma unroll
         for (int r = 0; r < 5; ++r)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) q[r][c] = ts2[i][y + r][x + c];
+            for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(ts2[i][y + r][x + c]);
+        // conv_5x4 keeps one partial sum per kernel row, added in row order
+        f2_t acc = 0ull;
 #pragma unroll
-        for (int hm = 0; hm < 2; ++hm) {
-            const int m = 2 * i + hm;
-            // conv_5x4 keeps one partial sum per kernel row, added in row order
-            float acc = 0.f;
+        for (int r = 0; r < 5; ++r) {
+            f2_t rs = f2_mul(q[r][0], f2_ld(W.k3p[i][4 * r]), nz);
 #pragma unroll
-            for (int r = 0; r < 5; ++r) {
-                float rs = fmul(q[r][0], W.k3[m][4 * r]);
-#pragma unroll
-                for (int c = 1; c < 4; ++c) rs = fadd(rs, fmul(q[r][c], W.k3[m][4 * r + c]));
-                acc = (r == 0) ? rs : fadd(acc, rs);
-            }
-            A[m] = lrelu_bn(acc, W.b3[m], W.w3a[m], W.w3b[m], W.bn3[m]);
+            for (int c = 1; c < 4; ++c) rs = f2_add(rs, f2_mul(q[r][c], f2_ld(W.k3p[i][4 * r + c]), nz));
+            acc = (r == 0) ? rs : f2_add(acc, rs);
         }
+        A[2 * i] = lrelu_bn(f2_lo(acc), W.b3[2 * i], W.w3a[2 * i], W.w3b[2 * i], W.bn3[2 * i]);
+        A[2 * i + 1] = lrelu_bn(f2_hi(acc), W.b3[2 * i + 1], W.w3a[2 * i + 1], W.w3b[2 * i + 1], W.bn3[2 * i + 1]);
     }
-    // hidden neurons n = 4*i + t read L3 maps i..i+3; the output sum runs in the same n order
+    // hidden neurons n = 4*i + t read L3 maps i..i+3 (neurons 2p, 2p+1 share them: packed); the
+    // output sum then runs over n in order
+    f2_t Ad[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) Ad[m] = f2_dup(A[m]);
     float out = 0.f;
 #pragma unroll
     for (int i = 0; i < Stage1W::kGroups; ++i) {
 #pragma unroll
-        for (int tt = 0; tt < Stage1W::kHS; ++tt) {
-            const int n = Stage1W::kHS * i + tt;
-            float s = W.hb[n];
+        for (int tp = 0; tp < Stage1W::kHS / 2; ++tp) {
+            const int n = Stage1W::kHS * i + 2 * tp;
+            f2_t s = f2_pack(W.hb[n], W.hb[n + 1]);
 #pragma unroll
-            for (int j = 0; j < Stage1W::kConn; ++j) s = fadd(s, fmul(A[i + j], W.hw[n][j]));
-            s = fmul(s, W.htw[i]);
-            s = tanh_rational(s);
-            s = fadd(fmul(0.5f, s), 0.5f);
-            const float h = fadd(fmul(W.hbnw[tt], s), W.hbnb[tt]);
-            out = (n == 0) ? fmul(h, W.ow[0]) : fadd(fmul(h, W.ow[n]), out);
+            for (int j = 0; j < Stage1W::kConn; ++j) s = f2_add(s, f2_mul(Ad[i + j], f2_ld(W.hwp[n / 2][j]), nz));
+            s = f2_mul(s, f2_dup(W.htw[i]), nz);
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int tt = 2 * tp + e;
+                float v = tanh_rational(e == 0 ? f2_lo(s) : f2_hi(s));
+                v = fadd(fmul(0.5f, v), 0.5f);
+                const float h = fadd(fmul(W.hbnw[tt], v), W.hbnb[tt]);
+                out = (n + e == 0) ? fmul(h, W.ow[0]) : fadd(fmul(h, W.ow[n + e]), out);
+            }
         }
     }
     float c = fmul(fadd(out, W.ob), W.otw);

@@ -49,27 +49,33 @@ __device__ __forceinline__ float win_in(const WindowSmem& S, int mode, int x, in
 
 template <class NW>
 __device__ void window_net(const NW& W, WindowSmem& S, int mode) {
-    // L1: conv 4x4 + folded BN/LReLU + 2x2 max, then neighbour sums (add / add2)
+    static_assert(NW::kM1 % 2 == 0 && NW::kM2 % 2 == 0 && NW::kM3 % 2 == 0 && NW::kHS % 2 == 0, "maps and neurons run in pairs");
+    const f2_t nz = f2_ld(W.negzero);
+    // L1: conv 4x4 + folded BN/LReLU + 2x2 max, then neighbour sums (add / add2); every map pair
+    // reads the same window, so it runs as one packed pair
     for (int p = threadIdx.x; p < kP1W * kP1H; p += kWT) {
         const int x = p % kP1W, y = p / kP1W;
-        float win[5][5];
+        f2_t win[5][5];
 #pragma unroll
         for (int r = 0; r < 5; ++r)
 #pragma unroll
-            for (int c = 0; c < 5; ++c) win[r][c] = win_in(S, mode, 2 * x + c, 2 * y + r);
+            for (int c = 0; c < 5; ++c) win[r][c] = f2_dup(win_in(S, mode, 2 * x + c, 2 * y + r));
         float P[NW::kM1];
 #pragma unroll
-        for (int m = 0; m < NW::kM1; ++m) {
-            float cv[4];
+        for (int mp = 0; mp < NW::kM1 / 2; ++mp) {
+            float cv[2][4];
 #pragma unroll
             for (int d = 0; d < 4; ++d) {
                 const int dy = d >> 1, dx = d & 1;
-                float acc = fmul(win[dy][dx], W.k1[m][0]);
+                f2_t acc = f2_mul(win[dy][dx], f2_ld(W.k1p[mp][0]), nz);
 #pragma unroll
-                for (int k = 1; k < 16; ++k) acc = fadd(acc, fmul(win[dy + (k >> 2)][dx + (k & 3)], W.k1[m][k]));
-                cv[d] = lrelu_bn(acc, W.b1[m], W.w1a[m], W.w1b[m], W.bn1[m]);
+                for (int k = 1; k < 16; ++k) acc = f2_add(acc, f2_mul(win[dy + (k >> 2)][dx + (k & 3)], f2_ld(W.k1p[mp][k]), nz));
+                const int m0 = 2 * mp, m1 = 2 * mp + 1;
+                cv[0][d] = lrelu_bn(f2_lo(acc), W.b1[m0], W.w1a[m0], W.w1b[m0], W.bn1[m0]);
+                cv[1][d] = lrelu_bn(f2_hi(acc), W.b1[m1], W.w1a[m1], W.w1b[m1], W.bn1[m1]);
             }
-            P[m] = fmaxf(fmaxf(cv[0], cv[1]), fmaxf(cv[2], cv[3]));
+            P[2 * mp] = fmaxf(fmaxf(cv[0][0], cv[0][1]), fmaxf(cv[0][2], cv[0][3]));
+            P[2 * mp + 1] = fmaxf(fmaxf(cv[1][0], cv[1][1]), fmaxf(cv[1][2], cv[1][3]));
         }
         S.s1[0][y][x] = fadd(P[0], P[1]);
 #pragma unroll
@@ -82,25 +88,23 @@ __device__ void window_net(const NW& W, WindowSmem& S, int mode) {
         const int i = it / (kP2W * kP2H);
         const int p = it - i * (kP2W * kP2H);
         const int x = p % kP2W, y = p / kP2W;
-        float q[4][4];
+        f2_t q[4][4];
 #pragma unroll
         for (int r = 0; r < 4; ++r)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) q[r][c] = S.s1[i][2 * y + r][2 * x + c];
+            for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(S.s1[i][2 * y + r][2 * x + c]);
+        float cv[2][4];
 #pragma unroll
-        for (int hm = 0; hm < 2; ++hm) {
-            const int m = 2 * i + hm;
-            float cv[4];
+        for (int d = 0; d < 4; ++d) {
+            const int dy = d >> 1, dx = d & 1;
+            f2_t acc = f2_mul(q[dy][dx], f2_ld(W.k2p[i][0]), nz);
 #pragma unroll
-            for (int d = 0; d < 4; ++d) {
-                const int dy = d >> 1, dx = d & 1;
-                float acc = fmul(q[dy][dx], W.k2[m][0]);
-#pragma unroll
-                for (int k = 1; k < 9; ++k) acc = fadd(acc, fmul(q[dy + k / 3][dx + k % 3], W.k2[m][k]));
-                cv[d] = lrelu_bn(acc, W.b2[m], W.w2a[m], W.w2b[m], W.bn2[m]);
-            }
-            S.p2[m][y][x] = fmaxf(fmaxf(cv[0], cv[1]), fmaxf(cv[2], cv[3]));
+            for (int k = 1; k < 9; ++k) acc = f2_add(acc, f2_mul(q[dy + k / 3][dx + k % 3], f2_ld(W.k2p[i][k]), nz));
+            cv[0][d] = lrelu_bn(f2_lo(acc), W.b2[2 * i], W.w2a[2 * i], W.w2b[2 * i], W.bn2[2 * i]);
+            cv[1][d] = lrelu_bn(f2_hi(acc), W.b2[2 * i + 1], W.w2a[2 * i + 1], W.w2b[2 * i + 1], W.bn2[2 * i + 1]);
         }
+        S.p2[2 * i][y][x] = fmaxf(fmaxf(cv[0][0], cv[0][1]), fmaxf(cv[0][2], cv[0][3]));
+        S.p2[2 * i + 1][y][x] = fmaxf(fmaxf(cv[1][0], cv[1][1]), fmaxf(cv[1][2], cv[1][3]));
     }
     __syncthreads();
     for (int p = threadIdx.x; p < kP2W * kP2H; p += kWT) {
@@ -111,29 +115,36 @@ __device__ void window_net(const NW& W, WindowSmem& S, int mode) {
         S.s2[M - 1][y][x] = fadd(S.p2[M - 2][y][x], S.p2[M - 1][y][x]);
     }
     __syncthreads();
-    // L3: 7w x 8h conv summed in one left-to-right chain (conv_8x7), BN/LReLU, no pooling
-    for (int it = threadIdx.x; it < NW::kM3 * kOutN; it += kWT) {
-        const int m = it / kOutN, o = it - m * kOutN;
+    // L3: 7w x 8h conv summed in one left-to-right chain (conv_8x7), BN/LReLU, no pooling;
+    // maps (2i, 2i+1) share the input: packed
+    for (int it = threadIdx.x; it < (NW::kM3 / 2) * kOutN; it += kWT) {
+        const int i = it / kOutN, o = it - i * kOutN;
         const int ox = o & 3, oy = o >> 2;
-        const int i = m >> 1;
-        float acc = fmul(S.s2[i][oy][ox], W.k3[m][0]);
+        f2_t acc = f2_mul(f2_dup(S.s2[i][oy][ox]), f2_ld(W.k3p[i][0]), nz);
 #pragma unroll
         for (int k = 1; k < NW::kK3W * NW::kK3H; ++k)
-            acc = fadd(acc, fmul(S.s2[i][oy + k / NW::kK3W][ox + k % NW::kK3W], W.k3[m][k]));
-        S.a3[m][o] = lrelu_bn(acc, W.b3[m], W.w3a[m], W.w3b[m], W.bn3[m]);
+            acc = f2_add(acc, f2_mul(f2_dup(S.s2[i][oy + k / NW::kK3W][ox + k % NW::kK3W]), f2_ld(W.k3p[i][k]), nz));
+        S.a3[2 * i][o] = lrelu_bn(f2_lo(acc), W.b3[2 * i], W.w3a[2 * i], W.w3b[2 * i], W.bn3[2 * i]);
+        S.a3[2 * i + 1][o] = lrelu_bn(f2_hi(acc), W.b3[2 * i + 1], W.w3a[2 * i + 1], W.w3b[2 * i + 1], W.bn3[2 * i + 1]);
     }
     __syncthreads();
-    // hidden neurons n = HS*i + t read L3 maps i .. i+CONN-1
-    for (int it = threadIdx.x; it < NW::kHL * kOutN; it += kWT) {
-        const int n = it / kOutN, o = it - n * kOutN;
-        const int i = n / NW::kHS, t = n - i * NW::kHS;
-        float s = W.hb[n];
+    // hidden neurons n = HS*i + t read L3 maps i .. i+CONN-1; neurons (2q, 2q+1) share the
+    // group, so they run as one packed pair
+    for (int it = threadIdx.x; it < (NW::kHL / 2) * kOutN; it += kWT) {
+        const int q = it / kOutN, o = it - q * kOutN;
+        const int n = 2 * q;
+        const int i = n / NW::kHS;
+        f2_t s = f2_pack(W.hb[n], W.hb[n + 1]);
 #pragma unroll
-        for (int j = 0; j < NW::kConn; ++j) s = fadd(s, fmul(S.a3[i + j][o], W.hw[n][j]));
-        s = fmul(s, W.htw[i]);
-        s = tanh_rational(s);
-        s = fadd(fmul(0.5f, s), 0.5f);
-        S.hbuf[n][o] = fadd(fmul(W.hbnw[t], s), W.hbnb[t]);
+        for (int j = 0; j < NW::kConn; ++j) s = f2_add(s, f2_mul(f2_dup(S.a3[i + j][o]), f2_ld(W.hwp[q][j]), nz));
+        s = f2_mul(s, f2_dup(W.htw[i]), nz);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int t = (n + e) - i * NW::kHS;
+            float v = tanh_rational(e == 0 ? f2_lo(s) : f2_hi(s));
+            v = fadd(fmul(0.5f, v), 0.5f);
+            S.hbuf[n + e][o] = fadd(fmul(W.hbnw[t], v), W.hbnb[t]);
+        }
     }
     __syncthreads();
     if (threadIdx.x < kOutN) {

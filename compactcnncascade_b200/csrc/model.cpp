@@ -134,12 +134,15 @@ bool pack_model(const RawModel& m, int index_output, NW* o, std::string* err) {
         return false;
     }
     std::memset(o, 0, sizeof(NW));
+    auto tap = [&](int l, int mm, int k) { return m.kernels[l][(size_t)mm * m.kw[l] * m.kh[l] + k]; };
     for (int mm = 0; mm < NW::kM1; ++mm)
-        for (int k = 0; k < NW::kK1W * NW::kK1H; ++k) o->k1[mm][k] = m.kernels[0][mm * NW::kK1W * NW::kK1H + k];
-    for (int mm = 0; mm < NW::kM2; ++mm)
-        for (int k = 0; k < NW::kK2W * NW::kK2H; ++k) o->k2[mm][k] = m.kernels[1][mm * NW::kK2W * NW::kK2H + k];
-    for (int mm = 0; mm < NW::kM3; ++mm)
-        for (int k = 0; k < NW::kK3W * NW::kK3H; ++k) o->k3[mm][k] = m.kernels[2][mm * NW::kK3W * NW::kK3H + k];
+        for (int k = 0; k < NW::kK1W * NW::kK1H; ++k) o->k1d[mm][k] = make_float2(tap(0, mm, k), tap(0, mm, k));
+    for (int i = 0; i < NW::kM1 / 2; ++i)
+        for (int k = 0; k < NW::kK1W * NW::kK1H; ++k) o->k1p[i][k] = make_float2(tap(0, 2 * i, k), tap(0, 2 * i + 1, k));
+    for (int i = 0; i < NW::kM2 / 2; ++i)
+        for (int k = 0; k < NW::kK2W * NW::kK2H; ++k) o->k2p[i][k] = make_float2(tap(1, 2 * i, k), tap(1, 2 * i + 1, k));
+    for (int i = 0; i < NW::kM3 / 2; ++i)
+        for (int k = 0; k < NW::kK3W * NW::kK3H; ++k) o->k3p[i][k] = make_float2(tap(2, 2 * i, k), tap(2, 2 * i + 1, k));
     auto act = [&](int l, int mm, int field) { return m.act[l][5 * mm + field]; };
     for (int mm = 0; mm < NW::kM1; ++mm) {
         o->b1[mm] = act(0, mm, 0);
@@ -159,10 +162,10 @@ bool pack_model(const RawModel& m, int index_output, NW* o, std::string* err) {
         o->w3b[mm] = act(2, mm, 2);
         o->bn3[mm] = act(2, mm, 4);
     }
-    for (int n = 0; n < NW::kHL; ++n) {
-        for (int j = 0; j < NW::kConn; ++j) o->hw[n][j] = m.hw[(size_t)n * NW::kConn + j];
-        o->hb[n] = m.hb[n];
-    }
+    for (int n = 0; n < NW::kHL; ++n) o->hb[n] = m.hb[n];
+    for (int q = 0; q < NW::kHL / 2; ++q)
+        for (int j = 0; j < NW::kConn; ++j)
+            o->hwp[q][j] = make_float2(m.hw[(size_t)(2 * q) * NW::kConn + j], m.hw[(size_t)(2 * q + 1) * NW::kConn + j]);
     for (int i = 0; i < NW::kGroups; ++i) o->htw[i] = m.htw[i];
     for (int t = 0; t < NW::kHS; ++t) {
         o->hbnw[t] = m.hbn[2 * t];
@@ -175,6 +178,7 @@ bool pack_model(const RawModel& m, int index_output, NW* o, std::string* err) {
     o->ob = m.ob[idx];
     o->otw = m.otw;
     o->af = idx == 0 ? -m.af_scale : m.af_scale;
+    o->negzero = make_float2(-0.f, -0.f);
     return true;
 }
 
