@@ -57,6 +57,17 @@ __device__ __forceinline__ f2_t f2_add(f2_t a, f2_t b) {
     return r;
 }
 
+__device__ __forceinline__ f2_t f2_sub(f2_t a, f2_t b) {
+    f2_t r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2_t f2_max0(f2_t c) { return f2_pack(fmaxf(0.f, f2_lo(c)), fmaxf(0.f, f2_hi(c))); }
+__device__ __forceinline__ f2_t f2_max4(f2_t a, f2_t b, f2_t c, f2_t d) {
+    return f2_pack(fmaxf(fmaxf(f2_lo(a), f2_lo(b)), fmaxf(f2_lo(c), f2_lo(d))),
+                   fmaxf(fmaxf(f2_hi(a), f2_hi(b)), fmaxf(f2_hi(c), f2_hi(d))));
+}
+
 // Rational tanh approximation of the reference (cnnpp_cplusplus.cpp:662-666, 680-683):
 //   s = sgn(c) * (1 - 1 / (((1 + |c|) + c*c) + (((a*c)*c)*c)*c)),  a = 1.41645
 __device__ __forceinline__ float tanh_rational(float c) {
@@ -75,6 +86,26 @@ __device__ __forceinline__ float lrelu_bn(float x, float b, float w1, float w2, 
     float c = fadd(x, b);
     return fadd(fadd(fmul(w1, c), fmul(w2, fmaxf(0.f, c))), bnb);
 }
+
+// Two independent lanes of tanh_rational. The reciprocal 1/den is the correctly rounded IEEE
+// value, the same number as the reference's 1.f / den.
+__device__ __forceinline__ f2_t tanh_rational2(f2_t c, f2_t nz) {
+    const f2_t one = f2_pack(1.f, 1.f), a = f2_pack(1.41645f, 1.41645f);
+    const float lo = f2_lo(c), hi = f2_hi(c);
+    const f2_t ac = f2_pack(fabsf(lo), fabsf(hi));
+    const f2_t c2 = f2_mul(c, c, nz);
+    const f2_t c4 = f2_mul(f2_mul(f2_mul(f2_mul(a, c, nz), c, nz), c, nz), c, nz);
+    const f2_t den = f2_add(f2_add(f2_add(one, ac), c2), c4);
+    const f2_t r = f2_pack(__frcp_rn(f2_lo(den)), __frcp_rn(f2_hi(den)));
+    const f2_t sgn = f2_pack(lo < 0.f ? -1.f : 1.f, hi < 0.f ? -1.f : 1.f);
+    return f2_mul(sgn, f2_sub(one, r), nz);
+}
+
+// Two lanes of lrelu_bn; p = {b, w1, w2, bn_b}, each a (lane 0, lane 1) pair.
+__device__ __forceinline__ f2_t lrelu_bn2(f2_t x, const float2* p, f2_t nz) {
+    const f2_t c = f2_add(x, f2_ld(p[0]));
+    return f2_add(f2_add(f2_mul(f2_ld(p[1]), c, nz), f2_mul(f2_ld(p[2]), f2_max0(c), nz)), f2_ld(p[3]));
+}
 #endif  // __CUDACC__
 
 // ---------------------------------------------------------------------------------------
@@ -91,10 +122,14 @@ struct NetWeights {
     float2 k1d[M1][K1W * K1H];      // L1 taps duplicated (w, w): two pixels of one map per packed op
     float2 k1p[M1 / 2][K1W * K1H];  // L1 taps of maps (2i, 2i+1), which read the same input
     float b1[M1], w1a[M1], w1b[M1], bn1[M1];
+    float2 a1d[M1][4];              // L1 {b, w1a, w1b, bn} of each map duplicated (v, v)
+    float2 a1p[M1 / 2][4];          // L1 {b, w1a, w1b, bn} of map pairs (2i, 2i+1)
     float2 k2p[M2 / 2][K2W * K2H];  // L2 taps of maps (2i, 2i+1), which read the same sum map i
     float b2[M2], w2a[M2], w2b[M2], bn2[M2];
+    float2 a2p[M2 / 2][4];          // L2 {b, w2a, w2b, bn} of map pairs
     float2 k3p[M3 / 2][K3W * K3H];  // L3 taps of maps (2i, 2i+1)
     float b3[M3], w3a[M3], w3b[M3], bn3[M3];
+    float2 a3p[M3 / 2][4];          // L3 {b, w3a, w3b, bn} of map pairs
     float2 hwp[HL / 2][CONN];       // hidden weights of neurons (2q, 2q+1); neuron n = HS*i + t reads
                                     // L3 maps i .. i+CONN-1 (HS even, so a pair shares its group)
     float hb[HL];
@@ -111,6 +146,19 @@ using Stage1W = NetWeights<4, 8, 16, 4, 4, 3, 3, 4, 5, 52, 4, 4>;
 using Stage2W = NetWeights<6, 12, 24, 4, 4, 3, 3, 7, 8, 84, 4, 4>;
 // cnn4face3_cntk.bin: 36x40 window, 6/12/24 maps, 4x4 / 3x3 / 7(w)x8(h), hidden 34 = 17 x 2
 using Stage3W = NetWeights<6, 12, 24, 4, 4, 3, 3, 7, 8, 34, 8, 2>;
+
+// Stage-1 parameters duplicated (v, v) for the back kernel, which runs every operation of the L3
+// maps, the hidden layer and the output neuron on two vertically adjacent response pixels at once.
+struct Stage1Dup {
+    float2 k3d[Stage1W::kM3][Stage1W::kK3W * Stage1W::kK3H];
+    float2 a3d[Stage1W::kM3][4];
+    float2 hwd[Stage1W::kHL][Stage1W::kConn];
+    float2 hbd[Stage1W::kHL];
+    float2 htwd[Stage1W::kGroups];
+    float2 hbnwd[Stage1W::kHS], hbnbd[Stage1W::kHS];
+    float2 owd[Stage1W::kHL];
+    float2 obd, otwd, afd;
+};
 
 struct WindowNets {
     Stage2W s2;
@@ -136,11 +184,41 @@ struct LevelDesc {
     int k1_tiles_x, k1_base;  // stage-1 front kernel tiles
     int k2_tiles_x, k2_base;  // stage-1 back kernel tiles
     int order;           // processing position of this level in the candidate scan (0 = first)
+    long long img_off;   // offset of this level's image in the level arena (floats)
+    int img_pitch;       // floats per level image row
+    int img_vec;         // 1: rows start 16-byte aligned and the pitch is a multiple of 4 floats
+    int pyr_base;        // first pyramid-kernel block of this level
+    int pyr_wq;          // pyramid-kernel column blocks per row band
 };
+
+// Level descriptors passed by value to the kernels that find their level per block (a frame's
+// pyramid is launched in groups of at most kParamLevels levels). Every block of a launch maps to
+// global block index first + blockIdx.x, whose level is found by binary search over the
+// descriptors' base fields, all in the constant bank.
+constexpr int kParamLevels = 32;
+struct LevelTable {
+    int n;      // levels in lv[]
+    int first;  // global block index of this launch's block 0
+    LevelDesc lv[kParamLevels];
+};
+
+#if defined(__CUDACC__)
+// Level of global block g: the last level whose first block is <= g (binary search over the
+// descriptors in the constant bank; FIELD selects the front or back kernel's tile base).
+template <int LevelDesc::*FIELD>
+__device__ __forceinline__ int find_level(const LevelTable& T, int g) {
+    int lo = 0, hi = T.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (T.lv[mid].*FIELD <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+#endif
 
 // stage-1 front kernel tile (pooled L1 pixels) and back kernel tile (response pixels)
 constexpr int kK1TileX = 32, kK1TileY = 16;
-constexpr int kK2TileX = 16, kK2TileY = 16;
+constexpr int kK2TileX = 32, kK2TileY = 16;
 
 // stage-1 window and the stage-2/3 crop geometry (cnn_detector_v3.cpp:54-55, 1489-1501)
 constexpr int kPatW = 23, kPatH = 27;           // stage-1 pattern

@@ -87,6 +87,7 @@ void Detector::free_slot(Slot& s) {
     if (s.exec) cudaGraphExecDestroy(s.exec);
     cudaFree(s.d_in);
     cudaFree(s.d_gray);
+    cudaFree(s.d_limg);
     cudaFree(s.d_s1);
     cudaFree(s.d_resp);
     cudaFree(s.d_counts);
@@ -237,13 +238,14 @@ ccnn_status Detector::init() {
     cfg_.rescale = (float)api_.min_face_height / (float)pat_h_;
 
     // capacities from the largest plans this configuration can produce
-    s1_cap_ = resp_cap_ = 0;
+    s1_cap_ = resp_cap_ = img_cap_ = 0;
     chunk_cap_ = 0;
     for (int ch : {1, 3}) {
         Plan tmp;
         ccnn_status st = build_plan(max_w_, max_h_, ch, (int)scales_.size(), &tmp);
         if (st != CCNN_OK) return st;
         s1_cap_ = std::max(s1_cap_, tmp.s1_floats);
+        img_cap_ = std::max(img_cap_, tmp.img_floats);
         resp_cap_ = std::max(resp_cap_, tmp.resp_floats);
         chunk_cap_ = std::max(chunk_cap_, (int)tmp.chunks.size());
     }
@@ -265,6 +267,7 @@ ccnn_status Detector::init() {
     // persistent stage-2/3 grid: 4 resident 256-thread CTAs per SM (register bound)
     window_grid_ = prop.multiProcessorCount * 4;
     CCNN_CUDA(replay_setup());
+    CCNN_CUDA(stage1_setup());
 
     inited_ = true;
     for (auto& s : slots_) {
@@ -284,6 +287,7 @@ ccnn_status Detector::alloc_slot(Slot& s) {
     CCNN_CUDA(cudaMalloc(&s.d_in, s.in_pitch * max_h_));
     s.gray_pitch = (int)round_up(max_w_, 16);
     CCNN_CUDA(cudaMalloc(&s.d_gray, sizeof(float) * (size_t)s.gray_pitch * max_h_));
+    CCNN_CUDA(cudaMalloc(&s.d_limg, sizeof(float) * std::max(4LL, img_cap_)));
     CCNN_CUDA(cudaMalloc(&s.d_s1, sizeof(float) * std::max(1LL, s1_cap_)));
     CCNN_CUDA(cudaMalloc(&s.d_resp, sizeof(float) * std::max(1LL, resp_cap_)));
     CCNN_CUDA(cudaMalloc(&s.d_counts, sizeof(int) * chunk_cap_));
@@ -324,8 +328,8 @@ ccnn_status Detector::build_plan(int w, int h, int ch, int num_scales, Plan* p) 
     }
     p->levels.clear();
     p->chunks.clear();
-    long long s1 = 0, resp = 0;
-    int k1 = 0, k2 = 0;
+    long long s1 = 0, resp = 0, img = 0;
+    int k1 = 0, k2 = 0, pyr = 0;
     int n = 0;
     for (int scl = 0; scl < num_scales && scl < (int)scales_.size(); ++scl) {
         LevelDesc L{};
@@ -354,6 +358,13 @@ ccnn_status Detector::build_plan(int w, int h, int ch, int num_scales, Plan* p) 
         L.k2_tiles_x = (L.ow + kK2TileX - 1) / kK2TileX;
         L.k2_base = k2;
         k2 += L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY);
+        L.img_pitch = (int)round_up(L.w, 4);
+        L.img_vec = 1;
+        L.img_off = img;
+        img += (long long)L.img_pitch * L.h;
+        L.pyr_wq = (L.img_pitch + kPyrCols - 1) / kPyrCols;
+        L.pyr_base = pyr;
+        pyr += L.pyr_wq * ((L.h + kPyrRows - 1) / kPyrRows);
         p->levels.push_back(L);
         ++n;
     }
@@ -368,6 +379,7 @@ ccnn_status Detector::build_plan(int w, int h, int ch, int num_scales, Plan* p) 
     p->k2_tiles = k2;
     p->s1_floats = s1;
     p->resp_floats = resp;
+    p->img_floats = img;
     return CCNN_OK;
 }
 
@@ -380,7 +392,8 @@ ccnn_status Detector::plan_for(int w, int h, int ch, const Plan** out) {
         std::unique_ptr<Plan> p(new Plan());
         ccnn_status st = build_plan(w, h, ch, num_scales_, p.get());
         if (st != CCNN_OK) return st;
-        if (p->s1_floats > s1_cap_ || p->resp_floats > resp_cap_ || (long long)p->chunks.size() > chunk_cap_) {
+        if (p->s1_floats > s1_cap_ || p->resp_floats > resp_cap_ || p->img_floats > img_cap_ ||
+            (long long)p->chunks.size() > chunk_cap_) {
             set_error("internal: pyramid plan exceeds the allocated buffers");
             return CCNN_ERR_CUDA;
         }
@@ -408,7 +421,8 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
     else
         e = launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st);
     CCNN_CUDA(e);
-    CCNN_CUDA(launch_stage1(w1_, p.d_levels, p.n_levels, p.k1_tiles, p.k2_tiles, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_s1, s.d_resp, s.st));
+    CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
+    CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st));
     CCNN_CUDA(launch_candidates(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                 (int)cand_cap_, s.st));
     if (detect_enabled_)
@@ -745,29 +759,25 @@ ccnn_status Detector::stage1_forward(const float* d_img, int w, int h, size_t st
     L.s1_plane = (long long)L.s1_pitch * L.p1h;
     L.k1_tiles_x = (L.p1w + kK1TileX - 1) / kK1TileX;
     L.k2_tiles_x = (L.ow + kK2TileX - 1) / kK2TileX;
-    const int k1 = L.k1_tiles_x * ((L.p1h + kK1TileY - 1) / kK1TileY);
-    const int k2 = L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY);
+    L.img_pitch = (int)(step / sizeof(float));
+    L.img_vec = (L.img_pitch % 4 == 0 && (reinterpret_cast<uintptr_t>(d_img) & 15) == 0) ? 1 : 0;
     *rw = L.ow;
     *rh = L.oh;
     if ((long long)L.ow * L.oh > cap) {
         set_error("response capacity too small");
         return CCNN_ERR_INVALID_ARG;
     }
-    LevelDesc* d_l = nullptr;
     float* d_s1 = nullptr;
-    CCNN_CUDA(cudaMallocAsync(&d_l, sizeof(LevelDesc), st));
     CCNN_CUDA(cudaMallocAsync(&d_s1, sizeof(float) * 4 * L.s1_plane, st));
-    CCNN_CUDA(cudaMemcpyAsync(d_l, &L, sizeof(LevelDesc), cudaMemcpyHostToDevice, st));
-    CCNN_CUDA(launch_stage1(w1_, d_l, 1, k1, k2, d_img, (int)(step / sizeof(float)), w, h, d_s1, d_resp, st));
+    CCNN_CUDA(launch_stage1(w1_, &L, 1, d_img, d_s1, d_resp, st));
     CCNN_CUDA(cudaFreeAsync(d_s1, st));
-    CCNN_CUDA(cudaFreeAsync(d_l, st));
     CCNN_CUDA(cudaStreamSynchronize(st));
     return CCNN_OK;
 }
 
 // Re-runs the last frame's kernel chain on slot 0 `iters` times with an event between every
-// two kernels; ms[k] gets the mean duration of kernel k: gray, stage-1 front, stage-1 back,
-// candidate count, candidate write, stage-2/3 windows, replay.
+// two kernels; ms[k] gets the mean duration of kernel k: gray, pyramid, stage-1 front, stage-1
+// back, candidate count, candidate write, stage-2/3 windows, replay.
 ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     std::lock_guard<std::mutex> lk(mu_);
     Slot& s = slots_[0];
@@ -777,7 +787,7 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     }
     cudaSetDevice(device_);
     const Plan& p = *s.last_plan;
-    constexpr int K = 7;
+    constexpr int K = 8;
     cudaEvent_t ev[K + 1];
     for (auto& e : ev) CCNN_CUDA(cudaEventCreate(&e));
     double acc[K] = {0};
@@ -807,22 +817,24 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         else
             CCNN_CUDA(launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st));
         CCNN_CUDA(cudaEventRecord(ev[1], s.st));
-        CCNN_CUDA(launch_stage1_front(w1_, p.d_levels, p.n_levels, p.k1_tiles, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_s1, s.st));
+        CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
         CCNN_CUDA(cudaEventRecord(ev[2], s.st));
-        CCNN_CUDA(launch_stage1_back(w1_, p.d_levels, p.n_levels, p.k2_tiles, s.d_s1, s.d_resp, s.st));
+        CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st));
         CCNN_CUDA(cudaEventRecord(ev[3], s.st));
-        CCNN_CUDA(launch_cand_count(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.st));
+        CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st));
         CCNN_CUDA(cudaEventRecord(ev[4], s.st));
+        CCNN_CUDA(launch_cand_count(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.st));
+        CCNN_CUDA(cudaEventRecord(ev[5], s.st));
         CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                     (int)cand_cap_, s.st));
-        CCNN_CUDA(cudaEventRecord(ev[5], s.st));
+        CCNN_CUDA(cudaEventRecord(ev[6], s.st));
         if (detect_enabled_)
             CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
                                     window_grid_, s.st));
-        CCNN_CUDA(cudaEventRecord(ev[6], s.st));
-        CCNN_CUDA(launch_replay(a, s.st));
         CCNN_CUDA(cudaEventRecord(ev[7], s.st));
-        CCNN_CUDA(cudaEventSynchronize(ev[7]));
+        CCNN_CUDA(launch_replay(a, s.st));
+        CCNN_CUDA(cudaEventRecord(ev[8], s.st));
+        CCNN_CUDA(cudaEventSynchronize(ev[8]));
         for (int k = 0; k < K; ++k) {
             float m = 0.f;
             CCNN_CUDA(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));

@@ -26,7 +26,7 @@ struct Plan {
     std::vector<LevelDesc> levels;
     std::vector<int4> chunks;        // candidate-scan chunks in visiting order
     int k1_tiles = 0, k2_tiles = 0;
-    long long s1_floats = 0, resp_floats = 0;
+    long long s1_floats = 0, resp_floats = 0, img_floats = 0;
     LevelDesc* d_levels = nullptr;
     int4* d_chunks = nullptr;
 };
@@ -39,6 +39,7 @@ struct Slot {
     size_t in_pitch = 0;
     float* d_gray = nullptr;
     int gray_pitch = 0;  // floats
+    float* d_limg = nullptr;  // level arena: every level image of the frame
     float* d_s1 = nullptr;
     float* d_resp = nullptr;
     int* d_counts = nullptr;
@@ -115,7 +116,7 @@ class Detector {
 
     CascadeConfig cfg_{};
     Slot slots_[kSlots];
-    long long cand_cap_ = 0, s1_cap_ = 0, resp_cap_ = 0;
+    long long cand_cap_ = 0, s1_cap_ = 0, resp_cap_ = 0, img_cap_ = 0;
     int chunk_cap_ = 0;
     int window_grid_ = 0;
     std::map<std::tuple<int, int, int, int>, std::unique_ptr<Plan>> plans_;

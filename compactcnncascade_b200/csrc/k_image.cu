@@ -93,8 +93,66 @@ cudaError_t launch_gray_u8_resized(const uint8_t* src, int spitch, int sw, int s
     return cudaGetLastError();
 }
 
-// Standalone float resize (ImageResizer::FastImageResize(Image_32f&...), image_resize.cpp:564-584);
-// the detector itself samples levels inside the stage-1 front kernel.
+// Pyramid: every processed level image of a frame in one launch (RunCPUDetect,
+// cnn_detector_v3.cpp:2090-2104: scale 1 copies the gray image, scale > 0.7 nearest neighbour,
+// else bilinear; ImageResizer::FastImageResize, image_resize.cpp:564-584). A block covers 256
+// consecutive columns x kPyrRows rows of one level: each thread keeps its column's resampling
+// weights for all its rows, and a warp's loads and stores walk consecutive columns. Columns between
+// the level width and the row pitch are written as zeros.
+__global__ void __launch_bounds__(kPyrCols) pyramid_kernel(const __grid_constant__ LevelTable LT, const float* __restrict__ gray,
+                                                           int gpitch, int gw, int gh, float* __restrict__ limg) {
+    const int g = LT.first + blockIdx.x;
+    const LevelDesc& L = LT.lv[find_level<&LevelDesc::pyr_base>(LT, g)];
+    const int local = g - L.pyr_base;
+    const int rb = local / L.pyr_wq;
+    const int x = (local - rb * L.pyr_wq) * kPyrCols + threadIdx.x;
+    if (x >= L.img_pitch) return;
+    float* out = limg + L.img_off + x;
+    const int y0 = rb * kPyrRows;
+    const int y1 = y0 + kPyrRows < L.h ? y0 + kPyrRows : L.h;
+    if (x >= L.w) {
+        for (int y = y0; y < y1; ++y) out[(long long)y * L.img_pitch] = 0.f;
+        return;
+    }
+    if (L.mode == 0) {
+        for (int y = y0; y < y1; ++y) out[(long long)y * L.img_pitch] = __ldg(gray + (size_t)y * gpitch + x);
+        return;
+    }
+    const AxisSample sx = sample_col(x, L.sclx, gw);
+    if (L.mode == 1) {
+        for (int y = y0; y < y1; ++y)
+            out[(long long)y * L.img_pitch] = __ldg(gray + (size_t)sample_row(y, L.scly, gh).idx * gpitch + sx.idx);
+        return;
+    }
+#pragma unroll 4
+    for (int y = y0; y < y1; ++y) {
+        const AxisSample sy = sample_row(y, L.scly, gh);
+        uint32_t py = sy.idx;
+        if (py + 1 >= (uint32_t)gh) py--;  // bilinear keeps a row below
+        const float* r0 = gray + (size_t)py * gpitch + sx.idx;
+        const float top = fadd(fmul(__ldg(r0), sx.c), fmul(__ldg(r0 + 1), sx.f));
+        const float bot = fadd(fmul(__ldg(r0 + gpitch), sx.c), fmul(__ldg(r0 + gpitch + 1), sx.f));
+        out[(long long)y * L.img_pitch] = fadd(fmul(top, sy.c), fmul(bot, sy.f));
+    }
+}
+
+cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* gray, int gpitch, int gw, int gh, float* limg,
+                           cudaStream_t st) {
+    for (int g0 = 0; g0 < n_levels; g0 += kParamLevels) {
+        LevelTable T;
+        T.n = n_levels - g0 < kParamLevels ? n_levels - g0 : kParamLevels;
+        for (int i = 0; i < T.n; ++i) T.lv[i] = levels[g0 + i];
+        T.first = T.lv[0].pyr_base;
+        const LevelDesc& last = T.lv[T.n - 1];
+        const int blocks = last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows) - T.first;
+        if (blocks > 0) pyramid_kernel<<<blocks, kPyrCols, 0, st>>>(T, gray, gpitch, gw, gh, limg);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Standalone float resize (ImageResizer::FastImageResize(Image_32f&...), image_resize.cpp:564-584).
 __global__ void __launch_bounds__(256) resize_f32_kernel(const float* __restrict__ src, int spitch, int sw, int sh,
                                                          float* __restrict__ dst, int dpitch, int dw, int dh, int mode) {
     int x = blockIdx.x * blockDim.x + threadIdx.x;

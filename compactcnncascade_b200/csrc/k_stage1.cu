@@ -5,90 +5,80 @@
 // add/add2 (:916-950), conv_3x3 (:36-91), conv_5x4 (:158-187), lrelu_bn (:623-645),
 // mulCN_add_tanhW (:646-672), mulC/mulC1_add (:952-984), tanhW (:673-690).
 //
-// front: one CTA per 32x16 tile of pooled L1 pixels of one level. The level image is never
-//        materialised: the CTA samples its (67 x 35) input tile straight from the gray frame
-//        with the pyramid's fixed-point resampler, runs the 4x4 conv + folded BN/LReLU + 2x2 max
-//        for the 4 L1 maps and writes the 4 neighbour-map sums that L2 consumes (S1 arena).
-// back:  one CTA per 16x16 tile of response pixels. It stages the S1 tile (4 x 42 x 40) in shared
-//        memory, computes the 8 pooled L2 maps and their sums on the 19 x 20 halo tile, then every
-//        thread finishes one response pixel: the 16 L3 maps (4w x 5h), the 52 hidden neurons and
-//        the output neuron.
+// front: one CTA per 32x16 tile of pooled L1 pixels of one level. The CTA stages its (67 x 35)
+//        input tile of the level image, runs the 4x4 conv + folded BN/LReLU + 2x2 max for the 4
+//        L1 maps and writes the 4 neighbour-map sums that L2 consumes (S1 arena).
+// back:  one CTA per 32x16 tile of response pixels. It stages the S1 tile (4 x 42 x 72) in shared
+//        memory, computes the 8 pooled L2 maps and their sums on the 35 x 20 halo tile, then every
+//        thread finishes two vertically adjacent response pixels: the 16 L3 maps (4w x 5h), the
+//        52 hidden neurons and the output neuron.
+// Packed f32x2 instructions run two identical chains of IEEE operations at once (two pixels, or
+// two maps that read the same input), so every value still sees the reference's roundings.
 // Every tile of every level is one block of the same grid; a block finds its level by binary
-// search over the level table, so a frame is two launches whatever its pyramid depth.
+// search over the level descriptors (kernel parameters), so a frame is two launches per group of
+// up to kParamLevels levels.
 #include "kernels.h"
 #include "resample.cuh"
 
 namespace ccnn {
 
-__device__ __forceinline__ int find_level(const LevelDesc* __restrict__ lv, int n, int tile, bool front) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        int base = front ? lv[mid].k1_base : lv[mid].k2_base;
-        if (base <= tile) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
 constexpr int kInW = 2 * kK1TileX + 3;  // 67
 constexpr int kInH = 2 * kK1TileY + 3;  // 35
 constexpr int kInWh = (kInW + 1) / 2;   // 34 columns of each parity
 
-// Tile layout for the front kernel: row r of the input tile is stored next to row r+2 as a packed
-// pair (a thread computes two vertically adjacent pooled pixels, whose windows are 2 rows apart),
-// and columns are split by parity so that the stride-2 column walk of a warp is conflict-free.
-__global__ void __launch_bounds__(256, 4) stage1_front_kernel(const __grid_constant__ Stage1W W, const LevelDesc* __restrict__ levels,
-                                                              int n_levels, const float* __restrict__ gray, int gpitch, int gw, int gh,
-                                                              float* __restrict__ s1) {
-    __shared__ float2 tinp[kInH - 2][2][kInWh];
-    __shared__ float tin_tail[2][kInW];        // the last two rows have no partner below
-    __shared__ uint32_t col_idx[kInW], row_idx[kInH];
-    __shared__ float col_f[kInW], col_c[kInW], row_f[kInH], row_c[kInH];
-    const int lvl = find_level(levels, n_levels, blockIdx.x, true);
-    const LevelDesc L = levels[lvl];
-    const int t = blockIdx.x - L.k1_base;
+// One input sample of the front tile: row r, column c (tile coordinates) = value v. Row r is
+// stored next to row r+2 as a packed pair (a thread computes two vertically adjacent pooled
+// pixels, whose windows are 2 rows apart), and columns are split by parity so that the stride-2
+// column walk of a warp is conflict-free.
+struct FrontTile {
+    float2 p[kInH - 2][2][kInWh];
+    float tail[2][kInW];  // the last two rows have no partner below
+    __device__ __forceinline__ void put(int r, int c, float v) {
+        if (r < kInH - 2)
+            p[r][c & 1][c >> 1].x = v;
+        else
+            tail[r - (kInH - 2)][c] = v;
+        if (r >= 2) p[r - 2][c & 1][c >> 1].y = v;
+    }
+};
+
+// Loads the (67 x 35) input tile of a front CTA from its level image. Rows that start 16-byte
+// aligned with a pitch of whole float4 groups are read as 17 float4 per row (columns past the
+// image width hold zeros or the caller's own padding; no stored pixel depends on them), other
+// images one float at a time.
+__device__ __forceinline__ void load_front_tile(FrontTile& T, const float* __restrict__ img, const LevelDesc& L, int ix0, int iy0) {
+    if (L.img_vec) {
+        constexpr int kV = (kInW + 3) / 4;  // 17
+        for (int i = threadIdx.x; i < kInH * kV; i += blockDim.x) {
+            const int r = i / kV, c4 = i - r * kV;
+            const int x = ix0 + 4 * c4, y = iy0 + r;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (y < L.h && x < L.img_pitch) v = __ldg(reinterpret_cast<const float4*>(img + (long long)y * L.img_pitch + x));
+            T.put(r, 4 * c4, v.x);
+            T.put(r, 4 * c4 + 1, v.y);
+            T.put(r, 4 * c4 + 2, v.z);
+            if (4 * c4 + 3 < kInW) T.put(r, 4 * c4 + 3, v.w);
+        }
+    } else {
+        for (int i = threadIdx.x; i < kInH * kInW; i += blockDim.x) {
+            const int r = i / kInW, c = i - r * kInW;
+            const int x = ix0 + c, y = iy0 + r;
+            T.put(r, c, (x < L.w && y < L.h) ? __ldg(img + (long long)y * L.img_pitch + x) : 0.f);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, 3) stage1_front_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ LevelTable LT,
+                                                              const float* __restrict__ limg, float* __restrict__ s1) {
+    __shared__ FrontTile T;
+    const int g = LT.first + blockIdx.x;
+    const LevelDesc& L = LT.lv[find_level<&LevelDesc::k1_base>(LT, g)];
+    const int t = g - L.k1_base;
     const int px0 = (t % L.k1_tiles_x) * kK1TileX;
     const int py0 = (t / L.k1_tiles_x) * kK1TileY;
     const int ix0 = 2 * px0, iy0 = 2 * py0;
 
-    // per-tile sampling table: one column / row of the resampler each
-    if (L.mode != 0) {
-        if (threadIdx.x < kInW) {
-            const AxisSample sx = sample_col(ix0 + threadIdx.x, L.sclx, gw);
-            col_idx[threadIdx.x] = sx.idx;
-            col_f[threadIdx.x] = sx.f;
-            col_c[threadIdx.x] = sx.c;
-        } else if (threadIdx.x >= 128 && threadIdx.x < 128 + kInH) {
-            const int r = threadIdx.x - 128;
-            const AxisSample sy = sample_row(iy0 + r, L.scly, gh);
-            uint32_t py = sy.idx;
-            if (L.mode == 2 && py + 1 >= (uint32_t)gh) py--;  // bilinear keeps a row below
-            row_idx[r] = py;
-            row_f[r] = sy.f;
-            row_c[r] = sy.c;
-        }
-        __syncthreads();
-    }
-    for (int i = threadIdx.x; i < kInH * kInW; i += blockDim.x) {
-        const int r = i / kInW, c = i - r * kInW;
-        const int lx = ix0 + c, ly = iy0 + r;
-        float v = 0.f;
-        if (lx < L.w && ly < L.h) {
-            if (L.mode == 0) {
-                v = gray[(size_t)ly * gpitch + lx];
-            } else if (L.mode == 1) {
-                v = gray[(size_t)row_idx[r] * gpitch + col_idx[c]];
-            } else {
-                const float* r0 = gray + (size_t)row_idx[r] * gpitch + col_idx[c];
-                const float top = fadd(fmul(r0[0], col_c[c]), fmul(r0[1], col_f[c]));
-                const float bot = fadd(fmul(r0[gpitch], col_c[c]), fmul(r0[gpitch + 1], col_f[c]));
-                v = fadd(fmul(top, row_c[r]), fmul(bot, row_f[r]));
-            }
-        }
-        float* lo = r < kInH - 2 ? &tinp[r][c & 1][c >> 1].x : &tin_tail[r - (kInH - 2)][c];
-        *lo = v;
-        if (r >= 2) tinp[r - 2][c & 1][c >> 1].y = v;
-    }
+    load_front_tile(T, limg + L.img_off, L, ix0, iy0);
     __syncthreads();
 
     const int qx = threadIdx.x & (kK1TileX - 1);
@@ -99,169 +89,253 @@ __global__ void __launch_bounds__(256, 4) stage1_front_kernel(const __grid_const
 #pragma unroll
     for (int r = 0; r < 5; ++r)
 #pragma unroll
-        for (int c = 0; c < 5; ++c) pr[r][c] = *reinterpret_cast<const f2_t*>(&tinp[2 * qy + r][c & 1][qx + (c >> 1)]);
+        for (int c = 0; c < 5; ++c) pr[r][c] = *reinterpret_cast<const f2_t*>(&T.p[2 * qy + r][c & 1][qx + (c >> 1)]);
 
-    float P[2][4];
+    // packed over the two pixels (lo = row qy, hi = row qy + 1)
+    f2_t P[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
-        float cv[2][4];
+        f2_t cv[4];
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
             const int dy = d >> 1, dx = d & 1;
             f2_t acc = f2_mul(pr[dy][dx], f2_ld(W.k1d[m][0]), nz);
 #pragma unroll
-            for (int k = 1; k < 16; ++k)
-                acc = f2_add(acc, f2_mul(pr[dy + (k >> 2)][dx + (k & 3)], f2_ld(W.k1d[m][k]), nz));
-            cv[0][d] = lrelu_bn(f2_lo(acc), W.b1[m], W.w1a[m], W.w1b[m], W.bn1[m]);
-            cv[1][d] = lrelu_bn(f2_hi(acc), W.b1[m], W.w1a[m], W.w1b[m], W.bn1[m]);
+            for (int k = 1; k < 16; ++k) acc = f2_add(acc, f2_mul(pr[dy + (k >> 2)][dx + (k & 3)], f2_ld(W.k1d[m][k]), nz));
+            cv[d] = lrelu_bn2(acc, W.a1d[m], nz);
         }
-#pragma unroll
-        for (int q = 0; q < 2; ++q) P[q][m] = fmaxf(fmaxf(cv[q][0], cv[q][1]), fmaxf(cv[q][2], cv[q][3]));
+        P[m] = f2_max4(cv[0], cv[1], cv[2], cv[3]);
     }
+    // neighbour-map sums consumed by L2 (add/add2 of the reference)
+    const f2_t s01 = f2_add(P[0], P[1]);
+    const f2_t o[4] = {s01, f2_add(s01, P[2]), f2_add(f2_add(P[1], P[2]), P[3]), f2_add(P[2], P[3])};
+    const int gx = px0 + qx, gy = py0 + qy;
+    if (gx < L.p1w) {
+        float* out = s1 + L.s1_off + (long long)gy * L.s1_pitch + gx;
+        if (gy < L.p1h) {
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        const int gx = px0 + qx, gy = py0 + qy + q;
-        if (gx < L.p1w && gy < L.p1h) {
-            float* o = s1 + L.s1_off + (long long)gy * L.s1_pitch + gx;
-            o[0] = fadd(P[q][0], P[q][1]);
-            o[L.s1_plane] = fadd(fadd(P[q][0], P[q][1]), P[q][2]);
-            o[2 * L.s1_plane] = fadd(fadd(P[q][1], P[q][2]), P[q][3]);
-            o[3 * L.s1_plane] = fadd(P[q][2], P[q][3]);
+            for (int k = 0; k < 4; ++k) out[k * L.s1_plane] = f2_lo(o[k]);
+        }
+        if (gy + 1 < L.p1h) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) out[k * L.s1_plane + L.s1_pitch] = f2_hi(o[k]);
         }
     }
 }
 
-constexpr int kP2TW = kK2TileX + 3;  // 19
-constexpr int kP2TH = kK2TileY + 4;  // 20
-constexpr int kS1TW = 2 * kP2TW + 2; // 40
-constexpr int kS1TH = 2 * kP2TH + 2; // 42
-constexpr int kS1TWh = kS1TW / 2 + 1; // 21 columns of each parity (+1 pad)
+constexpr int kP2TW = kK2TileX + 3;   // 35 pooled L2 columns (halo 3)
+constexpr int kP2TH = kK2TileY + 4;   // 20 pooled L2 rows (halo 4)
+constexpr int kS1TW = 2 * kP2TW + 2;  // 72
+constexpr int kS1TH = 2 * kP2TH + 2;  // 42
+constexpr int kS1TWh = kS1TW / 2;     // 36 columns of each parity
+constexpr int kS2P = kP2TW + 1;       // 36: ts2 row pitch
 
-__global__ void __launch_bounds__(256) stage1_back_kernel(const __grid_constant__ Stage1W W, const LevelDesc* __restrict__ levels,
-                                                          int n_levels, const float* __restrict__ s1, float* __restrict__ resp) {
-    __shared__ float ts1[4][kS1TH][2 * kS1TWh];  // column c stored at (c & 1) * kS1TWh + (c >> 1)
-    __shared__ float ts2[8][kP2TH][kP2TW + 1];
-    const int lvl = find_level(levels, n_levels, blockIdx.x, false);
-    const LevelDesc L = levels[lvl];
-    const int t = blockIdx.x - L.k2_base;
+struct BackSmem {
+    float s1[4][kS1TH][kS1TW];    // column c stored at (c & 1) * kS1TWh + (c >> 1)
+    float s2[8][kP2TH][kS2P];     // the 8 neighbour sums of the pooled L2 maps
+};
+constexpr int kBackSmemBytes = (int)sizeof(BackSmem);
+
+// back: one CTA per 32 x 16 tile of response pixels.
+//   A: the S1 tile (4 x 42 x 72) is staged in shared memory with 16-byte loads;
+//   B: the 8 pooled L2 maps and their sums on the 35 x 20 halo tile (maps 2i and 2i+1 read the
+//      same S1 map i: one packed pair);
+//   C: every thread finishes two vertically adjacent response pixels, every operation packed over
+//      the pair: the 16 L3 maps (4w x 5h), the 52 hidden neurons and the output neuron.
+__global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ Stage1Dup D,
+                                                             const __grid_constant__ LevelTable LT, const float* __restrict__ s1,
+                                                             float* __restrict__ resp) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BackSmem& S = *reinterpret_cast<BackSmem*>(smem_raw);
+    const int g = LT.first + blockIdx.x;
+    const LevelDesc& L = LT.lv[find_level<&LevelDesc::k2_base>(LT, g)];
+    const int t = g - L.k2_base;
     const int ox0 = (t % L.k2_tiles_x) * kK2TileX;
     const int oy0 = (t / L.k2_tiles_x) * kK2TileY;
     const int sx0 = 2 * ox0, sy0 = 2 * oy0;
 
-    for (int i = threadIdx.x; i < 4 * kS1TH * kS1TW; i += blockDim.x) {
-        int m = i / (kS1TH * kS1TW);
-        int rem = i - m * (kS1TH * kS1TW);
-        int r = rem / kS1TW, c = rem - r * kS1TW;
-        int x = sx0 + c, y = sy0 + r;
-        float v = 0.f;
-        if (x < L.p1w && y < L.p1h) v = s1[L.s1_off + m * L.s1_plane + (long long)y * L.s1_pitch + x];
-        ts1[m][r][(c & 1) * kS1TWh + (c >> 1)] = v;
+    // A: rows of 18 float4; columns past the plane pitch and rows past p1h read as 0 (no valid
+    // response pixel depends on them)
+    {
+        const float* base = s1 + L.s1_off;
+        constexpr int kV = kS1TW / 4;
+        for (int i = threadIdx.x; i < 4 * kS1TH * kV; i += blockDim.x) {
+            const int row = i / kV, c4 = i - row * kV;
+            const int m = row / kS1TH, rr = row - m * kS1TH;
+            const int x = sx0 + 4 * c4, y = sy0 + rr;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (y < L.p1h && x < L.s1_pitch)
+                v = __ldg(reinterpret_cast<const float4*>(base + m * L.s1_plane + (long long)y * L.s1_pitch + x));
+            *reinterpret_cast<float2*>(&S.s1[m][rr][2 * c4]) = make_float2(v.x, v.z);
+            *reinterpret_cast<float2*>(&S.s1[m][rr][kS1TWh + 2 * c4]) = make_float2(v.y, v.w);
+        }
     }
     __syncthreads();
 
     const f2_t nz = f2_ld(W.negzero);
-    // pooled L2 maps and their neighbour sums on the (19 x 20) halo tile; maps 2i and 2i+1 read the
-    // same sum map i, so they run as one packed pair
+    // B
     for (int p = threadIdx.x; p < kP2TW * kP2TH; p += blockDim.x) {
         const int x = p % kP2TW, y = p / kP2TW;
-        float P[8];
+        f2_t P[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             f2_t q[4][4];
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
-                for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(ts1[i][2 * y + r][(c & 1) * kS1TWh + x + (c >> 1)]);
-            float cv[2][4];
+                for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(S.s1[i][2 * y + r][(c & 1) * kS1TWh + x + (c >> 1)]);
+            f2_t cv[4];
 #pragma unroll
             for (int d = 0; d < 4; ++d) {
                 const int dy = d >> 1, dx = d & 1;
                 f2_t acc = f2_mul(q[dy][dx], f2_ld(W.k2p[i][0]), nz);
 #pragma unroll
                 for (int k = 1; k < 9; ++k) acc = f2_add(acc, f2_mul(q[dy + k / 3][dx + k % 3], f2_ld(W.k2p[i][k]), nz));
-                cv[0][d] = lrelu_bn(f2_lo(acc), W.b2[2 * i], W.w2a[2 * i], W.w2b[2 * i], W.bn2[2 * i]);
-                cv[1][d] = lrelu_bn(f2_hi(acc), W.b2[2 * i + 1], W.w2a[2 * i + 1], W.w2b[2 * i + 1], W.bn2[2 * i + 1]);
+                cv[d] = lrelu_bn2(acc, W.a2p[i], nz);
             }
-            P[2 * i] = fmaxf(fmaxf(cv[0][0], cv[0][1]), fmaxf(cv[0][2], cv[0][3]));
-            P[2 * i + 1] = fmaxf(fmaxf(cv[1][0], cv[1][1]), fmaxf(cv[1][2], cv[1][3]));
+            P[i] = f2_max4(cv[0], cv[1], cv[2], cv[3]);  // (map 2i, map 2i+1)
         }
-        ts2[0][y][x] = fadd(P[0], P[1]);
+        float Pm[8];
 #pragma unroll
-        for (int k = 1; k < 7; ++k) ts2[k][y][x] = fadd(fadd(P[k - 1], P[k]), P[k + 1]);
-        ts2[7][y][x] = fadd(P[6], P[7]);
+        for (int i = 0; i < 4; ++i) {
+            Pm[2 * i] = f2_lo(P[i]);
+            Pm[2 * i + 1] = f2_hi(P[i]);
+        }
+        S.s2[0][y][x] = fadd(Pm[0], Pm[1]);
+#pragma unroll
+        for (int k = 1; k < 7; ++k) S.s2[k][y][x] = fadd(fadd(Pm[k - 1], Pm[k]), Pm[k + 1]);
+        S.s2[7][y][x] = fadd(Pm[6], Pm[7]);
     }
     __syncthreads();
 
-    const int x = threadIdx.x & (kK2TileX - 1), y = threadIdx.x / kK2TileX;
-    float A[16];
+    // C: pixels (x, y) and (x, y + 1)
+    const int x = threadIdx.x & (kK2TileX - 1), y = (threadIdx.x / kK2TileX) * 2;
+    f2_t A[16];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        f2_t q[5][4];
+        float v[6][4];
 #pragma unroll
-        for (int r = 0; r < 5; ++r)
+        for (int r = 0; r < 6; ++r)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(ts2[i][y + r][x + c]);
-        // conv_5x4 keeps one partial sum per kernel row, added in row order
-        f2_t acc = 0ull;
+            for (int c = 0; c < 4; ++c) v[r][c] = S.s2[i][y + r][x + c];
 #pragma unroll
-        for (int r = 0; r < 5; ++r) {
-            f2_t rs = f2_mul(q[r][0], f2_ld(W.k3p[i][4 * r]), nz);
+        for (int e = 0; e < 2; ++e) {
+            const int mm = 2 * i + e;
+            // conv_5x4 keeps one partial sum per kernel row, added in row order
+            f2_t acc = 0ull;
 #pragma unroll
-            for (int c = 1; c < 4; ++c) rs = f2_add(rs, f2_mul(q[r][c], f2_ld(W.k3p[i][4 * r + c]), nz));
-            acc = (r == 0) ? rs : f2_add(acc, rs);
+            for (int r = 0; r < 5; ++r) {
+                f2_t rs = f2_mul(f2_pack(v[r][0], v[r + 1][0]), f2_ld(D.k3d[mm][4 * r]), nz);
+#pragma unroll
+                for (int c = 1; c < 4; ++c) rs = f2_add(rs, f2_mul(f2_pack(v[r][c], v[r + 1][c]), f2_ld(D.k3d[mm][4 * r + c]), nz));
+                acc = (r == 0) ? rs : f2_add(acc, rs);
+            }
+            A[mm] = lrelu_bn2(acc, D.a3d[mm], nz);
         }
-        A[2 * i] = lrelu_bn(f2_lo(acc), W.b3[2 * i], W.w3a[2 * i], W.w3b[2 * i], W.bn3[2 * i]);
-        A[2 * i + 1] = lrelu_bn(f2_hi(acc), W.b3[2 * i + 1], W.w3a[2 * i + 1], W.w3b[2 * i + 1], W.bn3[2 * i + 1]);
     }
-    // hidden neurons n = 4*i + t read L3 maps i..i+3 (neurons 2p, 2p+1 share them: packed); the
-    // output sum then runs over n in order
-    f2_t Ad[16];
-#pragma unroll
-    for (int m = 0; m < 16; ++m) Ad[m] = f2_dup(A[m]);
-    float out = 0.f;
+    // hidden neuron n = 4*i + t reads L3 maps i..i+3; the output sum runs over n in order
+    const f2_t half = f2_pack(0.5f, 0.5f);
+    f2_t out = 0ull;
 #pragma unroll
     for (int i = 0; i < Stage1W::kGroups; ++i) {
 #pragma unroll
-        for (int tp = 0; tp < Stage1W::kHS / 2; ++tp) {
-            const int n = Stage1W::kHS * i + 2 * tp;
-            f2_t s = f2_pack(W.hb[n], W.hb[n + 1]);
+        for (int tt = 0; tt < Stage1W::kHS; ++tt) {
+            const int n = Stage1W::kHS * i + tt;
+            f2_t s = f2_ld(D.hbd[n]);
 #pragma unroll
-            for (int j = 0; j < Stage1W::kConn; ++j) s = f2_add(s, f2_mul(Ad[i + j], f2_ld(W.hwp[n / 2][j]), nz));
-            s = f2_mul(s, f2_dup(W.htw[i]), nz);
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int tt = 2 * tp + e;
-                float v = tanh_rational(e == 0 ? f2_lo(s) : f2_hi(s));
-                v = fadd(fmul(0.5f, v), 0.5f);
-                const float h = fadd(fmul(W.hbnw[tt], v), W.hbnb[tt]);
-                out = (n + e == 0) ? fmul(h, W.ow[0]) : fadd(fmul(h, W.ow[n + e]), out);
-            }
+            for (int j = 0; j < Stage1W::kConn; ++j) s = f2_add(s, f2_mul(A[i + j], f2_ld(D.hwd[n][j]), nz));
+            s = f2_mul(s, f2_ld(D.htwd[i]), nz);
+            f2_t v = tanh_rational2(s, nz);
+            v = f2_add(f2_mul(half, v, nz), half);
+            const f2_t h = f2_add(f2_mul(f2_ld(D.hbnwd[tt]), v, nz), f2_ld(D.hbnbd[tt]));
+            out = (n == 0) ? f2_mul(h, f2_ld(D.owd[0]), nz) : f2_add(f2_mul(h, f2_ld(D.owd[n]), nz), out);
         }
     }
-    float c = fmul(fadd(out, W.ob), W.otw);
-    c = tanh_rational(c);
-    const float r = (W.af == 0.f) ? fadd(fmul(0.5f, c), 0.5f) : fmul(W.af, c);
+    f2_t c = f2_mul(f2_add(out, f2_ld(D.obd)), f2_ld(D.otwd), nz);
+    c = tanh_rational2(c, nz);
+    const f2_t r = (W.af == 0.f) ? f2_add(f2_mul(half, c, nz), half) : f2_mul(f2_ld(D.afd), c, nz);
     const int gx = ox0 + x, gy = oy0 + y;
-    if (gx < L.ow && gy < L.oh) resp[L.resp_off + (long long)gy * L.ow + gx] = r;
+    if (gx < L.ow) {
+        if (gy < L.oh) resp[L.resp_off + (long long)gy * L.ow + gx] = f2_lo(r);
+        if (gy + 1 < L.oh) resp[L.resp_off + (long long)(gy + 1) * L.ow + gx] = f2_hi(r);
+    }
 }
 
-cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, const float* gray, int gpitch,
-                                int gw, int gh, float* s1, cudaStream_t st) {
-    if (k1_tiles > 0) stage1_front_kernel<<<k1_tiles, 256, 0, st>>>(W, d_levels, n_levels, gray, gpitch, gw, gh, s1);
+// Duplicated stage-1 parameters for the back kernel, derived from the packed weight block.
+static Stage1Dup make_dup(const Stage1W& W) {
+    Stage1Dup D;
+    auto dup = [](float v) { return make_float2(v, v); };
+    for (int i = 0; i < Stage1W::kM3 / 2; ++i)
+        for (int k = 0; k < Stage1W::kK3W * Stage1W::kK3H; ++k) {
+            D.k3d[2 * i][k] = dup(W.k3p[i][k].x);
+            D.k3d[2 * i + 1][k] = dup(W.k3p[i][k].y);
+        }
+    for (int mm = 0; mm < Stage1W::kM3; ++mm) {
+        D.a3d[mm][0] = dup(W.b3[mm]);
+        D.a3d[mm][1] = dup(W.w3a[mm]);
+        D.a3d[mm][2] = dup(W.w3b[mm]);
+        D.a3d[mm][3] = dup(W.bn3[mm]);
+    }
+    for (int q = 0; q < Stage1W::kHL / 2; ++q)
+        for (int j = 0; j < Stage1W::kConn; ++j) {
+            D.hwd[2 * q][j] = dup(W.hwp[q][j].x);
+            D.hwd[2 * q + 1][j] = dup(W.hwp[q][j].y);
+        }
+    for (int n = 0; n < Stage1W::kHL; ++n) {
+        D.hbd[n] = dup(W.hb[n]);
+        D.owd[n] = dup(W.ow[n]);
+    }
+    for (int i = 0; i < Stage1W::kGroups; ++i) D.htwd[i] = dup(W.htw[i]);
+    for (int tt = 0; tt < Stage1W::kHS; ++tt) {
+        D.hbnwd[tt] = dup(W.hbnw[tt]);
+        D.hbnbd[tt] = dup(W.hbnb[tt]);
+    }
+    D.obd = dup(W.ob);
+    D.otwd = dup(W.otw);
+    D.afd = dup(W.af);
+    return D;
+}
+
+cudaError_t stage1_setup() {
+    return cudaFuncSetAttribute(stage1_back_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBackSmemBytes);
+}
+
+// Launches KERNEL once per group of at most kParamLevels levels; tiles(L) is a level's block count
+// and base(L) its first global block.
+template <class Launch, class Tiles>
+static cudaError_t launch_grouped(const LevelDesc* levels, int n_levels, int LevelDesc::*base, Tiles tiles, Launch launch) {
+    for (int g0 = 0; g0 < n_levels; g0 += kParamLevels) {
+        LevelTable T;
+        T.n = n_levels - g0 < kParamLevels ? n_levels - g0 : kParamLevels;
+        for (int i = 0; i < T.n; ++i) T.lv[i] = levels[g0 + i];
+        T.first = T.lv[0].*base;
+        const LevelDesc& last = T.lv[T.n - 1];
+        const int blocks = last.*base + tiles(last) - T.first;
+        if (blocks > 0) launch(T, blocks);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     return cudaGetLastError();
 }
 
-cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k2_tiles, const float* s1, float* resp,
-                               cudaStream_t st) {
-    if (k2_tiles > 0) stage1_back_kernel<<<k2_tiles, 256, 0, st>>>(W, d_levels, n_levels, s1, resp);
-    return cudaGetLastError();
+cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st) {
+    return launch_grouped(
+        levels, n_levels, &LevelDesc::k1_base, [](const LevelDesc& L) { return L.k1_tiles_x * ((L.p1h + kK1TileY - 1) / kK1TileY); },
+        [&](const LevelTable& T, int blocks) { stage1_front_kernel<<<blocks, 256, 0, st>>>(W, T, limg, s1); });
 }
 
-cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, int k2_tiles, const float* gray,
-                          int gpitch, int gw, int gh, float* s1, float* resp, cudaStream_t st) {
-    cudaError_t e = launch_stage1_front(W, d_levels, n_levels, k1_tiles, gray, gpitch, gw, gh, s1, st);
+cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st) {
+    const Stage1Dup D = make_dup(W);
+    return launch_grouped(
+        levels, n_levels, &LevelDesc::k2_base, [](const LevelDesc& L) { return L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY); },
+        [&](const LevelTable& T, int blocks) { stage1_back_kernel<<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp); });
+}
+
+cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
+                          cudaStream_t st) {
+    cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st);
     if (e != cudaSuccess) return e;
-    return launch_stage1_back(W, d_levels, n_levels, k2_tiles, s1, resp, st);
+    return launch_stage1_back(W, levels, n_levels, s1, resp, st);
 }
 
 }  // namespace ccnn

@@ -41,12 +41,19 @@ cudaError_t launch_gray_u8_resized(const uint8_t* src, int spitch, int sw, int s
                                    cudaStream_t st);
 cudaError_t launch_resize_f32(const float* src, int spitch, int sw, int sh, float* dst, int dpitch, int dw, int dh, int type,
                               cudaStream_t st);
-cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, int k2_tiles, const float* gray,
-                          int gpitch, int gw, int gh, float* s1, float* resp, cudaStream_t st);
-cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k1_tiles, const float* gray, int gpitch,
-                                int gw, int gh, float* s1, cudaStream_t st);
-cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* d_levels, int n_levels, int k2_tiles, const float* s1, float* resp,
-                               cudaStream_t st);
+// every level image of a frame into the level arena (img_off / img_pitch of each descriptor);
+// blocks of kPyrCols columns x kPyrRows rows (pyr_wq column blocks per level row band)
+constexpr int kPyrCols = 256, kPyrRows = 8;
+cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* gray, int gpitch, int gw, int gh, float* limg,
+                           cudaStream_t st);
+// stage-1 net over all levels; `levels` is a HOST array (the descriptors travel as kernel
+// parameters), level images at limg + img_off
+cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
+                          cudaStream_t st);
+cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st);
+// dynamic shared memory of the stage-1 back kernel (set once per device before any launch)
+cudaError_t stage1_setup();
+cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st);
 cudaError_t launch_cand_count(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
                               cudaStream_t st);
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,

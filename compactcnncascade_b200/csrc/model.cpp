@@ -162,6 +162,28 @@ bool pack_model(const RawModel& m, int index_output, NW* o, std::string* err) {
         o->w3b[mm] = act(2, mm, 2);
         o->bn3[mm] = act(2, mm, 4);
     }
+    for (int mm = 0; mm < NW::kM1; ++mm) {
+        const float v[4] = {o->b1[mm], o->w1a[mm], o->w1b[mm], o->bn1[mm]};
+        for (int f = 0; f < 4; ++f) o->a1d[mm][f] = make_float2(v[f], v[f]);
+    }
+    for (int i = 0; i < NW::kM1 / 2; ++i) {
+        o->a1p[i][0] = make_float2(o->b1[2 * i], o->b1[2 * i + 1]);
+        o->a1p[i][1] = make_float2(o->w1a[2 * i], o->w1a[2 * i + 1]);
+        o->a1p[i][2] = make_float2(o->w1b[2 * i], o->w1b[2 * i + 1]);
+        o->a1p[i][3] = make_float2(o->bn1[2 * i], o->bn1[2 * i + 1]);
+    }
+    for (int i = 0; i < NW::kM2 / 2; ++i) {
+        o->a2p[i][0] = make_float2(o->b2[2 * i], o->b2[2 * i + 1]);
+        o->a2p[i][1] = make_float2(o->w2a[2 * i], o->w2a[2 * i + 1]);
+        o->a2p[i][2] = make_float2(o->w2b[2 * i], o->w2b[2 * i + 1]);
+        o->a2p[i][3] = make_float2(o->bn2[2 * i], o->bn2[2 * i + 1]);
+    }
+    for (int i = 0; i < NW::kM3 / 2; ++i) {
+        o->a3p[i][0] = make_float2(o->b3[2 * i], o->b3[2 * i + 1]);
+        o->a3p[i][1] = make_float2(o->w3a[2 * i], o->w3a[2 * i + 1]);
+        o->a3p[i][2] = make_float2(o->w3b[2 * i], o->w3b[2 * i + 1]);
+        o->a3p[i][3] = make_float2(o->bn3[2 * i], o->bn3[2 * i + 1]);
+    }
     for (int n = 0; n < NW::kHL; ++n) o->hb[n] = m.hb[n];
     for (int q = 0; q < NW::kHL / 2; ++q)
         for (int j = 0; j < NW::kConn; ++j)

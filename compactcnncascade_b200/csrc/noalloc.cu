@@ -8,11 +8,11 @@
 // part of the library image instead.
 //
 // The scratch is a file-scope __device__ array: every GPU that loads the library holds it (9 MiB +
-// 256 B) until the process exits. It holds the level descriptor (first 256 bytes) and the four L1
-// neighbour-sum planes of the image (up to kStaticS1Floats floats). Every call shares it, and it keeps
-// the last call's contents; nothing in it has to start at zero, because each call writes the
-// descriptor and every plane value it later reads. Calls that overlap on the GPU (different
-// streams, or different host threads) race on the array.
+// 256 B) until the process exits. It holds the four L1 neighbour-sum planes of the image (up to
+// kStaticS1Floats floats) after a reserved first 256 bytes; the level descriptor travels as a
+// kernel parameter. Every call shares it, and it keeps the last call's contents; nothing in it has
+// to start at zero, because each call writes every plane value it later reads. Calls that overlap
+// on the GPU (different streams, or different host threads) race on the array.
 #include <cuda_runtime.h>
 
 #include <map>
@@ -30,8 +30,7 @@ void set_error(const std::string& msg);
 namespace {
 
 constexpr long long kStaticS1Floats = 2359296;  // 9 MiB of fp32: a 1920x1080 image needs 2,065,920
-constexpr size_t kDescBytes = 256;
-static_assert(sizeof(LevelDesc) <= kDescBytes, "level descriptor must fit its scratch slot");
+constexpr size_t kDescBytes = 256;  // reserved head of the array
 
 static __device__ __align__(256) unsigned char g_stage1_scratch[kDescBytes + sizeof(float) * kStaticS1Floats];
 
@@ -52,6 +51,11 @@ ccnn_status scratch_address(int dev, unsigned char** out) {
         const cudaError_t e = cudaGetSymbolAddress(&p, g_stage1_scratch);
         if (e != cudaSuccess) {
             set_error(std::string("cudaGetSymbolAddress(static stage-1 scratch): ") + cudaGetErrorString(e));
+            return CCNN_ERR_CUDA;
+        }
+        const cudaError_t e2 = stage1_setup();  // kernel attribute, no allocation
+        if (e2 != cudaSuccess) {
+            set_error(std::string("stage-1 kernel set-up: ") + cudaGetErrorString(e2));
             return CCNN_ERR_CUDA;
         }
         g_scratch_addr[dev] = p;
@@ -116,6 +120,9 @@ extern "C" CCNN_API ccnn_status ccnn_stage1_forward_static(const char* model_pat
     L.k2_tiles_x = (L.ow + kK2TileX - 1) / kK2TileX;
     L.k1_base = 0;
     L.k2_base = 0;
+    L.img_off = 0;
+    L.img_pitch = (int)(step / sizeof(float));
+    L.img_vec = (L.img_pitch % 4 == 0 && (reinterpret_cast<uintptr_t>(d_img) & 15) == 0) ? 1 : 0;
     *resp_cols = L.ow;
     *resp_rows = L.oh;
     if (4 * L.s1_plane > kStaticS1Floats) {
@@ -139,14 +146,10 @@ extern "C" CCNN_API ccnn_status ccnn_stage1_forward_static(const char* model_pat
     unsigned char* scratch = nullptr;
     st = scratch_address(dev, &scratch);
     if (st != CCNN_OK) return st;
-    LevelDesc* d_level = reinterpret_cast<LevelDesc*>(scratch);
     float* d_s1 = reinterpret_cast<float*>(scratch + kDescBytes);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int k1 = L.k1_tiles_x * ((L.p1h + kK1TileY - 1) / kK1TileY);
-    const int k2 = L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY);
-    e = cudaMemcpyAsync(d_level, &L, sizeof(LevelDesc), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = launch_stage1_front(w, d_level, 1, k1, d_img, (int)(step / sizeof(float)), cols, rows, d_s1, s);
-    if (e == cudaSuccess) e = launch_stage1_back(w, d_level, 1, k2, d_s1, d_resp, s);
+    e = launch_stage1_front(w, &L, 1, d_img, d_s1, s);
+    if (e == cudaSuccess) e = launch_stage1_back(w, &L, 1, d_s1, d_resp, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         set_error(std::string("static stage-1 forward: ") + cudaGetErrorString(e));
