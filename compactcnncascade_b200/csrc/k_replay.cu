@@ -15,8 +15,12 @@
 //
 // The scan test of a level against the detections of earlier levels has no order dependence,
 // so all 32 warps run it in parallel (one warp per candidate, 32 earlier boxes per ballot).
-// What depends on order (copies appended during the level's own scan, the survivors' pass,
-// the sort and the clustering) runs in warp 0 with ballots over 32 boxes at a time.
+// Every box a level appends has the geometry of one of that level's candidates, so the tests
+// against boxes appended during the level (its own scan, then the survivors' pass) are candidate
+// pairs: all warps evaluate them into bit matrices first, and warp 0 then replays the order-
+// dependent decisions with one ballot over the bit words per candidate. Levels with more than
+// kBitMax candidates take the direct route (warp 0 tests the appended boxes 32 at a time). The sort
+// permutes (scale, index) keys, and the clustering runs in warp 0.
 #include "kernels.h"
 #include "replay.cuh"
 
@@ -27,21 +31,6 @@ constexpr int kRT = 1024;
 __device__ __forceinline__ Det cand_rect(const Candidate& c, float inv_scale, float scale) {
     return make_det((int)((float)c.px * inv_scale), (int)((float)c.py * inv_scale), (int)((float)kPatW * inv_scale),
                     (int)((float)kPatH * inv_scale), 0.f, scale, 0);
-}
-
-__device__ __forceinline__ Det shfl_det(const Det& d, int src) {
-    Det r;
-    r.x = __shfl_sync(0xffffffffu, d.x, src);
-    r.y = __shfl_sync(0xffffffffu, d.y, src);
-    r.w = __shfl_sync(0xffffffffu, d.w, src);
-    r.h = __shfl_sync(0xffffffffu, d.h, src);
-    r.x2 = __shfl_sync(0xffffffffu, d.x2, src);
-    r.y2 = __shfl_sync(0xffffffffu, d.y2, src);
-    r.score = __shfl_sync(0xffffffffu, d.score, src);
-    r.scale = __shfl_sync(0xffffffffu, d.scale, src);
-    r.knn = __shfl_sync(0xffffffffu, d.knn, src);
-    r.num_detect = __shfl_sync(0xffffffffu, d.num_detect, src);
-    return r;
 }
 
 __device__ __forceinline__ void sort4(int* v) {
@@ -118,6 +107,9 @@ __device__ int merger_warp(const Det* in, int n, uint8_t* checked, Det* out, flo
                 if (pred && mt.s1_gt_s2 && lane < lim) checked[j] = 1;
                 if (mb) dropped = true;
             } else {
+                // the first lane (at or after `start`) whose box merges into the running cluster is
+                // absorbed; every lane then re-tests against the grown cluster box. The absorbed
+                // box is read by all lanes from shared memory (a broadcast), not shuffled.
                 int start = 0;
                 while (true) {
                     const MergeTest mt = merge_test(nmax, e, threshold);
@@ -125,13 +117,11 @@ __device__ int merger_warp(const Det* in, int n, uint8_t* checked, Det* out, flo
                     const unsigned m = __ballot_sync(0xffffffffu, pred);
                     if (!m) break;
                     const int f = __ffs(m) - 1;
-                    const Det ef = shfl_det(e, f);
-                    int X[4], Y[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        X[i] = __shfl_sync(0xffffffffu, mt.X[i], f);
-                        Y[i] = __shfl_sync(0xffffffffu, mt.Y[i], f);
-                    }
+                    const Det ef = in[base + f];
+                    int X[4] = {nmax.x, nmax.x2, ef.x, ef.x2};
+                    int Y[4] = {nmax.y, nmax.y2, ef.y, ef.y2};
+                    sort4(X);
+                    sort4(Y);
                     nmax.x = imin(nmax.x, X[0]);
                     nmax.y = imin(nmax.y, Y[0]);
                     nmax.x2 = imax(nmax.x2, X[3]);
@@ -205,10 +195,20 @@ __device__ __forceinline__ CandResult verdict(const WinOut* w, const Candidate& 
     return r;
 }
 
+constexpr int kBitMax = 256;              // candidates per level handled with bit matrices
+constexpr int kBitWords = kBitMax / 32;
+constexpr int kOwnVerdict = -kBitMax - 1;  // the candidate's own stage-2/3 verdict
+constexpr int kOwnScore = -kBitMax - 2;    // the candidate's stage-1 score (detection disabled)
+
 __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ int s_lvl_start[kMaxLevels + 1];
     __shared__ int s_nD, s_nS;
+    // bit j of word w of row i: drop_test(candidate i, box of candidate 32w + j) == 1 (A1) / == 2 (A2)
+    __shared__ uint32_t s_a1[kBitMax * kBitWords], s_a2[kBitMax * kBitWords];
+    __shared__ int s_didx[kBitMax];  // D index of the box a candidate appended, or -1
+    __shared__ int s_src[kBitMax];   // where that box's score/knn come from
+    __shared__ uint32_t s_S[kBitWords], s_T[kBitWords];  // candidate sets of the level (see below)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const CascadeConfig& C = a.cfg;
     const int n = *a.n_cand;
@@ -295,7 +295,163 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                 }
                 if (lane == 0) first_dec[c] = code;
             }
+            const int m = e - g;
+            const int W = (m + 31) >> 5;
+            if (m <= kBitMax) {
+                // candidate-pair tests of this level, one ballot per (row i, word w)
+                for (int it = warp; it < m * W; it += kRT / 32) {
+                    const int i = it / W, w = it - i * W;
+                    const int j = 32 * w + lane;
+                    int t = 0;
+                    if (j < i) {
+                        const Det nr = cand_rect(cands[g + i], inv_scale, scale);
+                        t = drop_test(nr, rect_shrink(nr, 0.7f), cand_rect(cands[g + j], inv_scale, scale));
+                    }
+                    const uint32_t b1 = __ballot_sync(0xffffffffu, t == 1), b2 = __ballot_sync(0xffffffffu, t == 2);
+                    if (lane == 0) {
+                        s_a1[i * W + w] = b1;
+                        s_a2[i * W + w] = b2;
+                    }
+                }
+            }
             __syncthreads();
+            if (m <= kBitMax) {
+                // The order-dependent decisions of the level as fixed points over candidate sets (bit
+                // j of word w = candidate 32w + j). Candidate i's decision depends only on candidates
+                // j < i, so after t rounds the first t candidates are final, and a round that changes
+                // nothing has reached the unique solution, which is the sequential one.
+                //   S: boxes appended during the scan: the first decisive box of candidate i (earlier
+                //      levels first, then S in order) has drop type 1;
+                //   T: boxes appended by the survivors' pass: survivor i overlaps (> 0.5) a box of T
+                //      (a copy), or its stage-2/3 verdict accepts it (or detection is disabled).
+                const bool thread_item = tid < m;  // candidate i = tid (m <= 256: warps 0..7)
+                const int i = tid;
+                int code = -1, acc = 0;
+                if (thread_item) {
+                    code = first_dec[g + i];
+                    acc = C.detect_enabled ? res[g + i].accepted : 1;
+                }
+                if (tid < kBitWords) {
+                    s_S[tid] = 0u;
+                    s_T[tid] = 0u;
+                }
+                __syncthreads();
+                bool inS = false;
+                for (int round = 0; round <= m; ++round) {
+                    bool in = false;
+                    if (thread_item) {
+                        if (code >= 0) {
+                            in = (code & 1) == 0;
+                        } else {
+                            for (int w = 0; w < W; ++w) {
+                                const uint32_t hit = (s_a1[i * W + w] | s_a2[i * W + w]) & s_S[w];
+                                if (hit) {
+                                    in = (s_a1[i * W + w] >> (__ffs(hit) - 1)) & 1u;
+                                    break;
+                                }
+                            }
+                        }
+                    }
+                    const uint32_t word = __ballot_sync(0xffffffffu, in);
+                    __syncthreads();  // every thread has read the previous round's S
+                    const bool changed = (lane == 0 && warp < W && s_S[warp] != word);
+                    if (lane == 0 && warp < W) s_S[warp] = word;
+                    inS = in;
+                    if (!__syncthreads_or(changed)) break;
+                }
+                // survivors: not decided by the scan
+                bool surv_i = false;
+                if (thread_item && code < 0) {
+                    surv_i = true;
+                    for (int w = 0; w < W; ++w)
+                        if ((s_a1[i * W + w] | s_a2[i * W + w]) & s_S[w]) {
+                            surv_i = false;
+                            break;
+                        }
+                }
+                const bool check = C.detect_enabled != 0;
+                for (int round = 0; round <= m; ++round) {
+                    bool in = false;
+                    if (surv_i) {
+                        in = acc != 0;
+                        if (check)
+                            for (int w = 0; w < W && !in; ++w) in = (s_a1[i * W + w] & s_T[w]) != 0u;
+                    }
+                    const uint32_t word = __ballot_sync(0xffffffffu, in);
+                    __syncthreads();
+                    const bool changed = (lane == 0 && warp < W && s_T[warp] != word);
+                    if (lane == 0 && warp < W) s_T[warp] = word;
+                    if (!__syncthreads_or(changed)) break;
+                }
+                // D index (scan appends in candidate order, then the survivors' appends) and the
+                // source of each box's score/knn
+                int nScan = 0, nSurv = 0;
+                for (int w = 0; w < W; ++w) {
+                    nScan += __popc(s_S[w]);
+                    nSurv += __popc(s_T[w]);
+                }
+                if (thread_item) {
+                    const uint32_t below = (1u << (i & 31)) - 1u;
+                    int dst = -1, src = 0;
+                    if (inS) {
+                        int r = 0;
+                        for (int w = 0; w < (i >> 5); ++w) r += __popc(s_S[w]);
+                        dst = nD + r + __popc(s_S[i >> 5] & below);
+                        if (code >= 0) {
+                            src = code >> 1;
+                        } else {
+                            for (int w = 0; w < W; ++w) {
+                                const uint32_t hit = (s_a1[i * W + w] | s_a2[i * W + w]) & s_S[w];
+                                if (hit) {
+                                    src = -1 - (32 * w + __ffs(hit) - 1);
+                                    break;
+                                }
+                            }
+                        }
+                    } else if ((s_T[i >> 5] >> (i & 31)) & 1u) {
+                        int r = 0;
+                        for (int w = 0; w < (i >> 5); ++w) r += __popc(s_T[w]);
+                        dst = nD + nScan + r + __popc(s_T[i >> 5] & below);
+                        src = C.detect_enabled ? kOwnVerdict : kOwnScore;
+                        if (check)
+                            for (int w = 0; w < W; ++w) {
+                                const uint32_t hit = s_a1[i * W + w] & s_T[w];
+                                if (hit) {
+                                    src = -1 - (32 * w + __ffs(hit) - 1);
+                                    break;
+                                }
+                            }
+                    }
+                    s_didx[i] = dst;
+                    s_src[i] = src;
+                }
+                __syncthreads();
+                // the boxes: rect of the candidate, score/knn from the end of its copy chain
+                if (thread_item && s_didx[i] >= 0) {
+                    int r = i, src = s_src[i];
+                    while (src < 0 && src > kOwnVerdict) {  // a box of this level: follow it
+                        r = -1 - src;
+                        src = s_src[r];
+                    }
+                    float sc;
+                    int kn;
+                    if (src >= 0) {
+                        sc = D[src].score;
+                        kn = D[src].knn;
+                    } else if (src == kOwnVerdict) {
+                        sc = res[g + r].score;
+                        kn = res[g + r].knn;
+                    } else {
+                        sc = cands[g + r].score;
+                        kn = 0;
+                    }
+                    const Det nr = cand_rect(cands[g + i], inv_scale, scale);
+                    D[s_didx[i]] = make_det(nr.x, nr.y, nr.w, nr.h, sc, scale, kn);
+                }
+                nD += nScan + nSurv;
+                __syncthreads();
+                continue;
+            }
             if (warp == 0) {
                 int nS = 0;
                 for (int c = g; c < e; ++c) {
@@ -390,17 +546,21 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
         nD = s_nD;
     }
 
-    // raw list (reference order) to global memory for inspection; reversed copy for the sort
+    // raw list (reference order) to global memory for inspection; the reversed list is sorted by
+    // permuting (scale, index) keys (the first region is free once the levels are done)
     if (fits)
         for (int i = tid; i < nD; i += kRT) a.D[i] = D[i];
-    for (int i = tid; i < nD; i += kRT) R[i] = D[nD - 1 - i];
+    ScaleKey* K = fits ? reinterpret_cast<ScaleKey*>(sm) : reinterpret_cast<ScaleKey*>(a.M);
+    for (int i = tid; i < nD; i += kRT) K[i] = ScaleKey{D[nD - 1 - i].scale, i};
+    __syncthreads();
+    if (nD > 16 && tid == 0) introsort_scale_desc(K, nD);  // n <= 16: insertion sort of a sorted list
+    __syncthreads();
+    for (int i = tid; i < nD; i += kRT) R[i] = D[nD - 1 - K[i].idx];
     __syncthreads();
 
     // post-processing in warp 0
     if (warp != 0) return;
     if (lane == 0) *a.n_raw = nD;
-    if (nD > 16 && lane == 0) introsort_scale_desc(R, nD);
-    __syncwarp();
     int nF = 0;
     const Det* fin = R;
     if (nD > 0) {

@@ -75,16 +75,27 @@ CCNN_HD int drop_test(const Det& nr, const Det& exp_r, const Det& e) {
 }
 
 // ---- libstdc++ introsort order for comp(a, b) = b.scale < a.scale ----
+// The steps only compare .scale and move whole elements, so they run on any element type with a
+// .scale member: sorting (scale, index) pairs gives the permutation that sorting the detections
+// themselves would apply.
 
-CCNN_HD bool comp_scale_desc(const Det& a, const Det& b) { return b.scale < a.scale; }
+struct ScaleKey {
+    float scale;
+    int idx;
+};
 
-CCNN_HD void swap_det(Det* a, Det* b) {
-    Det t = *a;
+template <class T>
+CCNN_HD bool comp_scale_desc(const T& a, const T& b) { return b.scale < a.scale; }
+
+template <class T>
+CCNN_HD void swap_el(T* a, T* b) {
+    T t = *a;
     *a = *b;
     *b = t;
 }
 
-CCNN_HD void push_heap_det(Det* first, int hole, int top, Det value) {
+template <class T>
+CCNN_HD void push_heap_el(T* first, int hole, int top, T value) {
     int parent = (hole - 1) / 2;
     while (hole > top && comp_scale_desc(first[parent], value)) {
         first[hole] = first[parent];
@@ -94,7 +105,8 @@ CCNN_HD void push_heap_det(Det* first, int hole, int top, Det value) {
     first[hole] = value;
 }
 
-CCNN_HD void adjust_heap_det(Det* first, int hole, int len, Det value) {
+template <class T>
+CCNN_HD void adjust_heap_el(T* first, int hole, int len, T value) {
     const int top = hole;
     int child = hole;
     while (child < (len - 1) / 2) {
@@ -108,15 +120,16 @@ CCNN_HD void adjust_heap_det(Det* first, int hole, int len, Det value) {
         first[hole] = first[child - 1];
         hole = child - 1;
     }
-    push_heap_det(first, hole, top, value);
+    push_heap_el(first, hole, top, value);
 }
 
-CCNN_HD void heap_sort_det(Det* first, int len) {
+template <class T>
+CCNN_HD void heap_sort_el(T* first, int len) {
     if (len >= 2) {  // make_heap
         int parent = (len - 2) / 2;
         while (true) {
-            Det v = first[parent];
-            adjust_heap_det(first, parent, len, v);
+            T v = first[parent];
+            adjust_heap_el(first, parent, len, v);
             if (parent == 0) break;
             parent--;
         }
@@ -125,35 +138,38 @@ CCNN_HD void heap_sort_det(Det* first, int len) {
     int last = len;
     while (last > 1) {
         --last;
-        Det v = first[last];
+        T v = first[last];
         first[last] = first[0];
-        adjust_heap_det(first, 0, last, v);
+        adjust_heap_el(first, 0, last, v);
     }
 }
 
-CCNN_HD void median_to_first(Det* result, Det* a, Det* b, Det* c) {
+template <class T>
+CCNN_HD void median_to_first(T* result, T* a, T* b, T* c) {
     if (comp_scale_desc(*a, *b)) {
-        if (comp_scale_desc(*b, *c)) swap_det(result, b);
-        else if (comp_scale_desc(*a, *c)) swap_det(result, c);
-        else swap_det(result, a);
-    } else if (comp_scale_desc(*a, *c)) swap_det(result, a);
-    else if (comp_scale_desc(*b, *c)) swap_det(result, c);
-    else swap_det(result, b);
+        if (comp_scale_desc(*b, *c)) swap_el(result, b);
+        else if (comp_scale_desc(*a, *c)) swap_el(result, c);
+        else swap_el(result, a);
+    } else if (comp_scale_desc(*a, *c)) swap_el(result, a);
+    else if (comp_scale_desc(*b, *c)) swap_el(result, c);
+    else swap_el(result, b);
 }
 
-CCNN_HD int unguarded_partition(Det* v, int first, int last, int pivot) {
+template <class T>
+CCNN_HD int unguarded_partition(T* v, int first, int last, int pivot) {
     while (true) {
         while (comp_scale_desc(v[first], v[pivot])) ++first;
         --last;
         while (comp_scale_desc(v[pivot], v[last])) --last;
         if (!(first < last)) return first;
-        swap_det(&v[first], &v[last]);
+        swap_el(&v[first], &v[last]);
         ++first;
     }
 }
 
-CCNN_HD void unguarded_linear_insert(Det* v, int last) {
-    Det val = v[last];
+template <class T>
+CCNN_HD void unguarded_linear_insert(T* v, int last) {
+    T val = v[last];
     int next = last - 1;
     while (comp_scale_desc(val, v[next])) {
         v[last] = v[next];
@@ -163,11 +179,12 @@ CCNN_HD void unguarded_linear_insert(Det* v, int last) {
     v[last] = val;
 }
 
-CCNN_HD void insertion_sort(Det* v, int first, int last) {
+template <class T>
+CCNN_HD void insertion_sort(T* v, int first, int last) {
     if (first == last) return;
     for (int i = first + 1; i != last; ++i) {
         if (comp_scale_desc(v[i], v[first])) {
-            Det val = v[i];
+            T val = v[i];
             for (int k = i; k > first; --k) v[k] = v[k - 1];
             v[first] = val;
         } else {
@@ -186,7 +203,8 @@ CCNN_HD int floor_log2(int n) {
 }
 
 // iterative form of the introsort loop: the recursion is on the right part, the loop on the left
-CCNN_HD void introsort_scale_desc(Det* v, int n) {
+template <class T>
+CCNN_HD void introsort_scale_desc(T* v, int n) {
     if (n <= 1) return;
     const int kThreshold = 16;
     // explicit stack of (first, last, depth) for the recursive calls
@@ -201,7 +219,7 @@ CCNN_HD void introsort_scale_desc(Det* v, int n) {
         int first = st_first[sp], last = st_last[sp], depth = st_depth[sp];
         while (last - first > kThreshold) {
             if (depth == 0) {
-                heap_sort_det(v + first, last - first);
+                heap_sort_el(v + first, last - first);
                 break;
             }
             --depth;
