@@ -12,7 +12,7 @@ import numpy as np
 from . import _capi
 from ._capi import CCNNError, Face, Image, Params
 
-__all__ = ["FaceDetector", "Param", "synth_frame", "CCNNError", "default_params"]
+__all__ = ["FaceDetector", "FaceServer", "Param", "synth_frame", "CCNNError", "default_params", "pinned_frame"]
 
 Pipeline = {"CPU": 0, "GPU": 1, "GPU_CPU": 2}
 DetectMode = {"disable": 0, "sync": 1, "async": 2}
@@ -188,6 +188,93 @@ class FaceDetector:
         buf = (_capi.Detection * max(1, n.value))()
         _capi.check(L.ccnn_inspect_raw_detections(self._h, buf, n.value, ctypes.byref(n)), "ccnn_inspect_raw_detections")
         return [(d.x, d.y, d.width, d.height, d.score, d.scale, d.knn, d.num_detect) for d in buf[: n.value]]
+
+
+class FaceServer:
+    """Serving loop over the B200 cascade (include/ccnn_server.h): submit frames of any resolution
+    as they arrive, collect each result by ticket. Frames must stay alive (and unmodified) until
+    their result has been taken; `pinned_frame` gives page-locked arrays that upload asynchronously."""
+
+    def __init__(self, param=None, models=None, hbm_budget_bytes=0, slots_per_class=0, max_queue=0):
+        L = _capi.lib()
+        p = param if param is not None else default_params()
+        cfg = _capi.ServerConfig(hbm_budget_bytes, slots_per_class, max_queue)
+        arr = None
+        if models is not None:
+            arr = (ctypes.c_char_p * 3)(*[(m.encode() if m else None) for m in models])
+        h = ctypes.c_void_p()
+        _capi.check(L.ccnn_server_create(ctypes.byref(p), arr, ctypes.byref(cfg), ctypes.byref(h)), "ccnn_server_create")
+        self._h = h
+        self._frames = {}
+
+    def close(self):
+        if self._h:
+            _capi.lib().ccnn_server_destroy(self._h)
+            self._h = None
+            self._frames.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, img):
+        """Queues a uint8 HxW / HxWxC frame; returns its ticket, or None when the queue is full."""
+        im, a = _as_image(img)
+        t = ctypes.c_longlong()
+        st = _capi.lib().ccnn_server_submit(self._h, ctypes.byref(im), ctypes.byref(t))
+        if st == _capi.BUSY:
+            return None
+        _capi.check(st, "ccnn_server_submit")
+        self._frames[t.value] = a  # keep the pixels alive until the result is taken
+        return t.value
+
+    def _take(self, fn, ticket, capacity):
+        faces = (Face * capacity)()
+        n = ctypes.c_int()
+        lat = ctypes.c_double()
+        st = fn(self._h, ticket, faces, capacity, ctypes.byref(n), ctypes.byref(lat))
+        if st == _capi.PENDING:
+            return None
+        self._frames.pop(ticket, None)
+        _capi.check(st, "ccnn_server result")
+        return [(f.x, f.y, f.width, f.height, f.score) for f in faces[: min(n.value, capacity)]], lat.value
+
+    def wait(self, ticket, capacity=4096):
+        """(faces, latency_ms) of a ticket, blocking until the frame is done."""
+        return self._take(_capi.lib().ccnn_server_wait, ticket, capacity)
+
+    def poll(self, ticket, capacity=4096):
+        """(faces, latency_ms) if the frame is done, else None."""
+        return self._take(_capi.lib().ccnn_server_poll, ticket, capacity)
+
+    def stats(self):
+        s = _capi.ServerStats()
+        _capi.check(_capi.lib().ccnn_server_stats_get(self._h, ctypes.byref(s)), "ccnn_server_stats_get")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+
+class _PinnedBuffer:
+    """Page-locked host bytes exposed to numpy; freed when the last array using them goes away."""
+
+    def __init__(self, n):
+        self._lib = _capi.lib()
+        self.ptr = self._lib.ccnn_host_alloc(max(1, n))
+        if not self.ptr:
+            raise MemoryError("ccnn_host_alloc failed")
+        self.__array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (self.ptr, False), "version": 3}
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            self._lib.ccnn_host_free(self.ptr)
+            self.ptr = None
+
+
+def pinned_frame(shape):
+    """A uint8 array of `shape` in page-locked host memory."""
+    n = int(np.prod(shape))
+    return np.asarray(_PinnedBuffer(n)).reshape(shape)
 
 
 def synth_frame(width, height, seed, n_faces, min_face, max_face, channels=3):

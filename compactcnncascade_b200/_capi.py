@@ -1,4 +1,5 @@
-"""ctypes binding of the C ABI declared in include/ccnn.h and include/ccnn_inspect.h.
+"""ctypes binding of the C ABI declared in include/ccnn.h, include/ccnn_inspect.h and
+include/ccnn_server.h.
 
 The shared library is built in-tree (compactcnncascade_b200/libccnn.so) by
 compactcnncascade_b200/build.py. Loading fails loudly when it is missing: there is no
@@ -14,6 +15,8 @@ SYNTH_PATH = os.path.join(_HERE, "libccnn_synth.so")
 # ccnn_status
 OK = 0
 TRUNCATED = 1
+PENDING = 2
+BUSY = 3
 ERR_INVALID_ARG = -1
 ERR_MODEL = -2
 ERR_CONFIG = -3
@@ -29,6 +32,8 @@ EXPORTED = [
     "ccnn_gray_u8_to_f32", "ccnn_resize_f32", "ccnn_stage1_forward", "ccnn_inspect_levels",
     "ccnn_inspect_response", "ccnn_inspect_candidates", "ccnn_inspect_raw_detections",
     "ccnn_sort_permutation", "ccnn_detect_device_batch", "ccnn_profile_last_frame", "ccnn_plan_levels", "ccnn_stage1_forward_static",
+    "ccnn_server_create", "ccnn_server_destroy", "ccnn_server_submit", "ccnn_server_poll", "ccnn_server_wait",
+    "ccnn_server_stats_get", "ccnn_host_alloc", "ccnn_host_free",
 ]
 
 
@@ -55,6 +60,16 @@ class Face(ctypes.Structure):
 class Image(ctypes.Structure):
     _fields_ = [("cols", ctypes.c_int), ("rows", ctypes.c_int), ("channels", ctypes.c_int),
                 ("data", ctypes.c_void_p), ("step", ctypes.c_size_t)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("slots_per_class", ctypes.c_int), ("max_queue", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+                ("queued", ctypes.c_int), ("in_flight", ctypes.c_int), ("classes", ctypes.c_int),
+                ("hbm_bytes", ctypes.c_size_t)]
 
 
 class LevelInfo(ctypes.Structure):
@@ -122,6 +137,17 @@ def lib():
         L.ccnn_profile_last_frame.argtypes = [vp, ci, P(ctypes.c_float), ci]
         L.ccnn_plan_levels.argtypes = [P(Params), ci, ci, ci, P(LevelInfo), ci, P(ci)]
         L.ccnn_stage1_forward_static.argtypes = [ctypes.c_char_p, vp, ci, ci, ctypes.c_size_t, vp, ci, P(ci), P(ci), vp]
+        ll = ctypes.c_longlong
+        L.ccnn_server_create.argtypes = [P(Params), P(ctypes.c_char_p), P(ServerConfig), P(vp)]
+        L.ccnn_server_destroy.argtypes = [vp]
+        L.ccnn_server_submit.argtypes = [vp, P(Image), P(ll)]
+        L.ccnn_server_poll.argtypes = [vp, ll, P(Face), ci, P(ci), P(ctypes.c_double)]
+        L.ccnn_server_wait.argtypes = [vp, ll, P(Face), ci, P(ci), P(ctypes.c_double)]
+        L.ccnn_server_stats_get.argtypes = [vp, P(ServerStats)]
+        L.ccnn_host_alloc.argtypes = [ctypes.c_size_t]
+        L.ccnn_host_alloc.restype = vp
+        L.ccnn_host_free.argtypes = [vp]
+        L.ccnn_host_free.restype = None
         _lib = L
     return _lib
 

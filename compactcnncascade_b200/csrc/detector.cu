@@ -161,8 +161,13 @@ ccnn_status Detector::apply_precision() {
     return CCNN_OK;
 }
 
-ccnn_status Detector::create(const ccnn_params& p, const char* const* model_paths) {
+ccnn_status Detector::create(const ccnn_params& p, const char* const* model_paths, int n_slots, bool colour_input) {
     api_ = p;
+    if (n_slots < 1) {
+        set_error("a detector needs at least one frame slot");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    slots_.assign(n_slots, Slot());
     if (p.facial_analysis) {
         set_error("facial_analysis is not supported by this detector");
         return CCNN_ERR_UNSUPPORTED;
@@ -172,7 +177,7 @@ ccnn_status Detector::create(const ccnn_params& p, const char* const* model_path
         static const char* kNames[3] = {"cnn4face1_cntk.bin", "cnn4face2_cntk.bin", "cnn4face3_cntk.bin"};
         model_paths_[i] = (mp && mp[0]) ? std::string(mp) : bundled_model_dir() + "/" + kNames[i];
     }
-    gray_image_only_ = true;
+    gray_image_only_ = !colour_input;
     max_w_ = p.max_image_width;
     max_h_ = p.max_image_height;
     return init();
@@ -575,6 +580,41 @@ ccnn_status Detector::detect(const ccnn_image& img, bool device_input, cudaStrea
     return collect(s, faces, cap, n);
 }
 
+ccnn_status Detector::launch(int k, const ccnn_image& img) {
+    if (k < 0 || k >= (int)slots_.size()) {
+        set_error("slot index out of range");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    if (img.cols != max_w_ || img.rows != max_h_ || (gray_image_only_ && img.channels != 1)) {
+        set_error("frame does not match the slot configuration");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(device_);
+    const Plan* p = nullptr;
+    bool empty = false;
+    ccnn_status st = prepare_frame(img, &p, &empty);
+    if (st != CCNN_OK) return st;
+    if (empty) {  // no level fits the stage-2/3 window: an empty result, nothing launched
+        *slots_[k].h_nfaces = 0;
+        CCNN_CUDA(cudaEventRecord(slots_[k].done, slots_[k].st));
+        return CCNN_OK;
+    }
+    return enqueue(slots_[k], *p, img, false, nullptr);
+}
+
+bool Detector::slot_done(int k) { return cudaEventQuery(slots_[k].done) != cudaErrorNotReady; }
+
+ccnn_status Detector::fetch(int k, ccnn_face* faces, int cap, int* n) { return collect(slots_[k], faces, cap, n); }
+
+size_t Detector::slot_bytes() const {
+    const size_t in = (size_t)round_up((long long)max_w_ * 4, 64) * max_h_;
+    const size_t gray = sizeof(float) * (size_t)round_up(max_w_, 16) * max_h_;
+    const size_t per_cand = sizeof(Candidate) + sizeof(CandResult) + 4 * sizeof(WinOut) + 4 * sizeof(Det) + 2 * sizeof(int) + 1;
+    const size_t per_slot = in + gray + sizeof(float) * (size_t)(std::max(4LL, img_cap_) + std::max(1LL, s1_cap_) + std::max(1LL, resp_cap_)) +
+                            sizeof(int) * chunk_cap_ + per_cand * (size_t)cand_cap_ + sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces);
+    return per_slot * slots_.size();
+}
+
 ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, bool device_input, ccnn_face* faces, int cap_per, int* n_faces,
                                    float* gpu_ms) {
     std::lock_guard<std::mutex> lk(mu_);
@@ -583,8 +623,8 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, bool devic
         return CCNN_ERR_INVALID_ARG;
     }
     cudaSetDevice(device_);
-    int pending[kSlots];
-    for (int k = 0; k < kSlots; ++k) pending[k] = -1;
+    const int n_sl = (int)slots_.size();
+    std::vector<int> pending(n_sl, -1);
     ccnn_status worst = CCNN_OK;
     // device time of the whole batch: from an event before the first frame's upload (both
     // slot streams wait on it) to an event after the last frame of either slot
@@ -593,10 +633,10 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, bool devic
         CCNN_CUDA(cudaEventCreate(&t0));
         CCNN_CUDA(cudaEventCreate(&t1));
         CCNN_CUDA(cudaEventRecord(t0, slots_[0].st));
-        for (int k = 1; k < kSlots; ++k) CCNN_CUDA(cudaStreamWaitEvent(slots_[k].st, t0, 0));
+        for (int k = 1; k < n_sl; ++k) CCNN_CUDA(cudaStreamWaitEvent(slots_[k].st, t0, 0));
     }
     for (int i = 0; i < n_img; ++i) {
-        const int k = i % kSlots;
+        const int k = i % n_sl;
         Slot& s = slots_[k];
         if (pending[k] >= 0) {
             ccnn_status st = collect(s, faces + (size_t)pending[k] * cap_per, cap_per, &n_faces[pending[k]]);
@@ -608,7 +648,7 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, bool devic
         bool empty = false;
         // frame admission may re-initialise (and so free the slots): drain in-flight frames first
         if (!inited_ || imgs[i].cols > max_w_ || imgs[i].rows > max_h_ || (gray_image_only_ && input_downscale_ && imgs[i].channels != 1)) {
-            for (int q = 0; q < kSlots; ++q)
+            for (int q = 0; q < n_sl; ++q)
                 if (pending[q] >= 0) {
                     ccnn_status st = collect(slots_[q], faces + (size_t)pending[q] * cap_per, cap_per, &n_faces[pending[q]]);
                     if (st < 0) return st;
@@ -628,11 +668,11 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, bool devic
     }
     if (t0) {
         if (inited_) {
-            for (int k = 1; k < kSlots; ++k) CCNN_CUDA(cudaStreamWaitEvent(slots_[0].st, slots_[k].done, 0));
+            for (int k = 1; k < n_sl; ++k) CCNN_CUDA(cudaStreamWaitEvent(slots_[0].st, slots_[k].done, 0));
             CCNN_CUDA(cudaEventRecord(t1, slots_[0].st));
         }
     }
-    for (int k = 0; k < kSlots; ++k)
+    for (int k = 0; k < n_sl; ++k)
         if (pending[k] >= 0) {
             ccnn_status st = collect(slots_[k], faces + (size_t)pending[k] * cap_per, cap_per, &n_faces[pending[k]]);
             if (st < 0) return st;

@@ -69,11 +69,24 @@ class Detector {
     Detector() = default;
     ~Detector();
 
-    ccnn_status create(const ccnn_params& p, const char* const* model_paths);
+    // n_slots: frames in flight (each slot owns a stream, buffers and a captured graph);
+    // colour_input: start in the state the reference reaches after its first colour frame
+    // (gray_image_only off), so that colour frames never re-initialise the detector
+    ccnn_status create(const ccnn_params& p, const char* const* model_paths, int n_slots = kSlots, bool colour_input = false);
     ccnn_status detect(const ccnn_image& img, bool device_input, cudaStream_t user_stream, ccnn_face* faces, int cap, int* n);
     ccnn_status detect_batch(const ccnn_image* imgs, int n_img, bool device_input, ccnn_face* faces, int cap_per, int* n_faces,
                              float* gpu_ms);
     ccnn_status profile(int iters, float* ms, int n_ms);
+
+    // Non-blocking use of one slot by a single scheduling thread (the serving loop): launch a
+    // host frame on slot k, test for completion, fetch the faces. Frames must have the size the
+    // detector was created for.
+    int n_slots() const { return (int)slots_.size(); }
+    ccnn_status launch(int k, const ccnn_image& img);
+    bool slot_done(int k);
+    ccnn_status fetch(int k, ccnn_face* faces, int cap, int* n);
+    // device bytes held by the frame slots
+    size_t slot_bytes() const;
 
     ccnn_status get_gray_device(const float** data, int* cols, int* rows, size_t* step);
     ccnn_status get_gray_host(float* out, int cap, int* cols, int* rows);
@@ -115,7 +128,7 @@ class Detector {
     int num_scales_ = 0;
 
     CascadeConfig cfg_{};
-    Slot slots_[kSlots];
+    std::vector<Slot> slots_;
     long long cand_cap_ = 0, s1_cap_ = 0, resp_cap_ = 0, img_cap_ = 0;
     int chunk_cap_ = 0;
     int window_grid_ = 0;

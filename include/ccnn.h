@@ -24,6 +24,8 @@ extern "C" {
 typedef enum {
     CCNN_OK = 0,
     CCNN_TRUNCATED = 1,          /* more faces than the output capacity; the first `capacity` were written */
+    CCNN_PENDING = 2,            /* serving loop: the frame is not finished yet (ccnn_server_poll) */
+    CCNN_BUSY = 3,               /* serving loop: the request queue is full; submit again later */
     CCNN_ERR_INVALID_ARG = -1,
     CCNN_ERR_MODEL = -2,         /* model file missing, truncated, wrong format version or unsupported shape */
     CCNN_ERR_CONFIG = -3,        /* parameters give an empty scale list (reference: "Invalid configuration") */
