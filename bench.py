@@ -53,6 +53,77 @@ def _frames(seeds, workers):
         return pool.map(_gen_frame, seeds)
 
 
+# ---------------- serving workload ----------------
+
+SERVE_MIX = [((640, 480), 0.3, 5, 40, 200), ((1280, 720), 0.3, 10, 30, 300), ((1920, 1080), 0.3, 20, 30, 300),
+             ((3840, 2160), 0.1, 60, 20, 600)]
+
+
+def _gen_serve_frame(args):
+    import compactcnncascade_b200 as ccnn
+    (w, h), seed, nf, lo, hi = args
+    return ccnn.synth_frame(w, h, seed, nf, lo, hi)[0]
+
+
+def serve_frames(per_res, seed0=900_000):
+    jobs = [(m[0], seed0 + 1000 * r + i, m[2], m[3], m[4]) for r, m in enumerate(SERVE_MIX) for i in range(per_res)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(min(len(jobs), os.cpu_count() or 4)) as pool:
+        imgs = pool.map(_gen_serve_frame, jobs)
+    out = {}
+    for (res, *_), img in zip(jobs, imgs):
+        out.setdefault(res, []).append(img)
+    return out
+
+
+def run_serving(frames_by_res, rate, n_frames, seed=1):
+    """Poisson arrivals (seeded exponential inter-arrival times) of frames drawn from the
+    resolution mix; every frame goes through the serving loop (ccnn_server_*). Returns latency
+    percentiles (submit -> result on the device side, measured by the server) and throughput."""
+    import compactcnncascade_b200 as ccnn
+    rng = np.random.default_rng(seed)
+    p = ccnn.default_params()
+    p.min_face_height, p.max_face_height, p.scale_factor = MIN_FACE, MAX_FACE, SCALE_FACTOR
+    p.detect_mode = 1
+    srv = ccnn.FaceServer(p, hbm_budget_bytes=32 << 30, slots_per_class=4)
+    pinned = {res: [] for res in frames_by_res}
+    for res, imgs in frames_by_res.items():
+        for img in imgs:
+            pf = ccnn.pinned_frame(img.shape)
+            pf[...] = img
+            pinned[res].append(pf)
+    # warm-up: every class once (detector creation and graph capture are not part of serving)
+    for res in pinned:
+        srv.wait(srv.submit(pinned[res][0]))
+    weights = np.array([m[1] for m in SERVE_MIX])
+    kinds = rng.choice(len(SERVE_MIX), size=n_frames, p=weights / weights.sum())
+    gaps = rng.exponential(1.0 / rate, size=n_frames)
+    tickets = []
+    t0 = time.perf_counter()
+    due = t0
+    for k, g in zip(kinds, gaps):
+        due += g
+        while time.perf_counter() < due:
+            pass
+        res = SERVE_MIX[k][0]
+        imgs = pinned[res]
+        t = None
+        while t is None:  # a full queue pushes back on the client
+            t = srv.submit(imgs[len(tickets) % len(imgs)])
+        tickets.append((res, t))
+    lat = {res: [] for res in pinned}
+    for res, t in tickets:
+        lat[res].append(srv.wait(t)[1])
+    wall = time.perf_counter() - t0
+    srv.close()
+    allv = np.concatenate([np.array(v) for v in lat.values() if v])
+    out = {"rate_per_s": rate, "frames": n_frames, "fps": round(n_frames / wall, 1),
+           "p50_ms": round(float(np.percentile(allv, 50)), 3), "p99_ms": round(float(np.percentile(allv, 99)), 3),
+           "per_resolution": {f"{r[0]}x{r[1]}": {"frames": len(v), "p50_ms": round(float(np.percentile(v, 50)), 3),
+                                                 "p99_ms": round(float(np.percentile(v, 99)), 3)} for r, v in lat.items() if v}}
+    return out
+
+
 # ---------------- reference CPU path (test oracle; never the measured product) ----------------
 
 def _ref_worker(args):
@@ -212,6 +283,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--latency-frames", type=int, default=200)
     ap.add_argument("--profile-iters", type=int, default=20)
+    ap.add_argument("--serve-frames", type=int, default=2000, help="frames of the serving-loop phase (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate of the serving phase, frames/s")
+    ap.add_argument("--serving", action="store_true",
+                    help="only the serving sweep: 10,000 mixed-resolution frames at 500, 1000, 2000, 4000 frames/s")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -222,10 +297,19 @@ def main():
         run_reference(args, world, rank)
         return
 
+    if args.serving:
+        if rank == 0:
+            fr = serve_frames(4)
+            sweep = [run_serving(fr, r, 10_000, seed=int(r)) for r in (500.0, 1000.0, 2000.0, 4000.0)]
+            print(json.dumps({"metric": "serving loop p50/p99 ms and fps, mixed 640x480/1280x720/1920x1080/3840x2160 at 30/30/30/10 %",
+                              "unit": "ms", "data": "synthetic (seeded generator)", "sweep": sweep}), flush=True)
+        return
+
     from compactcnncascade_b200.replicas import rank_seeds
     # frames and the CPU baseline use spawn pools, started before this process touches CUDA
     seeds = rank_seeds(rank, args.distinct)
     frames = _frames(seeds, os.cpu_count() or 4)
+    sframes = serve_frames(2) if (rank == 0 and args.serve_frames > 0) else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = reference_cpu(runs_per_worker=args.cpu_frames)
@@ -365,6 +449,7 @@ def main():
         "kernel_ms_all": {k: round(v, 4) for k, v in kernel_ms.items()},
     }
     fb = frame_bytes(levels, W, H)
+    serving = run_serving(sframes, args.serve_rate, args.serve_frames) if sframes else None
 
     line = {
         "metric": METRIC,
@@ -393,6 +478,9 @@ def main():
         "roofline": roofline,
         "wall_value": round(frames_timed / wall_dev, 2),
     }
+    if serving:
+        line["serving"] = dict(serving, note="serving loop (ccnn_server_*): Poisson arrivals of mixed 640x480/1280x720/"
+                                             "1920x1080/3840x2160 frames at 30/30/30/10 %, latency = submit to result")
     if cpu:
         fps, workers, nfr, secs, fast = cpu
         line["cpu_baseline"] = {"value": round(fps, 3), "unit": "frames/s", "cores": workers, "kind": "reference",
