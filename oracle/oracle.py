@@ -99,7 +99,7 @@ def detect(img, p=None, **kw):
     lh = np.empty(cap, np.int32)
     rw = np.empty(cap, np.int32)
     rh = np.empty(cap, np.int32)
-    resp = np.empty(w * h + 1024, np.float32)
+    resp = np.empty(2 * w * h + 1024, np.float32)  # upsampled pyramids hold more response pixels than the frame
     ccap = w * h // 4 + 1024
     cands = (OrcCand * ccap)()
     nc = ctypes.c_int()
