@@ -189,7 +189,11 @@ struct LevelDesc {
     int img_vec;         // 1: rows start 16-byte aligned and the pitch is a multiple of 4 floats
     int pyr_base;        // first pyramid-kernel block of this level
     int pyr_wq;          // pyramid-kernel column blocks per row band
+    int chunk_base;      // first candidate-scan chunk of this level
 };
+
+// candidate-scan chunk: response pixels of one level per compaction block, in raster order
+constexpr int kCandChunk = 2048;
 
 // Level descriptors passed by value to the kernels that find their level per block (a frame's
 // pyramid is launched in groups of at most kParamLevels levels). Every block of a launch maps to

@@ -38,7 +38,6 @@ ccnn_status cuda_status(cudaError_t e, const char* what) {
     } while (0)
 
 namespace {
-constexpr int kChunk = 2048;  // candidate-scan chunk (response pixels per block)
 inline long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 // Size * float with truncation (type.h:200-203)
 inline void size_scale(int w, int h, float s, int* ow, int* oh) {
@@ -377,8 +376,9 @@ ccnn_status Detector::build_plan(int w, int h, int ch, int num_scales, Plan* p) 
     for (int scl = n - 1; scl >= 0; --scl) {
         LevelDesc& L = p->levels[scl];
         L.order = n - 1 - scl;
+        L.chunk_base = (int)p->chunks.size();
         const int total = L.ow * L.oh;
-        for (int s = 0; s < total; s += kChunk) p->chunks.push_back(make_int4(scl, s, std::min(kChunk, total - s), 0));
+        for (int s = 0; s < total; s += kCandChunk) p->chunks.push_back(make_int4(scl, s, std::min(kCandChunk, total - s), 0));
     }
     p->k1_tiles = k1;
     p->k2_tiles = k2;
@@ -427,8 +427,10 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
         e = launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st);
     CCNN_CUDA(e);
     CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
-    CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st));
-    CCNN_CUDA(launch_candidates(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
+    // the back kernel counts each chunk's candidates as it writes the responses
+    if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
+    CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1));
+    CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                 (int)cand_cap_, s.st));
     if (detect_enabled_)
         CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
@@ -817,7 +819,8 @@ ccnn_status Detector::stage1_forward(const float* d_img, int w, int h, size_t st
 
 // Re-runs the last frame's kernel chain on slot 0 `iters` times with an event between every
 // two kernels; ms[k] gets the mean duration of kernel k: gray, pyramid, stage-1 front, stage-1
-// back, candidate count, candidate write, stage-2/3 windows, replay.
+// back (with the candidate count and the memset of the counts before it), candidate write,
+// stage-2/3 windows, replay.
 ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     std::lock_guard<std::mutex> lk(mu_);
     Slot& s = slots_[0];
@@ -827,7 +830,7 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     }
     cudaSetDevice(device_);
     const Plan& p = *s.last_plan;
-    constexpr int K = 8;
+    constexpr int K = 7;
     cudaEvent_t ev[K + 1];
     for (auto& e : ev) CCNN_CUDA(cudaEventCreate(&e));
     double acc[K] = {0};
@@ -861,20 +864,19 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         CCNN_CUDA(cudaEventRecord(ev[2], s.st));
         CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st));
         CCNN_CUDA(cudaEventRecord(ev[3], s.st));
-        CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st));
+        if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
+        CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1));
         CCNN_CUDA(cudaEventRecord(ev[4], s.st));
-        CCNN_CUDA(launch_cand_count(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.st));
-        CCNN_CUDA(cudaEventRecord(ev[5], s.st));
         CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                     (int)cand_cap_, s.st));
-        CCNN_CUDA(cudaEventRecord(ev[6], s.st));
+        CCNN_CUDA(cudaEventRecord(ev[5], s.st));
         if (detect_enabled_)
             CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
                                     window_grid_, s.st));
-        CCNN_CUDA(cudaEventRecord(ev[7], s.st));
+        CCNN_CUDA(cudaEventRecord(ev[6], s.st));
         CCNN_CUDA(launch_replay(a, s.st));
-        CCNN_CUDA(cudaEventRecord(ev[8], s.st));
-        CCNN_CUDA(cudaEventSynchronize(ev[8]));
+        CCNN_CUDA(cudaEventRecord(ev[7], s.st));
+        CCNN_CUDA(cudaEventSynchronize(ev[7]));
         for (int k = 0; k < K; ++k) {
             float m = 0.f;
             CCNN_CUDA(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));

@@ -6,9 +6,10 @@
 // (RunCheckDetectAsync :2041-2049). The output list keeps exactly that order.
 //
 // The scan space is cut into chunks that never straddle two levels (host-built chunk table,
-// chunks in visiting order). Pass 1 counts each chunk's hits with warp ballots; pass 2 gives
-// each chunk its offset (sum of the counts of earlier chunks) and writes its hits in order using
-// a ballot/popc prefix inside each warp and a warp-total scan across the block.
+// chunks in visiting order). The stage-1 back kernel counts each chunk's hits as it writes the
+// responses; this kernel gives each chunk its offset (sum of the counts of earlier chunks) and
+// writes its hits in order using a ballot/popc prefix inside each warp and a warp-total scan
+// across the block.
 #include "kernels.h"
 
 namespace ccnn {
@@ -52,22 +53,6 @@ __device__ __forceinline__ int block_sum(int v, int* warp_tot) {
     return t;
 }
 
-__global__ void __launch_bounds__(kChunkThreads) cand_count_kernel(const int4* __restrict__ chunks, const LevelDesc* __restrict__ levels,
-                                                                   const float* __restrict__ resp, float thr, int* __restrict__ counts) {
-    __shared__ int wt[32];
-    const int4 ck = chunks[blockIdx.x];  // (level, start, len, -)
-    const long long base = levels[ck.x].resp_off + ck.y;
-    int cnt = 0;
-    for (int b0 = 0; b0 < ck.z; b0 += blockDim.x) {
-        const int i = b0 + threadIdx.x;
-        const int hit = (i < ck.z) && resp[base + i] > thr;
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if ((threadIdx.x & 31) == 0) cnt += __popc(m);
-    }
-    const int tot = block_sum(cnt, wt);
-    if (threadIdx.x == 0) counts[blockIdx.x] = tot;
-}
-
 __global__ void __launch_bounds__(kChunkThreads) cand_write_kernel(const int4* __restrict__ chunks, int n_chunks,
                                                                    const LevelDesc* __restrict__ levels, const float* __restrict__ resp,
                                                                    float thr, const int* __restrict__ counts, Candidate* __restrict__ out,
@@ -105,24 +90,11 @@ __global__ void __launch_bounds__(kChunkThreads) cand_write_kernel(const int4* _
     }
 }
 
-cudaError_t launch_cand_count(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
-                              cudaStream_t st) {
-    if (n_chunks > 0) cand_count_kernel<<<n_chunks, kChunkThreads, 0, st>>>(d_chunks, d_levels, resp, thr, counts);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
                               const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st) {
     if (n_chunks <= 0) return cudaMemsetAsync(n_out, 0, sizeof(int), st);
     cand_write_kernel<<<n_chunks, kChunkThreads, 0, st>>>(d_chunks, n_chunks, d_levels, resp, thr, counts, out, n_out, cap);
     return cudaGetLastError();
-}
-
-cudaError_t launch_candidates(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
-                              Candidate* out, int* n_out, int cap, cudaStream_t st) {
-    cudaError_t e = launch_cand_count(d_chunks, n_chunks, d_levels, resp, thr, counts, st);
-    if (e != cudaSuccess) return e;
-    return launch_cand_write(d_chunks, n_chunks, d_levels, resp, thr, counts, out, n_out, cap, st);
 }
 
 }  // namespace ccnn

@@ -144,7 +144,7 @@ constexpr int kBackSmemBytes = (int)sizeof(BackSmem);
 //      the pair: the 16 L3 maps (4w x 5h), the 52 hidden neurons and the output neuron.
 __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ Stage1Dup D,
                                                              const __grid_constant__ LevelTable LT, const float* __restrict__ s1,
-                                                             float* __restrict__ resp) {
+                                                             float* __restrict__ resp, int* __restrict__ counts, float thr) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BackSmem& S = *reinterpret_cast<BackSmem*>(smem_raw);
     const int g = LT.first + blockIdx.x;
@@ -256,8 +256,15 @@ __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_consta
     const f2_t r = (W.af == 0.f) ? f2_add(f2_mul(half, c, nz), half) : f2_mul(f2_ld(D.afd), c, nz);
     const int gx = ox0 + x, gy = oy0 + y;
     if (gx < L.ow) {
-        if (gy < L.oh) resp[L.resp_off + (long long)gy * L.ow + gx] = f2_lo(r);
-        if (gy + 1 < L.oh) resp[L.resp_off + (long long)(gy + 1) * L.ow + gx] = f2_hi(r);
+        // candidates (response > treshold_1) are counted per scan chunk for the compaction
+        if (gy < L.oh) {
+            resp[L.resp_off + (long long)gy * L.ow + gx] = f2_lo(r);
+            if (counts && f2_lo(r) > thr) atomicAdd(&counts[L.chunk_base + (gy * L.ow + gx) / kCandChunk], 1);
+        }
+        if (gy + 1 < L.oh) {
+            resp[L.resp_off + (long long)(gy + 1) * L.ow + gx] = f2_hi(r);
+            if (counts && f2_hi(r) > thr) atomicAdd(&counts[L.chunk_base + ((gy + 1) * L.ow + gx) / kCandChunk], 1);
+        }
     }
 }
 
@@ -324,18 +331,19 @@ cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n
         [&](const LevelTable& T, int blocks) { stage1_front_kernel<<<blocks, 256, 0, st>>>(W, T, limg, s1); });
 }
 
-cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st) {
+cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
+                               int* counts, float thr) {
     const Stage1Dup D = make_dup(W);
     return launch_grouped(
         levels, n_levels, &LevelDesc::k2_base, [](const LevelDesc& L) { return L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY); },
-        [&](const LevelTable& T, int blocks) { stage1_back_kernel<<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp); });
+        [&](const LevelTable& T, int blocks) { stage1_back_kernel<<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp, counts, thr); });
 }
 
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
-                          cudaStream_t st) {
+                          cudaStream_t st, int* counts, float thr) {
     cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st);
     if (e != cudaSuccess) return e;
-    return launch_stage1_back(W, levels, n_levels, s1, resp, st);
+    return launch_stage1_back(W, levels, n_levels, s1, resp, st, counts, thr);
 }
 
 }  // namespace ccnn

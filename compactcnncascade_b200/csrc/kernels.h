@@ -48,18 +48,16 @@ cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* g
                            cudaStream_t st);
 // stage-1 net over all levels; `levels` is a HOST array (the descriptors travel as kernel
 // parameters), level images at limg + img_off
+// counts (optional, zeroed by the caller): per candidate-scan chunk, responses > thr
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
-                          cudaStream_t st);
+                          cudaStream_t st, int* counts = nullptr, float thr = 0.f);
 cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st);
 // dynamic shared memory of the stage-1 back kernel (set once per device before any launch)
 cudaError_t stage1_setup();
-cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st);
-cudaError_t launch_cand_count(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
-                              cudaStream_t st);
+cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
+                               int* counts = nullptr, float thr = 0.f);
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
                               const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st);
-cudaError_t launch_candidates(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr, int* counts,
-                              Candidate* out, int* n_out, int cap, cudaStream_t st);
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
                           const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st);
 int window_smem_bytes();

@@ -81,8 +81,8 @@ CCNN_API ccnn_status ccnn_plan_levels(const ccnn_params* p, int cols, int rows, 
                                       int* n_levels);
 
 /* Re-runs the handle's last frame `iters` times and writes the mean duration (ms, CUDA events)
- * of each kernel of the chain: [0] gray, [1] pyramid, [2] stage-1 front, [3] stage-1 back,
- * [4] candidate count, [5] candidate write, [6] stage-2/3 windows, [7] replay/sort/merge. */
+ * of each kernel of the chain: [0] gray, [1] pyramid, [2] stage-1 front, [3] stage-1 back (which also
+ * counts the candidates), [4] candidate write, [5] stage-2/3 windows, [6] replay/sort/merge. */
 CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* kernel_ms, int n_kernels);
 
 /* The permutation the detector's device sort applies to detections with the given scales
