@@ -38,6 +38,7 @@ struct WindowSmem {
     float a3[24][kOutN];
     float hbuf[84][kOutN];
     float out[kOutN];
+    float l1rest[32][6];  // pooled L1 maps of the partial pass's pixels
     int geo[4];
 };
 
@@ -52,9 +53,19 @@ __device__ void window_net(const NW& W, WindowSmem& S, int mode) {
     static_assert(NW::kM1 % 2 == 0 && NW::kM2 % 2 == 0 && NW::kM3 % 2 == 0 && NW::kHS % 2 == 0, "maps and neurons run in pairs");
     const f2_t nz = f2_ld(W.negzero);
     // L1: conv 4x4 + folded BN/LReLU + 2x2 max, then neighbour sums (add / add2); every map pair
-    // reads the same window, so it runs as one packed pair
-    for (int p = threadIdx.x; p < kP1W * kP1H; p += kWT) {
-        const int x = p % kP1W, y = p / kP1W;
+    // reads the same window, so it runs as one packed pair. Whole passes of kWT pixels run every map
+    // pair per thread; the pixels of the last, partial pass are split into (pixel, map pair) units,
+    // one warp per map pair, so that it takes a third of a pass.
+    constexpr int kFull = (kP1W * kP1H / kWT) * kWT;
+    constexpr int kRest = kP1W * kP1H - kFull;
+    constexpr int kMP = NW::kM1 / 2;
+    static_assert(kRest <= 32 && 32 * kMP <= kWT, "partial L1 pass must fit one warp per map pair");
+    for (int p = threadIdx.x; p < kFull + 32 * kMP; p += kWT) {
+        const bool unit = p >= kFull;  // one map pair (warp-uniform) of a pixel of the partial pass
+        if (unit && ((p - kFull) & 31) >= kRest) continue;
+        const int px = unit ? kFull + ((p - kFull) & 31) : p;
+        const int mp0 = unit ? (p - kFull) >> 5 : 0;
+        const int x = px % kP1W, y = px / kP1W;
         f2_t win[5][5];
 #pragma unroll
         for (int r = 0; r < 5; ++r)
@@ -62,25 +73,42 @@ __device__ void window_net(const NW& W, WindowSmem& S, int mode) {
             for (int c = 0; c < 5; ++c) win[r][c] = f2_dup(win_in(S, mode, 2 * x + c, 2 * y + r));
         float P[NW::kM1];
 #pragma unroll
-        for (int mp = 0; mp < NW::kM1 / 2; ++mp) {
-            float cv[2][4];
+        for (int mp = 0; mp < kMP; ++mp) {
+            if (unit && mp != mp0) continue;
+            f2_t cv[4];
 #pragma unroll
             for (int d = 0; d < 4; ++d) {
                 const int dy = d >> 1, dx = d & 1;
                 f2_t acc = f2_mul(win[dy][dx], f2_ld(W.k1p[mp][0]), nz);
 #pragma unroll
                 for (int k = 1; k < 16; ++k) acc = f2_add(acc, f2_mul(win[dy + (k >> 2)][dx + (k & 3)], f2_ld(W.k1p[mp][k]), nz));
-                const int m0 = 2 * mp, m1 = 2 * mp + 1;
-                cv[0][d] = lrelu_bn(f2_lo(acc), W.b1[m0], W.w1a[m0], W.w1b[m0], W.bn1[m0]);
-                cv[1][d] = lrelu_bn(f2_hi(acc), W.b1[m1], W.w1a[m1], W.w1b[m1], W.bn1[m1]);
+                cv[d] = lrelu_bn2(acc, W.a1p[mp], nz);  // maps (2mp, 2mp+1)
             }
-            P[2 * mp] = fmaxf(fmaxf(cv[0][0], cv[0][1]), fmaxf(cv[0][2], cv[0][3]));
-            P[2 * mp + 1] = fmaxf(fmaxf(cv[1][0], cv[1][1]), fmaxf(cv[1][2], cv[1][3]));
+            const f2_t pm = f2_max4(cv[0], cv[1], cv[2], cv[3]);
+            P[2 * mp] = f2_lo(pm);
+            P[2 * mp + 1] = f2_hi(pm);
+            if (unit) {
+                S.l1rest[px - kFull][2 * mp] = P[2 * mp];
+                S.l1rest[px - kFull][2 * mp + 1] = P[2 * mp + 1];
+            }
         }
+        if (unit) continue;
         S.s1[0][y][x] = fadd(P[0], P[1]);
 #pragma unroll
         for (int k = 1; k < NW::kM1 - 1; ++k) S.s1[k][y][x] = fadd(fadd(P[k - 1], P[k]), P[k + 1]);
         S.s1[NW::kM1 - 1][y][x] = fadd(P[NW::kM1 - 2], P[NW::kM1 - 1]);
+    }
+    if (kRest > 0) {
+        __syncthreads();
+        if (threadIdx.x < kRest) {
+            const int px = kFull + threadIdx.x;
+            const int x = px % kP1W, y = px / kP1W;
+            const float* P = S.l1rest[threadIdx.x];
+            S.s1[0][y][x] = fadd(P[0], P[1]);
+#pragma unroll
+            for (int k = 1; k < NW::kM1 - 1; ++k) S.s1[k][y][x] = fadd(fadd(P[k - 1], P[k]), P[k + 1]);
+            S.s1[NW::kM1 - 1][y][x] = fadd(P[NW::kM1 - 2], P[NW::kM1 - 1]);
+        }
     }
     __syncthreads();
     // L2: map pair (2i, 2i+1) convolves sum map i; 3x3 + BN/LReLU + 2x2 max
@@ -93,18 +121,18 @@ __device__ void window_net(const NW& W, WindowSmem& S, int mode) {
         for (int r = 0; r < 4; ++r)
 #pragma unroll
             for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(S.s1[i][2 * y + r][2 * x + c]);
-        float cv[2][4];
+        f2_t cv[4];
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
             const int dy = d >> 1, dx = d & 1;
             f2_t acc = f2_mul(q[dy][dx], f2_ld(W.k2p[i][0]), nz);
 #pragma unroll
             for (int k = 1; k < 9; ++k) acc = f2_add(acc, f2_mul(q[dy + k / 3][dx + k % 3], f2_ld(W.k2p[i][k]), nz));
-            cv[0][d] = lrelu_bn(f2_lo(acc), W.b2[2 * i], W.w2a[2 * i], W.w2b[2 * i], W.bn2[2 * i]);
-            cv[1][d] = lrelu_bn(f2_hi(acc), W.b2[2 * i + 1], W.w2a[2 * i + 1], W.w2b[2 * i + 1], W.bn2[2 * i + 1]);
+            cv[d] = lrelu_bn2(acc, W.a2p[i], nz);
         }
-        S.p2[2 * i][y][x] = fmaxf(fmaxf(cv[0][0], cv[0][1]), fmaxf(cv[0][2], cv[0][3]));
-        S.p2[2 * i + 1][y][x] = fmaxf(fmaxf(cv[1][0], cv[1][1]), fmaxf(cv[1][2], cv[1][3]));
+        const f2_t pm = f2_max4(cv[0], cv[1], cv[2], cv[3]);
+        S.p2[2 * i][y][x] = f2_lo(pm);
+        S.p2[2 * i + 1][y][x] = f2_hi(pm);
     }
     __syncthreads();
     for (int p = threadIdx.x; p < kP2W * kP2H; p += kWT) {
@@ -124,8 +152,9 @@ __device__ void window_net(const NW& W, WindowSmem& S, int mode) {
 #pragma unroll
         for (int k = 1; k < NW::kK3W * NW::kK3H; ++k)
             acc = f2_add(acc, f2_mul(f2_dup(S.s2[i][oy + k / NW::kK3W][ox + k % NW::kK3W]), f2_ld(W.k3p[i][k]), nz));
-        S.a3[2 * i][o] = lrelu_bn(f2_lo(acc), W.b3[2 * i], W.w3a[2 * i], W.w3b[2 * i], W.bn3[2 * i]);
-        S.a3[2 * i + 1][o] = lrelu_bn(f2_hi(acc), W.b3[2 * i + 1], W.w3a[2 * i + 1], W.w3b[2 * i + 1], W.bn3[2 * i + 1]);
+        const f2_t av = lrelu_bn2(acc, W.a3p[i], nz);
+        S.a3[2 * i][o] = f2_lo(av);
+        S.a3[2 * i + 1][o] = f2_hi(av);
     }
     __syncthreads();
     // hidden neurons n = HS*i + t read L3 maps i .. i+CONN-1; neurons (2q, 2q+1) share the
@@ -138,13 +167,12 @@ __device__ void window_net(const NW& W, WindowSmem& S, int mode) {
 #pragma unroll
         for (int j = 0; j < NW::kConn; ++j) s = f2_add(s, f2_mul(f2_dup(S.a3[i + j][o]), f2_ld(W.hwp[q][j]), nz));
         s = f2_mul(s, f2_dup(W.htw[i]), nz);
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const int t = (n + e) - i * NW::kHS;
-            float v = tanh_rational(e == 0 ? f2_lo(s) : f2_hi(s));
-            v = fadd(fmul(0.5f, v), 0.5f);
-            S.hbuf[n + e][o] = fadd(fmul(W.hbnw[t], v), W.hbnb[t]);
-        }
+        const f2_t half = f2_pack(0.5f, 0.5f);
+        const f2_t v = f2_add(f2_mul(half, tanh_rational2(s, nz), nz), half);
+        const int t = n - i * NW::kHS;  // neurons n, n+1 are slots t, t+1 of group i
+        const f2_t h = f2_add(f2_mul(f2_pack(W.hbnw[t], W.hbnw[t + 1]), v, nz), f2_pack(W.hbnb[t], W.hbnb[t + 1]));
+        S.hbuf[n][o] = f2_lo(h);
+        S.hbuf[n + 1][o] = f2_hi(h);
     }
     __syncthreads();
     if (threadIdx.x < kOutN) {
