@@ -80,8 +80,9 @@ class FaceDetector:
             pass
 
     # ---- detection ----
-    def Detect(self, img, capacity=4096):
-        """FaceDetector::Detect: returns a list of (x, y, width, height, score); raises on error."""
+    def Detect(self, img, capacity=4096, attributes=False):
+        """FaceDetector::Detect: returns a list of (x, y, width, height, score), with
+        (gender, smile, glasses) appended when `attributes` (set by facial analysis, else -1)."""
         if self._h is None:
             raise CCNNError(_capi.ERR_INVALID_ARG, "Detect (detector not initialised)")
         im, _keep = _as_image(img)
@@ -89,6 +90,8 @@ class FaceDetector:
         n = ctypes.c_int(0)
         st = _capi.lib().ccnn_detect(self._h, ctypes.byref(im), faces, capacity, ctypes.byref(n))
         _capi.check(st, "ccnn_detect")
+        if attributes:
+            return [(f.x, f.y, f.width, f.height, f.score, f.gender, f.smile, f.glasses) for f in faces[: min(n.value, capacity)]]
         return [(f.x, f.y, f.width, f.height, f.score) for f in faces[: min(n.value, capacity)]]
 
     def DetectBatch(self, imgs, capacity=4096):

@@ -160,6 +160,29 @@ struct Stage1Dup {
     float2 obd, otwd, afd;
 };
 
+// cnn4landmarks_cntk.bin (facial analysis): 49x51 window, 24/48/96 maps, 4x4 / 3x3 / 10(w)x11(h),
+// a fully connected hidden layer of 384 neurons over the 96 L3 values, 13 outputs (5 landmarks
+// (x, y) as fractions of the window, gender, smile, glasses). Too large for kernel parameters: it
+// lives in device memory.
+struct LandmarkNet {
+    static constexpr int kM1 = 24, kM2 = 48, kM3 = 96, kHL = 384, kOut = 13;
+    static constexpr int kInW = 49, kInH = 51, kK3W = 10, kK3H = 11;
+    float2 k1p[kM1 / 2][16];        // L1 taps of map pairs (2i, 2i+1)
+    float2 a1p[kM1 / 2][4];         // L1 {b, w1a, w1b, bn} of map pairs
+    float2 k2p[kM2 / 2][9];         // L2 maps (2i, 2i+1) read neighbour sum i
+    float2 a2p[kM2 / 2][4];
+    float2 k3p[kM3 / 2][kK3W * kK3H];  // L3 maps (2i, 2i+1) read neighbour sum i
+    float2 a3p[kM3 / 2][4];
+    float2 hwp[kHL / 2][kM3];       // hidden neurons (2q, 2q+1) over every L3 value
+    float2 hbp[kHL / 2];            // their biases
+    float2 hbnwp[kHL / 2], hbnbp[kHL / 2];
+    float htw;                      // tanh slope (one group)
+    float ow[kOut][kHL];
+    float ob[kOut];
+    float otw, af;
+    float2 negzero;
+};
+
 struct WindowNets {
     Stage2W s2;
     Stage3W s3;

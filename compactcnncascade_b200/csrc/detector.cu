@@ -80,13 +80,20 @@ bool compute_scales(const ccnn_params& p, bool gray_only, int pat_h, int max_h, 
     return !scales->empty();
 }
 
-Detector::~Detector() { clear(); }
+Detector::~Detector() {
+    clear();
+    if (d_lnet_) cudaFree(d_lnet_);
+}
 
 void Detector::free_slot(Slot& s) {
     if (s.exec) cudaGraphExecDestroy(s.exec);
     cudaFree(s.d_in);
     cudaFree(s.d_gray);
     cudaFree(s.d_limg);
+    cudaFree(s.d_attr);
+    cudaFree(s.d_fa);
+    s.d_attr = nullptr;
+    s.d_fa = nullptr;
     cudaFree(s.d_s1);
     cudaFree(s.d_resp);
     cudaFree(s.d_counts);
@@ -156,7 +163,7 @@ ccnn_status Detector::apply_precision() {
         case CCNN_PRECISION_ULTRA: type_check_ = 2; min_num_detect_ = 2; break;
         default: break;
     }
-    if (!detect_enabled_) drop_detect_ = false;
+    if (!detect_enabled_ || api_.facial_analysis) drop_detect_ = false;  // Init (:961-964)
     return CCNN_OK;
 }
 
@@ -167,10 +174,6 @@ ccnn_status Detector::create(const ccnn_params& p, const char* const* model_path
         return CCNN_ERR_INVALID_ARG;
     }
     slots_.assign(n_slots, Slot());
-    if (p.facial_analysis) {
-        set_error("facial_analysis is not supported by this detector");
-        return CCNN_ERR_UNSUPPORTED;
-    }
     for (int i = 0; i < 3; ++i) {
         const char* mp = model_paths ? model_paths[i] : nullptr;
         static const char* kNames[3] = {"cnn4face1_cntk.bin", "cnn4face2_cntk.bin", "cnn4face3_cntk.bin"};
@@ -202,6 +205,19 @@ ccnn_status Detector::init() {
         !pack_model(m[2], api_.index_output[2], &wn_->s3, &err)) {
         set_error(err);
         return CCNN_ERR_MODEL;
+    }
+    if (api_.facial_analysis && detect_enabled_) {
+        // InitCNNCheck (:792-810): the landmark network, bundled next to the library
+        RawModel lm;
+        std::unique_ptr<LandmarkNet> ln(new LandmarkNet());
+        if (!load_model_file(bundled_model_dir() + "/cnn4landmarks_cntk.bin", &lm, &err) || !pack_landmarks(lm, ln.get(), &err)) {
+            set_error(err);
+            return CCNN_ERR_MODEL;
+        }
+        int dev = api_.cuda_device_id;
+        CCNN_CUDA(cudaSetDevice(dev));
+        if (!d_lnet_) CCNN_CUDA(cudaMalloc(&d_lnet_, sizeof(LandmarkNet)));
+        CCNN_CUDA(cudaMemcpy(d_lnet_, ln.get(), sizeof(LandmarkNet), cudaMemcpyHostToDevice));
     }
     pat_w_ = m[0].min_w;
     pat_h_ = m[0].min_h;
@@ -270,8 +286,10 @@ ccnn_status Detector::init() {
     CCNN_CUDA(cudaGetDeviceProperties(&prop, device_));
     // persistent stage-2/3 grid: 4 resident 256-thread CTAs per SM (register bound)
     window_grid_ = prop.multiProcessorCount * 4;
+    facial_grid_ = prop.multiProcessorCount;  // one 118 KB-shared-memory block per SM
     CCNN_CUDA(replay_setup());
     CCNN_CUDA(stage1_setup());
+    CCNN_CUDA(facial_setup());
 
     inited_ = true;
     for (auto& s : slots_) {
@@ -311,6 +329,10 @@ ccnn_status Detector::alloc_slot(Slot& s) {
     CCNN_CUDA(cudaMalloc(&s.d_faces, sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces)));
     CCNN_CUDA(cudaMemset(s.d_faces, 0, sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces)));
     CCNN_CUDA(cudaMalloc(&s.d_nfaces, sizeof(int)));
+    if (d_lnet_ && api_.facial_analysis) {
+        CCNN_CUDA(cudaMalloc(&s.d_attr, sizeof(int4) * cand_cap_));
+        CCNN_CUDA(cudaMalloc(&s.d_fa, sizeof(int) * 5 * cand_cap_));
+    }
     CCNN_CUDA(cudaMallocHost(&s.h_nfaces, sizeof(int)));
     CCNN_CUDA(cudaMallocHost(&s.h_faces, sizeof(FaceOut) * kHostFaces));
     CCNN_CUDA(cudaMemsetAsync(s.d_ncand, 0, sizeof(int), s.st));
@@ -419,6 +441,31 @@ ccnn_status Detector::plan_for(int w, int h, int ch, const Plan** out) {
     return CCNN_OK;
 }
 
+ReplayArgs Detector::replay_args(Slot& s, const Plan& p) const {
+    ReplayArgs a;
+    a.cands = s.d_cands;
+    a.n_cand = s.d_ncand;
+    a.win = s.d_win;
+    a.results = s.d_results;
+    a.levels = p.d_levels;
+    a.n_levels = p.n_levels;
+    a.cfg = cfg_;
+    a.D = s.D;
+    a.R = s.R;
+    a.M = s.M;
+    a.F = s.F;
+    a.first_dec = s.first_dec;
+    a.survivors = s.survivors;
+    a.checked = s.checked;
+    a.attr = s.d_attr;
+    a.fa_scratch = s.d_fa;
+    a.n_raw = s.d_nraw;
+    a.faces = s.d_faces;
+    a.face_cap = (int)cand_cap_;
+    a.n_faces = s.d_nfaces;
+    return a;
+}
+
 ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
     cudaError_t e;
     if (p.downscale)
@@ -435,26 +482,10 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
     if (detect_enabled_)
         CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
                                 window_grid_, s.st));
-    ReplayArgs a;
-    a.cands = s.d_cands;
-    a.n_cand = s.d_ncand;
-    a.win = s.d_win;
-    a.results = s.d_results;
-    a.levels = p.d_levels;
-    a.n_levels = p.n_levels;
-    a.cfg = cfg_;
-    a.D = s.D;
-    a.R = s.R;
-    a.M = s.M;
-    a.F = s.F;
-    a.first_dec = s.first_dec;
-    a.survivors = s.survivors;
-    a.checked = s.checked;
-    a.n_raw = s.d_nraw;
-    a.faces = s.d_faces;
-    a.face_cap = (int)cand_cap_;
-    a.n_faces = s.d_nfaces;
-    CCNN_CUDA(launch_replay(a, s.st));
+    if (s.d_attr)
+        CCNN_CUDA(launch_facial(d_lnet_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_, s.d_attr,
+                                facial_grid_, s.st));
+    CCNN_CUDA(launch_replay(replay_args(s, p), s.st));
     CCNN_CUDA(cudaMemcpyAsync(s.h_nfaces, s.d_nfaces, sizeof(int), cudaMemcpyDeviceToHost, s.st));
     CCNN_CUDA(cudaMemcpyAsync(s.h_faces, s.d_faces, sizeof(FaceOut) * kHostFaces, cudaMemcpyDeviceToHost, s.st));
     return CCNN_OK;
@@ -504,7 +535,9 @@ ccnn_status Detector::collect(Slot& s, ccnn_face* faces, int cap, int* n) {
         faces[i].width = src[i].w;
         faces[i].height = src[i].h;
         faces[i].score = src[i].score;
-        faces[i].gender = faces[i].smile = faces[i].glasses = -1;
+        faces[i].gender = src[i].gender;
+        faces[i].smile = src[i].smile;
+        faces[i].glasses = src[i].glasses;
     }
     return nf > cap ? CCNN_TRUNCATED : CCNN_OK;
 }
@@ -733,10 +766,6 @@ ccnn_status Detector::get_params(ccnn_params* out) {
 
 ccnn_status Detector::set_params(const ccnn_params& p) {
     std::lock_guard<std::mutex> lk(mu_);
-    if (p.facial_analysis) {
-        set_error("facial_analysis is not supported by this detector");
-        return CCNN_ERR_UNSUPPORTED;
-    }
     clear();
     api_ = p;
     max_w_ = p.max_image_width;
@@ -834,25 +863,7 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     cudaEvent_t ev[K + 1];
     for (auto& e : ev) CCNN_CUDA(cudaEventCreate(&e));
     double acc[K] = {0};
-    ReplayArgs a;
-    a.cands = s.d_cands;
-    a.n_cand = s.d_ncand;
-    a.win = s.d_win;
-    a.results = s.d_results;
-    a.levels = p.d_levels;
-    a.n_levels = p.n_levels;
-    a.cfg = cfg_;
-    a.D = s.D;
-    a.R = s.R;
-    a.M = s.M;
-    a.F = s.F;
-    a.first_dec = s.first_dec;
-    a.survivors = s.survivors;
-    a.checked = s.checked;
-    a.n_raw = s.d_nraw;
-    a.faces = s.d_faces;
-    a.face_cap = (int)cand_cap_;
-    a.n_faces = s.d_nfaces;
+    const ReplayArgs a = replay_args(s, p);
     for (int it = 0; it < iters; ++it) {
         CCNN_CUDA(cudaEventRecord(ev[0], s.st));
         if (p.downscale)
@@ -873,6 +884,9 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         if (detect_enabled_)
             CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
                                     window_grid_, s.st));
+        if (s.d_attr)
+            CCNN_CUDA(launch_facial(d_lnet_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
+                                    s.d_attr, facial_grid_, s.st));
         CCNN_CUDA(cudaEventRecord(ev[6], s.st));
         CCNN_CUDA(launch_replay(a, s.st));
         CCNN_CUDA(cudaEventRecord(ev[7], s.st));

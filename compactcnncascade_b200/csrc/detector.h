@@ -56,6 +56,8 @@ struct Slot {
     int* d_nfaces = nullptr;
     int* h_nfaces = nullptr;   // pinned
     FaceOut* h_faces = nullptr;  // pinned, kHostFaces entries
+    int4* d_attr = nullptr;      // facial analysis: per candidate (dropped, gender, smile, glasses)
+    int* d_fa = nullptr;         // facial analysis: replay scratch (5 x candidate capacity)
     cudaGraphExec_t exec = nullptr;
     const Plan* exec_plan = nullptr;
     const Plan* last_plan = nullptr;  // plan of the last frame run on this slot
@@ -116,6 +118,7 @@ class Detector {
     std::string model_paths_[3];
     Stage1W w1_{};
     std::unique_ptr<WindowNets> wn_;
+    LandmarkNet* d_lnet_ = nullptr;  // facial-analysis network (device memory), when enabled
     int pat_w_ = kPatW, pat_h_ = kPatH;     // stage-1 window
     int ext_w_ = kWinW, ext_h_ = kWinH;     // smallest level processed
 
@@ -132,6 +135,7 @@ class Detector {
     long long cand_cap_ = 0, s1_cap_ = 0, resp_cap_ = 0, img_cap_ = 0;
     int chunk_cap_ = 0;
     int window_grid_ = 0;
+    int facial_grid_ = 0;
     std::map<std::tuple<int, int, int, int>, std::unique_ptr<Plan>> plans_;
     std::mutex mu_;
 
@@ -145,6 +149,7 @@ class Detector {
     ccnn_status enqueue_kernels(Slot& s, const Plan& p);
     ccnn_status prepare_frame(const ccnn_image& img, const Plan** plan, bool* empty);
     ccnn_status collect(Slot& s, ccnn_face* faces, int cap, int* n);
+    ReplayArgs replay_args(Slot& s, const Plan& p) const;
     ccnn_status apply_precision();
 };
 

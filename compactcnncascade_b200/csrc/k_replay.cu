@@ -23,6 +23,7 @@
 // permutes (scale, index) keys, and the clustering runs in warp 0.
 #include "kernels.h"
 #include "replay.cuh"
+#include "window_common.cuh"
 
 namespace ccnn {
 
@@ -86,7 +87,10 @@ __device__ __forceinline__ MergeTest merge_test(const Det& a, const Det& b, floa
 }
 
 // Merger (cnn_detector_v3.cpp:2814-2936) run by one warp. in[] is read-only; checked[] is scratch.
-__device__ int merger_warp(const Det* in, int n, uint8_t* checked, Det* out, float threshold, bool del) {
+// clus (optional): cluster (output index) of every input box; src (optional): input index of
+// every output box.
+__device__ int merger_warp(const Det* in, int n, uint8_t* checked, Det* out, float threshold, bool del, int* clus = nullptr,
+                           int* src = nullptr) {
     const int lane = threadIdx.x & 31;
     for (int k = lane; k < n; k += 32) checked[k] = 0;
     __syncwarp();
@@ -137,6 +141,7 @@ __device__ int merger_warp(const Det* in, int n, uint8_t* checked, Det* out, flo
                     if (lane == f) {
                         checked[j] = 1;
                         live = false;
+                        if (clus) clus[j] = nout;
                     }
                     start = f + 1;
                 }
@@ -144,6 +149,10 @@ __device__ int merger_warp(const Det* in, int n, uint8_t* checked, Det* out, flo
             __syncwarp();
         }
         if (del && dropped) continue;
+        if (lane == 0) {
+            if (clus) clus[i1] = nout;
+            if (src) src[nout] = i1;
+        }
         Det r = nmax;
         r.x = (nmin.x + nmax.x) >> 1;
         r.y = (nmin.y + nmax.y) >> 1;
@@ -160,40 +169,6 @@ __device__ int merger_warp(const Det* in, int n, uint8_t* checked, Det* out, flo
 
 constexpr int kMaxLevels = 1024;
 
-// stage-2/3 verdict of one candidate from its four speculative (max, count) pairs, applying the
-// reference's order: stage 2, early exits (:1698-1706), stage 3, accept rule (:1709-1725), retry
-// with the shrunken window when rejected and double_check is on (:1806-1811)
-__device__ __forceinline__ CandResult verdict(const WinOut* w, const Candidate& cd, float scale, const CascadeConfig& C) {
-    const int mn = (C.adapt_min_neighbors && scale > 0.7f && C.min_neighbors > 1) ? C.min_neighbors - 1 : C.min_neighbors;
-    CandResult r;
-    r.accepted = 0;
-    r.score = 0.f;
-    r.knn = 0;
-    r.pad = 0;
-    const int n_mod = C.double_check ? 2 : 1;
-    for (int mod = 0; mod < n_mod; ++mod) {
-        const float max1 = w[2 * mod].max;
-        const int k1 = w[2 * mod].knn;
-        const bool stop = (C.type_check == 0 && k1 >= mn) || (C.type_check > 0 && k1 <= 0) || (C.type_check == 2 && k1 < mn);
-        const float max2 = stop ? -10.f : w[2 * mod + 1].max;
-        const int k2 = stop ? 0 : w[2 * mod + 1].knn;
-        bool flag = false;
-        switch (C.type_check) {
-            case 0: flag = (k1 >= mn || k2 >= mn); break;
-            case 1: flag = (k1 >= mn && k2 > 0) || (k1 > 0 && k2 >= mn); break;
-            case 2: flag = (k1 >= mn && k2 >= mn); break;
-        }
-        if (flag) {
-            const float m1 = (-1.7159f < max1) ? max1 : -1.7159f;
-            const float m2 = (-1.7159f < max2) ? max2 : -1.7159f;
-            r.accepted = mod + 1;
-            r.score = fadd(fadd(cd.score, fmul((float)k1, m1)), fmul((float)k2, m2));
-            r.knn = imin(k1, k2);
-            return r;
-        }
-    }
-    return r;
-}
 
 constexpr int kBitMax = 256;              // candidates per level handled with bit matrices
 constexpr int kBitWords = kBitMax / 32;
@@ -330,6 +305,7 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                 if (thread_item) {
                     code = first_dec[g + i];
                     acc = C.detect_enabled ? res[g + i].accepted : 1;
+                    if (acc && a.attr && a.attr[g + i].x) acc = 0;  // facial analysis dropped it
                 }
                 if (tid < kBitWords) {
                     s_S[tid] = 0u;
@@ -447,6 +423,8 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                     }
                     const Det nr = cand_rect(cands[g + i], inv_scale, scale);
                     D[s_didx[i]] = make_det(nr.x, nr.y, nr.w, nr.h, sc, scale, kn);
+                    // facial data travels with a candidate's own accepted box, not with copies
+                    if (a.fa_scratch) a.fa_scratch[s_didx[i]] = (s_src[i] == kOwnVerdict) ? g + i : -1;
                 }
                 nD += nScan + nSurv;
                 __syncthreads();
@@ -482,6 +460,7 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                                 nr = cand_rect(cands[c], inv_scale, scale);
                                 const Det src = D[k0];
                                 D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, src.score, scale, src.knn);
+                                if (a.fa_scratch) a.fa_scratch[nD] = -1;
                             }
                             nD++;
                             __syncwarp();
@@ -522,6 +501,7 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                         if (lane == 0) {
                             const Det src = D[k0];
                             D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, src.score, scale, src.knn);
+                            if (a.fa_scratch) a.fa_scratch[nD] = -1;
                         }
                         nD++;
                         __syncwarp();
@@ -529,12 +509,19 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                     }
                 }
                 if (!C.detect_enabled) {
-                    if (lane == 0) D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, cd.score, scale, 0);
+                    if (lane == 0) {
+                        D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, cd.score, scale, 0);
+                        if (a.fa_scratch) a.fa_scratch[nD] = -1;
+                    }
                     nD++;
                 } else {
                     const CandResult r = res[c];
-                    if (r.accepted) {
-                        if (lane == 0) D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, r.score, scale, r.knn);
+                    // facial analysis drops a window whose landmarks collapse (cnn_detector_v3.cpp:1750)
+                    if (r.accepted && !(a.attr && a.attr[c].x)) {
+                        if (lane == 0) {
+                            D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, r.score, scale, r.knn);
+                            if (a.fa_scratch) a.fa_scratch[nD] = c;
+                        }
                         nD++;
                     }
                 }
@@ -555,7 +542,10 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
     __syncthreads();
     if (nD > 16 && tid == 0) introsort_scale_desc(K, nD);  // n <= 16: insertion sort of a sorted list
     __syncthreads();
-    for (int i = tid; i < nD; i += kRT) R[i] = D[nD - 1 - K[i].idx];
+    for (int i = tid; i < nD; i += kRT) {
+        R[i] = D[nD - 1 - K[i].idx];
+        if (a.fa_scratch) a.fa_scratch[a.face_cap + i] = a.fa_scratch[nD - 1 - K[i].idx];
+    }
     __syncthreads();
 
     // post-processing in warp 0
@@ -564,8 +554,16 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
     int nF = 0;
     const Det* fin = R;
     if (nD > 0) {
+        int* fa = a.fa_scratch;
+        const int cap = a.face_cap;
+        int* clus = fa ? fa + 2 * cap : nullptr;  // cluster of every sorted box
+        int* keepmap = fa ? fa + 3 * cap : nullptr;  // first-merge cluster of every kept box
+        int* fsrc = fa ? fa + 4 * cap : nullptr;     // kept box of every final box
         if (C.merger_detect) {
-            int nM = merger_warp(R, nD, checked, M, 0.5f, false);
+            int nM = merger_warp(R, nD, checked, M, 0.5f, false, clus);
+            if (keepmap)
+                for (int k = lane; k < nM; k += 32) keepmap[k] = k;
+            __syncwarp();
             if (C.min_num_detect > 1) {
                 // stable erase of clusters with fewer than min_num_detect merges
                 int w = 0;
@@ -576,19 +574,29 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                     const unsigned m = __ballot_sync(0xffffffffu, keep);
                     const int pos = w + __popc(m & ((1u << lane) - 1u));
                     __syncwarp();
-                    if (keep) M[pos] = v;
+                    if (keep) {
+                        M[pos] = v;
+                        if (keepmap) keepmap[pos] = kk;
+                    }
                     __syncwarp();
                     w += __popc(m);
                 }
                 nM = w;
             }
             if (nM > 0) {
-                nF = merger_warp(M, nM, checked, F, 0.2f, true);
+                nF = merger_warp(M, nM, checked, F, 0.2f, true, nullptr, fsrc);
                 fin = F;
             } else {
                 nF = 0;
             }
         } else {
+            if (fa)
+                for (int k = lane; k < nD; k += 32) {
+                    clus[k] = k;
+                    keepmap[k] = k;
+                    fsrc[k] = k;
+                }
+            __syncwarp();
             nF = nD;
             fin = R;
         }
@@ -608,6 +616,42 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
             f.h = d.h;
         }
         f.score = d.score;
+        f.gender = f.smile = f.glasses = -1;
+        if (a.fa_scratch) {
+            // CompactCNNLibAPI_v2.cpp:296-319: each attribute is the element at size/2 of the
+            // merged box's facial data sorted in descending order
+            const int c = a.fa_scratch[3 * a.face_cap + a.fa_scratch[4 * a.face_cap + i]];
+            const int* rcand = a.fa_scratch + a.face_cap;
+            const int* cl = a.fa_scratch + 2 * a.face_cap;
+            int size = 0;
+            for (int r = 0; r < nD; ++r)
+                if (cl[r] == c && rcand[r] >= 0) size++;
+            if (size > 0) {
+                const int k = size / 2;
+                int outv[3];
+                for (int q = 0; q < 3; ++q) {
+                    // the k-th largest value (0-based): a value v with #(> v) <= k < #(>= v)
+                    outv[q] = -1;
+                    for (int r = 0; r < nD && outv[q] == -1; ++r) {
+                        if (cl[r] != c || rcand[r] < 0) continue;
+                        const int4 at = a.attr[rcand[r]];
+                        const int v = q == 0 ? at.y : (q == 1 ? at.z : at.w);
+                        int gt = 0, ge = 0;
+                        for (int u = 0; u < nD; ++u) {
+                            if (cl[u] != c || rcand[u] < 0) continue;
+                            const int4 bu = a.attr[rcand[u]];
+                            const int w = q == 0 ? bu.y : (q == 1 ? bu.z : bu.w);
+                            gt += w > v;
+                            ge += w >= v;
+                        }
+                        if (gt <= k && k < ge) outv[q] = v;
+                    }
+                }
+                f.gender = outv[0];
+                f.smile = outv[1];
+                f.glasses = outv[2];
+            }
+        }
         a.faces[i] = f;
     }
     if (lane == 0) *a.n_faces = nF;

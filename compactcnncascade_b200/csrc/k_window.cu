@@ -20,6 +20,7 @@
 // 20x22 -> pooled 10x11), sums, L3 (24 maps, 7w x 8h -> 4x4), hidden layer and output neuron.
 #include "kernels.h"
 #include "resample.cuh"
+#include "window_common.cuh"
 
 namespace ccnn {
 
@@ -198,27 +199,7 @@ struct WinArgs {
 
 // crop + byte rounding + (optional) equalisation of one window into S.crop
 __device__ void prepare_window(const WinArgs& a, WindowSmem& S, const Candidate& cd, float inv_scale, int mod) {
-    if (threadIdx.x == 0) {
-        int x = (int)((float)(cd.px - (kExtOff + kXOff) / 2) * inv_scale);
-        int y = (int)((float)(cd.py - kExtOff / 2) * inv_scale);
-        int width = (int)((float)(kPatW + kExtOff + kXOff) * inv_scale);
-        int height = (int)((float)(kPatH + kExtOff) * inv_scale);
-        if (mod == 1) {
-            const float k = 0.15f;
-            x = (int)(fadd((float)x, fdiv(fmul((float)width, k), 2.f)));
-            width = (int)(fsub((float)width, fmul((float)width, k)));
-            y = (int)(fadd((float)y, fdiv(fmul((float)height, k), 2.f)));
-            height = (int)(fsub((float)height, fmul((float)height, k)));
-        }
-        const int rx = min(max(x, 0), a.gw);
-        const int ry = min(max(y, 0), a.gh);
-        const int rcols = min(max(x + width, 0), a.gw) - rx;
-        const int rrows = min(max(y + height, 0), a.gh) - ry;
-        S.geo[0] = rx;
-        S.geo[1] = ry;
-        S.geo[2] = rcols;
-        S.geo[3] = rrows;
-    }
+    if (threadIdx.x == 0) window_geometry(cd, inv_scale, mod, a.gw, a.gh, S.geo);
     if (threadIdx.x < 256) S.hist[threadIdx.x] = 0;
     __syncthreads();
     const int rx = S.geo[0], ry = S.geo[1], rcols = S.geo[2], rrows = S.geo[3];

@@ -11,6 +11,7 @@ namespace ccnn {
 struct FaceOut {
     int x, y, w, h;
     float score;
+    int gender, smile, glasses;  // facial analysis; -1 without it
 };
 
 struct ReplayArgs {
@@ -29,6 +30,10 @@ struct ReplayArgs {
     int* first_dec;  // per candidate: first decisive earlier box (scan test)
     int* survivors;  // per level: candidates surviving the scan
     uint8_t* checked;
+    // facial analysis (null when off): per candidate (dropped, gender, smile, glasses), and
+    // scratch of 5 x candidate-capacity ints for the attribute medians of merged boxes
+    const int4* attr;
+    int* fa_scratch;
     // outputs
     int* n_raw;
     FaceOut* faces;
@@ -61,6 +66,11 @@ cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDes
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
                           const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st);
 int window_smem_bytes();
+// facial analysis: dynamic shared memory attribute (once per device) and the landmark kernel
+cudaError_t facial_setup();
+cudaError_t launch_facial(const LandmarkNet* d_net, const float* gray, int gpitch, int gw, int gh, const Candidate* cands,
+                          const int* n_cand, const LevelDesc* levels, const WinOut* win, const CascadeConfig& cfg, int4* attr, int grid,
+                          cudaStream_t st);
 // dynamic shared memory of the replay kernel (set once per device before any launch)
 constexpr int kReplaySmemBytes = 200 * 1024;
 cudaError_t replay_setup();

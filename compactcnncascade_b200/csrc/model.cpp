@@ -208,6 +208,54 @@ template bool pack_model<Stage1W>(const RawModel&, int, Stage1W*, std::string*);
 template bool pack_model<Stage2W>(const RawModel&, int, Stage2W*, std::string*);
 template bool pack_model<Stage3W>(const RawModel&, int, Stage3W*, std::string*);
 
+bool pack_landmarks(const RawModel& m, LandmarkNet* o, std::string* err) {
+    using LN = LandmarkNet;
+    const bool shape_ok = m.min_w == LN::kInW && m.min_h == LN::kInH && m.maps[0] == LN::kM1 && m.maps[1] == LN::kM2 &&
+                          m.maps[2] == LN::kM3 && m.kw[0] == 4 && m.kh[0] == 4 && m.kw[1] == 3 && m.kh[1] == 3 &&
+                          m.kw[2] == LN::kK3W && m.kh[2] == LN::kK3H && m.full_connect && m.hl == LN::kHL && m.hs == LN::kHL &&
+                          m.nout == LN::kOut;
+    if (!shape_ok) {
+        *err = "facial-analysis model shape differs from cnn4landmarks_cntk.bin";
+        return false;
+    }
+    std::memset(o, 0, sizeof(LN));
+    auto tap = [&](int l, int mm, int k) { return m.kernels[l][(size_t)mm * m.kw[l] * m.kh[l] + k]; };
+    auto act = [&](int l, int mm, int field) { return m.act[l][5 * mm + field]; };
+    auto act_pair = [&](int l, int i, float2* out4) {
+        const int f[4] = {0, 1, 2, 4};  // conv bias, lrelu w1, lrelu w2, bn bias (bn weight folded)
+        for (int q = 0; q < 4; ++q) out4[q] = make_float2(act(l, 2 * i, f[q]), act(l, 2 * i + 1, f[q]));
+    };
+    for (int i = 0; i < LN::kM1 / 2; ++i) {
+        for (int k = 0; k < 16; ++k) o->k1p[i][k] = make_float2(tap(0, 2 * i, k), tap(0, 2 * i + 1, k));
+        act_pair(0, i, o->a1p[i]);
+    }
+    for (int i = 0; i < LN::kM2 / 2; ++i) {
+        for (int k = 0; k < 9; ++k) o->k2p[i][k] = make_float2(tap(1, 2 * i, k), tap(1, 2 * i + 1, k));
+        act_pair(1, i, o->a2p[i]);
+    }
+    for (int i = 0; i < LN::kM3 / 2; ++i) {
+        for (int k = 0; k < LN::kK3W * LN::kK3H; ++k) o->k3p[i][k] = make_float2(tap(2, 2 * i, k), tap(2, 2 * i + 1, k));
+        act_pair(2, i, o->a3p[i]);
+    }
+    for (int q = 0; q < LN::kHL / 2; ++q) {
+        for (int j = 0; j < LN::kM3; ++j)
+            o->hwp[q][j] = make_float2(m.hw[(size_t)(2 * q) * LN::kM3 + j], m.hw[(size_t)(2 * q + 1) * LN::kM3 + j]);
+        o->hbp[q] = make_float2(m.hb[2 * q], m.hb[2 * q + 1]);
+        o->hbnwp[q] = make_float2(m.hbn[2 * (2 * q)], m.hbn[2 * (2 * q + 1)]);
+        o->hbnbp[q] = make_float2(m.hbn[2 * (2 * q) + 1], m.hbn[2 * (2 * q + 1) + 1]);
+    }
+    o->htw = m.htw[0];
+    // one group, so the output sum visits the hidden neurons in order with weight index t
+    for (int k = 0; k < LN::kOut; ++k) {
+        for (int t = 0; t < LN::kHL; ++t) o->ow[k][t] = m.ow[(size_t)k * m.hl + t];
+        o->ob[k] = m.ob[k];
+    }
+    o->otw = m.otw;
+    o->af = m.af_scale;  // index_output -1: every output, no sign flip (cnn_simd_cntk.cpp:396-397)
+    o->negzero = make_float2(-0.f, -0.f);
+    return true;
+}
+
 std::string bundled_model_dir() {
     Dl_info info;
     if (dladdr(reinterpret_cast<void*>(&bundled_model_dir), &info) && info.dli_fname) {

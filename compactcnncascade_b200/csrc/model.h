@@ -39,6 +39,9 @@ bool load_model_file(const std::string& path, RawModel* m, std::string* err);
 template <class NW>
 bool pack_model(const RawModel& m, int index_output, NW* out, std::string* err);
 
+// Packs the facial-analysis (landmark) model; all 13 outputs are kept (index_output -1).
+bool pack_landmarks(const RawModel& m, LandmarkNet* out, std::string* err);
+
 // Directory holding the bundled model files (next to the shared library).
 std::string bundled_model_dir();
 

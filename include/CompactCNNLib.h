@@ -99,8 +99,12 @@ class FaceDetector {
         int n = 0;
         ccnn_status st = ccnn_detect(h_, &im, out.data(), capacity, &n);
         if (st < 0) return -1;
-        for (int i = 0; i < n && i < capacity; ++i)
+        for (int i = 0; i < n && i < capacity; ++i) {
             faces[i] = Face(out[i].x, out[i].y, out[i].width, out[i].height, out[i].score);
+            faces[i].gender = out[i].gender;  // facial analysis (else -1)
+            faces[i].smile = out[i].smile;
+            faces[i].glasses = out[i].glasses;
+        }
         return n;
     }
 

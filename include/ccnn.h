@@ -62,14 +62,15 @@ typedef struct {
     int device_info;
     int cuda_device_id;
     int cl_platform_id, cl_device_id;
-    int facial_analysis;                    /* must be 0: the landmark net is not part of this path */
+    int facial_analysis;                    /* 1: run the landmark network (bundled cnn4landmarks_cntk.bin) on
+                                               accepted windows: gender/smile/glasses, and drop_detect off */
 } ccnn_params;
 
 /* FaceDetector::Face (CompactCNNLibAPI_v2.h:66-82) */
 typedef struct {
     int x, y, width, height;
     float score;
-    int gender, smile, glasses;             /* always -1 (facial analysis off) */
+    int gender, smile, glasses;             /* facial analysis: median over the merged windows; else -1 */
 } ccnn_face;
 
 /* FaceDetector::ImageData (CompactCNNLibAPI_v2.h:84-95): 1 = gray, 3 = BGR, 4 = BGRA, row pitch in bytes */

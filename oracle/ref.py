@@ -23,6 +23,11 @@ class RefParams(ctypes.Structure):
                 ("equalize", ctypes.c_int), ("reflection", ctypes.c_int), ("detect_mode", ctypes.c_int)]
 
 
+class RefFace(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_int), ("y", ctypes.c_int), ("w", ctypes.c_int), ("h", ctypes.c_int),
+                ("score", ctypes.c_float), ("gender", ctypes.c_int), ("smile", ctypes.c_int), ("glasses", ctypes.c_int)]
+
+
 class RefDet(ctypes.Structure):
     _fields_ = [("x", ctypes.c_int), ("y", ctypes.c_int), ("w", ctypes.c_int), ("h", ctypes.c_int),
                 ("score", ctypes.c_float), ("scale", ctypes.c_float), ("knn", ctypes.c_int), ("num_detect", ctypes.c_int)]
@@ -48,6 +53,7 @@ def load(fast=False):
         L.ref_equalize.argtypes = [vp, ci, ci]
         L.ref_net_forward.argtypes = [ctypes.c_char_p, ci, vp, ci, ci, ci, vp, ci, P(ci), P(ci)]
         L.ref_face_detect.argtypes = [P(RefParams), vp, ci, ci, ci, ci, P(RefDet), ci]
+        L.ref_face_detect_fa.argtypes = [P(RefParams), vp, ci, ci, ci, ci, P(RefFace), ci]
         L.ref_api_init.argtypes = [P(RefParams)]
         L.ref_api_detect.argtypes = [vp, ci, ci, ci, ci, P(RefDet), ci]
         L.ref_detect_steps.argtypes = [P(RefParams), vp, ci, ci, ci, ci,
@@ -109,6 +115,18 @@ def face_detect(img, p, fast=False):
     if n < 0:
         raise RuntimeError(f"ref_face_detect failed ({n})")
     return [(d.x, d.y, d.w, d.h, d.score) for d in out[:n]]
+
+
+def face_detect_fa(img, p, fast=False):
+    """The reference's public Detect with facial analysis on: (x, y, w, h, score, gender, smile, glasses)."""
+    L = load(fast)
+    h, w = img.shape[:2]
+    ch = 1 if img.ndim == 2 else img.shape[2]
+    out = (RefFace * 65536)()
+    n = L.ref_face_detect_fa(ctypes.byref(p), img.ctypes.data, w, h, ch, img.strides[0], out, 65536)
+    if n < 0:
+        raise RuntimeError(f"ref_face_detect_fa failed ({n})")
+    return [(d.x, d.y, d.w, d.h, d.score, d.gender, d.smile, d.glasses) for d in out[:n]]
 
 
 def detect_steps(img, p, with_levels=True):

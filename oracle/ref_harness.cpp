@@ -166,6 +166,38 @@ int ref_face_detect(const ref_params* p, const uint8_t* img, int w, int h, int c
     return n;
 }
 
+// The same with facial analysis on (landmark network, CompactCNNLibAPI_v2.cpp:296-319): faces
+// carry gender / smile / glasses.
+typedef struct {
+    int x, y, w, h;
+    float score;
+    int gender, smile, glasses;
+} ref_face;
+
+int ref_face_detect_fa(const ref_params* p, const uint8_t* img, int w, int h, int ch, int step, ref_face* out, int cap) {
+    std::lock_guard<std::mutex> lk(g_api_mutex);
+    CompactCNNLib::FaceDetector fd;
+    CompactCNNLib::FaceDetector::Param q = to_api_param(p);
+    q.facial_analysis = true;
+    if (fd.Init(q) < 0) return -1;
+    std::vector<CompactCNNLib::FaceDetector::Face> faces(4096);
+    CompactCNNLib::FaceDetector::ImageData im(w, h, ch, const_cast<uint8_t*>(img), (size_t)step);
+    int n = fd.Detect(faces.data(), im);
+    if (n < 0) return n;
+    for (int i = 0; i < n && i < cap; ++i) {
+        out[i].x = faces[i].x;
+        out[i].y = faces[i].y;
+        out[i].w = faces[i].width;
+        out[i].h = faces[i].height;
+        out[i].score = faces[i].score;
+        out[i].gender = faces[i].gender;
+        out[i].smile = faces[i].smile;
+        out[i].glasses = faces[i].glasses;
+    }
+    fd.Clear();
+    return n;
+}
+
 // Persistent detector for repeated timing of the reference (bench reference arm).
 static CompactCNNLib::FaceDetector* g_fd = nullptr;
 
