@@ -159,8 +159,9 @@ class FaceDetector:
 
     @staticmethod
     def CNTKDump2Binary(binary_file, cntk_model_dump):
-        """The offline CNTK-dump converter is not part of the detection path."""
-        raise NotImplementedError("model conversion (cnn_models_converter.cpp) is offline tooling outside this path")
+        """FaceDetector::CNTKDump2Binary: converts a CNTK text dump into a binary model file
+        (".bin" appended when missing). Raises on a malformed dump."""
+        _capi.check(_capi.lib().ccnn_cntk_dump_to_binary(binary_file.encode(), cntk_model_dump.encode()), "ccnn_cntk_dump_to_binary")
 
     # ---- inspection (include/ccnn_inspect.h) ----
     def levels(self):

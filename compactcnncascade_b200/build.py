@@ -12,7 +12,7 @@ CSRC = os.path.join(HERE, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CU_SOURCES = ["capi.cu", "detector.cu", "k_image.cu", "k_stage1.cu", "k_candidates.cu", "k_window.cu", "k_replay.cu", "noalloc.cu", "server.cu", "k_facial.cu"]
-CPP_SOURCES = ["model.cpp"]
+CPP_SOURCES = ["model.cpp", "convert.cpp"]
 
 # -fmad=false: the kernels must reproduce the reference's uncontracted IEEE single arithmetic.
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-fmad=false", "-std=c++17",

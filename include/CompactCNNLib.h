@@ -12,13 +12,14 @@
 //    total count; the reference has no capacity argument;
 //  * getGrayImage32F(img, GPU) returns the device buffer, as the reference's GPU pipeline does;
 //    with Pipeline::CPU it returns a host copy owned by the facade;
-//  * CNTKDump2Binary (offline model conversion) is not provided by this library.
+//  * CNTKDump2Binary reports nothing on failure, like the reference; ccnn_cntk_dump_to_binary returns a status.
 #pragma once
 
 #include <cstddef>
 #include <vector>
 
 #include "ccnn.h"
+#include "ccnn_inspect.h"
 
 namespace CompactCNNLib {
 
@@ -106,6 +107,11 @@ class FaceDetector {
             faces[i].glasses = out[i].glasses;
         }
         return n;
+    }
+
+    // FaceDetector::CNTKDump2Binary (CompactCNNLibAPI_v2.cpp:509-519)
+    static void CNTKDump2Binary(const char* binary_file, const char* cntk_model_dump) {
+        ccnn_cntk_dump_to_binary(binary_file, cntk_model_dump);
     }
 
     int Clear() {

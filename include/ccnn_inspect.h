@@ -85,6 +85,11 @@ CCNN_API ccnn_status ccnn_plan_levels(const ccnn_params* p, int cols, int rows, 
  * counts the candidates), [4] candidate write, [5] stage-2/3 windows, [6] replay/sort/merge. */
 CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* kernel_ms, int n_kernels);
 
+/* FaceDetector::CNTKDump2Binary (src/CNNObjectDetector/CompactCNNLibAPI_v2.cpp:509-519): converts a
+ * CNTK text dump of a trained cascade network into the binary model format (version 1.1) that
+ * ccnn_create loads. ".bin" is appended to binary_file when it has no such extension. Host-only. */
+CCNN_API ccnn_status ccnn_cntk_dump_to_binary(const char* binary_file, const char* cntk_model_dump);
+
 /* The permutation the detector's device sort applies to detections with the given scales
  * (perm[i] = input index placed at slot i); equals std::sort with comp(a, b) = b < a. */
 CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm);

@@ -54,6 +54,7 @@ def load(fast=False):
         L.ref_net_forward.argtypes = [ctypes.c_char_p, ci, vp, ci, ci, ci, vp, ci, P(ci), P(ci)]
         L.ref_face_detect.argtypes = [P(RefParams), vp, ci, ci, ci, ci, P(RefDet), ci]
         L.ref_face_detect_fa.argtypes = [P(RefParams), vp, ci, ci, ci, ci, P(RefFace), ci]
+        L.ref_cntk_dump2binary.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
         L.ref_api_init.argtypes = [P(RefParams)]
         L.ref_api_detect.argtypes = [vp, ci, ci, ci, ci, P(RefDet), ci]
         L.ref_detect_steps.argtypes = [P(RefParams), vp, ci, ci, ci, ci,
@@ -127,6 +128,11 @@ def face_detect_fa(img, p, fast=False):
     if n < 0:
         raise RuntimeError(f"ref_face_detect_fa failed ({n})")
     return [(d.x, d.y, d.w, d.h, d.score, d.gender, d.smile, d.glasses) for d in out[:n]]
+
+
+def cntk_dump2binary(binary_file, dump_file):
+    """The reference's FaceDetector::CNTKDump2Binary."""
+    load().ref_cntk_dump2binary(binary_file.encode(), dump_file.encode())
 
 
 def detect_steps(img, p, with_levels=True):

@@ -198,6 +198,12 @@ int ref_face_detect_fa(const ref_params* p, const uint8_t* img, int w, int h, in
     return n;
 }
 
+// CNTK dump -> binary model (CompactCNNLibAPI_v2.cpp:509-519)
+int ref_cntk_dump2binary(const char* binary_file, const char* dump_file) {
+    CompactCNNLib::FaceDetector::CNTKDump2Binary(binary_file, dump_file);
+    return 0;
+}
+
 // Persistent detector for repeated timing of the reference (bench reference arm).
 static CompactCNNLib::FaceDetector* g_fd = nullptr;
 
