@@ -65,7 +65,7 @@ struct Slot {
 
 class Detector {
    public:
-    static constexpr int kSlots = 4;
+    static constexpr int kSlots = 8;
     static constexpr int kHostFaces = 1024;
 
     Detector() = default;
