@@ -34,6 +34,7 @@ EXPORTED = [
     "ccnn_sort_permutation", "ccnn_detect_device_batch", "ccnn_profile_last_frame", "ccnn_plan_levels", "ccnn_stage1_forward_static",
     "ccnn_server_create", "ccnn_server_destroy", "ccnn_server_submit", "ccnn_server_poll", "ccnn_server_wait",
     "ccnn_server_stats_get", "ccnn_host_alloc", "ccnn_host_free", "ccnn_cntk_dump_to_binary",
+    "ccnn_check_reciprocal",
 ]
 
 
@@ -149,6 +150,7 @@ def lib():
         L.ccnn_host_free.argtypes = [vp]
         L.ccnn_host_free.restype = None
         L.ccnn_cntk_dump_to_binary.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        L.ccnn_check_reciprocal.argtypes = [P(ctypes.c_longlong), P(ctypes.c_longlong)]
         _lib = L
     return _lib
 

@@ -269,3 +269,41 @@ CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm
 }
 
 }  // extern "C"
+
+// Exhaustive check of the packed reciprocal used by the rational tanh against the IEEE reciprocal.
+namespace ccnn {
+__global__ void rcp_check_kernel(uint32_t start, uint32_t pairs, unsigned long long* bad) {
+    unsigned long long local = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+        const float d0 = __uint_as_float(start + 2 * i), d1 = __uint_as_float(start + 2 * i + 1);
+        const f2_t r = f2_rcp(f2_pack(d0, d1));
+        local += (__float_as_uint(f2_lo(r)) != __float_as_uint(__frcp_rn(d0))) + (__float_as_uint(f2_hi(r)) != __float_as_uint(__frcp_rn(d1)));
+    }
+    if (local) atomicAdd(bad, local);
+}
+}  // namespace ccnn
+
+extern "C" CCNN_API ccnn_status ccnn_check_reciprocal(long long* mismatches, long long* checked) {
+    if (!mismatches || !checked) {
+        ccnn::set_error("invalid arguments");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    unsigned long long* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(unsigned long long));
+    const uint32_t lo = 0x3F800000u, hi = 0x7F800000u + 2u;  // 1.0 up to +inf and the first NaN
+    if (e == cudaSuccess) {
+        ccnn::rcp_check_kernel<<<148 * 8, 256>>>(lo, (hi - lo) / 2, d);
+        e = cudaDeviceSynchronize();
+    }
+    unsigned long long nb = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&nb, d, sizeof(nb), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        ccnn::set_error(std::string("reciprocal check: ") + cudaGetErrorString(e));
+        return CCNN_ERR_CUDA;
+    }
+    *mismatches = (long long)nb;
+    *checked = (long long)(hi - lo);
+    return CCNN_OK;
+}

@@ -87,6 +87,32 @@ __device__ __forceinline__ float lrelu_bn(float x, float b, float w1, float w2, 
     return fadd(fadd(fmul(w1, c), fmul(w2, fmaxf(0.f, c))), bnb);
 }
 
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
+    f2_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// Correctly rounded IEEE reciprocals of two values in [1, 2^126): the hardware approximation
+// (rcp.approx, within about an ulp) refined by two Newton-Raphson steps with fused residuals,
+// e = 1 - d*y, y' = y + y*e (Markstein's FMA iteration). For every float of that range the result
+// equals __frcp_rn bit for bit (compared exhaustively on B200, ccnn_check_reciprocal). Outside it
+// (subnormal results, infinity, NaN) both lanes take __frcp_rn.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ f2_t f2_rcp(f2_t d) {
+    const float d0 = f2_lo(d), d1 = f2_hi(d);
+    if (!(d0 >= 1.f && d0 < 0x1p126f && d1 >= 1.f && d1 < 0x1p126f)) return f2_pack(__frcp_rn(d0), __frcp_rn(d1));
+    const f2_t one = f2_pack(1.f, 1.f);
+    const f2_t nd = f2_pack(-d0, -d1);
+    f2_t y = f2_pack(rcp_approx(d0), rcp_approx(d1));
+    y = f2_fma(y, f2_fma(nd, y, one), y);
+    return f2_fma(y, f2_fma(nd, y, one), y);
+}
+
 // Two independent lanes of tanh_rational. The reciprocal 1/den is the correctly rounded IEEE
 // value, the same number as the reference's 1.f / den.
 __device__ __forceinline__ f2_t tanh_rational2(f2_t c, f2_t nz) {
@@ -96,7 +122,7 @@ __device__ __forceinline__ f2_t tanh_rational2(f2_t c, f2_t nz) {
     const f2_t c2 = f2_mul(c, c, nz);
     const f2_t c4 = f2_mul(f2_mul(f2_mul(f2_mul(a, c, nz), c, nz), c, nz), c, nz);
     const f2_t den = f2_add(f2_add(f2_add(one, ac), c2), c4);
-    const f2_t r = f2_pack(__frcp_rn(f2_lo(den)), __frcp_rn(f2_hi(den)));
+    const f2_t r = f2_rcp(den);  // den >= 1 (or NaN)
     const f2_t sgn = f2_pack(lo < 0.f ? -1.f : 1.f, hi < 0.f ? -1.f : 1.f);
     return f2_mul(sgn, f2_sub(one, r), nz);
 }

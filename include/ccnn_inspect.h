@@ -85,6 +85,11 @@ CCNN_API ccnn_status ccnn_plan_levels(const ccnn_params* p, int cols, int rows, 
  * counts the candidates), [4] candidate write, [5] stage-2/3 windows, [6] replay/sort/merge. */
 CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* kernel_ms, int n_kernels);
 
+/* Compares, on the current device, the packed reciprocal the kernels use in the rational tanh with the
+ * IEEE reciprocal for every float from 1.0 to +infinity (and the first NaN); *mismatches must be 0.
+ * No reference counterpart: the evidence behind replacing the division (cnnpp_cplusplus.cpp:662-666). */
+CCNN_API ccnn_status ccnn_check_reciprocal(long long* mismatches, long long* checked);
+
 /* FaceDetector::CNTKDump2Binary (src/CNNObjectDetector/CompactCNNLibAPI_v2.cpp:509-519): converts a
  * CNTK text dump of a trained cascade network into the binary model format (version 1.1) that
  * ccnn_create loads. ".bin" is appended to binary_file when it has no such extension. Host-only. */
