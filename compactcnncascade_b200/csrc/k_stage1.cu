@@ -210,18 +210,17 @@ __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_consta
 
     // C: pixels (x, y) and (x, y + 1)
     const int x = threadIdx.x & (kK2TileX - 1), y = (threadIdx.x / kK2TileX) * 2;
-    f2_t A[16];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    // L3 maps (2k, 2k+1) of the pixel pair, both from neighbour-sum map k; conv_5x4 keeps one
+    // partial sum per kernel row, added in row order
+    auto l3_pair = [&](int k, f2_t* m0, f2_t* m1) {
         float v[6][4];
 #pragma unroll
         for (int r = 0; r < 6; ++r)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) v[r][c] = S.s2[i][y + r][x + c];
+            for (int c = 0; c < 4; ++c) v[r][c] = S.s2[k][y + r][x + c];
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            const int mm = 2 * i + e;
-            // conv_5x4 keeps one partial sum per kernel row, added in row order
+            const int mm = 2 * k + e;
             f2_t acc = 0ull;
 #pragma unroll
             for (int r = 0; r < 5; ++r) {
@@ -230,26 +229,41 @@ __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_consta
                 for (int c = 1; c < 4; ++c) rs = f2_add(rs, f2_mul(f2_pack(v[r][c], v[r + 1][c]), f2_ld(D.k3d[mm][4 * r + c]), nz));
                 acc = (r == 0) ? rs : f2_add(acc, rs);
             }
-            A[mm] = lrelu_bn2(acc, D.a3d[mm], nz);
+            *(e == 0 ? m0 : m1) = lrelu_bn2(acc, D.a3d[mm], nz);
         }
-    }
-    // hidden neuron n = 4*i + t reads L3 maps i..i+3; the output sum runs over n in order
+    };
+    // hidden neuron n = 4*i + t reads L3 maps i..i+3: the groups run as a loop over a sliding window
+    // of four maps (a0..a3, with the second map of the last computed pair kept in `spare`), so the
+    // code stays small; the output sum runs over n in order
+    static_assert(Stage1W::kConn == 4 && Stage1W::kGroups + 3 == Stage1W::kM3, "sliding window of four L3 maps");
+    f2_t a0, a1, a2, a3, spare;
+    l3_pair(0, &a0, &a1);
+    l3_pair(1, &a2, &spare);
     const f2_t half = f2_pack(0.5f, 0.5f);
     f2_t out = 0ull;
-#pragma unroll
+#pragma unroll 1
     for (int i = 0; i < Stage1W::kGroups; ++i) {
+        const int m = i + 3;  // the group's newest map
+        if (m & 1) a3 = spare;
+        else l3_pair(m >> 1, &a3, &spare);
 #pragma unroll
         for (int tt = 0; tt < Stage1W::kHS; ++tt) {
             const int n = Stage1W::kHS * i + tt;
             f2_t s = f2_ld(D.hbd[n]);
-#pragma unroll
-            for (int j = 0; j < Stage1W::kConn; ++j) s = f2_add(s, f2_mul(A[i + j], f2_ld(D.hwd[n][j]), nz));
+            s = f2_add(s, f2_mul(a0, f2_ld(D.hwd[n][0]), nz));
+            s = f2_add(s, f2_mul(a1, f2_ld(D.hwd[n][1]), nz));
+            s = f2_add(s, f2_mul(a2, f2_ld(D.hwd[n][2]), nz));
+            s = f2_add(s, f2_mul(a3, f2_ld(D.hwd[n][3]), nz));
             s = f2_mul(s, f2_ld(D.htwd[i]), nz);
             f2_t v = tanh_rational2(s, nz);
             v = f2_add(f2_mul(half, v, nz), half);
             const f2_t h = f2_add(f2_mul(f2_ld(D.hbnwd[tt]), v, nz), f2_ld(D.hbnbd[tt]));
-            out = (n == 0) ? f2_mul(h, f2_ld(D.owd[0]), nz) : f2_add(f2_mul(h, f2_ld(D.owd[n]), nz), out);
+            const f2_t hw = f2_mul(h, f2_ld(D.owd[n]), nz);
+            out = (n == 0) ? hw : f2_add(hw, out);
         }
+        a0 = a1;
+        a1 = a2;
+        a2 = a3;
     }
     f2_t c = f2_mul(f2_add(out, f2_ld(D.obd)), f2_ld(D.otwd), nz);
     c = tanh_rational2(c, nz);
