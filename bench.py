@@ -285,6 +285,9 @@ def main():
     ap.add_argument("--profile-iters", type=int, default=20)
     ap.add_argument("--serve-frames", type=int, default=2000, help="frames of the serving-loop phase (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate of the serving phase, frames/s")
+    ap.add_argument("--no-gate", action="store_true", help="skip the batched+gated phase")
+    ap.add_argument("--gate-threshold", type=float, default=None, help="gate probability threshold (default: the weights' own)")
+    ap.add_argument("--gate-fallback", type=float, default=0.25, help="ambiguous-cell fraction that falls back to the full scan")
     ap.add_argument("--serving", action="store_true",
                     help="only the serving sweep: 10,000 mixed-resolution frames at 500, 1000, 2000, 4000 frames/s")
     args = ap.parse_args()
@@ -449,6 +452,62 @@ def main():
         "kernel_ms_all": {k: round(v, 4) for k, v in kernel_ms.items()},
     }
     fb = frame_bytes(levels, W, H)
+
+    # ---- batched+gated: the same frames with the learned gate in front of stage 1 ----
+    gated = None
+    from compactcnncascade_b200 import gate as gate_mod
+    if not args.no_gate and os.path.exists(gate_mod.WEIGHTS_1080P):
+        meta = gate_mod.load_meta()
+        thr = args.gate_threshold if args.gate_threshold is not None else meta.get("operating_threshold", 0.1)
+        plain_boxes = [det.Detect(f) for f in frames]
+        det.setGate(gate_mod.load(), thr, args.gate_fallback)
+        hit = tot = 0
+        tiles = np.zeros(5)
+        for f, ref_boxes in zip(frames, plain_boxes):
+            h_, t_ = gate_mod.box_recall(ref_boxes, det.Detect(f))
+            hit, tot = hit + h_, tot + t_
+            tiles += np.array(det.gateStats())
+        for s in range(args.warmup):
+            device_step(s)
+        barrier()
+        with ClockSampler(dev) as gclk:
+            g_ms = 0.0
+            for s in range(args.steps):
+                g_ms += device_step(args.warmup + s)
+            barrier()
+        g_value = args.steps * B * world / (g_ms / 1e3)
+        for s in range(args.warmup):
+            host_step(s)
+        barrier()
+        t0 = time.perf_counter()
+        for s in range(args.steps):
+            host_step(args.warmup + s)
+        barrier()
+        g_e2e = args.steps * B * world / (time.perf_counter() - t0)
+        glat = []
+        for i in range(args.latency_frames):
+            t = h_frames[i % len(frames)]
+            im = _capi.Image(W, H, 3, t.data_ptr(), W * 3)
+            t0 = time.perf_counter()
+            L.ccnn_detect(det._h, ctypes.byref(im), one, cap, ctypes.byref(n1))
+            glat.append((time.perf_counter() - t0) * 1e3)
+        glat = np.array(glat[min(5, len(glat) - 1):])
+        gk = (ctypes.c_float * (len(KERNELS) + 1))()
+        L.ccnn_profile_last_frame(det._h, args.profile_iters, gk, len(KERNELS) + 1)
+        det.disableGate()
+        gated = {"value": round(g_value, 2), "unit": "frames/s", "speedup_vs_plain": round(g_value / value, 3),
+                 "e2e": round(g_e2e, 2), "e2e_speedup_vs_plain": round(g_e2e / e2e, 3),
+                 "p50_ms": round(float(np.percentile(glat, 50)), 3), "p99_ms": round(float(np.percentile(glat, 99)), 3),
+                 "box_recall": round(hit / max(1, tot), 4), "boxes": tot, "recall_frames": len(frames), "threshold": thr,
+                 "fallback_fraction": args.gate_fallback,
+                 "front_tiles_run": round(tiles[0] / max(1, tiles[1]), 4), "back_tiles_run": round(tiles[2] / max(1, tiles[3]), 4),
+                 "fallback_frames": int(tiles[4]), "clocks": gclk.summary(),
+                 "kernel_ms_all": dict({KERNELS[i]: round(float(gk[i]), 4) for i in range(len(KERNELS))},
+                                       gate=round(float(gk[len(KERNELS)]), 4)),
+                 "weights": {k: meta.get(k) for k in ("train_frames", "epochs", "eval_frames")},
+                 "note": "same frames, detector and batch as `value`, with the learned gate (include/ccnn_gate.h) skipping "
+                         "stage-1 tiles; box recall = plain-cascade boxes matched by a gated box at IoU >= 0.5"}
+
     serving = run_serving(sframes, args.serve_rate, args.serve_frames) if sframes else None
 
     line = {
@@ -478,6 +537,8 @@ def main():
         "roofline": roofline,
         "wall_value": round(frames_timed / wall_dev, 2),
     }
+    if gated:
+        line["gated"] = gated
     if serving:
         line["serving"] = dict(serving, note="serving loop (ccnn_server_*): Poisson arrivals of mixed 640x480/1280x720/"
                                              "1920x1080/3840x2160 frames at 30/30/30/10 %, latency = submit to result")

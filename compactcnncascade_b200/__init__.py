@@ -12,7 +12,7 @@ import numpy as np
 from . import _capi
 from ._capi import CCNNError, Face, Image, Params
 
-__all__ = ["FaceDetector", "FaceServer", "Param", "synth_frame", "CCNNError", "default_params", "pinned_frame"]
+__all__ = ["FaceDetector", "FaceServer", "Param", "synth_frame", "synth_frame_device", "CCNNError", "default_params", "pinned_frame"]
 
 Pipeline = {"CPU": 0, "GPU": 1, "GPU_CPU": 2}
 DetectMode = {"disable": 0, "sync": 1, "async": 2}
@@ -113,6 +113,40 @@ class FaceDetector:
             fs = faces[i * capacity: i * capacity + min(ns[i], capacity)]
             out.append([(f.x, f.y, f.width, f.height, f.score) for f in fs])
         return out
+
+    def DetectDevice(self, data_ptr, width, height, channels, step, stream=None, capacity=4096):
+        """Detect on a frame already in device memory (uint8, interleaved, row pitch `step` bytes)."""
+        if self._h is None:
+            raise CCNNError(_capi.ERR_INVALID_ARG, "DetectDevice (detector not initialised)")
+        im = Image(width, height, channels, data_ptr, step)
+        faces = (Face * capacity)()
+        n = ctypes.c_int(0)
+        st = _capi.lib().ccnn_detect_device(self._h, ctypes.byref(im), stream, faces, capacity, ctypes.byref(n))
+        _capi.check(st, "ccnn_detect_device")
+        return [(f.x, f.y, f.width, f.height, f.score) for f in faces[: min(n.value, capacity)]]
+
+    # ---- learned gate (include/ccnn_gate.h) ----
+    def setGate(self, params, threshold=0.5, fallback_fraction=0.25):
+        """Skips stage-1 tiles that the gate network (700 fp32 parameters) finds unlikely."""
+        p = np.ascontiguousarray(params, np.float32)
+        _capi.check(_capi.lib().ccnn_gate_set(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), p.size, float(threshold),
+                                              float(fallback_fraction)), "ccnn_gate_set")
+
+    def disableGate(self):
+        _capi.check(_capi.lib().ccnn_gate_disable(self._h), "ccnn_gate_disable")
+
+    def gateStats(self):
+        """(front tiles run, front tiles, back tiles run, back tiles, fell back) of the last frame."""
+        v = [ctypes.c_int() for _ in range(5)]
+        _capi.check(_capi.lib().ccnn_gate_stats(self._h, *[ctypes.byref(x) for x in v]), "ccnn_gate_stats")
+        return tuple(x.value for x in v)
+
+    def grayDevice(self):
+        """(device pointer, cols, rows, step in bytes) of the last frame's fp32 gray image."""
+        ptr, w, h, step = ctypes.c_void_p(), ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
+        _capi.check(_capi.lib().ccnn_get_gray_device(self._h, ctypes.byref(ptr), ctypes.byref(w), ctypes.byref(h), ctypes.byref(step)),
+                    "ccnn_get_gray_device")
+        return ptr.value, w.value, h.value, step.value
 
     # ---- parameters ----
     def getParam(self):
@@ -279,6 +313,16 @@ def pinned_frame(shape):
     """A uint8 array of `shape` in page-locked host memory."""
     n = int(np.prod(shape))
     return np.asarray(_PinnedBuffer(n)).reshape(shape)
+
+
+def synth_frame_device(out_ptr, width, height, seed, n_faces, min_face, max_face, channels=3, step=None, stream=None):
+    """The same seeded frame as `synth_frame`, rendered on the device into `out_ptr` (device
+    memory, row pitch `step` bytes, default width * channels); returns the face patches."""
+    faces = (_capi.SynthFace * max(1, n_faces))()
+    st = _capi.lib().ccnn_synth_frame_device(out_ptr, width, height, channels, step or width * channels, seed, n_faces, min_face,
+                                             max_face, faces, stream)
+    _capi.check(st, "ccnn_synth_frame_device")
+    return [(f.cx, f.cy, f.w, f.h, f.angle_deg, f.contrast) for f in faces[:n_faces]]
 
 
 def synth_frame(width, height, seed, n_faces, min_face, max_face, channels=3):

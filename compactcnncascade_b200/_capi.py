@@ -34,7 +34,8 @@ EXPORTED = [
     "ccnn_sort_permutation", "ccnn_detect_device_batch", "ccnn_profile_last_frame", "ccnn_plan_levels", "ccnn_stage1_forward_static",
     "ccnn_server_create", "ccnn_server_destroy", "ccnn_server_submit", "ccnn_server_poll", "ccnn_server_wait",
     "ccnn_server_stats_get", "ccnn_host_alloc", "ccnn_host_free", "ccnn_cntk_dump_to_binary",
-    "ccnn_check_reciprocal",
+    "ccnn_check_reciprocal", "ccnn_synth_frame_device", "ccnn_gate_set", "ccnn_gate_disable", "ccnn_gate_stats",
+    "ccnn_gate_labels", "ccnn_gate_features", "ccnn_gate_gradient", "ccnn_gate_train",
 ]
 
 
@@ -151,6 +152,15 @@ def lib():
         L.ccnn_host_free.restype = None
         L.ccnn_cntk_dump_to_binary.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
         L.ccnn_check_reciprocal.argtypes = [P(ctypes.c_longlong), P(ctypes.c_longlong)]
+        L.ccnn_synth_frame_device.argtypes = [vp, ci, ci, ci, ctypes.c_size_t, ctypes.c_ulonglong, ci, ci, ci, vp, vp]
+        fp = P(ctypes.c_float)
+        L.ccnn_gate_set.argtypes = [vp, fp, ci, ctypes.c_float, ctypes.c_float]
+        L.ccnn_gate_disable.argtypes = [vp]
+        L.ccnn_gate_stats.argtypes = [vp, P(ci), P(ci), P(ci), P(ci), P(ci)]
+        L.ccnn_gate_labels.argtypes = [vp, vp, vp]
+        L.ccnn_gate_features.argtypes = [vp, ci, ci, ctypes.c_size_t, vp, vp]
+        L.ccnn_gate_gradient.argtypes = [vp, vp, vp, ci, ci, ci, ctypes.c_float, fp, fp]
+        L.ccnn_gate_train.argtypes = [fp, vp, vp, ci, ci, ci, ci, ci, ctypes.c_float, ctypes.c_float, fp]
         _lib = L
     return _lib
 

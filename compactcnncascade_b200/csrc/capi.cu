@@ -119,6 +119,26 @@ CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* ke
     return h->det.profile(iters, kernel_ms, n_kernels);
 }
 
+CCNN_API ccnn_status ccnn_gate_set(ccnn_handle h, const float* params, int n_params, float threshold, float fallback_fraction) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    return h->det.gate_set(params, n_params, threshold, fallback_fraction);
+}
+
+CCNN_API ccnn_status ccnn_gate_disable(ccnn_handle h) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    return h->det.gate_disable();
+}
+
+CCNN_API ccnn_status ccnn_gate_stats(ccnn_handle h, int* front_run, int* front_total, int* back_run, int* back_total, int* fallback) {
+    if (!h || !front_run || !front_total || !back_run || !back_total || !fallback) return CCNN_ERR_INVALID_ARG;
+    return h->det.gate_stats(front_run, front_total, back_run, back_total, fallback);
+}
+
+CCNN_API ccnn_status ccnn_gate_labels(ccnn_handle h, unsigned char* d_labels, void* stream) {
+    if (!h || !d_labels) return CCNN_ERR_INVALID_ARG;
+    return h->det.gate_labels(d_labels, (cudaStream_t)stream);
+}
+
 CCNN_API ccnn_status ccnn_get_gray_device(ccnn_handle h, const float** data, int* cols, int* rows, size_t* step) {
     if (!h || !data || !cols || !rows || !step) return CCNN_ERR_INVALID_ARG;
     return h->det.get_gray_device(data, cols, rows, step);

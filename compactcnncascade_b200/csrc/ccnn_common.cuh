@@ -239,6 +239,7 @@ struct LevelDesc {
     int pyr_base;        // first pyramid-kernel block of this level
     int pyr_wq;          // pyramid-kernel column blocks per row band
     int chunk_base;      // first candidate-scan chunk of this level
+    int octave;          // floor(log2(largest scale / scale)): the learned gate's output for this level
 };
 
 // candidate-scan chunk: response pixels of one level per compaction block, in raster order

@@ -16,6 +16,7 @@
 #include "model.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 namespace ccnn {
@@ -83,6 +84,7 @@ bool compute_scales(const ccnn_params& p, bool gray_only, int pat_h, int max_h, 
 Detector::~Detector() {
     clear();
     if (d_lnet_) cudaFree(d_lnet_);
+    if (d_gate_) cudaFree(d_gate_);
 }
 
 void Detector::free_slot(Slot& s) {
@@ -94,6 +96,12 @@ void Detector::free_slot(Slot& s) {
     cudaFree(s.d_fa);
     s.d_attr = nullptr;
     s.d_fa = nullptr;
+    cudaFree(s.gate.ambiguous);  // the bitmaps share its allocation
+    cudaFree(s.gate.prob);
+    cudaFree(s.d_front_on);
+    cudaFree(s.d_back_on);
+    s.gate = GateScratch{};
+    s.d_front_on = s.d_back_on = nullptr;
     cudaFree(s.d_s1);
     cudaFree(s.d_resp);
     cudaFree(s.d_counts);
@@ -259,6 +267,7 @@ ccnn_status Detector::init() {
 
     // capacities from the largest plans this configuration can produce
     s1_cap_ = resp_cap_ = img_cap_ = 0;
+    k1_cap_ = k2_cap_ = 0;
     chunk_cap_ = 0;
     for (int ch : {1, 3}) {
         Plan tmp;
@@ -266,6 +275,8 @@ ccnn_status Detector::init() {
         if (st != CCNN_OK) return st;
         s1_cap_ = std::max(s1_cap_, tmp.s1_floats);
         img_cap_ = std::max(img_cap_, tmp.img_floats);
+        k1_cap_ = std::max(k1_cap_, tmp.k1_tiles);
+        k2_cap_ = std::max(k2_cap_, tmp.k2_tiles);
         resp_cap_ = std::max(resp_cap_, tmp.resp_floats);
         chunk_cap_ = std::max(chunk_cap_, (int)tmp.chunks.size());
     }
@@ -329,6 +340,10 @@ ccnn_status Detector::alloc_slot(Slot& s) {
     CCNN_CUDA(cudaMalloc(&s.d_faces, sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces)));
     CCNN_CUDA(cudaMemset(s.d_faces, 0, sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces)));
     CCNN_CUDA(cudaMalloc(&s.d_nfaces, sizeof(int)));
+    if (gate_on_) {
+        ccnn_status st = alloc_gate(s);
+        if (st != CCNN_OK) return st;
+    }
     if (d_lnet_ && api_.facial_analysis) {
         CCNN_CUDA(cudaMalloc(&s.d_attr, sizeof(int4) * cand_cap_));
         CCNN_CUDA(cudaMalloc(&s.d_fa, sizeof(int) * 5 * cand_cap_));
@@ -399,6 +414,7 @@ ccnn_status Detector::build_plan(int w, int h, int ch, int num_scales, Plan* p) 
         LevelDesc& L = p->levels[scl];
         L.order = n - 1 - scl;
         L.chunk_base = (int)p->chunks.size();
+        L.octave = (int)std::floor(std::log2((double)scales_[0] / (double)scales_[scl]) + 1e-9);
         const int total = L.ow * L.oh;
         for (int s = 0; s < total; s += kCandChunk) p->chunks.push_back(make_int4(scl, s, std::min(kCandChunk, total - s), 0));
     }
@@ -441,6 +457,101 @@ ccnn_status Detector::plan_for(int w, int h, int ch, const Plan** out) {
     return CCNN_OK;
 }
 
+ccnn_status Detector::alloc_gate(Slot& s) {
+    if (s.gate.prob) return CCNN_OK;
+    const size_t w8 = (size_t)max_w_ / 8, h8 = (size_t)max_h_ / 8;
+    const size_t cells = (w8 / 2) * (h8 / 2);
+    void* words = nullptr;
+    CCNN_CUDA(cudaMalloc(&words, sizeof(uint32_t) * (1 + (size_t)gate_bitmap_words(max_w_, max_h_))));
+    s.gate.ambiguous = (int*)words;
+    s.gate.bits = (uint32_t*)words + 1;
+    CCNN_CUDA(cudaMalloc(&s.gate.prob, sizeof(float) * std::max<size_t>(1, kGK * cells)));
+    CCNN_CUDA(cudaMalloc(&s.d_front_on, std::max(1, k1_cap_)));
+    CCNN_CUDA(cudaMalloc(&s.d_back_on, std::max(1, k2_cap_)));
+    return CCNN_OK;
+}
+
+ccnn_status Detector::gate_set(const float* params, int n, float threshold, float fallback_fraction) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!params || n != kGateParams || !(threshold > 0.f && threshold < 1.f) || !(fallback_fraction >= 0.f)) {
+        set_error("gate: kGateParams parameters, a threshold in (0, 1) and a non-negative fallback fraction are needed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    if (!inited_) {
+        ccnn_status st = init();
+        if (st != CCNN_OK) return st;
+    }
+    cudaSetDevice(device_);
+    gate_params_.assign(params, params + n);
+    if (!d_gate_) CCNN_CUDA(cudaMalloc(&d_gate_, sizeof(float) * kGateParams));
+    CCNN_CUDA(cudaMemcpy(d_gate_, params, sizeof(float) * kGateParams, cudaMemcpyHostToDevice));
+    gate_on_ = true;
+    gate_thr_ = threshold;
+    gate_amb_frac_ = fallback_fraction;
+    for (auto& s : slots_) {
+        if (s.st) CCNN_CUDA(cudaStreamSynchronize(s.st));
+        ccnn_status st = alloc_gate(s);
+        if (st != CCNN_OK) return st;
+        s.exec_plan = nullptr;  // the per-frame graphs are captured again with the gate
+    }
+    return CCNN_OK;
+}
+
+ccnn_status Detector::gate_disable() {
+    std::lock_guard<std::mutex> lk(mu_);
+    gate_on_ = false;
+    for (auto& s : slots_) {
+        if (s.st) cudaStreamSynchronize(s.st);
+        s.exec_plan = nullptr;
+    }
+    return CCNN_OK;
+}
+
+ccnn_status Detector::gate_labels(uint8_t* d_labels, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(mu_);
+    Slot& s = slots_[0];
+    if (!inited_ || !s.last_plan || !detect_enabled_) {
+        set_error("no frame has been processed with stages 2 and 3");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(device_);
+    CCNN_CUDA(cudaStreamSynchronize(s.st));
+    const Plan& p = *s.last_plan;
+    CCNN_CUDA(launch_gate_labels(s.d_cands, s.d_results, s.d_ncand, (int)cand_cap_, p.d_levels, p.gw, p.gh, d_labels, st));
+    return CCNN_OK;
+}
+
+ccnn_status Detector::gate_stats(int* front_run, int* front_total, int* back_run, int* back_total, int* fallback) {
+    std::lock_guard<std::mutex> lk(mu_);
+    Slot& s = slots_[0];
+    if (!inited_ || !s.last_plan) {
+        set_error("no frame has been processed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(device_);
+    CCNN_CUDA(cudaStreamSynchronize(s.st));
+    const Plan& p = *s.last_plan;
+    const LevelDesc& last = p.levels[p.n_levels - 1];
+    const int nb = last.k2_base + last.k2_tiles_x * ((last.oh + kK2TileY - 1) / kK2TileY);
+    const int nf = last.k1_base + last.k1_tiles_x * ((last.p1h + kK1TileY - 1) / kK1TileY);
+    *front_total = nf;
+    *back_total = nb;
+    *front_run = nf;
+    *back_run = nb;
+    *fallback = 0;
+    if (!gate_on_ || !s.gate.prob || p.gw < 32 || p.gh < 32) return CCNN_OK;
+    std::vector<uint8_t> f(nf), b(nb);
+    CCNN_CUDA(cudaMemcpy(f.data(), s.d_front_on, nf, cudaMemcpyDeviceToHost));
+    CCNN_CUDA(cudaMemcpy(b.data(), s.d_back_on, nb, cudaMemcpyDeviceToHost));
+    int amb = 0;
+    CCNN_CUDA(cudaMemcpy(&amb, s.gate.ambiguous, sizeof(int), cudaMemcpyDeviceToHost));
+    *front_run = (int)std::count(f.begin(), f.end(), (uint8_t)1);
+    *back_run = (int)std::count(b.begin(), b.end(), (uint8_t)1);
+    const int w16 = (p.gw / 8) / 2, h16 = (p.gh / 8) / 2;
+    *fallback = amb > (int)(gate_amb_frac_ * (float)(w16 * h16 * kGK)) ? 1 : 0;
+    return CCNN_OK;
+}
+
 ReplayArgs Detector::replay_args(Slot& s, const Plan& p) const {
     ReplayArgs a;
     a.cands = s.d_cands;
@@ -474,9 +585,16 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
         e = launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st);
     CCNN_CUDA(e);
     CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
+    // the learned gate decides which stage-1 tiles run
+    const bool gated = gate_on_ && s.gate.prob && p.gw >= 32 && p.gh >= 32;
+    if (gated) {
+        CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_, gate_amb_frac_,
+                              s.d_back_on, s.d_front_on, s.st));
+    }
     // the back kernel counts each chunk's candidates as it writes the responses
     if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
-    CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1));
+    CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
+                            gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr));
     CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                 (int)cand_cap_, s.st));
     if (detect_enabled_)
@@ -860,9 +978,10 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     cudaSetDevice(device_);
     const Plan& p = *s.last_plan;
     constexpr int K = 7;
-    cudaEvent_t ev[K + 1];
+    cudaEvent_t ev[K + 2];  // ev[K + 1]: end of the learned gate, when it runs
     for (auto& e : ev) CCNN_CUDA(cudaEventCreate(&e));
-    double acc[K] = {0};
+    double acc[K + 1] = {0};
+    const bool gated = gate_on_ && s.gate.prob && p.gw >= 32 && p.gh >= 32;
     const ReplayArgs a = replay_args(s, p);
     for (int it = 0; it < iters; ++it) {
         CCNN_CUDA(cudaEventRecord(ev[0], s.st));
@@ -873,10 +992,16 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         CCNN_CUDA(cudaEventRecord(ev[1], s.st));
         CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
         CCNN_CUDA(cudaEventRecord(ev[2], s.st));
-        CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st));
+        if (gated) {
+            CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_,
+                                  gate_amb_frac_, s.d_back_on, s.d_front_on, s.st));
+        }
+        CCNN_CUDA(cudaEventRecord(ev[K + 1], s.st));
+        CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st, gated ? s.d_front_on : nullptr));
         CCNN_CUDA(cudaEventRecord(ev[3], s.st));
         if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
-        CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1));
+        CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
+                                     gated ? s.d_back_on : nullptr));
         CCNN_CUDA(cudaEventRecord(ev[4], s.st));
         CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                     (int)cand_cap_, s.st));
@@ -893,12 +1018,15 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         CCNN_CUDA(cudaEventSynchronize(ev[7]));
         for (int k = 0; k < K; ++k) {
             float m = 0.f;
-            CCNN_CUDA(cudaEventElapsedTime(&m, ev[k], ev[k + 1]));
+            CCNN_CUDA(cudaEventElapsedTime(&m, k == 2 ? ev[K + 1] : ev[k], ev[k + 1]));
             acc[k] += m;
         }
+        float m = 0.f;
+        CCNN_CUDA(cudaEventElapsedTime(&m, ev[2], ev[K + 1]));
+        acc[K] += m;
     }
     for (auto& e : ev) cudaEventDestroy(e);
-    for (int k = 0; k < n_ms && k < K; ++k) ms[k] = (float)(acc[k] / iters);
+    for (int k = 0; k < n_ms && k < K + 1; ++k) ms[k] = (float)(acc[k] / iters);
     return CCNN_OK;
 }
 

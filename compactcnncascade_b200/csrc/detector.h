@@ -13,6 +13,7 @@
 
 #include "../../include/ccnn.h"
 #include "../../include/ccnn_inspect.h"
+#include "../../include/ccnn_gate.h"
 #include "kernels.h"
 
 namespace ccnn {
@@ -56,6 +57,9 @@ struct Slot {
     int* d_nfaces = nullptr;
     int* h_nfaces = nullptr;   // pinned
     FaceOut* h_faces = nullptr;  // pinned, kHostFaces entries
+    GateScratch gate{};          // learned gate: features, activations, probabilities (when enabled)
+    uint8_t* d_front_on = nullptr;  // learned gate: stage-1 tile activity
+    uint8_t* d_back_on = nullptr;
     int4* d_attr = nullptr;      // facial analysis: per candidate (dropped, gender, smile, glasses)
     int* d_fa = nullptr;         // facial analysis: replay scratch (5 x candidate capacity)
     cudaGraphExec_t exec = nullptr;
@@ -79,6 +83,14 @@ class Detector {
     ccnn_status detect_batch(const ccnn_image* imgs, int n_img, bool device_input, ccnn_face* faces, int cap_per, int* n_faces,
                              float* gpu_ms);
     ccnn_status profile(int iters, float* ms, int n_ms);
+    // learned scale/region gate: parameters (kGateParams floats), probability threshold, and the
+    // fraction of ambiguous cells above which a frame falls back to the full scan
+    ccnn_status gate_set(const float* params, int n, float threshold, float fallback_fraction);
+    ccnn_status gate_disable();
+    // training labels of the last frame (slot 0): uint8 [4][gh/16][gw/16], device memory
+    ccnn_status gate_labels(uint8_t* d_labels, cudaStream_t st);
+    // stage-1 tiles the gate let run in the last frame (slot 0), of all, and whether it fell back
+    ccnn_status gate_stats(int* front_run, int* front_total, int* back_run, int* back_total, int* fallback);
 
     // Non-blocking use of one slot by a single scheduling thread (the serving loop): launch a
     // host frame on slot k, test for completion, fetch the faces. Frames must have the size the
@@ -119,6 +131,11 @@ class Detector {
     Stage1W w1_{};
     std::unique_ptr<WindowNets> wn_;
     LandmarkNet* d_lnet_ = nullptr;  // facial-analysis network (device memory), when enabled
+    float* d_gate_ = nullptr;        // learned gate parameters (device memory)
+    bool gate_on_ = false;
+    float gate_thr_ = 0.5f, gate_amb_frac_ = 0.25f;
+    std::vector<float> gate_params_;
+    ccnn_status alloc_gate(Slot& s);
     int pat_w_ = kPatW, pat_h_ = kPatH;     // stage-1 window
     int ext_w_ = kWinW, ext_h_ = kWinH;     // smallest level processed
 
@@ -133,6 +150,7 @@ class Detector {
     CascadeConfig cfg_{};
     std::vector<Slot> slots_;
     long long cand_cap_ = 0, s1_cap_ = 0, resp_cap_ = 0, img_cap_ = 0;
+    int k1_cap_ = 0, k2_cap_ = 0;
     int chunk_cap_ = 0;
     int window_grid_ = 0;
     int facial_grid_ = 0;

@@ -69,9 +69,11 @@ __device__ __forceinline__ void load_front_tile(FrontTile& T, const float* __res
 }
 
 __global__ void __launch_bounds__(256, 3) stage1_front_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ LevelTable LT,
-                                                              const float* __restrict__ limg, float* __restrict__ s1) {
+                                                              const float* __restrict__ limg, float* __restrict__ s1,
+                                                              const uint8_t* __restrict__ front_on) {
     __shared__ FrontTile T;
     const int g = LT.first + blockIdx.x;
+    if (front_on && !front_on[g]) return;  // gated off: no back tile reads this one
     const LevelDesc& L = LT.lv[find_level<&LevelDesc::k1_base>(LT, g)];
     const int t = g - L.k1_base;
     const int px0 = (t % L.k1_tiles_x) * kK1TileX;
@@ -144,7 +146,8 @@ constexpr int kBackSmemBytes = (int)sizeof(BackSmem);
 //      the pair: the 16 L3 maps (4w x 5h), the 52 hidden neurons and the output neuron.
 __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ Stage1Dup D,
                                                              const __grid_constant__ LevelTable LT, const float* __restrict__ s1,
-                                                             float* __restrict__ resp, int* __restrict__ counts, float thr) {
+                                                             float* __restrict__ resp, int* __restrict__ counts, float thr,
+                                                             const uint8_t* __restrict__ back_on) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BackSmem& S = *reinterpret_cast<BackSmem*>(smem_raw);
     const int g = LT.first + blockIdx.x;
@@ -152,6 +155,13 @@ __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_consta
     const int t = g - L.k2_base;
     const int ox0 = (t % L.k2_tiles_x) * kK2TileX;
     const int oy0 = (t / L.k2_tiles_x) * kK2TileY;
+    if (back_on && !back_on[g]) {  // gated off: responses below any stage-1 threshold
+        for (int i = threadIdx.x; i < kK2TileX * kK2TileY; i += blockDim.x) {
+            const int gx = ox0 + (i & (kK2TileX - 1)), gy = oy0 + i / kK2TileX;
+            if (gx < L.ow && gy < L.oh) resp[L.resp_off + (long long)gy * L.ow + gx] = -1e30f;
+        }
+        return;
+    }
     const int sx0 = 2 * ox0, sy0 = 2 * oy0;
 
     // A: rows of 18 float4; columns past the plane pitch and rows past p1h read as 0 (no valid
@@ -339,25 +349,26 @@ static cudaError_t launch_grouped(const LevelDesc* levels, int n_levels, int Lev
     return cudaGetLastError();
 }
 
-cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st) {
+cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st,
+                                const uint8_t* front_on) {
     return launch_grouped(
         levels, n_levels, &LevelDesc::k1_base, [](const LevelDesc& L) { return L.k1_tiles_x * ((L.p1h + kK1TileY - 1) / kK1TileY); },
-        [&](const LevelTable& T, int blocks) { stage1_front_kernel<<<blocks, 256, 0, st>>>(W, T, limg, s1); });
+        [&](const LevelTable& T, int blocks) { stage1_front_kernel<<<blocks, 256, 0, st>>>(W, T, limg, s1, front_on); });
 }
 
 cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
-                               int* counts, float thr) {
+                               int* counts, float thr, const uint8_t* back_on) {
     const Stage1Dup D = make_dup(W);
     return launch_grouped(
         levels, n_levels, &LevelDesc::k2_base, [](const LevelDesc& L) { return L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY); },
-        [&](const LevelTable& T, int blocks) { stage1_back_kernel<<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp, counts, thr); });
+        [&](const LevelTable& T, int blocks) { stage1_back_kernel<<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp, counts, thr, back_on); });
 }
 
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
-                          cudaStream_t st, int* counts, float thr) {
-    cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st);
+                          cudaStream_t st, int* counts, float thr, const uint8_t* front_on, const uint8_t* back_on) {
+    cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st, front_on);
     if (e != cudaSuccess) return e;
-    return launch_stage1_back(W, levels, n_levels, s1, resp, st, counts, thr);
+    return launch_stage1_back(W, levels, n_levels, s1, resp, st, counts, thr, back_on);
 }
 
 }  // namespace ccnn

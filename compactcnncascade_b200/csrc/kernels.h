@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "ccnn_common.cuh"
@@ -46,6 +47,22 @@ cudaError_t launch_gray_u8_resized(const uint8_t* src, int spitch, int sw, int s
                                    cudaStream_t st);
 cudaError_t launch_resize_f32(const float* src, int spitch, int sw, int sh, float* dst, int dpitch, int dw, int dh, int type,
                               cudaStream_t st);
+// learned scale/region gate (gate.cu): octaves predicted, parameter count, per-frame scratch
+constexpr int kGK = 4;
+constexpr int kGateParams = 8 * 9 + 8 + 8 * 8 * 9 + 8 + kGK * 8 + kGK;  // 700
+struct GateScratch {
+    int* ambiguous;  // cells with a probability in [thr / 4, thr); the bitmaps follow it
+    uint32_t* bits;  // per octave, per cell row: one bit per cell at or above the threshold
+    float* prob;     // kGK x (W/16 x H/16) probabilities
+};
+// words of the octave row bitmaps for a gw x gh gray frame
+int gate_bitmap_words(int gw, int gh);
+// the gate network on the frame's gray image, then the stage-1 tile activity of every level
+cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, int gw, int gh, const LevelDesc* levels, int n_levels, GateScratch sc,
+                        float thr, float amb_frac, uint8_t* back_on, uint8_t* front_on, cudaStream_t st);
+cudaError_t launch_gate_labels(const Candidate* cands, const CandResult* res, const int* ncand, int cap, const LevelDesc* d_levels, int gw, int gh,
+                               uint8_t* labels, cudaStream_t st);
+
 // every level image of a frame into the level arena (img_off / img_pitch of each descriptor);
 // blocks of kPyrCols columns x kPyrRows rows (pyr_wq column blocks per level row band)
 constexpr int kPyrCols = 256, kPyrRows = 8;
@@ -55,12 +72,16 @@ cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* g
 // parameters), level images at limg + img_off
 // counts (optional, zeroed by the caller): per candidate-scan chunk, responses > thr
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
-                          cudaStream_t st, int* counts = nullptr, float thr = 0.f);
-cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st);
+                          cudaStream_t st, int* counts = nullptr, float thr = 0.f, const uint8_t* front_on = nullptr,
+                          const uint8_t* back_on = nullptr);
+// front_on / back_on (optional): per-tile activity from the gate; inactive back tiles write
+// responses below every threshold
+cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st,
+                                const uint8_t* front_on = nullptr);
 // dynamic shared memory of the stage-1 back kernel (set once per device before any launch)
 cudaError_t stage1_setup();
 cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
-                               int* counts = nullptr, float thr = 0.f);
+                               int* counts = nullptr, float thr = 0.f, const uint8_t* back_on = nullptr);
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
                               const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st);
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,

@@ -3,6 +3,8 @@
 #ifndef CCNN_SYNTH_FRAME_H
 #define CCNN_SYNTH_FRAME_H
 #include <stdint.h>
+
+#include "synth_common.h"
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -20,6 +22,14 @@ typedef struct {
  * arguments (-1) or allocation failure (-2). */
 int ccnn_synth_frame(uint8_t* out, int width, int height, int channels, int step, uint64_t seed, int n_faces,
                      int min_face, int max_face, ccnn_synth_face* faces_out);
+
+/* The host half of the generator, shared with the device renderer: the background tables
+ * (`tables`: cos/sin of the 4 column phases [4][width] x2, then of the 4 row phases [4][height]
+ * x2, 8 * (width + height) doubles), each face's geometry (`geom`, n_faces entries), the channel
+ * jitter (4 ints) and the PCG32 state (state, inc) from which the noise takes two draws per pixel
+ * in raster order. Returns n_faces or -1. */
+int ccnn_synth_plan(int width, int height, uint64_t seed, int n_faces, int min_face, int max_face, double* tables,
+                    ccnn_synth_geom* geom, int* jitter, uint64_t* noise_state, ccnn_synth_face* faces_out);
 
 #ifdef __cplusplus
 }

@@ -95,6 +95,14 @@ CCNN_API ccnn_status ccnn_check_reciprocal(long long* mismatches, long long* che
  * ccnn_create loads. ".bin" is appended to binary_file when it has no such extension. Host-only. */
 CCNN_API ccnn_status ccnn_cntk_dump_to_binary(const char* binary_file, const char* cntk_model_dump);
 
+/* The seeded synthetic frame of the benchmarks and tests, rendered on the device into d_out
+ * (channels 1, 3 = BGR or 4 = BGRA interleaved, row pitch `step` bytes) on `stream`; byte-identical
+ * to the host generator for every seed and size. faces_out (host, may be NULL) receives n_faces
+ * records {int cx, cy, w, h; float angle_deg, contrast}. Returns when the frame is written.
+ * No reference counterpart (the reference publishes no benchmark inputs). */
+CCNN_API ccnn_status ccnn_synth_frame_device(void* d_out, int width, int height, int channels, size_t step, unsigned long long seed,
+                                             int n_faces, int min_face, int max_face, void* faces_out, void* stream);
+
 /* The permutation the detector's device sort applies to detections with the given scales
  * (perm[i] = input index placed at slot i); equals std::sort with comp(a, b) = b < a. */
 CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm);

@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared():
     names = []
-    for h in ("ccnn.h", "ccnn_inspect.h", "ccnn_server.h"):
+    for h in ("ccnn.h", "ccnn_inspect.h", "ccnn_server.h", "ccnn_gate.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
         names += re.findall(r"CCNN_API\s+[\w\s\*]+?\b(ccnn_\w+)\s*\(", src)
     return sorted(set(names))
