@@ -584,13 +584,13 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
     else
         e = launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st);
     CCNN_CUDA(e);
-    CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
-    // the learned gate decides which stage-1 tiles run
+    // the learned gate decides which stage-1 tiles run, and so which parts of the pyramid are read
     const bool gated = gate_on_ && s.gate.prob && p.gw >= 32 && p.gh >= 32;
     if (gated) {
         CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_, gate_amb_frac_,
                               s.d_back_on, s.d_front_on, s.st));
     }
+    CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st, gated ? s.d_front_on : nullptr));
     // the back kernel counts each chunk's candidates as it writes the responses
     if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
     CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
@@ -990,13 +990,14 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         else
             CCNN_CUDA(launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st));
         CCNN_CUDA(cudaEventRecord(ev[1], s.st));
-        CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
-        CCNN_CUDA(cudaEventRecord(ev[2], s.st));
         if (gated) {
             CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_,
                                   gate_amb_frac_, s.d_back_on, s.d_front_on, s.st));
         }
         CCNN_CUDA(cudaEventRecord(ev[K + 1], s.st));
+        CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st,
+                                 gated ? s.d_front_on : nullptr));
+        CCNN_CUDA(cudaEventRecord(ev[2], s.st));
         CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st, gated ? s.d_front_on : nullptr));
         CCNN_CUDA(cudaEventRecord(ev[3], s.st));
         if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
@@ -1018,11 +1019,11 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         CCNN_CUDA(cudaEventSynchronize(ev[7]));
         for (int k = 0; k < K; ++k) {
             float m = 0.f;
-            CCNN_CUDA(cudaEventElapsedTime(&m, k == 2 ? ev[K + 1] : ev[k], ev[k + 1]));
+            CCNN_CUDA(cudaEventElapsedTime(&m, k == 1 ? ev[K + 1] : ev[k], ev[k + 1]));
             acc[k] += m;
         }
         float m = 0.f;
-        CCNN_CUDA(cudaEventElapsedTime(&m, ev[2], ev[K + 1]));
+        CCNN_CUDA(cudaEventElapsedTime(&m, ev[1], ev[K + 1]));
         acc[K] += m;
     }
     for (auto& e : ev) cudaEventDestroy(e);

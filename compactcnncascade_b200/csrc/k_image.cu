@@ -100,12 +100,31 @@ cudaError_t launch_gray_u8_resized(const uint8_t* src, int spitch, int sw, int s
 // weights for all its rows, and a warp's loads and stores walk consecutive columns. Columns between
 // the level width and the row pitch are written as zeros.
 __global__ void __launch_bounds__(kPyrCols) pyramid_kernel(const __grid_constant__ LevelTable LT, const float* __restrict__ gray,
-                                                           int gpitch, int gw, int gh, float* __restrict__ limg) {
+                                                           int gpitch, int gw, int gh, float* __restrict__ limg,
+                                                           const uint8_t* __restrict__ front_on) {
     const int g = LT.first + blockIdx.x;
     const LevelDesc& L = LT.lv[find_level<&LevelDesc::pyr_base>(LT, g)];
     const int local = g - L.pyr_base;
     const int rb = local / L.pyr_wq;
-    const int x = (local - rb * L.pyr_wq) * kPyrCols + threadIdx.x;
+    const int cb = local - rb * L.pyr_wq;
+    if (front_on) {
+        // with the learned gate only the stage-1 front tiles that run read the level image: a block
+        // that none of them reads is left out (front tile (tx, ty) reads rows [32 ty, 32 ty + 35)
+        // and columns [64 tx, 64 tx + 68))
+        const int ty0 = max(0, (kPyrRows * rb - (2 * kK1TileY + 3) + 2 * kK1TileY) / (2 * kK1TileY));
+        const int ty1 = min((L.p1h + kK1TileY - 1) / kK1TileY - 1, (kPyrRows * rb + kPyrRows - 1) / (2 * kK1TileY));
+        const int tx0 = max(0, (kPyrCols * cb - (2 * kK1TileX + 4) + 2 * kK1TileX) / (2 * kK1TileX));
+        const int tx1 = min(L.k1_tiles_x - 1, (kPyrCols * cb + kPyrCols - 1) / (2 * kK1TileX));
+        bool need = false;
+        for (int ty = ty0; ty <= ty1 && !need; ++ty)
+            for (int tx = tx0; tx <= tx1; ++tx)
+                if (front_on[L.k1_base + ty * L.k1_tiles_x + tx]) {
+                    need = true;
+                    break;
+                }
+        if (!need) return;
+    }
+    const int x = cb * kPyrCols + threadIdx.x;
     if (x >= L.img_pitch) return;
     float* out = limg + L.img_off + x;
     const int y0 = rb * kPyrRows;
@@ -137,7 +156,7 @@ __global__ void __launch_bounds__(kPyrCols) pyramid_kernel(const __grid_constant
 }
 
 cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* gray, int gpitch, int gw, int gh, float* limg,
-                           cudaStream_t st) {
+                           cudaStream_t st, const uint8_t* front_on) {
     for (int g0 = 0; g0 < n_levels; g0 += kParamLevels) {
         LevelTable T;
         T.n = n_levels - g0 < kParamLevels ? n_levels - g0 : kParamLevels;
@@ -145,7 +164,7 @@ cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* g
         T.first = T.lv[0].pyr_base;
         const LevelDesc& last = T.lv[T.n - 1];
         const int blocks = last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows) - T.first;
-        if (blocks > 0) pyramid_kernel<<<blocks, kPyrCols, 0, st>>>(T, gray, gpitch, gw, gh, limg);
+        if (blocks > 0) pyramid_kernel<<<blocks, kPyrCols, 0, st>>>(T, gray, gpitch, gw, gh, limg, front_on);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

@@ -11,9 +11,9 @@
 //   (:1655-1706) and the accept rule (:1709-1725); score s0 + k1*max(-1.7159, m1) + k2*max(-1.7159, m2).
 //
 // Every candidate is evaluated speculatively: both nets on both the first and the retry window,
-// as four independent CTA work items. Which of them the reference would have reached (early
-// exits, retry, drop_detect) is decided by the replay kernel, so the verdicts are the same while
-// all items run in parallel.
+// as independent CTA work items. Which of them the reference would have reached (early exits,
+// retry, drop_detect) is decided by the replay kernel, so the verdicts are the same while all
+// items run in parallel.
 //
 // One CTA (256 threads) per work item, persistent over the item list. The networks run
 // entirely in shared memory: L1 (6 maps, 44x48 -> pooled 22x24), neighbour sums, L2 (12 maps,
@@ -256,9 +256,11 @@ __device__ void prepare_window(const WinArgs& a, WindowSmem& S, const Candidate&
 }
 
 // One work item = (candidate, window): window 0 is the first crop, window 1 the shrunken retry
-// crop. Both windows of a candidate run in parallel (the retry is speculative: whether the
-// reference reaches it is decided by the replay kernel). Inside an item, stage 3 runs only when
-// stage 2 does not end the check (the reference's early exits, cnn_detector_v3.cpp:1698-1706);
+// crop. Both windows of a candidate run in parallel (the retry is speculative: the verdict reads it
+// only when window 0 is rejected, cnn_detector_v3.cpp:1806-1811); running it on demand instead
+// would save the ~10 % of retries whose first window accepts but put the two windows of a rejected
+// candidate one after the other, doubling the kernel's latency. Inside an item, stage 3 runs only
+// when stage 2 does not end the check (the reference's early exits, cnn_detector_v3.cpp:1698-1706);
 // otherwise its slot keeps (max -10, count 0), exactly what the reference leaves behind.
 __global__ void __launch_bounds__(kWT, 4) window_kernel(const __grid_constant__ WindowNets N, const WinArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -67,7 +67,8 @@ cudaError_t launch_gate_labels(const Candidate* cands, const CandResult* res, co
 // blocks of kPyrCols columns x kPyrRows rows (pyr_wq column blocks per level row band)
 constexpr int kPyrCols = 256, kPyrRows = 8;
 cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* gray, int gpitch, int gw, int gh, float* limg,
-                           cudaStream_t st);
+                           cudaStream_t st,
+                           const uint8_t* front_on = nullptr);
 // stage-1 net over all levels; `levels` is a HOST array (the descriptors travel as kernel
 // parameters), level images at limg + img_off
 // counts (optional, zeroed by the caller): per candidate-scan chunk, responses > thr

@@ -29,7 +29,17 @@ __device__ __forceinline__ void window_geometry(const Candidate& cd, float inv_s
     geo[3] = min(max(y + height, 0), gh) - ry;
 }
 
-// stage-2/3 verdict of one candidate from its four speculative (max, count) pairs, applying the
+// the accept rule of one window from its stage-2 and stage-3 counts (cnn_detector_v3.cpp:1709-1725)
+__device__ __forceinline__ bool window_accepts(int k1, int k2, int mn, const CascadeConfig& C) {
+    switch (C.type_check) {
+        case 0: return k1 >= mn || k2 >= mn;
+        case 1: return (k1 >= mn && k2 > 0) || (k1 > 0 && k2 >= mn);
+        case 2: return k1 >= mn && k2 >= mn;
+    }
+    return false;
+}
+
+// stage-2/3 verdict of one candidate from its (max, count) pairs, applying the
 // reference's order: stage 2, early exits (:1698-1706), stage 3, accept rule (:1709-1725), retry
 // with the shrunken window when rejected and double_check is on (:1806-1811)
 __device__ __forceinline__ CandResult verdict(const WinOut* w, const Candidate& cd, float scale, const CascadeConfig& C) {
@@ -46,13 +56,7 @@ __device__ __forceinline__ CandResult verdict(const WinOut* w, const Candidate& 
         const bool stop = (C.type_check == 0 && k1 >= mn) || (C.type_check > 0 && k1 <= 0) || (C.type_check == 2 && k1 < mn);
         const float max2 = stop ? -10.f : w[2 * mod + 1].max;
         const int k2 = stop ? 0 : w[2 * mod + 1].knn;
-        bool flag = false;
-        switch (C.type_check) {
-            case 0: flag = (k1 >= mn || k2 >= mn); break;
-            case 1: flag = (k1 >= mn && k2 > 0) || (k1 > 0 && k2 >= mn); break;
-            case 2: flag = (k1 >= mn && k2 >= mn); break;
-        }
-        if (flag) {
+        if (window_accepts(k1, k2, mn, C)) {
             const float m1 = (-1.7159f < max1) ? max1 : -1.7159f;
             const float m2 = (-1.7159f < max2) ? max2 : -1.7159f;
             r.accepted = mod + 1;
