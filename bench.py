@@ -76,7 +76,7 @@ def serve_frames(per_res, seed0=900_000):
     return out
 
 
-def run_serving(frames_by_res, rate, n_frames, seed=1):
+def run_serving(frames_by_res, rate, n_frames, seed=1, gate=None):
     """Poisson arrivals (seeded exponential inter-arrival times) of frames drawn from the
     resolution mix; every frame goes through the serving loop (ccnn_server_*). Returns latency
     percentiles (submit -> result on the device side, measured by the server) and throughput."""
@@ -86,6 +86,8 @@ def run_serving(frames_by_res, rate, n_frames, seed=1):
     p.min_face_height, p.max_face_height, p.scale_factor = MIN_FACE, MAX_FACE, SCALE_FACTOR
     p.detect_mode = 1
     srv = ccnn.FaceServer(p, hbm_budget_bytes=32 << 30, slots_per_class=4)
+    if gate is not None:
+        srv.set_gate(*gate)
     pinned = {res: [] for res in frames_by_res}
     for res, imgs in frames_by_res.items():
         for img in imgs:
@@ -121,6 +123,65 @@ def run_serving(frames_by_res, rate, n_frames, seed=1):
            "p50_ms": round(float(np.percentile(allv, 50)), 3), "p99_ms": round(float(np.percentile(allv, 99)), 3),
            "per_resolution": {f"{r[0]}x{r[1]}": {"frames": len(v), "p50_ms": round(float(np.percentile(v, 50)), 3),
                                                  "p99_ms": round(float(np.percentile(v, 99)), 3)} for r, v in lat.items() if v}}
+    return out
+
+
+# ---------------- batched pyramid: many uneven levels ----------------
+
+BATCHED = [((3840, 2160), 60, 20, 600), ((4800, 2400), 60, 20, 600)]
+
+
+def run_batched_pyramid(dev, args):
+    """Scale 1.05, min face 20, no max face (the largest level is an upsampled 1.35x copy): 80+
+    pyramid levels of uneven sizes per frame, run as 8-frame pipelined batches of device-resident
+    frames (rendered on the device by the seeded generator). Device time from the library's events."""
+    import torch
+    import compactcnncascade_b200 as ccnn
+    from compactcnncascade_b200 import _capi
+    L = _capi.lib()
+    out = {}
+    B = args.batched_frames
+    for (w, h), nf, lo, hi in BATCHED:
+        p = ccnn.default_params()
+        p.max_image_width, p.max_image_height = w, h
+        p.min_face_height, p.max_face_height, p.scale_factor = 20, 0, 1.05
+        p.detect_mode = 1
+        p.cuda_device_id = dev
+        det = ccnn.FaceDetector()
+        if det.Init(p) != 0:
+            raise SystemExit(f"detector init failed: {_capi.last_error()}")
+        frames = []
+        for i in range(B):
+            t = torch.empty((h, w, 3), dtype=torch.uint8, device=f"cuda:{dev}")
+            ccnn.synth_frame_device(t.data_ptr(), w, h, 700_000 + 1000 * w + i, nf, lo, hi)
+            frames.append(t)
+        arr = (_capi.Image * B)(*[_capi.Image(w, h, 3, t.data_ptr(), w * 3) for t in frames])
+        cap = 1024
+        faces = (_capi.Face * (B * cap))()
+        nfaces = (ctypes.c_int * B)()
+        gms = ctypes.c_float()
+
+        def step():
+            if L.ccnn_detect_device_batch(det._h, arr, B, faces, cap, nfaces, ctypes.byref(gms)) < 0:
+                raise SystemExit(f"ccnn_detect_device_batch failed: {_capi.last_error()}")
+            return gms.value
+
+        for _ in range(max(3, args.warmup)):
+            step()
+        steps = max(3, args.steps // 4)
+        ms = sum(step() for _ in range(steps))
+        lat = []
+        for i in range(10):
+            t0 = time.perf_counter()
+            det.DetectDevice(frames[i % B].data_ptr(), w, h, 3, w * 3)
+            lat.append((time.perf_counter() - t0) * 1e3)
+        out[f"{w}x{h}"] = {"frames_per_s": round(steps * B / (ms / 1e3), 1), "levels": len(det.levels()),
+                           "faces_per_frame": round(sum(nfaces[j] for j in range(B)) / B, 1),
+                           "p50_ms": round(float(np.percentile(lat[2:], 50)), 3), "batch": B, "steps": steps}
+        det.Clear()
+    out["note"] = ("seeded frames with 60 face patches 20-600 px, scale 1.05, min face 20, no max face; all levels of a "
+                   "frame in one launch per kernel (level tables of at most 32 levels per launch), every frame's chain "
+                   "a CUDA graph, 8 frames in flight; device-resident frames, device time from CUDA events")
     return out
 
 
@@ -288,6 +349,8 @@ def main():
     ap.add_argument("--no-gate", action="store_true", help="skip the batched+gated phase")
     ap.add_argument("--gate-threshold", type=float, default=None, help="gate probability threshold (default: the weights' own)")
     ap.add_argument("--gate-fallback", type=float, default=0.25, help="ambiguous-cell fraction that falls back to the full scan")
+    ap.add_argument("--batched-frames", type=int, default=8,
+                    help="frames per batch of the batched-pyramid phase (3840x2160 and 4800x2400; 0: skip)")
     ap.add_argument("--serving", action="store_true",
                     help="only the serving sweep: 10,000 mixed-resolution frames at 500, 1000, 2000, 4000 frames/s")
     args = ap.parse_args()
@@ -508,7 +571,12 @@ def main():
                  "note": "same frames, detector and batch as `value`, with the learned gate (include/ccnn_gate.h) skipping "
                          "stage-1 tiles; box recall = plain-cascade boxes matched by a gated box at IoU >= 0.5"}
 
+    batched = run_batched_pyramid(dev, args) if (rank == 0 and args.batched_frames > 0) else None
     serving = run_serving(sframes, args.serve_rate, args.serve_frames) if sframes else None
+    serving_gated = None
+    if serving and gated:
+        serving_gated = run_serving(sframes, args.serve_rate, args.serve_frames,
+                                    gate=(gate_mod.load(), gated["threshold"], args.gate_fallback))
 
     line = {
         "metric": METRIC,
@@ -539,9 +607,14 @@ def main():
     }
     if gated:
         line["gated"] = gated
+    if batched:
+        line["batched_pyramid"] = batched
     if serving:
         line["serving"] = dict(serving, note="serving loop (ccnn_server_*): Poisson arrivals of mixed 640x480/1280x720/"
                                              "1920x1080/3840x2160 frames at 30/30/30/10 %, latency = submit to result")
+    if serving_gated:
+        line["serving"]["gated"] = dict(serving_gated, note="the same stream with the learned gate on in every resolution "
+                                                            "class (weights trained at 1080p; recall measured at 1080p only)")
     if cpu:
         fps, workers, nfr, secs, fast = cpu
         line["cpu_baseline"] = {"value": round(fps, 3), "unit": "frames/s", "cores": workers, "kind": "reference",

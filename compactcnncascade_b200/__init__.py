@@ -257,6 +257,12 @@ class FaceServer:
         except Exception:
             pass
 
+    def set_gate(self, params, threshold=0.5, fallback_fraction=0.25):
+        """The learned gate (FaceDetector.setGate) for every resolution class; before the first submit."""
+        p = np.ascontiguousarray(params, np.float32)
+        _capi.check(_capi.lib().ccnn_server_set_gate(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), p.size,
+                                                     float(threshold), float(fallback_fraction)), "ccnn_server_set_gate")
+
     def submit(self, img):
         """Queues a uint8 HxW / HxWxC frame; returns its ticket, or None when the queue is full."""
         im, a = _as_image(img)

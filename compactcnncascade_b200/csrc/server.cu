@@ -16,6 +16,7 @@
 #include <list>
 #include <memory>
 #include <thread>
+#include <vector>
 #include <unordered_map>
 
 #include "../../include/ccnn_server.h"
@@ -57,6 +58,7 @@ class Server {
     ccnn_status create(const ccnn_params& p, const char* const* models, const ccnn_server_config* cfg);
     ~Server();
     ccnn_status submit(const ccnn_image& img, long long* ticket);
+    ccnn_status set_gate(const float* params, int n, float threshold, float fallback_fraction);
     ccnn_status take(long long ticket, bool block, ccnn_face* faces, int cap, int* n, double* lat);
     void stats(ccnn_server_stats* out);
 
@@ -69,6 +71,8 @@ class Server {
     void fail(const std::shared_ptr<Request>& r, ccnn_status st, const std::string& why);
 
     ccnn_params params_{};
+    std::vector<float> gate_;  // learned-gate parameters for every class (empty: full scan)
+    float gate_thr_ = 0.5f, gate_fb_ = 0.25f;
     std::string models_[3];
     bool has_models_ = false;
     size_t budget_ = 0;
@@ -119,6 +123,23 @@ Server::~Server() {
     }
     cv_work_.notify_all();
     if (thread_.joinable()) thread_.join();
+}
+
+// The gate is fixed before the first frame: every class is then created with it.
+ccnn_status Server::set_gate(const float* params, int n, float threshold, float fallback_fraction) {
+    if (!params || n != kGateParams || !(threshold > 0.f && threshold < 1.f) || !(fallback_fraction >= 0.f)) {
+        set_error("gate: kGateParams parameters, a threshold in (0, 1) and a non-negative fallback fraction are needed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> lk(mu_);
+    if (submitted_ > 0) {
+        set_error("the gate must be set before the first frame is submitted");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    gate_.assign(params, params + n);
+    gate_thr_ = threshold;
+    gate_fb_ = fallback_fraction;
+    return CCNN_OK;
 }
 
 ccnn_status Server::submit(const ccnn_image& img, long long* ticket) {
@@ -218,6 +239,10 @@ ccnn_status Server::make_class(const ccnn_image& img, ResClass** out, bool* retr
         c->det.reset(new Detector());
         ccnn_status st = c->det->create(p, has_models_ ? mp : nullptr, slots, img.channels != 1);
         if (st != CCNN_OK) return st;
+        if (!gate_.empty()) {
+            st = c->det->gate_set(gate_.data(), (int)gate_.size(), gate_thr_, gate_fb_);
+            if (st != CCNN_OK) return st;
+        }
         c->bytes = c->det->slot_bytes();
         // make room: evict idle classes, least recently used first
         while (held_ + c->bytes > budget_) {
@@ -391,6 +416,15 @@ extern "C" CCNN_API ccnn_status ccnn_server_create(const ccnn_params* params, co
     if (st != CCNN_OK) return st;
     *out = s.release();
     return CCNN_OK;
+}
+
+extern "C" CCNN_API ccnn_status ccnn_server_set_gate(ccnn_server s, const float* params, int n_params, float threshold,
+                                                     float fallback_fraction) {
+    if (!s) {
+        ccnn::set_error("invalid arguments");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    return s->srv.set_gate(params, n_params, threshold, fallback_fraction);
 }
 
 extern "C" CCNN_API ccnn_status ccnn_server_destroy(ccnn_server s) {

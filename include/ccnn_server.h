@@ -47,6 +47,9 @@ typedef struct {
 CCNN_API ccnn_status ccnn_server_create(const ccnn_params* params, const char* const* model_paths, const ccnn_server_config* config,
                                         ccnn_server* out);
 CCNN_API ccnn_status ccnn_server_destroy(ccnn_server s);
+/* Turns the learned gate (include/ccnn_gate.h, ccnn_gate_set) on for every resolution class the
+ * server creates; only before the first frame is submitted (CCNN_ERR_INVALID_ARG after). */
+CCNN_API ccnn_status ccnn_server_set_gate(ccnn_server s, const float* params, int n_params, float threshold, float fallback_fraction);
 /* Queues one frame; *ticket identifies its result. CCNN_BUSY when max_queue requests wait. */
 CCNN_API ccnn_status ccnn_server_submit(ccnn_server s, const ccnn_image* img, long long* ticket);
 /* Result of a ticket: CCNN_PENDING while unfinished (poll), or blocks until it is done (wait).

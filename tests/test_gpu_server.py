@@ -63,6 +63,32 @@ def test_mixed_resolutions_match_alone(mix):
     srv.close()
 
 
+def test_gated_server_matches_gated_detector(mix):
+    """With the learned gate on, every frame of a mixed stream gives what a gated detector sized for
+    it gives alone; the gate cannot be changed once frames were submitted."""
+    from compactcnncascade_b200 import gate
+    if not __import__("os").path.exists(gate.WEIGHTS_1080P):
+        pytest.skip("no trained gate weights in the package")
+    w, thr = gate.load(), 0.2
+    alone = []
+    for f in mix:
+        p = _params()
+        p.max_image_width, p.max_image_height = f.shape[1], f.shape[0]
+        d = ccnn.FaceDetector()
+        assert d.Init(p) == 0
+        d.setGate(w, thr, 0.25)
+        alone.append(d.Detect(f))
+        d.Clear()
+    srv = ccnn.FaceServer(_params(), slots_per_class=2)
+    srv.set_gate(w, thr, 0.25)
+    tickets = [(i, srv.submit(mix[i])) for i in (2, 0, 1, 4, 3, 2, 0)]
+    for i, t in tickets:
+        assert srv.wait(t)[0] == alone[i], f"frame {i} differs in the mix"
+    with pytest.raises(ccnn.CCNNError):
+        srv.set_gate(w, thr, 0.25)
+    srv.close()
+
+
 def test_server_frame_matches_oracle(mix):
     srv = ccnn.FaceServer(_params())
     t = srv.submit(mix[0])
