@@ -242,6 +242,31 @@ struct LevelDesc {
     int octave;          // floor(log2(largest scale / scale)): the learned gate's output for this level
 };
 
+// The learned gate's per-octave cell bitmaps as the stage-1 back kernel reads them: bits == nullptr
+// means no gate. Rows of wwords words, one bit per 16x16-pixel cell of the frame.
+struct GateCells {
+    const uint32_t* bits;
+    const int* ambiguous;  // frames with more ambiguous cells than amb_limit are scanned in full
+    int amb_limit, wwords, w16, h16;
+};
+
+// any set bit of octave row bitmaps `B` in cells [cx0, cx1] x [cy0, cy1]
+__device__ __forceinline__ bool gate_any_bit(const uint32_t* __restrict__ B, int wwords, int cx0, int cx1, int cy0, int cy1) {
+    if (cx0 > cx1 || cy0 > cy1) return false;
+    const int w0 = cx0 >> 5, w1 = cx1 >> 5;
+    const uint32_t m0 = 0xffffffffu << (cx0 & 31), m1 = 0xffffffffu >> (31 - (cx1 & 31));
+    for (int y = cy0; y <= cy1; ++y) {
+        const uint32_t* row = B + (long long)y * wwords;
+        for (int w = w0; w <= w1; ++w) {
+            uint32_t m = 0xffffffffu;
+            if (w == w0) m &= m0;
+            if (w == w1) m &= m1;
+            if (row[w] & m) return true;
+        }
+    }
+    return false;
+}
+
 // candidate-scan chunk: response pixels of one level per compaction block, in raster order
 constexpr int kCandChunk = 2048;
 

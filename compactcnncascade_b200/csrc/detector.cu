@@ -594,7 +594,8 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
     // the back kernel counts each chunk's candidates as it writes the responses
     if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
     CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
-                            gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr));
+                            gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr,
+                            gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}));
     CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                 (int)cand_cap_, s.st));
     if (detect_enabled_)
@@ -1002,7 +1003,7 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         CCNN_CUDA(cudaEventRecord(ev[3], s.st));
         if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
         CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
-                                     gated ? s.d_back_on : nullptr));
+                                     gated ? s.d_back_on : nullptr, gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}));
         CCNN_CUDA(cudaEventRecord(ev[4], s.st));
         CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                     (int)cand_cap_, s.st));

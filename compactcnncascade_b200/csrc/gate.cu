@@ -351,23 +351,6 @@ __global__ void __launch_bounds__(256) gate_infer_kernel(const float* __restrict
     if (tid == 0 && samb) atomicAdd(ambiguous, samb);
 }
 
-// any set bit of octave row bitmaps `B` (wwords words a row) in cells [cx0, cx1] x [cy0, cy1]
-__device__ __forceinline__ bool any_bit(const uint32_t* __restrict__ B, int wwords, int cx0, int cx1, int cy0, int cy1) {
-    if (cx0 > cx1 || cy0 > cy1) return false;
-    const int w0 = cx0 >> 5, w1 = cx1 >> 5;
-    const uint32_t m0 = 0xffffffffu << (cx0 & 31), m1 = 0xffffffffu >> (31 - (cx1 & 31));
-    for (int y = cy0; y <= cy1; ++y) {
-        const uint32_t* row = B + (long long)y * wwords;
-        for (int w = w0; w <= w1; ++w) {
-            uint32_t m = 0xffffffffu;
-            if (w == w0) m &= m0;
-            if (w == w1) m &= m1;
-            if (row[w] & m) return true;
-        }
-    }
-    return false;
-}
-
 // cells within one cell of the window centres ((4*o + 11.5) / s, (4*o + 13.5) / s) of the
 // response pixels o in [ox0, ox1] x [oy0, oy1] of a level
 __device__ __forceinline__ void centre_cells(const LevelDesc& L, int ox0, int ox1, int oy0, int oy1, int w16, int h16, int* r) {
@@ -397,7 +380,7 @@ __global__ void gate_mask_kernel(const __grid_constant__ LevelTable LT, int nb, 
         const int ox0 = (t % L.k2_tiles_x) * kK2TileX, oy0 = (t / L.k2_tiles_x) * kK2TileY;
         int r[4];
         centre_cells(L, ox0, min(ox0 + kK2TileX, L.ow) - 1, oy0, min(oy0 + kK2TileY, L.oh) - 1, w16, h16, r);
-        back_on[g] = any_bit(bits + (long long)min(L.octave, kGK - 1) * h16 * wwords, wwords, r[0], r[1], r[2], r[3]) ? 1 : 0;
+        back_on[g] = gate_any_bit(bits + (long long)min(L.octave, kGK - 1) * h16 * wwords, wwords, r[0], r[1], r[2], r[3]) ? 1 : 0;
         return;
     }
     const int g = LT.lv[0].k1_base + (i - nb);
@@ -419,10 +402,22 @@ __global__ void gate_mask_kernel(const __grid_constant__ LevelTable LT, int nb, 
     }
     int r[4];
     centre_cells(L, bx0 * kK2TileX, min((bx1 + 1) * kK2TileX, L.ow) - 1, by0 * kK2TileY, min((by1 + 1) * kK2TileY, L.oh) - 1, w16, h16, r);
-    front_on[g] = any_bit(bits + (long long)min(L.octave, kGK - 1) * h16 * wwords, wwords, r[0], r[1], r[2], r[3]) ? 1 : 0;
+    front_on[g] = gate_any_bit(bits + (long long)min(L.octave, kGK - 1) * h16 * wwords, wwords, r[0], r[1], r[2], r[3]) ? 1 : 0;
 }
 
 }  // namespace
+
+GateCells gate_cells(GateScratch sc, int gw, int gh, float amb_frac) {
+    const int w16 = (gw / 8) / 2, h16 = (gh / 8) / 2;
+    GateCells c;
+    c.bits = sc.bits;
+    c.ambiguous = sc.ambiguous;
+    c.amb_limit = (int)(amb_frac * (float)(w16 * h16 * kGK));
+    c.wwords = (w16 + 31) / 32;
+    c.w16 = w16;
+    c.h16 = h16;
+    return c;
+}
 
 int gate_bitmap_words(int gw, int gh) {
     const int w16 = (gw / 8) / 2, h16 = (gh / 8) / 2;
@@ -438,7 +433,7 @@ cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, in
     if (e != cudaSuccess) return e;
     gate_infer_kernel<<<dim3((w8 + kIX - 1) / kIX, (h8 + kIY - 1) / kIY), 256, 0, st>>>(d_params, gray, gpitch, w8, h8, thr, 0.25f * thr, sc.bits,
                                                                                        wwords, sc.prob, sc.ambiguous);
-    const int amb_limit = (int)(amb_frac * (float)(w16 * h16 * kGK));
+    const int amb_limit = gate_cells(sc, gw, gh, amb_frac).amb_limit;
     for (int g0 = 0; g0 < n_levels; g0 += kParamLevels) {
         LevelTable T;
         T.n = n_levels - g0 < kParamLevels ? n_levels - g0 : kParamLevels;

@@ -147,7 +147,7 @@ constexpr int kBackSmemBytes = (int)sizeof(BackSmem);
 __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ Stage1Dup D,
                                                              const __grid_constant__ LevelTable LT, const float* __restrict__ s1,
                                                              float* __restrict__ resp, int* __restrict__ counts, float thr,
-                                                             const uint8_t* __restrict__ back_on) {
+                                                             const uint8_t* __restrict__ back_on, const GateCells cells) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BackSmem& S = *reinterpret_cast<BackSmem*>(smem_raw);
     const int g = LT.first + blockIdx.x;
@@ -280,14 +280,27 @@ __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_consta
     const f2_t r = (W.af == 0.f) ? f2_add(f2_mul(half, c, nz), half) : f2_mul(f2_ld(D.afd), c, nz);
     const int gx = ox0 + x, gy = oy0 + y;
     if (gx < L.ow) {
+        float rv[2] = {f2_lo(r), f2_hi(r)};
+        if (cells.bits && (rv[0] > thr || rv[1] > thr) && *cells.ambiguous <= cells.amb_limit) {
+            // learned gate, per candidate: its window centre ((4x + 11.5) / s, (4y + 13.5) / s) needs a
+            // likely cell of its octave within one cell
+            const uint32_t* B = cells.bits + (long long)min(L.octave, kGK - 1) * cells.h16 * cells.wwords;
+            const int cx = (int)((4.f * gx + 11.5f) * L.inv_scale) / 16;
+            for (int k = 0; k < 2; ++k) {
+                if (!(rv[k] > thr)) continue;
+                const int cy = (int)((4.f * (gy + k) + 13.5f) * L.inv_scale) / 16;
+                if (!gate_any_bit(B, cells.wwords, max(0, cx - 1), min(cells.w16 - 1, cx + 1), max(0, cy - 1), min(cells.h16 - 1, cy + 1)))
+                    rv[k] = -1e30f;
+            }
+        }
         // candidates (response > treshold_1) are counted per scan chunk for the compaction
         if (gy < L.oh) {
-            resp[L.resp_off + (long long)gy * L.ow + gx] = f2_lo(r);
-            if (counts && f2_lo(r) > thr) atomicAdd(&counts[L.chunk_base + (gy * L.ow + gx) / kCandChunk], 1);
+            resp[L.resp_off + (long long)gy * L.ow + gx] = rv[0];
+            if (counts && rv[0] > thr) atomicAdd(&counts[L.chunk_base + (gy * L.ow + gx) / kCandChunk], 1);
         }
         if (gy + 1 < L.oh) {
-            resp[L.resp_off + (long long)(gy + 1) * L.ow + gx] = f2_hi(r);
-            if (counts && f2_hi(r) > thr) atomicAdd(&counts[L.chunk_base + ((gy + 1) * L.ow + gx) / kCandChunk], 1);
+            resp[L.resp_off + (long long)(gy + 1) * L.ow + gx] = rv[1];
+            if (counts && rv[1] > thr) atomicAdd(&counts[L.chunk_base + ((gy + 1) * L.ow + gx) / kCandChunk], 1);
         }
     }
 }
@@ -357,18 +370,18 @@ cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n
 }
 
 cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
-                               int* counts, float thr, const uint8_t* back_on) {
+                               int* counts, float thr, const uint8_t* back_on, GateCells cells) {
     const Stage1Dup D = make_dup(W);
     return launch_grouped(
         levels, n_levels, &LevelDesc::k2_base, [](const LevelDesc& L) { return L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY); },
-        [&](const LevelTable& T, int blocks) { stage1_back_kernel<<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp, counts, thr, back_on); });
+        [&](const LevelTable& T, int blocks) { stage1_back_kernel<<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp, counts, thr, back_on, cells); });
 }
 
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
-                          cudaStream_t st, int* counts, float thr, const uint8_t* front_on, const uint8_t* back_on) {
+                          cudaStream_t st, int* counts, float thr, const uint8_t* front_on, const uint8_t* back_on, GateCells cells) {
     cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st, front_on);
     if (e != cudaSuccess) return e;
-    return launch_stage1_back(W, levels, n_levels, s1, resp, st, counts, thr, back_on);
+    return launch_stage1_back(W, levels, n_levels, s1, resp, st, counts, thr, back_on, cells);
 }
 
 }  // namespace ccnn

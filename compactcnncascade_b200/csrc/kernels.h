@@ -58,6 +58,8 @@ struct GateScratch {
 // words of the octave row bitmaps for a gw x gh gray frame
 int gate_bitmap_words(int gw, int gh);
 // the gate network on the frame's gray image, then the stage-1 tile activity of every level
+// the cell bitmaps of a gated frame for the stage-1 back kernel
+GateCells gate_cells(GateScratch sc, int gw, int gh, float amb_frac);
 cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, int gw, int gh, const LevelDesc* levels, int n_levels, GateScratch sc,
                         float thr, float amb_frac, uint8_t* back_on, uint8_t* front_on, cudaStream_t st);
 cudaError_t launch_gate_labels(const Candidate* cands, const CandResult* res, const int* ncand, int cap, const LevelDesc* d_levels, int gw, int gh,
@@ -72,9 +74,11 @@ cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* g
 // stage-1 net over all levels; `levels` is a HOST array (the descriptors travel as kernel
 // parameters), level images at limg + img_off
 // counts (optional, zeroed by the caller): per candidate-scan chunk, responses > thr
+// cells (optional): the gate's cell bitmaps; a response above thr whose window centre has no likely
+// cell within one cell of it (in its level's octave) is written below every threshold
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
                           cudaStream_t st, int* counts = nullptr, float thr = 0.f, const uint8_t* front_on = nullptr,
-                          const uint8_t* back_on = nullptr);
+                          const uint8_t* back_on = nullptr, GateCells cells = GateCells{});
 // front_on / back_on (optional): per-tile activity from the gate; inactive back tiles write
 // responses below every threshold
 cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st,
@@ -82,7 +86,7 @@ cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n
 // dynamic shared memory of the stage-1 back kernel (set once per device before any launch)
 cudaError_t stage1_setup();
 cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
-                               int* counts = nullptr, float thr = 0.f, const uint8_t* back_on = nullptr);
+                               int* counts = nullptr, float thr = 0.f, const uint8_t* back_on = nullptr, GateCells cells = GateCells{});
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
                               const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st);
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,

@@ -216,24 +216,44 @@ def evaluate(det, seeds, params, thresholds, fallback_fraction=0.25, width=FRAME
     return out
 
 
+def _operating_point(ev, thresholds):
+    """The highest threshold that kept >= 99.8% of the plain boxes (a margin over the 99% recall
+    target for frames outside the evaluation set)."""
+    ok = [r["threshold"] for r in ev if r["box_recall"] >= 0.998]
+    return max(ok) if ok else min(thresholds)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description="train the learned gate on frames labelled by the plain cascade")
     ap.add_argument("--train-frames", type=int, default=20000)
     ap.add_argument("--eval-frames", type=int, default=1000)
-    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--lr", type=float, default=3e-3)
-    ap.add_argument("--pos-weight", type=float, default=20.0)
+    ap.add_argument("--pos-weight", type=float, default=40.0)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--thresholds", default="0.05,0.1,0.2,0.3,0.4,0.5")
+    ap.add_argument("--thresholds", default="0.02,0.05,0.1,0.2,0.3")
     ap.add_argument("--fallback", type=float, default=0.25)
     ap.add_argument("--out", default=WEIGHTS_1080P)
     ap.add_argument("--report", default=None, help="write the evaluation as JSON here")
+    ap.add_argument("--eval-only", action="store_true",
+                    help="keep the weights in --out, evaluate them again and rewrite their description")
     a = ap.parse_args(argv)
     from . import FaceDetector
     det = FaceDetector()
     if det.Init(detector_params()) != 0:
         raise RuntimeError(_capi.last_error())
+    thr = [float(x) for x in a.thresholds.split(",")]
+    if a.eval_only:
+        params, meta = load(a.out), load_meta(a.out)
+        ev = evaluate(det, range(EVAL_SEED0, EVAL_SEED0 + a.eval_frames), params, thr, a.fallback)
+        for r in ev:
+            print(json.dumps(r), flush=True)
+        meta.update(eval=ev, eval_frames=a.eval_frames, eval_seeds=[EVAL_SEED0, EVAL_SEED0 + a.eval_frames],
+                    operating_threshold=_operating_point(ev, thr))
+        print(f"operating threshold {meta['operating_threshold']}", flush=True)
+        save(a.out, params, meta)
+        return 0
     t0 = time.time()
     ds = collect(det, range(TRAIN_SEED0, TRAIN_SEED0 + a.train_frames))
     t1 = time.time()
@@ -242,14 +262,10 @@ def main(argv=None):
     t2 = time.time()
     print(f"trained {a.epochs} epochs in {t2 - t1:.1f} s; loss {losses[0]:.4f} -> {losses[-1]:.4f}", flush=True)
     del ds
-    thr = [float(x) for x in a.thresholds.split(",")]
     ev = evaluate(det, range(EVAL_SEED0, EVAL_SEED0 + a.eval_frames), params, thr, a.fallback)
     for r in ev:
         print(json.dumps(r), flush=True)
-    # the operating point: the highest threshold that kept >= 99.8% of the plain boxes (a margin
-    # over the 99% recall target for frames outside the evaluation set)
-    ok = [r["threshold"] for r in ev if r["box_recall"] >= 0.998]
-    op = max(ok) if ok else min(thr)
+    op = _operating_point(ev, thr)
     print(f"operating threshold {op}", flush=True)
     meta = {"operating_threshold": op, "train_frames": a.train_frames, "train_seeds": [TRAIN_SEED0, TRAIN_SEED0 + a.train_frames], "epochs": a.epochs,
             "batch": a.batch, "lr": a.lr, "pos_weight": a.pos_weight, "init_seed": a.seed,
