@@ -279,12 +279,18 @@ __global__ void __launch_bounds__(256) gate_infer_kernel(const float* __restrict
         const int fx = x0 - 2 + tid % kFX, fy = y0 - 2 + tid / kFX;
         float v = 0.f;  // zero padding of the first convolution
         if (fx >= 0 && fx < w8 && fy >= 0 && fy < h8) {
-            float s = 0.f;
-            for (int r = 0; r < 8; ++r) {
-                const float* row = gray + (size_t)(8 * fy + r) * gpitch + 8 * fx;
+            // the detector's gray rows are 64-byte aligned with a pitch of 16 floats: 16-byte loads,
+            // summed in the same order as gate_features_kernel
+            float4 q[16];
 #pragma unroll
-                for (int c = 0; c < 8; ++c) s += row[c];
+            for (int r = 0; r < 8; ++r) {
+                const float4* row = reinterpret_cast<const float4*>(gray + (size_t)(8 * fy + r) * gpitch + 8 * fx);
+                q[2 * r] = __ldg(row);
+                q[2 * r + 1] = __ldg(row + 1);
             }
+            float s = 0.f;
+#pragma unroll
+            for (int r = 0; r < 16; ++r) s = (((s + q[r].x) + q[r].y) + q[r].z) + q[r].w;
             v = (s * (1.f / 64.f) - 128.f) * (1.f / 64.f);
         }
         sf[tid / kFX][tid % kFX] = __float2half(v);
@@ -364,11 +370,24 @@ __device__ __forceinline__ void centre_cells(const LevelDesc& L, int ox0, int ox
 // pixels: active when a likely cell of the level's octave lies near their window centres), the
 // rest the front tiles (active when a back tile that reads their S1 pixels can be: the union of
 // those back tiles' cell ranges is tested). A frame with too many ambiguous cells runs in full.
-__global__ void gate_mask_kernel(const __grid_constant__ LevelTable LT, int nb, const uint32_t* __restrict__ bits, int wwords, int w16, int h16,
-                                 const int* __restrict__ ambiguous, int amb_limit, uint8_t* __restrict__ back_on, uint8_t* __restrict__ front_on) {
+// The bitmaps are staged in shared memory first (a query walks up to a few dozen rows, which as
+// dependent global loads took longer than the rest of the kernel); frames whose bitmaps exceed
+// kMaskSmemWords read them from global memory.
+constexpr int kMaskSmemWords = 12288;
+
+__global__ void gate_mask_kernel(const __grid_constant__ LevelTable LT, int nb, const uint32_t* __restrict__ gbits, int n_words, int wwords,
+                                 int w16, int h16, const int* __restrict__ ambiguous, int amb_limit, uint8_t* __restrict__ back_on,
+                                 uint8_t* __restrict__ front_on) {
+    extern __shared__ uint32_t sbits[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const LevelDesc& last = LT.lv[LT.n - 1];
     const bool full = *ambiguous > amb_limit;
+    const bool staged = n_words <= kMaskSmemWords;
+    if (staged && !full) {
+        for (int k = threadIdx.x; k < n_words; k += blockDim.x) sbits[k] = gbits[k];
+        __syncthreads();  // `full` is uniform over the grid
+    }
+    const uint32_t* bits = staged ? sbits : gbits;
     if (i < nb) {
         const int g = LT.lv[0].k2_base + i;
         if (full) {
@@ -434,6 +453,7 @@ cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, in
     gate_infer_kernel<<<dim3((w8 + kIX - 1) / kIX, (h8 + kIY - 1) / kIY), 256, 0, st>>>(d_params, gray, gpitch, w8, h8, thr, 0.25f * thr, sc.bits,
                                                                                        wwords, sc.prob, sc.ambiguous);
     const int amb_limit = gate_cells(sc, gw, gh, amb_frac).amb_limit;
+    const int n_words = gate_bitmap_words(gw, gh);
     for (int g0 = 0; g0 < n_levels; g0 += kParamLevels) {
         LevelTable T;
         T.n = n_levels - g0 < kParamLevels ? n_levels - g0 : kParamLevels;
@@ -443,7 +463,8 @@ cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, in
         const int nb = last.k2_base + last.k2_tiles_x * ((last.oh + kK2TileY - 1) / kK2TileY) - T.lv[0].k2_base;
         const int nf = last.k1_base + last.k1_tiles_x * ((last.p1h + kK1TileY - 1) / kK1TileY) - T.lv[0].k1_base;
         if (nb + nf > 0)
-            gate_mask_kernel<<<blocks(nb + nf, 128), 128, 0, st>>>(T, nb, sc.bits, wwords, w16, h16, sc.ambiguous, amb_limit, back_on, front_on);
+            gate_mask_kernel<<<blocks(nb + nf, 128), 128, n_words <= kMaskSmemWords ? sizeof(uint32_t) * n_words : 0, st>>>(
+                T, nb, sc.bits, n_words, wwords, w16, h16, sc.ambiguous, amb_limit, back_on, front_on);
     }
     return cudaGetLastError();
 }
