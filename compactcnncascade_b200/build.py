@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CU_SOURCES = ["capi.cu", "detector.cu", "k_image.cu", "k_stage1.cu", "k_candidates.cu", "k_window.cu", "k_replay.cu", "noalloc.cu", "server.cu", "k_facial.cu", "gate.cu", "synth_device.cu"]
+CU_SOURCES = ["capi.cu", "detector.cu", "k_image.cu", "k_stage1.cu", "k_candidates.cu", "k_window.cu", "k_replay.cu", "noalloc.cu", "server.cu", "k_facial.cu", "gate.cu", "synth_device.cu", "k_legacy.cu"]
 CPP_SOURCES = ["model.cpp", "convert.cpp"]
 
 # -fmad=false: the kernels must reproduce the reference's uncontracted IEEE single arithmetic.

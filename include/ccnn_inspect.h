@@ -103,6 +103,18 @@ CCNN_API ccnn_status ccnn_cntk_dump_to_binary(const char* binary_file, const cha
 CCNN_API ccnn_status ccnn_synth_frame_device(void* d_out, int width, int height, int channels, size_t step, unsigned long long seed,
                                              int n_faces, int min_face, int max_face, void* faces_out, void* stream);
 
+/* Legacy cascade networks (model format 1.0, the cnn4face{1,2,3}_new.bin family: tanh activations,
+ * max or average pooling; reader SIMD::ConvNeuralNetwork::Init, src/CNNObjectDetector/cnn_simd.cpp:40-336,
+ * forward pass Run_single_thread, cnn_simd.cpp:551-874, in the reference's plain-C++ build).
+ * ccnn_legacy_model_info parses a model file (host only) into info[10] = {max_pool, min_w, min_h,
+ * maps L1, maps L2, maps L3, L3 kernel width, L3 kernel height, fully connected hidden layer,
+ * hidden neurons}. ccnn_legacy_net_forward runs the network on a device fp32 image (step in bytes)
+ * and writes the dense ow x oh response map to d_resp (device memory of resp_cap floats);
+ * returns when the map is written. */
+CCNN_API ccnn_status ccnn_legacy_model_info(const char* model_path, int* info, int n_info);
+CCNN_API ccnn_status ccnn_legacy_net_forward(const char* model_path, const float* d_img, int cols, int rows, size_t step, float* d_resp,
+                                             int resp_cap, int* ow, int* oh, void* stream);
+
 /* The permutation the detector's device sort applies to detections with the given scales
  * (perm[i] = input index placed at slot i); equals std::sort with comp(a, b) = b < a. */
 CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm);

@@ -13,6 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_STRICT = os.path.join(HERE, "_ref", "libccnn_ref.so")
 REF_FAST = os.path.join(HERE, "_ref", "libccnn_ref_fast.so")
+REF_LEGACY = os.path.join(HERE, "_ref", "libccnn_ref_legacy.so")
 MODELS = os.path.join(HERE, "..", "compactcnncascade_b200", "models")
 
 
@@ -187,3 +188,41 @@ def sort_perm(keys):
     perm = np.empty(len(keys), np.int32)
     L.ref_sort_by_scale_desc(keys.ctypes.data, len(keys), perm.ctypes.data)
     return perm
+
+
+# ---- legacy model family (format 1.0, the `_new.bin` networks) ----
+
+def legacy_available():
+    return os.path.exists(REF_LEGACY)
+
+
+def legacy_net_forward(model_path, img):
+    """Response map of the reference's legacy network (SIMD::ConvNeuralNetwork of
+    src/CNNObjectDetector/cnn_simd.cpp, plain-C++ build) on a float32 H x W image, in this process.
+    The model is passed as its bytes: the legacy reader cannot open a path (its file stream shadows
+    the stream it parses, cnn_simd.cpp:40-60)."""
+    if REF_LEGACY not in _libs:
+        L = ctypes.CDLL(REF_LEGACY)
+        ci, vp, P = ctypes.c_int, ctypes.c_void_p, ctypes.POINTER
+        L.ref_net_forward_bytes.argtypes = [ctypes.c_char_p, ci, vp, ci, ci, ci, vp, ci, P(ci), P(ci)]
+        _libs[REF_LEGACY] = L
+    L = _libs[REF_LEGACY]
+    with open(model_path, "rb") as f:
+        blob = f.read()
+    a = np.ascontiguousarray(img, np.float32)
+    h, w = a.shape
+    out = np.zeros(w * h, np.float32)
+    ow, oh = ctypes.c_int(), ctypes.c_int()
+    r = L.ref_net_forward_bytes(blob, len(blob), a.ctypes.data, w, h, w, out.ctypes.data, out.size, ctypes.byref(ow), ctypes.byref(oh))
+    if r != 0:
+        raise RuntimeError(f"reference legacy forward failed ({r})")
+    return out[: ow.value * oh.value].reshape(oh.value, ow.value)
+
+
+def legacy_net_forward_isolated(model_path, img):
+    """legacy_net_forward in a fresh process. The reference's fully connected 24-map route keeps the
+    pointers of the first network that ran it in a function-local static (mulC24_add_tanh call,
+    cnn_simd.cpp:806-809), so in one process only the first network instance computes correctly."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(1, maxtasksperchild=1) as pool:
+        return pool.apply(legacy_net_forward, (model_path, img))

@@ -129,6 +129,29 @@ int ref_net_forward(const char* model_path, int index_output, const float* img, 
     return 0;
 }
 
+// The same with the model given as its bytes. The legacy loader (format 1.0,
+// src/CNNObjectDetector/cnn_simd.cpp:40-60) reads a path into a stream that shadows the one it parses,
+// so only the in-memory form (a string of 255 bytes or more, as the detector passes its embedded
+// models) loads.
+int ref_net_forward_bytes(const char* model, int model_bytes, const float* img, int w, int h, int stride, float* out, int out_cap, int* ow,
+                          int* oh) {
+    SIMD::ConvNeuralNetwork net;
+    net.Init(std::string(model, (size_t)model_bytes), 0, nullptr);
+    if (net.isEmpty()) return -1;
+    Size mn = net.getMinInputImgSize();
+    if (w < mn.width || h < mn.height) return -2;
+    net.AllocateMemory(Size(w, h));
+    SIMD::Image_32f in(w, h, 1, const_cast<float*>(img), stride);
+    SIMD::Image_32f resp;
+    net.Forward(resp, in);
+    *ow = resp.width;
+    *oh = resp.height;
+    if (resp.width * resp.height > out_cap) return -3;
+    for (int y = 0; y < resp.height; ++y)
+        for (int x = 0; x < resp.width; ++x) out[y * resp.width + x] = resp.data[y * resp.widthStep + x];
+    return 0;
+}
+
 int ref_net_min_size(const char* model_path, int* w, int* h) {
     SIMD::ConvNeuralNetwork net;
     net.Init(std::string(model_path), 0, nullptr);
