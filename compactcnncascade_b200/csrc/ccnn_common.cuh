@@ -345,6 +345,7 @@ struct CascadeConfig {
     int min_num_detect;
     int rescale_output;   // gray_image_only input downscale: rects scaled back
     float rescale;        // min_obj_size.height / pattern height
+    int pat_w, pat_h;     // stage-1 pattern (the stage-1 network's smallest input)
 };
 
 }  // namespace ccnn

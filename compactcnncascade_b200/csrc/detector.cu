@@ -85,6 +85,7 @@ Detector::~Detector() {
     clear();
     if (d_lnet_) cudaFree(d_lnet_);
     if (d_gate_) cudaFree(d_gate_);
+    if (d_lg_) cudaFree(d_lg_);
 }
 
 void Detector::free_slot(Slot& s) {
@@ -200,17 +201,49 @@ ccnn_status Detector::init() {
         return CCNN_ERR_INVALID_ARG;
     }
 
-    // models (InitCNN / InitCNNCheck)
+    // models (InitCNN / InitCNNCheck). The family follows the files: format 1.0 (`_new.bin`) is
+    // the legacy tanh family the reference builds without USE_CNTK_MODELS (then with facial
+    // analysis off, cnn_detector_v3.cpp:911-915); otherwise the CNTK format.
     RawModel m[3];
     std::string err;
-    for (int i = 0; i < 3; ++i)
+    {
+        std::unique_ptr<LegacyNet[]> lg(new LegacyNet[3]);
+        std::string lerr;
+        legacy_ = load_legacy_model_file(model_paths_[0], &lg[0], &lerr);
+        if (legacy_) {
+            for (int i = 1; i < 3; ++i)
+                if (!load_legacy_model_file(model_paths_[i], &lg[i], &lerr)) {
+                    set_error("legacy cascade: " + lerr + " (all three models must be format 1.0)");
+                    return CCNN_ERR_MODEL;
+                }
+            if (lg[1].min_w != 36 || lg[1].min_h != 40 || lg[2].min_w != 36 || lg[2].min_h != 40) {
+                set_error("legacy cascade: stage-2/3 networks must take 36x40 windows");
+                return CCNN_ERR_MODEL;
+            }
+            for (int i = 1; i < 3; ++i)
+                if (lg[i].m0 > 6 || lg[i].m2 > 24 || lg[i].hl > 84 || lg[i].k3w != 7 || lg[i].k3h != 8) {
+                    set_error("legacy cascade: stage-2/3 networks larger than 6/12/24 maps, 84 hidden neurons or a 7x8 third layer are not supported");
+                    return CCNN_ERR_MODEL;
+                }
+            api_.facial_analysis = 0;
+            CCNN_CUDA(cudaSetDevice(api_.cuda_device_id));
+            if (!d_lg_) CCNN_CUDA(cudaMalloc(&d_lg_, 3 * sizeof(LegacyNet)));
+            CCNN_CUDA(cudaMemcpy(d_lg_, lg.get(), 3 * sizeof(LegacyNet), cudaMemcpyHostToDevice));
+            h_lg_ = std::move(lg);
+            for (int i = 0; i < 3; ++i) {
+                m[i].min_w = h_lg_[i].min_w;
+                m[i].min_h = h_lg_[i].min_h;
+            }
+        }
+    }
+    for (int i = 0; i < 3 && !legacy_; ++i)
         if (!load_model_file(model_paths_[i], &m[i], &err)) {
             set_error(err);
             return CCNN_ERR_MODEL;
         }
     if (!wn_) wn_.reset(new WindowNets());
-    if (!pack_model(m[0], api_.index_output[0], &w1_, &err) || !pack_model(m[1], api_.index_output[1], &wn_->s2, &err) ||
-        !pack_model(m[2], api_.index_output[2], &wn_->s3, &err)) {
+    if (!legacy_ && (!pack_model(m[0], api_.index_output[0], &w1_, &err) || !pack_model(m[1], api_.index_output[1], &wn_->s2, &err) ||
+                     !pack_model(m[2], api_.index_output[2], &wn_->s3, &err))) {
         set_error(err);
         return CCNN_ERR_MODEL;
     }
@@ -229,7 +262,7 @@ ccnn_status Detector::init() {
     }
     pat_w_ = m[0].min_w;
     pat_h_ = m[0].min_h;
-    if (pat_w_ != kPatW || pat_h_ != kPatH || m[1].min_w != 36 || m[1].min_h != 40 || m[2].min_w != 36 || m[2].min_h != 40) {
+    if ((!legacy_ && (pat_w_ != kPatW || pat_h_ != kPatH)) || m[1].min_w != 36 || m[1].min_h != 40 || m[2].min_w != 36 || m[2].min_h != 40) {
         set_error("model window sizes differ from the cascade prototype (23x27 / 36x40)");
         return CCNN_ERR_MODEL;
     }
@@ -264,6 +297,8 @@ ccnn_status Detector::init() {
     cfg_.min_num_detect = min_num_detect_;
     cfg_.rescale_output = input_downscale_ ? 1 : 0;
     cfg_.rescale = (float)api_.min_face_height / (float)pat_h_;
+    cfg_.pat_w = pat_w_;
+    cfg_.pat_h = pat_h_;
 
     // capacities from the largest plans this configuration can produce
     s1_cap_ = resp_cap_ = img_cap_ = 0;
@@ -391,6 +426,13 @@ ccnn_status Detector::build_plan(int w, int h, int ch, int num_scales, Plan* p) 
         L.s1_plane = (long long)L.s1_pitch * L.p1h;
         L.s1_off = s1;
         s1 += 4 * L.s1_plane;
+        if (legacy_) {
+            // the legacy stage-1 network's response map, and its pooled L1 and L2 maps in the S1 arena
+            const LegacyNet& n = h_lg_[0];
+            legacy_output_size(n, L.w, L.h, &L.ow, &L.oh);
+            s1 -= 4 * L.s1_plane;  // L.s1_off stays this level's start
+            s1 += (long long)n.m0 * L.p1w * L.p1h + (long long)n.m1 * L.p2w * L.p2h;
+        }
         L.resp_off = resp;
         resp += (long long)L.ow * L.oh;
         L.k1_tiles_x = (L.p1w + kK1TileX - 1) / kK1TileX;
@@ -480,6 +522,10 @@ ccnn_status Detector::gate_set(const float* params, int n, float threshold, floa
     if (!inited_) {
         ccnn_status st = init();
         if (st != CCNN_OK) return st;
+    }
+    if (legacy_) {
+        set_error("gate: the learned gate is trained for the CNTK cascade, not the legacy model family");
+        return CCNN_ERR_UNSUPPORTED;
     }
     cudaSetDevice(device_);
     gate_params_.assign(params, params + n);
@@ -593,20 +639,36 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
     CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st, gated ? s.d_front_on : nullptr));
     // the back kernel counts each chunk's candidates as it writes the responses
     if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
-    CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
-                            gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr,
-                            gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}));
+    if (legacy_) {
+        const ccnn_status ls = enqueue_legacy_stage1(s, p);
+        if (ls != CCNN_OK) return ls;
+    } else {
+        CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
+                                gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr,
+                                gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}));
+    }
     CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                 (int)cand_cap_, s.st));
     if (detect_enabled_)
         CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
-                                window_grid_, s.st));
+                                window_grid_, s.st, legacy_ ? d_lg_ : nullptr));
     if (s.d_attr)
         CCNN_CUDA(launch_facial(d_lnet_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_, s.d_attr,
                                 facial_grid_, s.st));
     CCNN_CUDA(launch_replay(replay_args(s, p), s.st));
     CCNN_CUDA(cudaMemcpyAsync(s.h_nfaces, s.d_nfaces, sizeof(int), cudaMemcpyDeviceToHost, s.st));
     CCNN_CUDA(cudaMemcpyAsync(s.h_faces, s.d_faces, sizeof(FaceOut) * kHostFaces, cudaMemcpyDeviceToHost, s.st));
+    return CCNN_OK;
+}
+
+// Stage 1 of the legacy family: the legacy network on every level image, its pooled maps in the
+// S1 arena, candidates counted per scan chunk.
+ccnn_status Detector::enqueue_legacy_stage1(Slot& s, const Plan& p) {
+    for (int i = 0; i < p.n_levels; ++i) {
+        const LevelDesc& L = p.levels[i];
+        CCNN_CUDA(launch_legacy_forward(d_lg_, h_lg_[0], s.d_limg + L.img_off, L.img_pitch, L.w, L.h, s.d_s1 + L.s1_off, s.d_resp + L.resp_off, s.st,
+                                        s.d_counts, L.chunk_base, cfg_.thr1));
+    }
     return CCNN_OK;
 }
 
@@ -932,6 +994,10 @@ ccnn_status Detector::stage1_forward(const float* d_img, int w, int h, size_t st
         set_error("image smaller than the stage-1 window or misaligned step");
         return CCNN_ERR_INVALID_ARG;
     }
+    if (legacy_) {
+        set_error("stage-1 inspection covers the CNTK family; use ccnn_legacy_net_forward for legacy models");
+        return CCNN_ERR_UNSUPPORTED;
+    }
     cudaSetDevice(device_);
     LevelDesc L{};
     L.w = w;
@@ -999,18 +1065,22 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st,
                                  gated ? s.d_front_on : nullptr));
         CCNN_CUDA(cudaEventRecord(ev[2], s.st));
-        CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st, gated ? s.d_front_on : nullptr));
+        if (!legacy_) CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st, gated ? s.d_front_on : nullptr));
         CCNN_CUDA(cudaEventRecord(ev[3], s.st));
         if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
-        CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
-                                     gated ? s.d_back_on : nullptr, gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}));
+        if (legacy_) {  // the legacy network's three layers all count as the back entry
+            const ccnn_status ls = enqueue_legacy_stage1(s, p);
+            if (ls != CCNN_OK) return ls;
+        } else
+            CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
+                                         gated ? s.d_back_on : nullptr, gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}));
         CCNN_CUDA(cudaEventRecord(ev[4], s.st));
         CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                     (int)cand_cap_, s.st));
         CCNN_CUDA(cudaEventRecord(ev[5], s.st));
         if (detect_enabled_)
             CCNN_CUDA(launch_window(*wn_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
-                                    window_grid_, s.st));
+                                    window_grid_, s.st, legacy_ ? d_lg_ : nullptr));
         if (s.d_attr)
             CCNN_CUDA(launch_facial(d_lnet_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_cands, s.d_ncand, p.d_levels, s.d_win, cfg_,
                                     s.d_attr, facial_grid_, s.st));

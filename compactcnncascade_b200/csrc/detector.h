@@ -14,6 +14,7 @@
 #include "../../include/ccnn.h"
 #include "../../include/ccnn_inspect.h"
 #include "../../include/ccnn_gate.h"
+#include "legacy.h"
 #include "kernels.h"
 
 namespace ccnn {
@@ -131,6 +132,11 @@ class Detector {
     Stage1W w1_{};
     std::unique_ptr<WindowNets> wn_;
     LandmarkNet* d_lnet_ = nullptr;  // facial-analysis network (device memory), when enabled
+    // legacy model family (format 1.0): the three networks on the host and in device memory
+    bool legacy_ = false;
+    std::unique_ptr<LegacyNet[]> h_lg_;
+    LegacyNet* d_lg_ = nullptr;
+    ccnn_status enqueue_legacy_stage1(Slot& s, const Plan& p);
     float* d_gate_ = nullptr;        // learned gate parameters (device memory)
     bool gate_on_ = false;
     float gate_thr_ = 0.5f, gate_amb_frac_ = 0.25f;

@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(kFT, 1) facial_kernel(const FacialArgs a) {
             const LevelDesc& L = a.levels[cd.level];
             const CandResult r = verdict(a.win + (size_t)ci * 4, cd, L.scale, a.cfg);
             S.accepted = r.accepted;
-            if (r.accepted) window_geometry(cd, L.inv_scale, r.accepted - 1, a.gw, a.gh, S.geo);
+            if (r.accepted) window_geometry(cd, L.inv_scale, r.accepted - 1, a.gw, a.gh, a.cfg.pat_w, a.cfg.pat_h, S.geo);
             a.attr[ci] = make_int4(0, -1, -1, -1);
         }
         __syncthreads();

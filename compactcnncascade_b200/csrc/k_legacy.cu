@@ -24,6 +24,7 @@
 #include "../../include/ccnn_inspect.h"
 #include "ccnn_common.cuh"
 #include "legacy.h"
+#include "legacy_dev.cuh"
 
 namespace ccnn {
 
@@ -145,22 +146,6 @@ bool load_legacy_model_file(const std::string& path, LegacyNet* net, std::string
 
 namespace {
 
-// tanh(c + b) of the four convolution outputs of a 2x2 window, max or sum, tanh(w * p + b) * af
-__device__ __forceinline__ float lg_pool_tanh(const float c[4], int max_pool, float cb, float sw, float sb, float af) {
-    float t[4];
-#pragma unroll
-    for (int d = 0; d < 4; ++d) t[d] = tanh_rational(fadd(c[d], cb));
-    const float p = max_pool ? fmaxf(fmaxf(t[0], t[1]), fmaxf(t[2], t[3])) : fadd(fadd(fadd(t[0], t[1]), t[2]), t[3]);
-    return fmul(af, tanh_rational(fadd(fmul(sw, p), sb)));
-}
-
-// neighbouring-map sum i of `count` maps (add / add2 as the reference orders them)
-__device__ __forceinline__ float lg_map_sum(const float* __restrict__ planes, long long plane, int count, int i, long long o) {
-    if (i == 0) return fadd(planes[o], planes[plane + o]);
-    if (i == count - 1) return fadd(planes[(count - 2) * plane + o], planes[(count - 1) * plane + o]);
-    return fadd(fadd(planes[(i - 1) * plane + o], planes[i * plane + o]), planes[(i + 1) * plane + o]);
-}
-
 __global__ void legacy_l1_kernel(const LegacyNet* __restrict__ N, const float* __restrict__ img, int pitch, int p1w, int p1h,
                                  float* __restrict__ pool1) {
     const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y, m = blockIdx.z;
@@ -202,63 +187,41 @@ __global__ void legacy_l2_kernel(const LegacyNet* __restrict__ N, const float* _
     pool2[((long long)m * p2h + y) * p2w + x] = lg_pool_tanh(c, N->max_pool, N->cb[1][m], N->sw[1][m], N->sb[1][m], N->af);
 }
 
-__global__ void legacy_out_kernel(const LegacyNet* __restrict__ N, const float* __restrict__ pool2, int p2w, int p2h, int ow, int oh,
-                                  float* __restrict__ resp) {
+__global__ void legacy_out_kernel(const LegacyNet* __restrict__ Np, const float* __restrict__ pool2, int p2w, int p2h, int ow, int oh,
+                                  float* __restrict__ resp, int* __restrict__ counts, int chunk_base, float thr) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= ow || y >= oh) return;
+    const LegacyNet& N = *Np;
     const long long plane = (long long)p2w * p2h;
-    const int it2 = N->m2 >> 1, kw = N->k3w, kt = N->k3w * N->k3h;
-    const float af = N->af;
+    const int it2 = N.m2 >> 1, kw = N.k3w;
     float vals[kLgMaxM2];
     float acc = 0.f;
     for (int i = 0; i < it2; ++i) {
-        float v[2];
-        for (int h = 0; h < 2; ++h) {
-            const int m = 2 * i + h;
-            const float* k = N->k3[m];
-            float c = fmul(lg_map_sum(pool2, plane, N->m1, i, (long long)y * p2w + x), k[0]);
-            for (int t = 1; t < kt; ++t) c = fadd(c, fmul(lg_map_sum(pool2, plane, N->m1, i, (long long)(y + t / kw) * p2w + x + t % kw), k[t]));
-            c = tanh_rational(fadd(c, N->cb[2][m]));
-            c = tanh_rational(fadd(fmul(N->sw[2][m], c), N->sb[2][m]));
-            if (N->full_connect) {
-                v[h] = fmul(af, c);  // tanh_tanh
-            } else {
-                // tanh_tanh_2tanh: hidden neurons 2m and 2m + 1 of this map
-                const float c1 = tanh_rational(fadd(fmul(fmul(af, N->hw[2 * m]), c), N->hb[2 * m]));
-                const float c2 = tanh_rational(fadd(fmul(fmul(af, N->hw[2 * m + 1]), c), N->hb[2 * m + 1]));
-                v[h] = fmul(af, fadd(fmul(N->ow[2 * m], c1), fmul(N->ow[2 * m + 1], c2)));
-            }
-        }
-        if (N->full_connect) {
-            vals[2 * i] = v[0];
-            vals[2 * i + 1] = v[1];
+        const auto in = [&](int t) { return lg_map_sum(pool2, plane, N.m1, i, (long long)(y + t / kw) * p2w + x + t % kw); };
+        const float v0 = lg_l3_value(N, 2 * i, in), v1 = lg_l3_value(N, 2 * i + 1, in);
+        if (N.full_connect) {
+            vals[2 * i] = v0;
+            vals[2 * i + 1] = v1;
         } else {
-            const float pair = fadd(v[1], v[0]);
+            const float pair = fadd(v1, v0);
             acc = (i == 0) ? pair : fadd(acc, pair);
         }
     }
-    if (N->full_connect) {
-        for (int n = 0; n < N->hl; ++n) {
-            float h;
-            if (N->m2 == 24) {  // mulC24_add_tanh: bias first, then the 24 maps
-                float s = N->hb[n];
-                for (int j = 0; j < 24; ++j) s = fadd(s, fmul(vals[j], N->hwfc[n][j]));
-                h = fmul(fmul(af, tanh_rational(s)), N->ow[n]);
-            } else {  // mulC2_add, mulC1_add, tanh: the output weight is not applied on this route
-                float s = fadd(fmul(vals[0], N->hwfc[n][0]), fmul(vals[1], N->hwfc[n][1]));
-                for (int j = 2; j < N->m2; ++j) s = fadd(fmul(vals[j], N->hwfc[n][j]), s);
-                h = fmul(af, tanh_rational(fadd(s, N->hb[n])));
-            }
+    if (N.full_connect)
+        for (int n = 0; n < N.hl; ++n) {
+            const float h = lg_hidden_fc(N, n, vals);
             acc = (n == 0) ? h : fadd(acc, h);
         }
-    }
-    resp[(long long)y * ow + x] = fmul(af, tanh_rational(fadd(acc, N->ob)));
+    const float r = lg_finish(N, acc);
+    resp[(long long)y * ow + x] = r;
+    // candidates (response > treshold_1) counted per scan chunk, as the CNTK stage-1 back kernel does
+    if (counts && r > thr) atomicAdd(&counts[chunk_base + (y * ow + x) / kCandChunk], 1);
 }
 
 }  // namespace
 
 cudaError_t launch_legacy_forward(const LegacyNet* d_net, const LegacyNet& h_net, const float* img, int pitch, int w, int h, float* scratch,
-                                  float* resp, cudaStream_t st) {
+                                  float* resp, cudaStream_t st, int* counts, int chunk_base, float thr) {
     const int p1w = (w - 3) >> 1, p1h = (h - 3) >> 1;
     const int p2w = (((w - 3) >> 1) - 2) >> 1, p2h = (((h - 3) >> 1) - 2) >> 1;
     int ow, oh;
@@ -268,7 +231,7 @@ cudaError_t launch_legacy_forward(const LegacyNet* d_net, const LegacyNet& h_net
     const dim3 b(32, 8);
     legacy_l1_kernel<<<dim3((p1w + 31) / 32, (p1h + 7) / 8, h_net.m0), b, 0, st>>>(d_net, img, pitch, p1w, p1h, pool1);
     legacy_l2_kernel<<<dim3((p2w + 31) / 32, (p2h + 7) / 8, h_net.m1), b, 0, st>>>(d_net, pool1, p1w, p1h, p2w, p2h, pool2);
-    legacy_out_kernel<<<dim3((ow + 31) / 32, (oh + 7) / 8), b, 0, st>>>(d_net, pool2, p2w, p2h, ow, oh, resp);
+    if (ow > 0 && oh > 0) legacy_out_kernel<<<dim3((ow + 31) / 32, (oh + 7) / 8), b, 0, st>>>(d_net, pool2, p2w, p2h, ow, oh, resp, counts, chunk_base, thr);
     return cudaGetLastError();
 }
 
@@ -326,7 +289,7 @@ extern "C" CCNN_API ccnn_status ccnn_legacy_net_forward(const char* model_path, 
     if (e == cudaSuccess) e = cudaMemcpyAsync(buf, &net, sizeof(LegacyNet), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = launch_legacy_forward((const LegacyNet*)buf, net, d_img, (int)(step / sizeof(float)), cols, rows,
-                                  (float*)((char*)buf + sizeof(LegacyNet)), d_resp, st);
+                                  (float*)((char*)buf + sizeof(LegacyNet)), d_resp, st, nullptr, 0, 0.f);
     if (buf) {
         const cudaError_t f = cudaFreeAsync(buf, st);
         if (e == cudaSuccess) e = f;

@@ -29,9 +29,11 @@ namespace ccnn {
 
 constexpr int kRT = 1024;
 
-__device__ __forceinline__ Det cand_rect(const Candidate& c, float inv_scale, float scale) {
-    return make_det((int)((float)c.px * inv_scale), (int)((float)c.py * inv_scale), (int)((float)kPatW * inv_scale),
-                    (int)((float)kPatH * inv_scale), 0.f, scale, 0);
+// the candidate's stage-1 pattern rectangle (new_rect, cnn_detector_v3.cpp:1497-1501); the pattern is
+// the stage-1 network's smallest input
+__device__ __forceinline__ Det cand_rect(const Candidate& c, float inv_scale, float scale, int pat_w, int pat_h) {
+    return make_det((int)((float)c.px * inv_scale), (int)((float)c.py * inv_scale), (int)((float)pat_w * inv_scale),
+                    (int)((float)pat_h * inv_scale), 0.f, scale, 0);
 }
 
 __device__ __forceinline__ void sort4(int* v) {
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
         if (C.drop_detect) {
             // scan test against the detections of earlier levels, one warp per candidate
             for (int c = g + warp; c < e; c += kRT / 32) {
-                const Det nr = cand_rect(cands[c], inv_scale, scale);
+                const Det nr = cand_rect(cands[c], inv_scale, scale, C.pat_w, C.pat_h);
                 const Det ex = rect_shrink(nr, 0.7f);
                 int code = -1;
                 for (int base = 0; base < n_prefix; base += 32) {
@@ -279,8 +281,8 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                     const int j = 32 * w + lane;
                     int t = 0;
                     if (j < i) {
-                        const Det nr = cand_rect(cands[g + i], inv_scale, scale);
-                        t = drop_test(nr, rect_shrink(nr, 0.7f), cand_rect(cands[g + j], inv_scale, scale));
+                        const Det nr = cand_rect(cands[g + i], inv_scale, scale, C.pat_w, C.pat_h);
+                        t = drop_test(nr, rect_shrink(nr, 0.7f), cand_rect(cands[g + j], inv_scale, scale, C.pat_w, C.pat_h));
                     }
                     const uint32_t b1 = __ballot_sync(0xffffffffu, t == 1), b2 = __ballot_sync(0xffffffffu, t == 2);
                     if (lane == 0) {
@@ -421,7 +423,7 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                         sc = cands[g + r].score;
                         kn = 0;
                     }
-                    const Det nr = cand_rect(cands[g + i], inv_scale, scale);
+                    const Det nr = cand_rect(cands[g + i], inv_scale, scale, C.pat_w, C.pat_h);
                     D[s_didx[i]] = make_det(nr.x, nr.y, nr.w, nr.h, sc, scale, kn);
                     // facial data travels with a candidate's own accepted box, not with copies
                     if (a.fa_scratch) a.fa_scratch[s_didx[i]] = (s_src[i] == kOwnVerdict) ? g + i : -1;
@@ -440,7 +442,7 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                         k0 = code >> 1;
                         type = (code & 1) + 1;
                     } else if (nD > n_prefix) {
-                        nr = cand_rect(cands[c], inv_scale, scale);
+                        nr = cand_rect(cands[c], inv_scale, scale, C.pat_w, C.pat_h);
                         const Det ex = rect_shrink(nr, 0.7f);
                         for (int base = n_prefix; base < nD; base += 32) {
                             const int kk = base + lane;
@@ -457,7 +459,7 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                     if (k0 >= 0) {
                         if (type == 1) {
                             if (lane == 0) {
-                                nr = cand_rect(cands[c], inv_scale, scale);
+                                nr = cand_rect(cands[c], inv_scale, scale, C.pat_w, C.pat_h);
                                 const Det src = D[k0];
                                 D[nD] = make_det(nr.x, nr.y, nr.w, nr.h, src.score, scale, src.knn);
                                 if (a.fa_scratch) a.fa_scratch[nD] = -1;
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
             for (int si = 0; si < nS; ++si) {
                 const int c = C.drop_detect ? surv[si] : g + si;
                 const Candidate cd = cands[c];
-                const Det nr = cand_rect(cd, inv_scale, scale);
+                const Det nr = cand_rect(cd, inv_scale, scale, C.pat_w, C.pat_h);
                 if (C.drop_detect && C.detect_enabled && nD > rect_size) {
                     int k0 = -1;
                     for (int base = rect_size; base < nD; base += 32) {

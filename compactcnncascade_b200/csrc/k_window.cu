@@ -21,6 +21,7 @@
 #include "kernels.h"
 #include "resample.cuh"
 #include "window_common.cuh"
+#include "legacy_dev.cuh"
 
 namespace ccnn {
 
@@ -187,6 +188,82 @@ __device__ void window_net(const NW& W, WindowSmem& S, int mode) {
     __syncthreads();
 }
 
+// The legacy (format 1.0) stage-2/3 networks on the window in shared memory: L1 (6 maps, 22x24
+// pooled) in S.s1, L2 (12 maps, 10x11) in S.p2, the L3 values of the 16 outputs in S.a3, fully
+// connected hidden neurons in S.hbuf; the arithmetic of the standalone legacy forward pass
+// (legacy_dev.cuh), spread over the block.
+__device__ void legacy_window_net(const LegacyNet& W, WindowSmem& S, int mode) {
+    constexpr int kP1 = kP1W * kP1H, kP2 = kP2W * kP2H;
+    constexpr long long kS1Plane = kP1H * (kP1W + 1), kP2Plane = kP2H * (kP2W + 1);
+    for (int it = threadIdx.x; it < W.m0 * kP1; it += kWT) {
+        const int m = it / kP1, p = it - m * kP1;
+        const int x = p % kP1W, y = p / kP1W;
+        const float* k = W.k1[m];
+        float c[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const int x0 = 2 * x + (d & 1), y0 = 2 * y + (d >> 1);
+            float acc = fmul(win_in(S, mode, x0, y0), k[0]);
+#pragma unroll
+            for (int t = 1; t < 16; ++t) acc = fadd(acc, fmul(win_in(S, mode, x0 + (t & 3), y0 + (t >> 2)), k[t]));
+            c[d] = acc;
+        }
+        S.s1[m][y][x] = lg_pool_tanh(c, W.max_pool, W.cb[0][m], W.sw[0][m], W.sb[0][m], W.af);
+    }
+    __syncthreads();
+    const float* s1 = &S.s1[0][0][0];
+    for (int it = threadIdx.x; it < W.m1 * kP2; it += kWT) {
+        const int m = it / kP2, p = it - m * kP2;
+        const int x = p % kP2W, y = p / kP2W, i = m >> 1;
+        float Q[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) Q[r][q] = lg_map_sum(s1, kS1Plane, W.m0, i, (2 * y + r) * (kP1W + 1) + 2 * x + q);
+        const float* k = W.k2[m];
+        float c[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const int dy = d >> 1, dx = d & 1;
+            float acc = fmul(Q[dy][dx], k[0]);
+#pragma unroll
+            for (int t = 1; t < 9; ++t) acc = fadd(acc, fmul(Q[dy + t / 3][dx + t % 3], k[t]));
+            c[d] = acc;
+        }
+        S.p2[m][y][x] = lg_pool_tanh(c, W.max_pool, W.cb[1][m], W.sw[1][m], W.sb[1][m], W.af);
+    }
+    __syncthreads();
+    const float* p2 = &S.p2[0][0][0];
+    for (int it = threadIdx.x; it < W.m2 * kOutN; it += kWT) {
+        const int m = it / kOutN, o = it - m * kOutN;
+        const int ox = o & 3, oy = o >> 2, i = m >> 1, kw = W.k3w;
+        S.a3[m][o] = lg_l3_value(W, m, [&](int t) { return lg_map_sum(p2, kP2Plane, W.m1, i, (oy + t / kw) * (kP2W + 1) + ox + t % kw); });
+    }
+    __syncthreads();
+    if (W.full_connect) {
+        for (int it = threadIdx.x; it < W.hl * kOutN; it += kWT) {
+            const int n = it / kOutN, o = it - n * kOutN;
+            float vals[kLgMaxM2];
+            for (int j = 0; j < W.m2; ++j) vals[j] = S.a3[j][o];
+            S.hbuf[n][o] = lg_hidden_fc(W, n, vals);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < kOutN) {
+        const int o = threadIdx.x;
+        float acc;
+        if (W.full_connect) {
+            acc = S.hbuf[0][o];
+            for (int n = 1; n < W.hl; ++n) acc = fadd(acc, S.hbuf[n][o]);
+        } else {
+            acc = fadd(S.a3[1][o], S.a3[0][o]);
+            for (int i = 1; i < W.m2 / 2; ++i) acc = fadd(acc, fadd(S.a3[2 * i + 1][o], S.a3[2 * i][o]));
+        }
+        S.out[o] = lg_finish(W, acc);
+    }
+    __syncthreads();
+}
+
 struct WinArgs {
     const float* gray;
     int gpitch, gw, gh;
@@ -195,11 +272,12 @@ struct WinArgs {
     const LevelDesc* levels;
     WinOut* out;
     CascadeConfig cfg;
+    const LegacyNet* lg;  // legacy networks ([1] stage 2, [2] stage 3) instead of the CNTK ones, or null
 };
 
 // crop + byte rounding + (optional) equalisation of one window into S.crop
 __device__ void prepare_window(const WinArgs& a, WindowSmem& S, const Candidate& cd, float inv_scale, int mod) {
-    if (threadIdx.x == 0) window_geometry(cd, inv_scale, mod, a.gw, a.gh, S.geo);
+    if (threadIdx.x == 0) window_geometry(cd, inv_scale, mod, a.gw, a.gh, a.cfg.pat_w, a.cfg.pat_h, S.geo);
     if (threadIdx.x < 256) S.hist[threadIdx.x] = 0;
     __syncthreads();
     const int rx = S.geo[0], ry = S.geo[1], rcols = S.geo[2], rrows = S.geo[3];
@@ -262,6 +340,7 @@ __device__ void prepare_window(const WinArgs& a, WindowSmem& S, const Candidate&
 // candidate one after the other, doubling the kernel's latency. Inside an item, stage 3 runs only
 // when stage 2 does not end the check (the reference's early exits, cnn_detector_v3.cpp:1698-1706);
 // otherwise its slot keeps (max -10, count 0), exactly what the reference leaves behind.
+template <bool kLegacy>
 __global__ void __launch_bounds__(kWT, 4) window_kernel(const __grid_constant__ WindowNets N, const WinArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WindowSmem& S = *reinterpret_cast<WindowSmem*>(smem_raw);
@@ -280,7 +359,9 @@ __global__ void __launch_bounds__(kWT, 4) window_kernel(const __grid_constant__ 
         r[1].max = -10.f;
         r[1].knn = 0;
         for (int stage = 0; stage < 2; ++stage) {
-            if (stage == 0)
+            if constexpr (kLegacy)
+                legacy_window_net(a.lg[1 + stage], S, stage == 0 ? 0 : (C.reflection ? 1 : 2));
+            else if (stage == 0)
                 window_net(N.s2, S, 0);
             else
                 window_net(N.s3, S, C.reflection ? 1 : 2);
@@ -312,7 +393,7 @@ __global__ void __launch_bounds__(kWT, 4) window_kernel(const __grid_constant__ 
 int window_smem_bytes() { return (int)sizeof(WindowSmem); }
 
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
-                          const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st) {
+                          const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st, const LegacyNet* lg) {
     static_assert(sizeof(WindowSmem) + 64 <= 48 * 1024, "window kernel shared memory must stay under the default 48 KB");
     WinArgs a;
     a.gray = gray;
@@ -324,7 +405,11 @@ cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, in
     a.levels = levels;
     a.out = out;
     a.cfg = cfg;
-    window_kernel<<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
+    a.lg = lg;
+    if (lg)
+        window_kernel<true><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
+    else
+        window_kernel<false><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
     return cudaGetLastError();
 }
 

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "ccnn_common.cuh"
+#include "legacy.h"
 
 namespace ccnn {
 
@@ -89,8 +90,14 @@ cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_
                                int* counts = nullptr, float thr = 0.f, const uint8_t* back_on = nullptr, GateCells cells = GateCells{});
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
                               const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st);
+// lg (optional): the legacy networks (device memory, [1] stage 2, [2] stage 3) replace N
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
-                          const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st);
+                          const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st,
+                          const LegacyNet* lg = nullptr);
+// one legacy (format 1.0) network on a w x h image (pitch floats): scratch holds its pooled L1 and
+// L2 maps; counts (optional) gets each scan chunk's responses above thr
+cudaError_t launch_legacy_forward(const LegacyNet* d_net, const LegacyNet& h_net, const float* img, int pitch, int w, int h, float* scratch,
+                                  float* resp, cudaStream_t st, int* counts, int chunk_base, float thr);
 int window_smem_bytes();
 // facial analysis: dynamic shared memory attribute (once per device) and the landmark kernel
 cudaError_t facial_setup();

@@ -9,11 +9,11 @@ namespace ccnn {
 // Crop of a candidate's check window in gray-frame coordinates (cnn_detector_v3.cpp:1489-1556):
 // the extended pattern around the stage-1 point, for mod 1 the retry window shrunk by 15 %, then
 // clamped to the frame. geo = {x, y, cols, rows}.
-__device__ __forceinline__ void window_geometry(const Candidate& cd, float inv_scale, int mod, int gw, int gh, int* geo) {
+__device__ __forceinline__ void window_geometry(const Candidate& cd, float inv_scale, int mod, int gw, int gh, int pat_w, int pat_h, int* geo) {
     int x = (int)((float)(cd.px - (kExtOff + kXOff) / 2) * inv_scale);
     int y = (int)((float)(cd.py - kExtOff / 2) * inv_scale);
-    int width = (int)((float)(kPatW + kExtOff + kXOff) * inv_scale);
-    int height = (int)((float)(kPatH + kExtOff) * inv_scale);
+    int width = (int)((float)(pat_w + kExtOff + kXOff) * inv_scale);
+    int height = (int)((float)(pat_h + kExtOff) * inv_scale);
     if (mod == 1) {
         const float k = 0.15f;
         x = (int)(fadd((float)x, fdiv(fmul((float)width, k), 2.f)));

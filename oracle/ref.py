@@ -226,3 +226,27 @@ def legacy_net_forward_isolated(model_path, img):
     import multiprocessing as mp
     with mp.get_context("spawn").Pool(1, maxtasksperchild=1) as pool:
         return pool.apply(legacy_net_forward, (model_path, img))
+
+
+def _legacy_face_detect_worker(img, pargs):
+    L = ctypes.CDLL(REF_LEGACY)
+    L.ref_face_detect.argtypes = [ctypes.POINTER(RefParams), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(RefDet), ctypes.c_int]
+    p = params(**pargs)
+    a = np.ascontiguousarray(img)
+    h, w = a.shape[:2]
+    ch = 1 if a.ndim == 2 else a.shape[2]
+    out = (RefDet * 65536)()
+    n = L.ref_face_detect(ctypes.byref(p), a.ctypes.data, w, h, ch, a.strides[0], out, 65536)
+    if n < 0:
+        raise RuntimeError(f"ref_face_detect (legacy) failed ({n})")
+    return [(d.x, d.y, d.w, d.h, d.score) for d in out[:n]]
+
+
+def legacy_face_detect(img, **pargs):
+    """The reference's public FaceDetector::Detect built for the legacy model family (its embedded
+    cnn4face{1,2,3}_new.bin), in a fresh process for the reason given at legacy_net_forward_isolated.
+    pargs are params() keywords."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(1, maxtasksperchild=1) as pool:
+        return pool.apply(_legacy_face_detect_worker, (img, pargs))

@@ -68,3 +68,40 @@ def test_legacy_forward_matches_reference(name, img, pad):
 def test_legacy_forward_rejects_small_images():
     with pytest.raises(ccnn.CCNNError):
         _device_forward("cnn4face2_new.bin", np.zeros((39, 35), np.float32))
+
+
+def _legacy_detector(w, h, min_face=40, max_face=240, scale=1.15):
+    p = ccnn.default_params()
+    p.max_image_width, p.max_image_height = w, h
+    p.min_face_height, p.max_face_height, p.scale_factor = min_face, max_face, scale
+    p.detect_mode = 1
+    d = ccnn.FaceDetector()
+    assert d.Init(p, models=[os.path.join(MODELS, f"cnn4face{i}_new.bin") for i in (1, 2, 3)]) == 0, _capi.last_error()
+    return d
+
+
+DETECT_CASES = [(640, 480, 1, 5, 40, 200, 3), (640, 480, 2, 5, 40, 200, 3), (640, 480, 3, 5, 40, 200, 3), (640, 480, 4, 5, 40, 200, 1),
+                (1280, 720, 5, 10, 30, 300, 3), (1920, 1080, 7, 20, 30, 300, 3)]
+
+
+@pytest.mark.parametrize("w,h,seed,nf,lo,hi,ch", DETECT_CASES)
+def test_legacy_cascade_matches_reference(w, h, seed, nf, lo, hi, ch):
+    """The whole cascade with the legacy models gives the reference's own faces (built for the legacy
+    family) on the same frame, box for box and score for score."""
+    img = ccnn.synth_frame(w, h, seed, nf, lo, hi, channels=ch)[0]
+    d = _legacy_detector(w, h)
+    got = d.Detect(img)
+    d.Clear()
+    want = ref.legacy_face_detect(img, max_w=w, max_h=h)
+    assert got == want
+    assert len(want) > 0 or seed == 4
+
+
+def test_legacy_detector_refuses_mixed_families_and_the_gate():
+    p = ccnn.default_params()
+    d = ccnn.FaceDetector()
+    mixed = [os.path.join(MODELS, "cnn4face1_new.bin"), os.path.join(MODELS, "cnn4face2_cntk.bin"), os.path.join(MODELS, "cnn4face3_new.bin")]
+    assert d.Init(p, models=mixed) == -1
+    d = _legacy_detector(640, 480)
+    with pytest.raises(ccnn.CCNNError):
+        d.setGate(np.zeros(700, np.float32), 0.5)
