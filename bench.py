@@ -599,7 +599,9 @@ def main():
         "p99_ms": round(float(np.percentile(lat, 99)), 3),
         "hbm_frac_frame_bytes": round(value / world * fb / (hbm_peak * 1e9), 5),
         "clocks": clocks,
-        "e2e": {"value": round(e2e, 2), "unit": "frames/s", "h2d_bytes_per_step": B * W * H * 3,
+        "e2e": {"value": round(e2e, 2), "unit": "frames/s", "h2d_gbs": round(e2e * W * H * 3 / 1e9, 2),
+                "bound_note": "host frames cross PCIe: h2d_gbs is the upload rate this throughput implies",
+                "h2d_bytes_per_step": B * W * H * 3,
                 "d2h_bytes_per_step": B * (4 + 1024 * 20)},
         "gpu_launches": len(KERNELS) * args.steps * B,
         "roofline": roofline,
