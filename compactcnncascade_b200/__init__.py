@@ -47,8 +47,10 @@ class FaceDetector:
         self._models = [None, None, None]
 
     # ---- lifecycle ----
-    def Init(self, param=None, models=None):
-        """FaceDetector::Init (CompactCNNLibAPI_v2.cpp:373-407). Returns 0 or -1."""
+    def Init(self, param=None, models=None, schedule=None):
+        """FaceDetector::Init (CompactCNNLibAPI_v2.cpp:373-407). Returns 0 or -1. `schedule`:
+        None (defaults), "auto" (the autotuner's entry for these parameters, when it has one) or
+        (frame_slots, window_ctas_per_sm)."""
         if self._h is not None:
             self.Clear()
         self._param = param if param is not None else default_params()
@@ -61,6 +63,11 @@ class FaceDetector:
             self.last_status = st
             return -1
         self._h = h
+        if schedule is not None:
+            from . import autotune
+            sched = autotune.lookup(self._param) if schedule == "auto" else tuple(schedule)
+            if sched is not None:
+                autotune.set_schedule(self, *sched)
         return 0
 
     def Clear(self):

@@ -36,7 +36,7 @@ EXPORTED = [
     "ccnn_server_stats_get", "ccnn_host_alloc", "ccnn_host_free", "ccnn_cntk_dump_to_binary",
     "ccnn_check_reciprocal", "ccnn_synth_frame_device", "ccnn_gate_set", "ccnn_gate_disable", "ccnn_gate_stats",
     "ccnn_gate_labels", "ccnn_gate_features", "ccnn_gate_gradient", "ccnn_gate_train", "ccnn_server_set_gate",
-    "ccnn_legacy_model_info", "ccnn_legacy_net_forward",
+    "ccnn_legacy_model_info", "ccnn_legacy_net_forward", "ccnn_set_schedule", "ccnn_get_schedule",
 ]
 
 
@@ -159,6 +159,8 @@ def lib():
         L.ccnn_gate_disable.argtypes = [vp]
         L.ccnn_server_set_gate.argtypes = [vp, fp, ci, ctypes.c_float, ctypes.c_float]
         L.ccnn_legacy_model_info.argtypes = [ctypes.c_char_p, P(ci), ci]
+        L.ccnn_set_schedule.argtypes = [vp, ci, ci]
+        L.ccnn_get_schedule.argtypes = [vp, P(ci), P(ci)]
         L.ccnn_legacy_net_forward.argtypes = [ctypes.c_char_p, vp, ci, ci, ctypes.c_size_t, vp, ci, P(ci), P(ci), vp]
         L.ccnn_gate_stats.argtypes = [vp, P(ci), P(ci), P(ci), P(ci), P(ci)]
         L.ccnn_gate_labels.argtypes = [vp, vp, vp]

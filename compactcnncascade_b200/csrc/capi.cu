@@ -119,6 +119,17 @@ CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* ke
     return h->det.profile(iters, kernel_ms, n_kernels);
 }
 
+CCNN_API ccnn_status ccnn_set_schedule(ccnn_handle h, int frame_slots, int window_ctas_per_sm) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    return h->det.set_schedule(frame_slots, window_ctas_per_sm);
+}
+
+CCNN_API ccnn_status ccnn_get_schedule(ccnn_handle h, int* frame_slots, int* window_ctas_per_sm) {
+    if (!h || !frame_slots || !window_ctas_per_sm) return CCNN_ERR_INVALID_ARG;
+    h->det.get_schedule(frame_slots, window_ctas_per_sm);
+    return CCNN_OK;
+}
+
 CCNN_API ccnn_status ccnn_gate_set(ccnn_handle h, const float* params, int n_params, float threshold, float fallback_fraction) {
     if (!h) return CCNN_ERR_INVALID_ARG;
     return h->det.gate_set(params, n_params, threshold, fallback_fraction);

@@ -331,7 +331,7 @@ ccnn_status Detector::init() {
     cudaDeviceProp prop;
     CCNN_CUDA(cudaGetDeviceProperties(&prop, device_));
     // persistent stage-2/3 grid: 4 resident 256-thread CTAs per SM (register bound)
-    window_grid_ = prop.multiProcessorCount * 4;
+    window_grid_ = prop.multiProcessorCount * window_ctas_per_sm_;
     facial_grid_ = prop.multiProcessorCount;  // one 118 KB-shared-memory block per SM
     CCNN_CUDA(replay_setup());
     CCNN_CUDA(stage1_setup());
@@ -541,6 +541,23 @@ ccnn_status Detector::gate_set(const float* params, int n, float threshold, floa
         s.exec_plan = nullptr;  // the per-frame graphs are captured again with the gate
     }
     return CCNN_OK;
+}
+
+ccnn_status Detector::set_schedule(int frame_slots, int window_ctas_per_sm) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (frame_slots < 0 || frame_slots > 64 || window_ctas_per_sm < 0 || window_ctas_per_sm > 4) {
+        set_error("schedule: 1-64 frame slots and 1-4 stage-2/3 blocks per SM (0 keeps the current value)");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    clear();
+    if (frame_slots > 0) slots_.assign(frame_slots, Slot());
+    if (window_ctas_per_sm > 0) window_ctas_per_sm_ = window_ctas_per_sm;
+    return init();
+}
+
+void Detector::get_schedule(int* frame_slots, int* window_ctas_per_sm) const {
+    *frame_slots = (int)slots_.size();
+    *window_ctas_per_sm = window_ctas_per_sm_;
 }
 
 ccnn_status Detector::gate_disable() {

@@ -103,6 +103,14 @@ CCNN_API ccnn_status ccnn_cntk_dump_to_binary(const char* binary_file, const cha
 CCNN_API ccnn_status ccnn_synth_frame_device(void* d_out, int width, int height, int channels, size_t step, unsigned long long seed,
                                              int n_faces, int min_face, int max_face, void* faces_out, void* stream);
 
+/* Schedule of a handle, as the autotuner (compactcnncascade_b200/autotune.py) picks it per frame size:
+ * frames in flight (1-64, default 8) and resident blocks per SM of the persistent stage-2/3 window
+ * kernel (1-4, default 4); 0 keeps a value. Rebuilds the handle's device state (as a re-Init does).
+ * Results do not depend on the schedule. No reference counterpart (the reference has no GPU
+ * schedule to tune). */
+CCNN_API ccnn_status ccnn_set_schedule(ccnn_handle h, int frame_slots, int window_ctas_per_sm);
+CCNN_API ccnn_status ccnn_get_schedule(ccnn_handle h, int* frame_slots, int* window_ctas_per_sm);
+
 /* Legacy cascade networks (model format 1.0, the cnn4face{1,2,3}_new.bin family: tanh activations,
  * max or average pooling; reader SIMD::ConvNeuralNetwork::Init, src/CNNObjectDetector/cnn_simd.cpp:40-336,
  * forward pass Run_single_thread, cnn_simd.cpp:551-874, in the reference's plain-C++ build).
