@@ -2,7 +2,7 @@
 // pyramid octave and per 16x16 cell of the frame, whether the plain cascade's stage 2/3 will accept
 // a window centred there. Stage-1 tiles whose footprint holds no likely cell are skipped.
 //
-// No reference counterpart: this is an addition to the cascade, judged against the plain (full
+// No reference counterpart: this is an addition to the cascade, evaluated against the plain (full
 // scan) cascade by box recall. Network (fp16 storage, fp32 accumulation):
 //   f  = (8x8 box average of the gray frame - 128) / 64             (W/8 x H/8, 1 channel)
 //   a1 = LReLU_0.1(conv3x3(f; 8 maps) + b1)                          (zero padding)

@@ -9,7 +9,7 @@ no cell above the threshold are skipped, and a frame with many cells just below 
 scanned in full.
 
 No reference counterpart: the reference scans every level in full (CNNDetector::RunCPUDetect,
-src/CNNObjectDetector/cnn_detector_v3.cpp:2063-2235); the gate is judged against that full scan by
+src/CNNObjectDetector/cnn_detector_v3.cpp:2063-2235); the gate is evaluated against that full scan by
 box recall.
 
     python -m compactcnncascade_b200.gate --train-frames 20000 --eval-frames 1000 --out weights.bin

@@ -2,7 +2,7 @@
  *
  * No reference counterpart: the reference scans every pyramid level in full
  * (CNNDetector::RunCPUDetect, src/CNNObjectDetector/cnn_detector_v3.cpp:2063-2235). The gate is
- * an addition judged against that full scan by box recall: a small network on an 8x8-averaged
+ * an addition evaluated against that full scan by box recall: a small network on an 8x8-averaged
  * copy of the gray frame predicts, for each pyramid octave and each 16x16-pixel cell of the
  * frame, whether the cascade will accept a window centred in that cell. Stage-1 tiles whose
  * candidates' window centres lie in no likely cell (with one cell of margin) are skipped; a frame
