@@ -134,6 +134,25 @@ def test_partial_gate_recomputes_every_active_tile(seeds):
     assert skipped > 0
 
 
+@pytest.mark.parametrize("w,h", [(47, 51), (64, 64), (100, 80), (333, 211)])
+def test_gate_on_small_and_odd_frames(w, h):
+    """Frames down to the stage-2/3 window: a gate that keeps every tile changes nothing, one that keeps
+    none leaves no face (frames under 32x32 gray pixels would always run in full)."""
+    p = ccnn.default_params()
+    p.max_image_width, p.max_image_height = w, h
+    p.min_face_height, p.max_face_height, p.scale_factor = 40, 240, 1.15
+    d = ccnn.FaceDetector()
+    assert d.Init(p) == 0
+    img = ccnn.synth_frame(w, h, 90 + w, 2, 40, max(41, min(w, h) - 2))[0]
+    plain = d.Detect(img)
+    d.setGate(_const_params(0.999), 0.5, 0.25)
+    assert d.Detect(img) == plain
+    fr, ft, br, bt, fb = d.gateStats()
+    assert (fr, br) == (ft, bt)
+    d.setGate(_const_params(1e-6), 0.5, 0.25)
+    assert d.Detect(img) == []
+
+
 def test_gate_rejects_bad_arguments():
     d = _det()
     with pytest.raises(ccnn.CCNNError):
