@@ -594,6 +594,11 @@ ccnn_status Detector::gate_stats(int* front_run, int* front_total, int* back_run
     cudaSetDevice(device_);
     CCNN_CUDA(cudaStreamSynchronize(s.st));
     const Plan& p = *s.last_plan;
+    *fallback = 0;
+    if (p.n_levels <= 0) {  // a frame too small for any level scans nothing
+        *front_run = *front_total = *back_run = *back_total = 0;
+        return CCNN_OK;
+    }
     const LevelDesc& last = p.levels[p.n_levels - 1];
     const int nb = last.k2_base + last.k2_tiles_x * ((last.oh + kK2TileY - 1) / kK2TileY);
     const int nf = last.k1_base + last.k1_tiles_x * ((last.p1h + kK1TileY - 1) / kK1TileY);
