@@ -74,7 +74,7 @@ CCNN_API ccnn_status ccnn_inspect_response(ccnn_handle h, int level, float* out,
 CCNN_API ccnn_status ccnn_inspect_candidates(ccnn_handle h, ccnn_candidate* out, int capacity, int* n);
 CCNN_API ccnn_status ccnn_inspect_raw_detections(ccnn_handle h, ccnn_detection* out, int capacity, int* n);
 
-/* The pyramid a freshly created handle processes for a frame of this size and channel count
+/* The pyramid a freshly created handle (with the CNTK models) processes for a frame of this size and channel count
  * (CNNDetector::InitScales, cnn_detector_v3.cpp:289-346, with the level-size rule of RunCPUDetect
  * :2080-2088 and the re-initialisation rules of Detect :2499-2546). Host-only; needs no GPU. */
 CCNN_API ccnn_status ccnn_plan_levels(const ccnn_params* p, int cols, int rows, int channels, ccnn_level_info* out, int capacity,
