@@ -540,7 +540,7 @@ def main():
             for s in range(args.steps):
                 g_ms += device_step(args.warmup + s)
             barrier()
-        g_value = args.steps * B * world / (g_ms / 1e3)
+        g_wall_e2e = None
         for s in range(args.warmup):
             host_step(s)
         barrier()
@@ -548,7 +548,14 @@ def main():
         for s in range(args.steps):
             host_step(args.warmup + s)
         barrier()
-        g_e2e = args.steps * B * world / (time.perf_counter() - t0)
+        g_wall_e2e = time.perf_counter() - t0
+        g_t = g_ms / 1e3
+        if dist:  # the slowest rank sets the job's time, as for `value`
+            t = torch.tensor([g_t, g_wall_e2e], device=f"cuda:{dev}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            g_t, g_wall_e2e = float(t[0]), float(t[1])
+        g_value = args.steps * B * world / g_t
+        g_e2e = args.steps * B * world / g_wall_e2e
         glat = []
         for i in range(args.latency_frames):
             t = h_frames[i % len(frames)]
