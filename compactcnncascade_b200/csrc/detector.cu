@@ -395,6 +395,7 @@ ccnn_status Detector::build_plan(int w, int h, int ch, int num_scales, Plan* p) 
     p->in_w = w;
     p->in_h = h;
     p->ch = ch;
+    p->in_pitch = (size_t)round_up((long long)w * ch, 64);
     p->downscale = input_downscale_ && ch == 1;
     if (p->downscale)
         size_scale(w, h, input_scale_, &p->gw, &p->gh);
@@ -648,9 +649,9 @@ ReplayArgs Detector::replay_args(Slot& s, const Plan& p) const {
 ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
     cudaError_t e;
     if (p.downscale)
-        e = launch_gray_u8_resized(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, s.d_gray, s.gray_pitch, p.gw, p.gh, s.st);
+        e = launch_gray_u8_resized(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, s.d_gray, s.gray_pitch, p.gw, p.gh, s.st);
     else
-        e = launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st);
+        e = launch_gray(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st);
     CCNN_CUDA(e);
     // the learned gate decides which stage-1 tiles run, and so which parts of the pyramid are read
     const bool gated = gate_on_ && s.gate.prob && p.gw >= 32 && p.gh >= 32;
@@ -695,9 +696,15 @@ ccnn_status Detector::enqueue_legacy_stage1(Slot& s, const Plan& p) {
 }
 
 ccnn_status Detector::enqueue(Slot& s, const Plan& p, const ccnn_image& img, bool device_input, cudaStream_t) {
+    // the frame's rows packed at the plan's pitch: a frame whose own step is that pitch (any 8-bit
+    // frame whose row is a multiple of 64 bytes, such as 1920 x 3) goes up as one contiguous copy,
+    // which the copy engines move faster over PCIe than row-by-row descriptors
     const size_t row = (size_t)img.cols * img.channels;
-    CCNN_CUDA(cudaMemcpy2DAsync(s.d_in, s.in_pitch, img.data, img.step, row, img.rows,
-                                device_input ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s.st));
+    const cudaMemcpyKind kind = device_input ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (img.step == p.in_pitch)
+        CCNN_CUDA(cudaMemcpyAsync(s.d_in, img.data, p.in_pitch * (size_t)(img.rows - 1) + row, kind, s.st));
+    else
+        CCNN_CUDA(cudaMemcpy2DAsync(s.d_in, p.in_pitch, img.data, img.step, row, img.rows, kind, s.st));
     if (s.exec_plan != &p) {
         if (s.exec) {
             cudaGraphExecDestroy(s.exec);
@@ -1075,9 +1082,9 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     for (int it = 0; it < iters; ++it) {
         CCNN_CUDA(cudaEventRecord(ev[0], s.st));
         if (p.downscale)
-            CCNN_CUDA(launch_gray_u8_resized(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, s.d_gray, s.gray_pitch, p.gw, p.gh, s.st));
+            CCNN_CUDA(launch_gray_u8_resized(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, s.d_gray, s.gray_pitch, p.gw, p.gh, s.st));
         else
-            CCNN_CUDA(launch_gray(s.d_in, (int)s.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st));
+            CCNN_CUDA(launch_gray(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st));
         CCNN_CUDA(cudaEventRecord(ev[1], s.st));
         if (gated) {
             CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_,

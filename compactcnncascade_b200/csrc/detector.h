@@ -22,6 +22,7 @@ namespace ccnn {
 // One pyramid plan: everything that depends on the frame size and the level count in force.
 struct Plan {
     int in_w = 0, in_h = 0, ch = 0;  // input frame
+    size_t in_pitch = 0;             // bytes per row of the frame in the slot's input buffer (packed to 64)
     int gw = 0, gh = 0;              // gray image (after the optional 8-bit downscale)
     bool downscale = false;
     int n_levels = 0;                // processed levels scl = 0 .. n_levels-1
