@@ -16,6 +16,7 @@
 #include "model.h"
 
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <cstring>
 
@@ -90,6 +91,7 @@ Detector::~Detector() {
 
 void Detector::free_slot(Slot& s) {
     if (s.exec) cudaGraphExecDestroy(s.exec);
+    if (s.graph) cudaGraphDestroy(s.graph);
     cudaFree(s.d_in);
     cudaFree(s.d_gray);
     cudaFree(s.d_limg);
@@ -695,21 +697,29 @@ ccnn_status Detector::enqueue_legacy_stage1(Slot& s, const Plan& p) {
     return CCNN_OK;
 }
 
+// Points the graph's gray-conversion node at `src` (row pitch `spitch` bytes) for the next launches.
+static cudaError_t retarget_gray(Slot& s, const Plan& p, const uint8_t* src, int spitch) {
+    int w = p.in_w, h = p.in_h, dpitch = s.gray_pitch;
+    float* dst = s.d_gray;
+    void* args[6] = {&src, &spitch, &w, &h, &dst, &dpitch};
+    cudaKernelNodeParams kp = s.gray_kp;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    return cudaGraphExecKernelNodeSetParams(s.exec, s.gray_node, &kp);
+}
+
 ccnn_status Detector::enqueue(Slot& s, const Plan& p, const ccnn_image& img, bool device_input, cudaStream_t) {
-    // the frame's rows packed at the plan's pitch: a frame whose own step is that pitch (any 8-bit
-    // frame whose row is a multiple of 64 bytes, such as 1920 x 3) goes up as one contiguous copy,
-    // which the copy engines move faster over PCIe than row-by-row descriptors
-    const size_t row = (size_t)img.cols * img.channels;
-    const cudaMemcpyKind kind = device_input ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if (img.step == p.in_pitch)
-        CCNN_CUDA(cudaMemcpyAsync(s.d_in, img.data, p.in_pitch * (size_t)(img.rows - 1) + row, kind, s.st));
-    else
-        CCNN_CUDA(cudaMemcpy2DAsync(s.d_in, p.in_pitch, img.data, img.step, row, img.rows, kind, s.st));
     if (s.exec_plan != &p) {
         if (s.exec) {
             cudaGraphExecDestroy(s.exec);
             s.exec = nullptr;
         }
+        if (s.graph) {
+            cudaGraphDestroy(s.graph);
+            s.graph = nullptr;
+        }
+        s.gray_node = nullptr;
+        s.gray_in_place = false;
         cudaGraph_t g;
         CCNN_CUDA(cudaStreamBeginCapture(s.st, cudaStreamCaptureModeThreadLocal));
         ccnn_status st = enqueue_kernels(s, p);
@@ -717,10 +727,51 @@ ccnn_status Detector::enqueue(Slot& s, const Plan& p, const ccnn_image& img, boo
         if (st != CCNN_OK) return st;
         CCNN_CUDA(ce);
         ce = cudaGraphInstantiate(&s.exec, g, 0);
-        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) cudaGraphDestroy(g);
         CCNN_CUDA(ce);
+        s.graph = g;
         s.exec_plan = &p;
+        // the gray-conversion node, so that device frames can be read where they are
+        if (!p.downscale) {
+            size_t nn = 0;
+            CCNN_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+            std::vector<cudaGraphNode_t> nodes(nn);
+            if (nn) CCNN_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+            const void* fn = gray_kernel_fn(p.ch);
+            for (cudaGraphNode_t nd : nodes) {
+                cudaGraphNodeType t;
+                CCNN_CUDA(cudaGraphNodeGetType(nd, &t));
+                if (t != cudaGraphNodeTypeKernel) continue;
+                cudaKernelNodeParams kp;
+                CCNN_CUDA(cudaGraphKernelNodeGetParams(nd, &kp));
+                if (kp.func == fn) {
+                    s.gray_node = nd;
+                    s.gray_kp = kp;
+                    break;
+                }
+            }
+        }
     }
+    // A device frame with the gray kernel's alignment (64-byte base and step) is read in place;
+    // anything else is packed into the slot's input buffer at the plan's pitch, as one contiguous
+    // copy when the frame's step already is that pitch (the copy engines move it faster than rows).
+    const bool in_place = device_input && s.gray_node && !((uintptr_t)img.data & 63) && !(img.step & 63) && img.step <= (size_t)INT32_MAX;
+    if (in_place) {
+        CCNN_CUDA(retarget_gray(s, p, (const uint8_t*)img.data, (int)img.step));
+        s.gray_in_place = true;
+    } else {
+        if (s.gray_in_place) {
+            CCNN_CUDA(retarget_gray(s, p, s.d_in, (int)p.in_pitch));
+            s.gray_in_place = false;
+        }
+        const size_t row = (size_t)img.cols * img.channels;
+        const cudaMemcpyKind kind = device_input ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        if (img.step == p.in_pitch)
+            CCNN_CUDA(cudaMemcpyAsync(s.d_in, img.data, p.in_pitch * (size_t)(img.rows - 1) + row, kind, s.st));
+        else
+            CCNN_CUDA(cudaMemcpy2DAsync(s.d_in, p.in_pitch, img.data, img.step, row, img.rows, kind, s.st));
+    }
+    s.last_in_place = in_place;
     CCNN_CUDA(cudaGraphLaunch(s.exec, s.st));
     CCNN_CUDA(cudaEventRecord(s.done, s.st));
     s.last_plan = &p;
@@ -1070,6 +1121,11 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     if (!inited_ || !s.last_plan || iters <= 0) {
         set_error("no frame has been processed");
         return CCNN_ERR_INVALID_ARG;
+    }
+    if (s.last_in_place) {
+        // the last frame was read from the caller's device memory, which may be gone by now
+        set_error("the last frame was read in place from device memory; profile a frame given from host memory");
+        return CCNN_ERR_UNSUPPORTED;
     }
     cudaSetDevice(device_);
     const Plan& p = *s.last_plan;

@@ -66,6 +66,11 @@ struct Slot {
     int* d_fa = nullptr;         // facial analysis: replay scratch (5 x candidate capacity)
     cudaGraphExec_t exec = nullptr;
     const Plan* exec_plan = nullptr;
+    cudaGraph_t graph = nullptr;          // kept while `exec` lives: its gray-kernel node is updated per frame
+    cudaGraphNode_t gray_node = nullptr;  // the gray conversion, retargeted at a device frame read in place
+    cudaKernelNodeParams gray_kp{};
+    bool gray_in_place = false;           // the node currently reads the caller's frame
+    bool last_in_place = false;           // the last frame was not copied into d_in
     const Plan* last_plan = nullptr;  // plan of the last frame run on this slot
 };
 

@@ -50,6 +50,15 @@ __global__ void __launch_bounds__(256) gray_kernel(const uint8_t* __restrict__ s
     }
 }
 
+const void* gray_kernel_fn(int ch) {
+    switch (ch) {
+        case 1: return reinterpret_cast<const void*>(gray_kernel<1>);
+        case 3: return reinterpret_cast<const void*>(gray_kernel<3>);
+        case 4: return reinterpret_cast<const void*>(gray_kernel<4>);
+    }
+    return nullptr;
+}
+
 cudaError_t launch_gray(const uint8_t* src, int spitch, int w, int h, int ch, float* dst, int dpitch, cudaStream_t st) {
     if ((spitch & 63) || (dpitch & 15) || (reinterpret_cast<uintptr_t>(src) & 63) || (reinterpret_cast<uintptr_t>(dst) & 63))
         return cudaErrorMisalignedAddress;  // the staging buffers are allocated 64-byte aligned

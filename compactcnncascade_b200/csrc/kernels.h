@@ -43,6 +43,8 @@ struct ReplayArgs {
     int* n_faces;
 };
 
+// the gray kernel instantiation for `ch` channels (to find its node in a captured graph)
+const void* gray_kernel_fn(int ch);
 cudaError_t launch_gray(const uint8_t* src, int spitch, int w, int h, int ch, float* dst, int dpitch, cudaStream_t st);
 cudaError_t launch_gray_u8_resized(const uint8_t* src, int spitch, int sw, int sh, float* dst, int dpitch, int dw, int dh,
                                    cudaStream_t st);

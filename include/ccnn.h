@@ -98,7 +98,8 @@ CCNN_API ccnn_status ccnn_destroy(ccnn_handle h);
 CCNN_API ccnn_status ccnn_detect(ccnn_handle h, const ccnn_image* img, ccnn_face* faces, int capacity, int* n_faces);
 
 /* Same, for an image already in device memory (img->data is a device pointer). `stream` is a
- * cudaStream_t (NULL = the handle's own stream); the call returns after the result is on the host. */
+ * cudaStream_t (NULL = the handle's own stream); the call returns after the result is on the host.
+ * A frame whose base and row step are multiples of 64 bytes is read in place (not copied). */
 CCNN_API ccnn_status ccnn_detect_device(ccnn_handle h, const ccnn_image* img, void* stream, ccnn_face* faces, int capacity,
                                         int* n_faces);
 

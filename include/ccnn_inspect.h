@@ -80,8 +80,8 @@ CCNN_API ccnn_status ccnn_inspect_raw_detections(ccnn_handle h, ccnn_detection* 
 CCNN_API ccnn_status ccnn_plan_levels(const ccnn_params* p, int cols, int rows, int channels, ccnn_level_info* out, int capacity,
                                       int* n_levels);
 
-/* Re-runs the handle's last frame `iters` times and writes the mean duration (ms, CUDA events)
- * of each kernel of the chain: [0] gray, [1] pyramid, [2] stage-1 front, [3] stage-1 back (which also
+/* Re-runs the handle's last frame `iters` times (CCNN_ERR_UNSUPPORTED when that frame was read in
+ * place from device memory) and writes the mean duration (ms, CUDA events) of each kernel of the chain: [0] gray, [1] pyramid, [2] stage-1 front, [3] stage-1 back (which also
  * counts the candidates), [4] candidate write, [5] stage-2/3 windows, [6] replay/sort/merge. */
 CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* kernel_ms, int n_kernels);
 
