@@ -37,3 +37,23 @@ def test_reader_refuses_other_files(tmp_path):
     assert _capi.lib().ccnn_legacy_model_info(str(cut).encode(), info, 10) == _capi.ERR_MODEL
     assert "truncated" in _capi.last_error()
     assert _capi.lib().ccnn_legacy_model_info(b"/nonexistent/model.bin", info, 10) == _capi.ERR_MODEL
+
+
+# ---- the float32 restatement (oracle/legacy_ref.py) against the reference's legacy build ----
+
+import numpy as np  # noqa: E402
+
+from oracle import legacy_ref, ref  # noqa: E402
+
+
+@pytest.mark.skipif(not ref.legacy_available(), reason="legacy reference build (oracle/_ref) not available")
+@pytest.mark.parametrize("name,shape,seed", [("cnn4face1_new.bin", (150, 200), 1), ("cnn4face1_new.bin", (31, 27), 2),
+                                             ("cnn4face2_new.bin", (51, 47), 3), ("cnn4face2_new.bin", (64, 80), 4),
+                                             ("cnn4face3_new.bin", (51, 47), 5), ("cnn4face3_new.bin", (70, 90), 6)])
+def test_restatement_matches_reference(name, shape, seed):
+    img = np.random.default_rng(seed).uniform(0, 255, shape).astype(np.float32)
+    path = os.path.join(MODELS, name)
+    got = legacy_ref.forward(legacy_ref.load(path), img)
+    want = ref.legacy_net_forward_isolated(path, img)
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), float(np.abs(got - want).max())
