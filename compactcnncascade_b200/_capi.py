@@ -37,6 +37,8 @@ EXPORTED = [
     "ccnn_check_reciprocal", "ccnn_synth_frame_device", "ccnn_gate_set", "ccnn_gate_disable", "ccnn_gate_stats",
     "ccnn_gate_labels", "ccnn_gate_features", "ccnn_gate_gradient", "ccnn_gate_train", "ccnn_server_set_gate",
     "ccnn_legacy_model_info", "ccnn_legacy_net_forward", "ccnn_set_schedule", "ccnn_get_schedule",
+    "ccnn_measure_fp32_peak", "ccnn_cnn_default_params", "ccnn_cnn_create", "ccnn_cnn_detect", "ccnn_cnn_nms",
+    "ccnn_cnn_get_params", "ccnn_cnn_set_params",
 ]
 
 
@@ -91,6 +93,25 @@ class Detection(ctypes.Structure):
                 ("num_detect", ctypes.c_int)]
 
 
+class CnnParam(ctypes.Structure):
+    """ccnn_cnn_param: CNNDetector::Param (include/ccnn_cnn.h)."""
+    _fields_ = [("pipeline", ctypes.c_int), ("max_image_width", ctypes.c_int), ("max_image_height", ctypes.c_int),
+                ("min_obj_width", ctypes.c_int), ("min_obj_height", ctypes.c_int), ("max_obj_width", ctypes.c_int),
+                ("max_obj_height", ctypes.c_int), ("scale_factor", ctypes.c_float), ("min_neighbors", ctypes.c_int),
+                ("num_threads", ctypes.c_int)]
+
+
+class CnnAdvancedParam(ctypes.Structure):
+    """ccnn_cnn_advanced_param: CNNDetector::AdvancedParam (include/ccnn_cnn.h)."""
+    _fields_ = [(n, ctypes.c_int) for n in ("detect_mode", "detect_precision", "packet_detection", "gray_image_only",
+                                            "facial_analysis", "equalize", "reflection", "type_check")] + \
+               [(n, ctypes.c_float) for n in ("treshold_1", "treshold_2", "treshold_3")] + \
+               [(n, ctypes.c_int) for n in ("adapt_min_neighbors", "double_check", "drop_detect", "min_num_detect", "device_info",
+                                            "cuda_device_id", "cl_platform_id", "cl_device_id", "concurrent_kernels",
+                                            "num_cnn_copy", "blur", "img_resize", "uniform_noise", "merger_detect")] + \
+               [("index_output", ctypes.c_int * 4)]
+
+
 class SynthFace(ctypes.Structure):
     _fields_ = [("cx", ctypes.c_int), ("cy", ctypes.c_int), ("w", ctypes.c_int), ("h", ctypes.c_int),
                 ("angle_deg", ctypes.c_float), ("contrast", ctypes.c_float)]
@@ -131,6 +152,14 @@ def lib():
         L.ccnn_gray_u8_to_f32.argtypes = [vp, ci, ci, ci, ctypes.c_size_t, vp, ctypes.c_size_t, vp]
         L.ccnn_resize_f32.argtypes = [vp, ci, ci, ctypes.c_size_t, vp, ci, ci, ctypes.c_size_t, ci, vp]
         L.ccnn_stage1_forward.argtypes = [vp, vp, ci, ci, ctypes.c_size_t, vp, ci, P(ci), P(ci), vp]
+        L.ccnn_measure_fp32_peak.argtypes = [ci, ci, P(ctypes.c_double), P(ctypes.c_float)]
+        L.ccnn_cnn_default_params.argtypes = [P(CnnParam), P(CnnAdvancedParam)]
+        L.ccnn_cnn_default_params.restype = None
+        L.ccnn_cnn_create.argtypes = [P(CnnParam), P(CnnAdvancedParam), P(ctypes.c_char_p), P(vp)]
+        L.ccnn_cnn_detect.argtypes = [vp, P(Image), P(Detection), ci, P(Detection), ci, P(ci)]
+        L.ccnn_cnn_nms.argtypes = [vp, P(Detection), ci, P(Detection), ci, P(ci)]
+        L.ccnn_cnn_get_params.argtypes = [vp, P(CnnParam), P(CnnAdvancedParam)]
+        L.ccnn_cnn_set_params.argtypes = [vp, P(CnnParam), P(CnnAdvancedParam)]
         L.ccnn_inspect_levels.argtypes = [vp, P(LevelInfo), ci, P(ci)]
         L.ccnn_inspect_response.argtypes = [vp, ci, vp, ci]
         L.ccnn_inspect_candidates.argtypes = [vp, P(CandidateInfo), ci, P(ci)]

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CU_SOURCES = ["capi.cu", "detector.cu", "k_image.cu", "k_stage1.cu", "k_candidates.cu", "k_window.cu", "k_replay.cu", "noalloc.cu", "server.cu", "k_facial.cu", "gate.cu", "synth_device.cu", "k_legacy.cu"]
+CU_SOURCES = ["capi.cu", "detector.cu", "k_image.cu", "k_stage1.cu", "k_candidates.cu", "k_window.cu", "k_replay.cu", "noalloc.cu", "server.cu", "k_facial.cu", "gate.cu", "synth_device.cu", "k_legacy.cu", "k_peak.cu"]
 CPP_SOURCES = ["model.cpp", "convert.cpp"]
 
 # -fmad=false: the kernels must reproduce the reference's uncontracted IEEE single arithmetic.
@@ -36,7 +36,7 @@ def build(verbose=False, force=False):
     out = os.path.join(HERE, "libccnn.so")
     srcs = [os.path.join(CSRC, s) for s in CU_SOURCES + CPP_SOURCES]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh", ".c"))]
-    deps += [os.path.join(HERE, "..", "include", f) for f in ("ccnn.h", "ccnn_inspect.h", "ccnn_server.h", "ccnn_gate.h")]
+    deps += [os.path.join(HERE, "..", "include", f) for f in ("ccnn.h", "ccnn_inspect.h", "ccnn_server.h", "ccnn_gate.h", "ccnn_cnn.h")]
     if force or _stale(out, deps):
         tmp = out + ".tmp"
         if os.path.exists(out):

@@ -119,6 +119,106 @@ CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* ke
     return h->det.profile(iters, kernel_ms, n_kernels);
 }
 
+// ---- the internal CNNDetector class: include/ccnn_cnn.h ----
+
+CCNN_API void ccnn_cnn_default_params(ccnn_cnn_param* p, ccnn_cnn_advanced_param* ap) {
+    // member defaults of CNNDetector::Param / AdvancedParam (cnn_detector_v3.h:114-175)
+    if (p) {
+        std::memset(p, 0, sizeof(*p));
+        p->pipeline = CCNN_PIPELINE_CPU;
+        p->max_image_width = 1280;
+        p->max_image_height = 720;
+        p->min_obj_width = 48;
+        p->min_obj_height = 48;
+        p->max_obj_width = 0;
+        p->max_obj_height = 0;
+        p->scale_factor = 1.2f;
+        p->min_neighbors = 2;
+        p->num_threads = 0;
+    }
+    if (ap) {
+        std::memset(ap, 0, sizeof(*ap));
+        ap->detect_mode = CCNN_DETECT_SYNC;
+        ap->detect_precision = CCNN_PRECISION_NORMAL;
+        ap->packet_detection = 0;
+        ap->gray_image_only = 0;
+        ap->facial_analysis = 0;
+        ap->equalize = 1;
+        ap->reflection = 1;
+        ap->type_check = 1;
+        ap->treshold_1 = ap->treshold_2 = ap->treshold_3 = 0.f;
+        ap->adapt_min_neighbors = 0;
+        ap->double_check = 1;
+        ap->drop_detect = 1;
+        ap->min_num_detect = 1;
+        ap->device_info = 0;
+        ap->cuda_device_id = 0;
+        ap->cl_platform_id = -1;
+        ap->cl_device_id = -1;
+        ap->concurrent_kernels = 3;
+        ap->num_cnn_copy = 1;
+        ap->blur = 0;
+        ap->img_resize = 0;  // ImgResize::NearestNeighbor
+        ap->uniform_noise = 0;
+        ap->merger_detect = 1;
+        ap->index_output[0] = 1;
+        ap->index_output[1] = 0;
+        ap->index_output[2] = 0;
+        ap->index_output[3] = -1;
+    }
+}
+
+CCNN_API ccnn_status ccnn_cnn_create(const ccnn_cnn_param* p, const ccnn_cnn_advanced_param* ap, const char* const* model_paths,
+                                     ccnn_handle* out) {
+    if (!out) {
+        set_error("null argument");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    ccnn_cnn_param dp;
+    ccnn_cnn_advanced_param dap;
+    ccnn_cnn_default_params(&dp, &dap);  // CNNDetector(Param* = 0, AdvancedParam* = 0): the defaults
+    ccnn_detector* h = new (std::nothrow) ccnn_detector();
+    if (!h) {
+        set_error("out of host memory");
+        return CCNN_ERR_OOM;
+    }
+    ccnn_status st = h->det.create_cnn(p ? *p : dp, ap ? *ap : dap, model_paths);
+    if (st != CCNN_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return CCNN_OK;
+}
+
+CCNN_API ccnn_status ccnn_cnn_detect(ccnn_handle h, const ccnn_image* img, const ccnn_detection* prior, int n_prior, ccnn_detection* out,
+                                     int capacity, int* n) {
+    if (!h || !img) {
+        set_error("null argument");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    return h->det.detect_cnn(*img, prior, n_prior, out, capacity, n);
+}
+
+CCNN_API ccnn_status ccnn_cnn_nms(ccnn_handle h, const ccnn_detection* rect, int n_rect, ccnn_detection* out, int capacity, int* n_out) {
+    if (!h) {
+        set_error("null argument");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    return h->det.nms(rect, n_rect, out, capacity, n_out);
+}
+
+CCNN_API ccnn_status ccnn_cnn_get_params(ccnn_handle h, ccnn_cnn_param* p, ccnn_cnn_advanced_param* ap) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    return h->det.get_cnn_params(p, ap);
+}
+
+CCNN_API ccnn_status ccnn_cnn_set_params(ccnn_handle h, const ccnn_cnn_param* p, const ccnn_cnn_advanced_param* ap) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    return h->det.set_cnn_params(p, ap);
+}
+
 CCNN_API ccnn_status ccnn_set_schedule(ccnn_handle h, int frame_slots, int window_ctas_per_sm) {
     if (!h) return CCNN_ERR_INVALID_ARG;
     return h->det.set_schedule(frame_slots, window_ctas_per_sm);

@@ -84,6 +84,7 @@ bool compute_scales(const ccnn_params& p, bool gray_only, int pat_h, int max_h, 
 
 Detector::~Detector() {
     clear();
+    if (order_ev_) cudaEventDestroy(order_ev_);
     if (d_lnet_) cudaFree(d_lnet_);
     if (d_gate_) cudaFree(d_gate_);
     if (d_lg_) cudaFree(d_lg_);
@@ -122,6 +123,8 @@ void Detector::free_slot(Slot& s) {
     cudaFree(s.d_nraw);
     cudaFree(s.d_faces);
     cudaFree(s.d_nfaces);
+    cudaFree(s.d_mk);
+    cudaFree(s.d_nmk);
     cudaFreeHost(s.h_nfaces);
     cudaFreeHost(s.h_faces);
     if (s.done) cudaEventDestroy(s.done);
@@ -156,6 +159,14 @@ ccnn_status Detector::apply_precision() {
     double_check_ = true;
     detect_enabled_ = api_.detect_mode != CCNN_DETECT_DISABLE;
     merger_detect_ = detect_enabled_;
+    if (has_cnn_) {
+        // CNNDetector's own AdvancedParam instead of the values paramConverter fixes
+        type_check_ = cnn_ap_.type_check;
+        min_num_detect_ = cnn_ap_.min_num_detect;
+        adapt_min_neighbors_ = cnn_ap_.adapt_min_neighbors != 0;
+        double_check_ = cnn_ap_.double_check != 0;
+        merger_detect_ = cnn_ap_.merger_detect != 0;
+    }
     if (api_.detect_precision == CCNN_PRECISION_DEF) {
         gray_image_only_ = true;
         type_check_ = 1;
@@ -196,7 +207,7 @@ ccnn_status Detector::create(const ccnn_params& p, const char* const* model_path
     return init();
 }
 
-ccnn_status Detector::init() {
+ccnn_status Detector::init_host() {
     apply_precision();
     if (max_w_ <= 0 || max_h_ <= 0) {
         set_error("max_image_size must be positive");
@@ -228,9 +239,6 @@ ccnn_status Detector::init() {
                     return CCNN_ERR_MODEL;
                 }
             api_.facial_analysis = 0;
-            CCNN_CUDA(cudaSetDevice(api_.cuda_device_id));
-            if (!d_lg_) CCNN_CUDA(cudaMalloc(&d_lg_, 3 * sizeof(LegacyNet)));
-            CCNN_CUDA(cudaMemcpy(d_lg_, lg.get(), 3 * sizeof(LegacyNet), cudaMemcpyHostToDevice));
             h_lg_ = std::move(lg);
             for (int i = 0; i < 3; ++i) {
                 m[i].min_w = h_lg_[i].min_w;
@@ -249,6 +257,7 @@ ccnn_status Detector::init() {
         set_error(err);
         return CCNN_ERR_MODEL;
     }
+    h_lnet_.reset();
     if (api_.facial_analysis && detect_enabled_) {
         // InitCNNCheck (:792-810): the landmark network, bundled next to the library
         RawModel lm;
@@ -257,10 +266,7 @@ ccnn_status Detector::init() {
             set_error(err);
             return CCNN_ERR_MODEL;
         }
-        int dev = api_.cuda_device_id;
-        CCNN_CUDA(cudaSetDevice(dev));
-        if (!d_lnet_) CCNN_CUDA(cudaMalloc(&d_lnet_, sizeof(LandmarkNet)));
-        CCNN_CUDA(cudaMemcpy(d_lnet_, ln.get(), sizeof(LandmarkNet), cudaMemcpyHostToDevice));
+        h_lnet_ = std::move(ln);
     }
     pat_w_ = m[0].min_w;
     pat_h_ = m[0].min_h;
@@ -319,6 +325,12 @@ ccnn_status Detector::init() {
     }
     cand_cap_ = std::max(1LL, resp_cap_);
     chunk_cap_ = std::max(chunk_cap_, 1);
+    return CCNN_OK;
+}
+
+ccnn_status Detector::init() {
+    ccnn_status hs = init_host();
+    if (hs != CCNN_OK) return hs;
     device_ = api_.cuda_device_id;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -330,6 +342,15 @@ ccnn_status Detector::init() {
         return CCNN_ERR_INVALID_ARG;
     }
     CCNN_CUDA(cudaSetDevice(device_));
+    if (legacy_) {
+        if (!d_lg_) CCNN_CUDA(cudaMalloc(&d_lg_, 3 * sizeof(LegacyNet)));
+        CCNN_CUDA(cudaMemcpy(d_lg_, h_lg_.get(), 3 * sizeof(LegacyNet), cudaMemcpyHostToDevice));
+    }
+    if (h_lnet_) {
+        if (!d_lnet_) CCNN_CUDA(cudaMalloc(&d_lnet_, sizeof(LandmarkNet)));
+        CCNN_CUDA(cudaMemcpy(d_lnet_, h_lnet_.get(), sizeof(LandmarkNet), cudaMemcpyHostToDevice));
+    }
+    if (!order_ev_) CCNN_CUDA(cudaEventCreateWithFlags(&order_ev_, cudaEventDisableTiming));
     cudaDeviceProp prop;
     CCNN_CUDA(cudaGetDeviceProperties(&prop, device_));
     // persistent stage-2/3 grid: 4 resident 256-thread CTAs per SM (register bound)
@@ -340,6 +361,7 @@ ccnn_status Detector::init() {
     CCNN_CUDA(facial_setup());
 
     inited_ = true;
+    ++init_gen_;
     for (auto& s : slots_) {
         ccnn_status st = alloc_slot(s);
         if (st != CCNN_OK) {
@@ -347,6 +369,30 @@ ccnn_status Detector::init() {
             return st;
         }
     }
+    return CCNN_OK;
+}
+
+ccnn_status Detector::estimate_bytes(const ccnn_params& p, const char* const* model_paths, int n_slots, bool colour_input,
+                                     bool with_gate, size_t* bytes) {
+    Detector d;
+    d.gate_on_ = with_gate;
+    d.api_ = p;
+    if (n_slots < 1) {
+        set_error("a detector needs at least one frame slot");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    d.slots_.assign(n_slots, Slot());
+    for (int i = 0; i < 3; ++i) {
+        const char* mp = model_paths ? model_paths[i] : nullptr;
+        static const char* kNames[3] = {"cnn4face1_cntk.bin", "cnn4face2_cntk.bin", "cnn4face3_cntk.bin"};
+        d.model_paths_[i] = (mp && mp[0]) ? std::string(mp) : bundled_model_dir() + "/" + kNames[i];
+    }
+    d.gray_image_only_ = !colour_input;
+    d.max_w_ = p.max_image_width;
+    d.max_h_ = p.max_image_height;
+    const ccnn_status st = d.init_host();
+    if (st != CCNN_OK) return st;
+    *bytes = d.slot_bytes();
     return CCNN_OK;
 }
 
@@ -377,6 +423,8 @@ ccnn_status Detector::alloc_slot(Slot& s) {
     CCNN_CUDA(cudaMalloc(&s.d_faces, sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces)));
     CCNN_CUDA(cudaMemset(s.d_faces, 0, sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces)));
     CCNN_CUDA(cudaMalloc(&s.d_nfaces, sizeof(int)));
+    CCNN_CUDA(cudaMalloc(&s.d_mk, sizeof(Det) * cand_cap_));
+    CCNN_CUDA(cudaMalloc(&s.d_nmk, sizeof(int)));
     if (gate_on_) {
         ccnn_status st = alloc_gate(s);
         if (st != CCNN_OK) return st;
@@ -645,6 +693,8 @@ ReplayArgs Detector::replay_args(Slot& s, const Plan& p) const {
     a.faces = s.d_faces;
     a.face_cap = (int)cand_cap_;
     a.n_faces = s.d_nfaces;
+    a.m_out = s.d_mk;
+    a.n_m_out = s.d_nmk;
     return a;
 }
 
@@ -682,7 +732,7 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
                                 facial_grid_, s.st));
     CCNN_CUDA(launch_replay(replay_args(s, p), s.st));
     CCNN_CUDA(cudaMemcpyAsync(s.h_nfaces, s.d_nfaces, sizeof(int), cudaMemcpyDeviceToHost, s.st));
-    CCNN_CUDA(cudaMemcpyAsync(s.h_faces, s.d_faces, sizeof(FaceOut) * kHostFaces, cudaMemcpyDeviceToHost, s.st));
+    CCNN_CUDA(cudaMemcpyAsync(s.h_faces, s.d_faces, sizeof(FaceOut) * kGraphFaces, cudaMemcpyDeviceToHost, s.st));
     return CCNN_OK;
 }
 
@@ -778,18 +828,35 @@ ccnn_status Detector::enqueue(Slot& s, const Plan& p, const ccnn_image& img, boo
     return CCNN_OK;
 }
 
-ccnn_status Detector::collect(Slot& s, ccnn_face* faces, int cap, int* n) {
+// Waits for slot s's frame and returns its faces: the graph downloads the first kGraphFaces; more
+// (up to `cap`) are fetched here. *src points at `cap`-or-fewer FaceOut entries valid until the
+// next call on the slot.
+ccnn_status Detector::collect_raw(Slot& s, int cap, int* n, const FaceOut** src) {
     CCNN_CUDA(cudaEventSynchronize(s.done));
     CCNN_CUDA(cudaGetLastError());
     const int nf = *s.h_nfaces;
     *n = nf;
     const int take = std::min(nf, cap);
-    std::vector<FaceOut> extra;
-    if (take > kHostFaces) {
-        extra.resize(take);
-        CCNN_CUDA(cudaMemcpy(extra.data(), s.d_faces, sizeof(FaceOut) * take, cudaMemcpyDeviceToHost));
+    *src = s.h_faces;
+    if (take > kGraphFaces) {
+        if (take > kHostFaces) {
+            s.h_extra.resize(take);
+            CCNN_CUDA(cudaMemcpy(s.h_extra.data(), s.d_faces, sizeof(FaceOut) * take, cudaMemcpyDeviceToHost));
+            *src = s.h_extra.data();
+        } else {
+            CCNN_CUDA(cudaMemcpy(s.h_faces + kGraphFaces, s.d_faces + kGraphFaces, sizeof(FaceOut) * (take - kGraphFaces),
+                                 cudaMemcpyDeviceToHost));
+        }
     }
-    const FaceOut* src = take > kHostFaces ? extra.data() : s.h_faces;
+    return CCNN_OK;
+}
+
+ccnn_status Detector::collect(Slot& s, ccnn_face* faces, int cap, int* n) {
+    const FaceOut* src = nullptr;
+    ccnn_status st = collect_raw(s, cap, n, &src);
+    if (st != CCNN_OK) return st;
+    const int nf = *n;
+    const int take = std::min(nf, cap);
     for (int i = 0; i < take; ++i) {
         faces[i].x = src[i].x;
         faces[i].y = src[i].y;
@@ -863,17 +930,21 @@ ccnn_status Detector::detect(const ccnn_image& img, bool device_input, cudaStrea
         return CCNN_OK;
     }
     Slot& s = slots_[0];
-    if (user_stream) {
-        // order the frame after the caller's pending work on its stream
-        cudaEvent_t ev;
-        CCNN_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        cudaEventRecord(ev, user_stream);
-        cudaStreamWaitEvent(s.st, ev, 0);
-        cudaEventDestroy(ev);
+    // a device frame is read on the slot's stream: order it after the caller's pending work on its
+    // stream (the legacy default stream when none is given), which may still be writing the frame
+    if (device_input) {
+        st = order_after(user_stream, 1);
+        if (st != CCNN_OK) return st;
     }
     st = enqueue(s, *p, img, device_input, user_stream);
     if (st != CCNN_OK) return st;
     return collect(s, faces, cap, n);
+}
+
+ccnn_status Detector::order_after(cudaStream_t user_stream, int n_slots) {
+    CCNN_CUDA(cudaEventRecord(order_ev_, user_stream ? user_stream : cudaStreamLegacy));
+    for (int k = 0; k < n_slots && k < (int)slots_.size(); ++k) CCNN_CUDA(cudaStreamWaitEvent(slots_[k].st, order_ev_, 0));
+    return CCNN_OK;
 }
 
 ccnn_status Detector::launch(int k, const ccnn_image& img) {
@@ -905,9 +976,15 @@ ccnn_status Detector::fetch(int k, ccnn_face* faces, int cap, int* n) { return c
 size_t Detector::slot_bytes() const {
     const size_t in = (size_t)round_up((long long)max_w_ * 4, 64) * max_h_;
     const size_t gray = sizeof(float) * (size_t)round_up(max_w_, 16) * max_h_;
-    const size_t per_cand = sizeof(Candidate) + sizeof(CandResult) + 4 * sizeof(WinOut) + 4 * sizeof(Det) + 2 * sizeof(int) + 1;
-    const size_t per_slot = in + gray + sizeof(float) * (size_t)(std::max(4LL, img_cap_) + std::max(1LL, s1_cap_) + std::max(1LL, resp_cap_)) +
-                            sizeof(int) * chunk_cap_ + per_cand * (size_t)cand_cap_ + sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces);
+    const size_t per_cand = sizeof(Candidate) + sizeof(CandResult) + 4 * sizeof(WinOut) + 5 * sizeof(Det) + 2 * sizeof(int) + 1;
+    size_t per_slot = in + gray + sizeof(float) * (size_t)(std::max(4LL, img_cap_) + std::max(1LL, s1_cap_) + std::max(1LL, resp_cap_)) +
+                      sizeof(int) * chunk_cap_ + per_cand * (size_t)cand_cap_ + sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces);
+    if (gate_on_) {
+        const size_t cells = ((size_t)max_w_ / 16) * ((size_t)max_h_ / 16);
+        per_slot += sizeof(uint32_t) * (1 + (size_t)gate_bitmap_words(max_w_, max_h_)) + sizeof(float) * std::max<size_t>(1, kGK * cells) +
+                    (size_t)std::max(1, k1_cap_) + (size_t)std::max(1, k2_cap_);
+    }
+    if (h_lnet_) per_slot += (sizeof(int4) + 5 * sizeof(int)) * (size_t)cand_cap_;
     return per_slot * slots_.size();
 }
 
@@ -921,6 +998,11 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, bool devic
     cudaSetDevice(device_);
     const int n_sl = (int)slots_.size();
     std::vector<int> pending(n_sl, -1);
+    // device frames: a slot stream waits for the work queued on the legacy default stream (where a
+    // caller without a stream of its own, torch included, wrote them) before its first frame of the
+    // batch, and again after a re-initialisation recreated the slots
+    int ordered_gen = -1;
+    std::vector<char> waited(n_sl, 0);
     ccnn_status worst = CCNN_OK;
     // device time of the whole batch: from an event before the first frame's upload (both
     // slot streams wait on it) to an event after the last frame of either slot
@@ -957,6 +1039,17 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, bool devic
         if (empty) {
             n_faces[i] = 0;
             continue;
+        }
+        if (device_input) {
+            if (ordered_gen != init_gen_) {
+                CCNN_CUDA(cudaEventRecord(order_ev_, cudaStreamLegacy));
+                std::fill(waited.begin(), waited.end(), 0);
+                ordered_gen = init_gen_;
+            }
+            if (!waited[k]) {
+                CCNN_CUDA(cudaStreamWaitEvent(slots_[k].st, order_ev_, 0));
+                waited[k] = 1;
+            }
         }
         st = enqueue(slots_[k], *p, imgs[i], device_input, nullptr);
         if (st != CCNN_OK) return st;
@@ -1275,6 +1368,275 @@ ccnn_status Detector::inspect_raw(ccnn_detection* out, int cap, int* n) {
         out[i].num_detect = d[i].num_detect;
     }
     return CCNN_OK;
+}
+
+// ---------------- the internal CNNDetector class (cnn_detector_v3.h:82-453) ----------------
+
+// CNNDetector::Param + AdvancedParam -> the FaceDetector-shaped parameters the rest of the detector
+// reads (the inverse of paramConverter, CompactCNNLibAPI_v2.cpp:51-88).
+void Detector::cnn_to_api() {
+    ccnn_default_params(&api_);
+    api_.max_image_width = cnn_p_.max_image_width;
+    api_.max_image_height = cnn_p_.max_image_height;
+    api_.min_face_height = cnn_p_.min_obj_height;
+    api_.max_face_height = cnn_p_.max_obj_height;
+    api_.scale_factor = cnn_p_.scale_factor;
+    api_.min_neighbors = cnn_p_.min_neighbors;
+    api_.num_threads = cnn_p_.num_threads;
+    api_.pipeline = cnn_p_.pipeline;
+    api_.detect_precision = cnn_ap_.detect_precision;
+    api_.treshold[0] = cnn_ap_.treshold_1;
+    api_.treshold[1] = cnn_ap_.treshold_2;
+    api_.treshold[2] = cnn_ap_.treshold_3;
+    api_.drop_detect = cnn_ap_.drop_detect;
+    api_.equalize = cnn_ap_.equalize;
+    api_.reflection = cnn_ap_.reflection;
+    api_.detect_mode = cnn_ap_.detect_mode;
+    for (int i = 0; i < 3; ++i) api_.index_output[i] = cnn_ap_.index_output[i];
+    api_.device_info = cnn_ap_.device_info;
+    api_.cuda_device_id = cnn_ap_.cuda_device_id;
+    api_.cl_platform_id = cnn_ap_.cl_platform_id;
+    api_.cl_device_id = cnn_ap_.cl_device_id;
+    api_.facial_analysis = cnn_ap_.facial_analysis;
+}
+
+static ccnn_status check_cnn_params(const ccnn_cnn_advanced_param& ap) {
+    if (ap.blur || ap.uniform_noise) {
+        // CNNDetector::Init resets both only for precision `def`; the reference's CPU path never reads
+        // blur, and uniform_noise draws from std::rand, which no parity contract can pin
+        if (ap.detect_precision != CCNN_PRECISION_DEF) {
+            set_error("AdvancedParam: blur and uniform_noise are not supported");
+            return CCNN_ERR_UNSUPPORTED;
+        }
+    }
+    return CCNN_OK;
+}
+
+ccnn_status Detector::create_cnn(const ccnn_cnn_param& p, const ccnn_cnn_advanced_param& ap, const char* const* model_paths) {
+    const ccnn_status cs = check_cnn_params(ap);
+    if (cs != CCNN_OK) return cs;
+    has_cnn_ = true;
+    cnn_p_ = p;
+    cnn_ap_ = ap;
+    cnn_to_api();
+    slots_.assign(1, Slot());  // Detect is synchronous: one frame slot
+    for (int i = 0; i < 3; ++i) {
+        const char* mp = model_paths ? model_paths[i] : nullptr;
+        static const char* kNames[3] = {"cnn4face1_cntk.bin", "cnn4face2_cntk.bin", "cnn4face3_cntk.bin"};
+        model_paths_[i] = (mp && mp[0]) ? std::string(mp) : bundled_model_dir() + "/" + kNames[i];
+    }
+    gray_image_only_ = ap.gray_image_only != 0;
+    max_w_ = p.max_image_width;
+    max_h_ = p.max_image_height;
+    return init();
+}
+
+static Det det_from(const ccnn_detection& d) {
+    Det r;
+    r.x = d.x;
+    r.y = d.y;
+    r.w = d.width;
+    r.h = d.height;
+    r.x2 = d.x + d.width;
+    r.y2 = d.y + d.height;
+    r.score = d.score;
+    r.scale = d.scale;
+    r.knn = d.knn;
+    r.num_detect = d.num_detect;
+    return r;
+}
+
+static ccnn_detection detection_from(const Det& d) {
+    ccnn_detection r;
+    r.x = d.x;
+    r.y = d.y;
+    r.width = d.w;
+    r.height = d.h;
+    r.score = d.score;
+    r.scale = d.scale;
+    r.knn = d.knn;
+    r.num_detect = d.num_detect;
+    return r;
+}
+
+ccnn_status Detector::detect_cnn(const ccnn_image& img, const ccnn_detection* prior, int n_prior, ccnn_detection* out, int cap, int* n) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!n || cap < 0 || (cap > 0 && !out) || n_prior < 0 || (n_prior > 0 && !prior)) {
+        set_error("invalid output arguments");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(device_);
+    std::vector<ccnn_detection> keep(prior, prior + n_prior);  // `prior` may alias `out`
+    auto give = [&](const std::vector<ccnn_detection>& v) {
+        *n = (int)v.size();
+        for (int i = 0; i < (int)v.size() && i < cap; ++i) out[i] = v[i];
+        return (int)v.size() > cap ? CCNN_TRUNCATED : CCNN_OK;
+    };
+    const Plan* p = nullptr;
+    bool empty = false;
+    ccnn_status st = prepare_frame(img, &p, &empty);
+    if (st != CCNN_OK) return st;
+    if (empty) return give(keep);  // a frame smaller than the check window: detections untouched (:2494-2497)
+    Slot& s = slots_[0];
+    st = enqueue(s, *p, img, false, nullptr);
+    if (st != CCNN_OK) return st;
+    int nf = 0;
+    const FaceOut* src = nullptr;
+    st = collect_raw(s, (int)std::min<long long>(std::max<long long>(cand_cap_, kHostFaces), INT32_MAX), &nf, &src);
+    if (st != CCNN_OK) return st;
+    std::vector<ccnn_detection> res;
+    if (n_prior == 0 || !merger_detect_) {
+        // the priors are dropped when the raw list is copied out unmerged (:2775-2779)
+        int nraw = 0;
+        if (n_prior > 0) CCNN_CUDA(cudaMemcpy(&nraw, s.d_nraw, sizeof(int), cudaMemcpyDeviceToHost));
+        if (n_prior > 0 && nraw == 0) return give(keep);
+        res.resize(nf);
+        for (int i = 0; i < nf; ++i) {
+            res[i].x = src[i].x;
+            res[i].y = src[i].y;
+            res[i].width = src[i].w;
+            res[i].height = src[i].h;
+            res[i].score = src[i].score;
+            res[i].scale = src[i].scale;
+            res[i].knn = src[i].knn;
+            res[i].num_detect = src[i].num_detect;
+        }
+        return give(res);
+    }
+    int nraw = 0;
+    CCNN_CUDA(cudaMemcpy(&nraw, s.d_nraw, sizeof(int), cudaMemcpyDeviceToHost));
+    if (nraw == 0) return give(keep);  // no new raw detection: the vector is left as it was (:2749)
+    int nmk = 0;
+    CCNN_CUDA(cudaMemcpy(&nmk, s.d_nmk, sizeof(int), cudaMemcpyDeviceToHost));
+    // [priors, new clusters] -> filter -> Merger(0.2, del) -> rescale, on the device
+    const int total = n_prior + nmk;
+    std::vector<Det> h_prior(n_prior);
+    for (int i = 0; i < n_prior; ++i) h_prior[i] = det_from(keep[i]);
+    Det *d_prior = nullptr, *d_list = nullptr, *d_out = nullptr;
+    uint8_t* d_checked = nullptr;
+    int* d_n = nullptr;
+    cudaError_t e = cudaMallocAsync(&d_prior, sizeof(Det) * n_prior, s.st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_list, sizeof(Det) * 2 * (size_t)total, s.st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_out, sizeof(Det) * (size_t)total, s.st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_checked, (size_t)total, s.st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_n, sizeof(int), s.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_prior, h_prior.data(), sizeof(Det) * n_prior, cudaMemcpyHostToDevice, s.st);
+    if (e == cudaSuccess) e = launch_prior_merge(d_prior, n_prior, s.d_mk, s.d_nmk, cfg_, d_list, d_checked, d_out, d_n, s.st);
+    int nout = 0;
+    std::vector<Det> h_out((size_t)total);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nout, d_n, sizeof(int), cudaMemcpyDeviceToHost, s.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_out.data(), d_out, sizeof(Det) * (size_t)total, cudaMemcpyDeviceToHost, s.st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.st);
+    for (void* q : {(void*)d_prior, (void*)d_list, (void*)d_out, (void*)d_checked, (void*)d_n})
+        if (q) cudaFreeAsync(q, s.st);
+    CCNN_CUDA(e);
+    CCNN_CUDA(cudaStreamSynchronize(s.st));
+    if (nout == 0 && total == 0) return give(keep);
+    res.resize(nout);
+    for (int i = 0; i < nout; ++i) res[i] = detection_from(h_out[i]);
+    return give(res);
+}
+
+ccnn_status Detector::nms(const ccnn_detection* rect, int n_rect, ccnn_detection* out, int cap, int* n_out) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!n_out || n_rect < 0 || (n_rect > 0 && !rect) || cap < 0 || (cap > 0 && !out)) {
+        set_error("invalid arguments");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    *n_out = 0;
+    if (n_rect == 0) return CCNN_OK;
+    if (!inited_) {
+        ccnn_status st = init();
+        if (st != CCNN_OK) return st;
+    }
+    cudaSetDevice(device_);
+    Slot& s = slots_[0];
+    std::vector<Det> h_in(n_rect);
+    for (int i = 0; i < n_rect; ++i) h_in[i] = det_from(rect[i]);
+    Det *d_in = nullptr, *d_out = nullptr;
+    uint8_t* d_checked = nullptr;
+    int* d_n = nullptr;
+    cudaError_t e = cudaMallocAsync(&d_in, sizeof(Det) * n_rect, s.st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_out, sizeof(Det) * n_rect, s.st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_checked, n_rect, s.st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_n, sizeof(int), s.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_in, h_in.data(), sizeof(Det) * n_rect, cudaMemcpyHostToDevice, s.st);
+    if (e == cudaSuccess) e = launch_nms(d_in, n_rect, d_checked, d_out, d_n, s.st);
+    int nout = 0;
+    std::vector<Det> h_out(n_rect);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nout, d_n, sizeof(int), cudaMemcpyDeviceToHost, s.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_out.data(), d_out, sizeof(Det) * n_rect, cudaMemcpyDeviceToHost, s.st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.st);
+    for (void* q : {(void*)d_in, (void*)d_out, (void*)d_checked, (void*)d_n})
+        if (q) cudaFreeAsync(q, s.st);
+    CCNN_CUDA(e);
+    CCNN_CUDA(cudaStreamSynchronize(s.st));
+    *n_out = nout;
+    for (int i = 0; i < nout && i < cap; ++i) out[i] = detection_from(h_out[i]);
+    return nout > cap ? CCNN_TRUNCATED : CCNN_OK;
+}
+
+ccnn_status Detector::get_cnn_params(ccnn_cnn_param* p, ccnn_cnn_advanced_param* ap) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!has_cnn_) {
+        set_error("the handle was not created through the CNNDetector API");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    if (p) {
+        *p = cnn_p_;
+        p->max_image_width = max_w_;
+        p->max_image_height = max_h_;
+        // InitDevice of a CUDA build (cnn_detector_v3.cpp:73-84): packet mode forces the GPU pipeline
+        if (cnn_ap_.packet_detection && cnn_p_.pipeline > 0 && cnn_ap_.detect_precision != CCNN_PRECISION_DEF) p->pipeline = CCNN_PIPELINE_GPU;
+    }
+    if (ap) {
+        *ap = cnn_ap_;
+        // the values CNNDetector::Init leaves in advanced_param (:922-963), and what Detect changed since
+        // (apply_precision derives them again from the given values at every initialisation; the
+        // gray-only state is Detect's, kept as it is)
+        const bool gray_only = gray_image_only_;
+        apply_precision();
+        gray_image_only_ = gray_only;
+        ap->type_check = type_check_;
+        ap->min_num_detect = min_num_detect_;
+        ap->drop_detect = drop_detect_;
+        ap->equalize = equalize_;
+        ap->reflection = reflection_;
+        ap->adapt_min_neighbors = adapt_min_neighbors_;
+        ap->double_check = double_check_;
+        ap->merger_detect = merger_detect_;
+        ap->gray_image_only = gray_image_only_;
+        ap->facial_analysis = api_.facial_analysis;
+        if (cnn_ap_.detect_precision == CCNN_PRECISION_DEF) {
+            ap->packet_detection = 0;
+            ap->blur = 0;
+            ap->uniform_noise = 0;
+        }
+        if (cnn_p_.pipeline == CCNN_PIPELINE_CPU) ap->packet_detection = 0;  // InitDevice (:73-84)
+    }
+    return CCNN_OK;
+}
+
+ccnn_status Detector::set_cnn_params(const ccnn_cnn_param* p, const ccnn_cnn_advanced_param* ap) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!has_cnn_) {
+        set_error("the handle was not created through the CNNDetector API");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    if (ap) {
+        const ccnn_status cs = check_cnn_params(*ap);
+        if (cs != CCNN_OK) return cs;
+    }
+    clear();  // setParam / setAdvancedParam clear the detector (cnn_detector_v3.h:407-416)
+    if (p) cnn_p_ = *p;
+    if (ap) {
+        cnn_ap_ = *ap;
+        gray_image_only_ = ap->gray_image_only != 0;
+    }
+    cnn_to_api();
+    max_w_ = cnn_p_.max_image_width;
+    max_h_ = cnn_p_.max_image_height;
+    return CCNN_OK;  // the next Detect initialises again (:2485-2492)
 }
 
 }  // namespace ccnn

@@ -14,6 +14,7 @@
 #include "../../include/ccnn.h"
 #include "../../include/ccnn_inspect.h"
 #include "../../include/ccnn_gate.h"
+#include "../../include/ccnn_cnn.h"
 #include "legacy.h"
 #include "kernels.h"
 
@@ -64,6 +65,8 @@ struct Slot {
     uint8_t* d_back_on = nullptr;
     int4* d_attr = nullptr;      // facial analysis: per candidate (dropped, gender, smile, glasses)
     int* d_fa = nullptr;         // facial analysis: replay scratch (5 x candidate capacity)
+    Det* d_mk = nullptr;         // the first merge's filtered clusters of the last frame
+    int* d_nmk = nullptr;
     cudaGraphExec_t exec = nullptr;
     const Plan* exec_plan = nullptr;
     cudaGraph_t graph = nullptr;          // kept while `exec` lives: its gray-kernel node is updated per frame
@@ -72,12 +75,14 @@ struct Slot {
     bool gray_in_place = false;           // the node currently reads the caller's frame
     bool last_in_place = false;           // the last frame was not copied into d_in
     const Plan* last_plan = nullptr;  // plan of the last frame run on this slot
+    std::vector<FaceOut> h_extra;     // faces beyond the pinned buffer's kHostFaces
 };
 
 class Detector {
    public:
     static constexpr int kSlots = 8;
     static constexpr int kHostFaces = 1024;
+    static constexpr int kGraphFaces = 64;  // faces each frame's graph downloads; more are fetched on demand
 
     Detector() = default;
     ~Detector();
@@ -87,6 +92,14 @@ class Detector {
     // (gray_image_only off), so that colour frames never re-initialise the detector
     ccnn_status create(const ccnn_params& p, const char* const* model_paths, int n_slots = kSlots, bool colour_input = false);
     ccnn_status detect(const ccnn_image& img, bool device_input, cudaStream_t user_stream, ccnn_face* faces, int cap, int* n);
+
+    // The internal CNNDetector class (cnn_detector_v3.h:82-453): its Param + AdvancedParam instead of
+    // FaceDetector::Param, raw Detection results, the caller's prior detections, NMS.
+    ccnn_status create_cnn(const ccnn_cnn_param& p, const ccnn_cnn_advanced_param& ap, const char* const* model_paths);
+    ccnn_status detect_cnn(const ccnn_image& img, const ccnn_detection* prior, int n_prior, ccnn_detection* out, int cap, int* n);
+    ccnn_status nms(const ccnn_detection* rect, int n_rect, ccnn_detection* out, int cap, int* n_out);
+    ccnn_status get_cnn_params(ccnn_cnn_param* p, ccnn_cnn_advanced_param* ap);
+    ccnn_status set_cnn_params(const ccnn_cnn_param* p, const ccnn_cnn_advanced_param* ap);
     ccnn_status detect_batch(const ccnn_image* imgs, int n_img, bool device_input, ccnn_face* faces, int cap_per, int* n_faces,
                              float* gpu_ms);
     ccnn_status profile(int iters, float* ms, int n_ms);
@@ -112,6 +125,10 @@ class Detector {
     ccnn_status fetch(int k, ccnn_face* faces, int cap, int* n);
     // device bytes held by the frame slots
     size_t slot_bytes() const;
+    // the device bytes create() would allocate for these arguments, computed on the host without
+    // touching the device (so that a caller can make room before allocating)
+    static ccnn_status estimate_bytes(const ccnn_params& p, const char* const* model_paths, int n_slots, bool colour_input,
+                                      bool with_gate, size_t* bytes);
 
     ccnn_status get_gray_device(const float** data, int* cols, int* rows, size_t* step);
     ccnn_status get_gray_host(float* out, int cap, int* cols, int* rows);
@@ -131,6 +148,12 @@ class Detector {
    private:
     // configuration (FaceDetector::Param + the AdvancedParam the API derives from it)
     ccnn_params api_{};
+    // created through the CNNDetector API: its Param and AdvancedParam as given (the precision
+    // rules are applied on top at every initialisation)
+    bool has_cnn_ = false;
+    ccnn_cnn_param cnn_p_{};
+    ccnn_cnn_advanced_param cnn_ap_{};
+    void cnn_to_api();
     int device_ = 0;
     bool gray_image_only_ = true;
     int type_check_ = 2, min_num_detect_ = 1;
@@ -142,6 +165,7 @@ class Detector {
     Stage1W w1_{};
     std::unique_ptr<WindowNets> wn_;
     LandmarkNet* d_lnet_ = nullptr;  // facial-analysis network (device memory), when enabled
+    std::unique_ptr<LandmarkNet> h_lnet_;  // its host copy
     // legacy model family (format 1.0): the three networks on the host and in device memory
     bool legacy_ = false;
     std::unique_ptr<LegacyNet[]> h_lg_;
@@ -173,8 +197,16 @@ class Detector {
     int facial_grid_ = 0;
     std::map<std::tuple<int, int, int, int>, std::unique_ptr<Plan>> plans_;
     std::mutex mu_;
+    // orders device frames after the caller's work on the legacy default stream
+    cudaEvent_t order_ev_ = nullptr;
+    int init_gen_ = 0;  // counts initialisations (each recreates the slot streams)
 
     ccnn_status init();
+    // the host half of init(): models, scales, plan capacities; touches no device
+    ccnn_status init_host();
+    // the slot streams wait for the work queued so far on `user_stream`, or on the legacy default
+    // stream when it is null (the stream a caller without one of its own, torch included, writes on)
+    ccnn_status order_after(cudaStream_t user_stream, int n_slots);
     void clear();
     ccnn_status alloc_slot(Slot& s);
     void free_slot(Slot& s);
@@ -184,6 +216,7 @@ class Detector {
     ccnn_status enqueue_kernels(Slot& s, const Plan& p);
     ccnn_status prepare_frame(const ccnn_image& img, const Plan** plan, bool* empty);
     ccnn_status collect(Slot& s, ccnn_face* faces, int cap, int* n);
+    ccnn_status collect_raw(Slot& s, int cap, int* n, const FaceOut** src);
     ReplayArgs replay_args(Slot& s, const Plan& p) const;
     ccnn_status apply_precision();
 };

@@ -552,7 +552,11 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
 
     // post-processing in warp 0
     if (warp != 0) return;
-    if (lane == 0) *a.n_raw = nD;
+    if (lane == 0) {
+        *a.n_raw = nD;
+        if (a.n_m_out) *a.n_m_out = 0;
+    }
+    __syncwarp();
     int nF = 0;
     const Det* fin = R;
     if (nD > 0) {
@@ -584,6 +588,11 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
                     w += __popc(m);
                 }
                 nM = w;
+            }
+            if (a.m_out) {
+                for (int k = lane; k < nM; k += 32) a.m_out[k] = M[k];
+                if (lane == 0) *a.n_m_out = nM;
+                __syncwarp();
             }
             if (nM > 0) {
                 nF = merger_warp(M, nM, checked, F, 0.2f, true, nullptr, fsrc);
@@ -618,6 +627,10 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
             f.h = d.h;
         }
         f.score = d.score;
+        f.scale = d.scale;
+        f.knn = d.knn;
+        f.num_detect = d.num_detect;
+        f.pad = 0;
         f.gender = f.smile = f.glasses = -1;
         if (a.fa_scratch) {
             // CompactCNNLibAPI_v2.cpp:296-319: each attribute is the element at size/2 of the
@@ -657,6 +670,55 @@ __global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
         a.faces[i] = f;
     }
     if (lane == 0) *a.n_faces = nF;
+}
+
+// Detect with the caller's detections in front (cnn_detector_v3.cpp:2753-2806), one warp: the
+// priors pass the stable min_num_detect filter (the new clusters arrive filtered), then the
+// whole list goes through Merger(0.2, del) and the optional rescale of a shrunken input frame.
+__global__ void __launch_bounds__(32, 1) prior_merge_kernel(const Det* prior, int n_prior, const Det* clusters, const int* n_clusters,
+                                                            const CascadeConfig C, Det* list, uint8_t* checked, Det* out, int* n_out) {
+    const int lane = threadIdx.x;
+    const int nc = *n_clusters;
+    int n = 0;
+    for (int base = 0; base < n_prior; base += 32) {  // stable erase of priors below min_num_detect
+        const int k = base + lane;
+        const bool keep = k < n_prior && (C.min_num_detect <= 1 || prior[k].num_detect >= C.min_num_detect);
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) list[n + __popc(m & ((1u << lane) - 1u))] = prior[k];
+        n += __popc(m);
+    }
+    for (int k = lane; k < nc; k += 32) list[n + k] = clusters[k];
+    n += nc;
+    __syncwarp();
+    const int nf = n > 0 ? merger_warp(list, n, checked, list + n, 0.2f, true) : 0;
+    for (int i = lane; i < nf; i += 32) {
+        Det d = list[n + i];
+        if (C.rescale_output) {
+            d.x = (int)((float)d.x * C.rescale);
+            d.y = (int)((float)d.y * C.rescale);
+            d.w = (int)((float)d.w * C.rescale);
+            d.h = (int)((float)d.h * C.rescale);
+        }
+        out[i] = d;
+    }
+    if (lane == 0) *n_out = nf;
+}
+
+// CNNDetector::NMS: Merger(detections, rect, 0.5) of the caller's boxes, one warp
+__global__ void __launch_bounds__(32, 1) nms_kernel(const Det* in, int n, uint8_t* checked, Det* out, int* n_out) {
+    const int nf = merger_warp(in, n, checked, out, 0.5f, false);
+    if (threadIdx.x == 0) *n_out = nf;
+}
+
+cudaError_t launch_prior_merge(const Det* prior, int n_prior, const Det* clusters, const int* n_clusters, const CascadeConfig& cfg, Det* scratch,
+                               uint8_t* checked, Det* out, int* n_out, cudaStream_t st) {
+    prior_merge_kernel<<<1, 32, 0, st>>>(prior, n_prior, clusters, n_clusters, cfg, scratch, checked, out, n_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nms(const Det* in, int n, uint8_t* checked, Det* out, int* n_out, cudaStream_t st) {
+    nms_kernel<<<1, 32, 0, st>>>(in, n, checked, out, n_out);
+    return cudaGetLastError();
 }
 
 cudaError_t replay_setup() { return cudaFuncSetAttribute(replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReplaySmemBytes); }

@@ -14,6 +14,9 @@ struct FaceOut {
     int x, y, w, h;
     float score;
     int gender, smile, glasses;  // facial analysis; -1 without it
+    float scale;                 // the merged detection's scale, neighbour count and cluster size
+    int knn, num_detect;         // (CNNDetector::Detection, cnn_detector_v3.h:186-217)
+    int pad;
 };
 
 struct ReplayArgs {
@@ -41,6 +44,10 @@ struct ReplayArgs {
     FaceOut* faces;
     int face_cap;
     int* n_faces;
+    // the first merge's clusters after the min_num_detect filter (the second merge's input) and
+    // their count, for callers that merge them again with detections of their own
+    Det* m_out;
+    int* n_m_out;
 };
 
 // the gray kernel instantiation for `ch` channels (to find its node in a captured graph)
@@ -110,5 +117,13 @@ cudaError_t launch_facial(const LandmarkNet* d_net, const float* gray, int gpitc
 constexpr int kReplaySmemBytes = 200 * 1024;
 cudaError_t replay_setup();
 cudaError_t launch_replay(const ReplayArgs& a, cudaStream_t st);
+// CNNDetector::Detect with detections already in the caller's vector (cnn_detector_v3.cpp:2753-2806):
+// [prior, new clusters] through the min_num_detect filter (applied to the priors here; the clusters
+// come filtered) and Merger(0.2, del), then the optional rescale; scratch holds 2 * (n_prior + n_new)
+// Det and as many bytes. The result goes to out / *n_out.
+cudaError_t launch_prior_merge(const Det* prior, int n_prior, const Det* clusters, const int* n_clusters, const CascadeConfig& cfg, Det* scratch,
+                               uint8_t* checked, Det* out, int* n_out, cudaStream_t st);
+// CNNDetector::NMS = Merger(detections, rect, 0.5) (cnn_detector_v3.cpp:2814-2936) of n boxes
+cudaError_t launch_nms(const Det* in, int n, uint8_t* checked, Det* out, int* n_out, cudaStream_t st);
 
 }  // namespace ccnn

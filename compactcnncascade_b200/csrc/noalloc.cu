@@ -12,7 +12,9 @@
 // kStaticS1Floats floats) after a reserved first 256 bytes; the level descriptor travels as a
 // kernel parameter. Every call shares it, and it keeps the last call's contents; nothing in it has
 // to start at zero, because each call writes every plane value it later reads. Calls that overlap
-// on the GPU (different streams, or different host threads) race on the array.
+// on the GPU (different streams, or different host threads) race on the array. The array's device
+// address is looked up once per CUDA context, so a device reset between calls is handled (the next
+// call looks it up again in the new context).
 #include <cuda_runtime.h>
 
 #include <map>
@@ -34,19 +36,50 @@ constexpr size_t kDescBytes = 256;  // reserved head of the array
 
 static __device__ __align__(256) unsigned char g_stage1_scratch[kDescBytes + sizeof(float) * kStaticS1Floats];
 
-constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};
+std::map<unsigned long long, void*> g_scratch_addr;  // per CUDA context: the array's device address
 std::map<std::string, Stage1W> g_weights;
 
-// One-time set-up per device (with that device current): the device address of the array.
-ccnn_status scratch_address(int dev, unsigned char** out) {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (dev < 0 || dev >= kMaxDevices) {
-        set_error("device index out of range for the static scratch table");
-        return CCNN_ERR_INVALID_ARG;
+// Identity of the calling thread's current CUDA context. A device reset (cudaDeviceReset) ends the
+// context and reloads the library's module into the next one, which moves the array and drops the
+// kernel attributes, so both are cached per context rather than per device ordinal. The driver's
+// cuCtxGetCurrent / cuCtxGetId are reached through the runtime's entry-point query, so the library
+// does not link libcuda itself.
+ccnn_status current_context_id(unsigned long long* id) {
+    typedef int (*GetCurrentFn)(void**);
+    typedef int (*GetIdFn)(void*, unsigned long long*);
+    static GetCurrentFn get_current = nullptr;
+    static GetIdFn get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        cudaDriverEntryPointQueryResult q1, q2;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrentFn>(f1);
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) == cudaSuccess &&
+            q2 == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetIdFn>(f2);
+        looked_up = true;
     }
-    if (!g_scratch_addr[dev]) {
+    void* ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, id) != 0) {
+        set_error("static stage-1 scratch: cannot identify the current CUDA context (driver entry points cuCtxGetCurrent/cuCtxGetId)");
+        return CCNN_ERR_CUDA;
+    }
+    return CCNN_OK;
+}
+
+// One-time set-up per CUDA context (the calling thread's device current): the device address of
+// the array and the stage-1 kernel attribute. Neither allocates.
+ccnn_status scratch_address(unsigned char** out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    unsigned long long ctx = 0;
+    const ccnn_status cs = current_context_id(&ctx);
+    if (cs != CCNN_OK) return cs;
+    auto it = g_scratch_addr.find(ctx);
+    if (it == g_scratch_addr.end()) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_stage1_scratch);
         if (e != cudaSuccess) {
@@ -58,9 +91,9 @@ ccnn_status scratch_address(int dev, unsigned char** out) {
             set_error(std::string("stage-1 kernel set-up: ") + cudaGetErrorString(e2));
             return CCNN_ERR_CUDA;
         }
-        g_scratch_addr[dev] = p;
+        it = g_scratch_addr.emplace(ctx, p).first;
     }
-    *out = static_cast<unsigned char*>(g_scratch_addr[dev]);
+    *out = static_cast<unsigned char*>(it->second);
     return CCNN_OK;
 }
 
@@ -137,14 +170,17 @@ extern "C" CCNN_API ccnn_status ccnn_stage1_forward_static(const char* model_pat
     Stage1W w;
     ccnn_status st = stage1_weights(model_path, &w);
     if (st != CCNN_OK) return st;
+    // cudaSetDevice on the current device makes sure its primary context exists and is current
+    // before the context is identified (it allocates nothing)
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaSetDevice(dev);
     if (e != cudaSuccess) {
-        set_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+        set_error(std::string("cudaGetDevice/cudaSetDevice: ") + cudaGetErrorString(e));
         return CCNN_ERR_CUDA;
     }
     unsigned char* scratch = nullptr;
-    st = scratch_address(dev, &scratch);
+    st = scratch_address(&scratch);
     if (st != CCNN_OK) return st;
     float* d_s1 = reinterpret_cast<float*>(scratch + kDescBytes);
     cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -231,43 +231,66 @@ ccnn_status Server::make_class(const ccnn_image& img, ResClass** out, bool* retr
     p.max_image_width = img.cols;
     p.max_image_height = img.rows;
     const char* mp[3] = {models_[0].c_str(), models_[1].c_str(), models_[2].c_str()};
+    const char* const* models = has_models_ ? mp : nullptr;
+    const bool colour = img.channels != 1;
+    // evicts the least recently used idle class; false when every class is busy
+    auto evict_one = [&]() {
+        ResClass* victim = nullptr;
+        for (auto& o : classes_)
+            if (o->busy == 0 && (!victim || o->last_used < victim->last_used)) victim = o.get();
+        if (!victim) return false;
+        held_ -= victim->bytes;
+        classes_.remove_if([&](const std::unique_ptr<ResClass>& o) { return o.get() == victim; });
+        n_classes_ = (int)classes_.size();
+        return true;
+    };
     for (int slots = slots_per_class_; slots >= 1; slots /= 2) {
+        // the class's device bytes are known from its plan before anything is allocated, so room
+        // is made first (idle classes evicted, least recently used first) and the budget is never
+        // exceeded, not even briefly
+        size_t bytes = 0;
+        ccnn_status st = Detector::estimate_bytes(p, models, slots, colour, !gate_.empty(), &bytes);
+        if (st != CCNN_OK) return st;
+        while (held_ + bytes > budget_ && evict_one()) {
+        }
+        if (held_ + bytes > budget_) {
+            bool busy = false;
+            for (auto& o : classes_) busy |= o->busy > 0;
+            if (busy) {  // room comes back when running frames finish
+                *retry_later = true;
+                return CCNN_OK;
+            }
+            continue;  // fewer slots
+        }
         std::unique_ptr<ResClass> c(new ResClass());
         c->w = img.cols;
         c->h = img.rows;
         c->c = img.channels;
-        c->det.reset(new Detector());
-        ccnn_status st = c->det->create(p, has_models_ ? mp : nullptr, slots, img.channels != 1);
+        // the device itself may hold less than the budget: on OOM, evict another idle class and retry
+        for (;;) {
+            c->det.reset(new Detector());
+            st = c->det->create(p, models, slots, colour);
+            if (st == CCNN_OK && !gate_.empty()) st = c->det->gate_set(gate_.data(), (int)gate_.size(), gate_thr_, gate_fb_);
+            if (st != CCNN_ERR_OOM || !evict_one()) break;
+        }
+        if (st == CCNN_ERR_OOM) {
+            c->det.reset();
+            bool busy = false;
+            for (auto& o : classes_) busy |= o->busy > 0;
+            if (busy) {
+                *retry_later = true;
+                return CCNN_OK;
+            }
+            continue;  // fewer slots
+        }
         if (st != CCNN_OK) return st;
-        if (!gate_.empty()) {
-            st = c->det->gate_set(gate_.data(), (int)gate_.size(), gate_thr_, gate_fb_);
-            if (st != CCNN_OK) return st;
-        }
         c->bytes = c->det->slot_bytes();
-        // make room: evict idle classes, least recently used first
-        while (held_ + c->bytes > budget_) {
-            ResClass* victim = nullptr;
-            for (auto& o : classes_)
-                if (o->busy == 0 && (!victim || o->last_used < victim->last_used)) victim = o.get();
-            if (!victim) break;
-            held_ -= victim->bytes;
-            classes_.remove_if([&](const std::unique_ptr<ResClass>& o) { return o.get() == victim; });
-            n_classes_ = (int)classes_.size();
-        }
-        if (held_ + c->bytes <= budget_) {
-            c->slot_req.assign(slots, nullptr);
-            held_ += c->bytes;
-            classes_.push_back(std::move(c));
-            n_classes_ = (int)classes_.size();
-            *out = classes_.back().get();
-            return CCNN_OK;
-        }
-        bool busy = false;
-        for (auto& o : classes_) busy |= o->busy > 0;
-        if (busy) {  // room comes back when running frames finish
-            *retry_later = true;
-            return CCNN_OK;
-        }
+        c->slot_req.assign(slots, nullptr);
+        held_ += c->bytes;
+        classes_.push_back(std::move(c));
+        n_classes_ = (int)classes_.size();
+        *out = classes_.back().get();
+        return CCNN_OK;
     }
     set_error("a frame of this size does not fit the server's HBM budget");
     return CCNN_ERR_OOM;

@@ -5,7 +5,11 @@
 // names and return conventions (0 / -1, Detect returns the face count or -1).
 //
 // Differences a caller can observe:
-//  * instances are independent detectors (the reference shares one process-global detector);
+//  * instances are independent detectors by default. The reference shares one process-global
+//    detector behind one mutex (CompactCNNLibAPI_v2.cpp:32-33): every instance's Init replaces it,
+//    every Clear (and destructor) deletes it. FaceDetector::setSingleton(true), called before the
+//    first Init, or defining CCNN_FACEDETECTOR_SINGLETON before including this header, gives exactly
+//    those semantics;
 //  * Param::models are honoured when set (the reference ignores them and always uses its embedded
 //    models, which are the same files as the bundled defaults);
 //  * Detect writes at most `capacity` faces (default 1000, the demos' buffer size) and returns the
@@ -16,6 +20,7 @@
 #pragma once
 
 #include <cstddef>
+#include <mutex>
 #include <vector>
 
 #include "ccnn.h"
@@ -86,19 +91,28 @@ class FaceDetector {
     FaceDetector(const FaceDetector&) = delete;
     FaceDetector& operator=(const FaceDetector&) = delete;
 
+    // The reference's process-global detector (CompactCNNLibAPI_v2.cpp:32-33) instead of one detector
+    // per instance; switch it before the first Init of the process.
+    static void setSingleton(bool on) { global().singleton = on; }
+    static bool isSingleton() { return global().singleton; }
+
     int Init(Param& param) {
         if (!isEmpty()) Clear();
+        Lock lk(this);
         param_ = param;
+        if (global().singleton) global().param = param;
         ccnn_params p = to_c(param);
-        return ccnn_create(&p, param.models, &h_) == CCNN_OK ? 0 : (h_ = nullptr, -1);
+        ccnn_handle& h = handle();
+        return ccnn_create(&p, param.models, &h) == CCNN_OK ? 0 : (h = nullptr, -1);
     }
 
     int Detect(Face* faces, ImageData& img, int capacity = 1000) {
         if (isEmpty() || faces == nullptr) return -1;
+        Lock lk(this);
         ccnn_image im{img.cols, img.rows, img.channels, img.data, img.step};
         std::vector<ccnn_face> out((size_t)(capacity > 0 ? capacity : 1));
         int n = 0;
-        ccnn_status st = ccnn_detect(h_, &im, out.data(), capacity, &n);
+        ccnn_status st = ccnn_detect(handle(), &im, out.data(), capacity, &n);
         if (st < 0) return -1;
         for (int i = 0; i < n && i < capacity; ++i) {
             faces[i] = Face(out[i].x, out[i].y, out[i].width, out[i].height, out[i].score);
@@ -116,18 +130,21 @@ class FaceDetector {
 
     int Clear() {
         if (isEmpty()) return -1;
-        ccnn_destroy(h_);
-        h_ = nullptr;
+        Lock lk(this);
+        ccnn_handle& h = handle();
+        ccnn_destroy(h);
+        h = nullptr;
         return 0;
     }
 
-    bool isEmpty() const { return h_ == nullptr; }
+    bool isEmpty() const { return handle() == nullptr; }
 
     Param getParam() const {
-        if (isEmpty()) return param_;
+        const Param& mine = global().singleton ? global().param : param_;
+        if (isEmpty()) return mine;
         ccnn_params p;
-        ccnn_get_params(h_, &p);
-        Param r = param_;
+        ccnn_get_params(handle(), &p);
+        Param r = mine;
         r.max_image_size = Size(p.max_image_width, p.max_image_height);
         r.min_face_height = p.min_face_height;
         r.max_face_height = p.max_face_height;
@@ -137,26 +154,27 @@ class FaceDetector {
     }
     void setParam(Param& param) {
         param_ = param;
+        if (global().singleton) global().param = param;
         if (isEmpty()) return;
         ccnn_params p = to_c(param);
-        ccnn_set_params(h_, &p);
+        ccnn_set_params(handle(), &p);
     }
 
     Size getMaxImageSize() const { return getParam().max_image_size; }
     void setMaxImageSize(Size s) {
-        if (!isEmpty()) ccnn_set_max_image_size(h_, s.width, s.height);
+        if (!isEmpty()) ccnn_set_max_image_size(handle(), s.width, s.height);
     }
     int getMinObjectHeight() const { return getParam().min_face_height; }
     void setMinObjectHeight(int v) {
-        if (!isEmpty()) ccnn_set_min_object_height(h_, v);
+        if (!isEmpty()) ccnn_set_min_object_height(handle(), v);
     }
     int getMaxObjectHeight() const { return getParam().max_face_height; }
     void setMaxObjectHeight(int v) {
-        if (!isEmpty()) ccnn_set_max_object_height(h_, v);
+        if (!isEmpty()) ccnn_set_max_object_height(handle(), v);
     }
     int getNumThreads() const { return getParam().num_threads; }
     void setNumThreads(int v) {
-        if (!isEmpty()) ccnn_set_num_threads(h_, v);
+        if (!isEmpty()) ccnn_set_num_threads(handle(), v);
     }
 
     int getGrayImage32F(ImageData* img, Pipeline pipeline) {
@@ -164,10 +182,10 @@ class FaceDetector {
         const float* d = nullptr;
         int w = 0, h = 0;
         size_t step = 0;
-        if (ccnn_get_gray_device(h_, &d, &w, &h, &step) != CCNN_OK) return -1;
+        if (ccnn_get_gray_device(handle(), &d, &w, &h, &step) != CCNN_OK) return -1;
         if (pipeline == Pipeline::CPU) {
             gray_host_.resize((size_t)w * h);
-            if (ccnn_get_gray_host(h_, gray_host_.data(), (int)gray_host_.size(), &w, &h) != CCNN_OK) return -1;
+            if (ccnn_get_gray_host(handle(), gray_host_.data(), (int)gray_host_.size(), &w, &h) != CCNN_OK) return -1;
             *img = ImageData(w, h, 1, reinterpret_cast<unsigned char*>(gray_host_.data()), sizeof(float) * (size_t)w);
         } else {
             *img = ImageData(w, h, 1, reinterpret_cast<unsigned char*>(const_cast<float*>(d)), step);
@@ -179,6 +197,31 @@ class FaceDetector {
     ccnn_handle h_ = nullptr;
     Param param_;
     std::vector<float> gray_host_;
+
+    // the process-global detector and its mutex, used when the singleton semantics are on
+    struct Global {
+#ifdef CCNN_FACEDETECTOR_SINGLETON
+        bool singleton = true;
+#else
+        bool singleton = false;
+#endif
+        ccnn_handle h = nullptr;
+        Param param;
+        std::recursive_mutex mu;
+    };
+    static Global& global() {
+        static Global g;
+        return g;
+    }
+    ccnn_handle& handle() { return global().singleton ? global().h : h_; }
+    ccnn_handle handle() const { return global().singleton ? global().h : h_; }
+    // serialises Init / Detect / Clear across instances in singleton mode, as the reference's mutex does
+    struct Lock {
+        std::unique_lock<std::recursive_mutex> lk;
+        explicit Lock(const FaceDetector*) {
+            if (global().singleton) lk = std::unique_lock<std::recursive_mutex>(global().mu);
+        }
+    };
 
     static ccnn_params to_c(const Param& q) {
         ccnn_params p;

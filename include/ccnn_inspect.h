@@ -61,12 +61,20 @@ CCNN_API ccnn_status ccnn_stage1_forward(ccnn_handle h, const float* d_img, int 
  * compiled into the library (9 MiB + 256 B per GPU that loads the library, held until exit):
  * images up to 2,359,296 floats of L1 planes (about 1920x1080, 2^21 pixels) are accepted, larger
  * ones are refused with CCNN_ERR_INVALID_ARG and a message naming the limit. model_path may be NULL
- * for the bundled cnn4face1_cntk.bin. The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call before any stream capture.
+ * for the bundled cnn4face1_cntk.bin. The first call in each CUDA context (on each device, and again
+ * after a device reset) looks up the array's device address (cudaGetSymbolAddress, with that device
+ * current); make that first call before any stream capture.
  * All calls share the array and it keeps the last call's contents; calls that overlap on the GPU
  * (other streams or threads) race on it. Returns after the response map is written. */
 CCNN_API ccnn_status ccnn_stage1_forward_static(const char* model_path, const float* d_img, int cols, int rows, size_t step,
                                                 float* d_resp, int resp_cap, int* resp_cols, int* resp_rows, void* stream);
+
+/* Measured ceiling of the fp32 pipe on the current device for the instructions the exact kernels
+ * issue (packed add.rn.f32x2 and the packed product fma.rn.f32x2 with a (-0, -0) addend): lane
+ * operations per second, each packed instruction counting two per thread, best of `reps` timed
+ * launches of `iters` loop trips after one warm-up launch. No counterpart in the reference: it is the
+ * denominator of the stage-1 kernels' roofline. Allocates a small sink buffer; synchronous. */
+CCNN_API ccnn_status ccnn_measure_fp32_peak(int iters, int reps, double* lane_ops_per_s, float* best_ms);
 
 /* Intermediates of the handle's last frame. */
 CCNN_API ccnn_status ccnn_inspect_levels(ccnn_handle h, ccnn_level_info* out, int capacity, int* n_levels);

@@ -54,6 +54,10 @@ def load(fast=False):
         L.ref_equalize.argtypes = [vp, ci, ci]
         L.ref_net_forward.argtypes = [ctypes.c_char_p, ci, vp, ci, ci, ci, vp, ci, P(ci), P(ci)]
         L.ref_face_detect.argtypes = [P(RefParams), vp, ci, ci, ci, ci, P(RefDet), ci]
+        if hasattr(L, "ref_cnn_detect"):
+            from compactcnncascade_b200._capi import CnnAdvancedParam, CnnParam
+            L.ref_cnn_detect.argtypes = [P(CnnParam), P(CnnAdvancedParam), vp, ci, ci, ci, ci, P(RefDet), ci, P(RefDet), ci,
+                                         P(CnnParam), P(CnnAdvancedParam)]
         L.ref_face_detect_fa.argtypes = [P(RefParams), vp, ci, ci, ci, ci, P(RefFace), ci]
         L.ref_cntk_dump2binary.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
         L.ref_api_init.argtypes = [P(RefParams)]
@@ -119,6 +123,35 @@ def face_detect(img, p, fast=False):
     return [(d.x, d.y, d.w, d.h, d.score) for d in out[:n]]
 
 
+def cnn_detect(img, p, ap, prior=()):
+    """The reference's own CNNDetector(&param, &advanced_param) + Detect(detections, image) with `prior`
+    (tuples x, y, w, h, score, scale, knn, num_detect) already in the vector. `p` / `ap` are
+    ccnn_cnn_param / ccnn_cnn_advanced_param structures (the harness shares their layout). Returns
+    (detections, param after, advanced param after)."""
+    from compactcnncascade_b200._capi import CnnAdvancedParam, CnnParam
+    L = load()
+    h, w = img.shape[:2]
+    ch = 1 if img.ndim == 2 else img.shape[2]
+    img = np.ascontiguousarray(img)
+    pr = (RefDet * max(1, len(prior)))(*[RefDet(*d) for d in prior])
+    out = (RefDet * 65536)()
+    pa, apa = CnnParam(), CnnAdvancedParam()
+    n = L.ref_cnn_detect(ctypes.byref(p), ctypes.byref(ap), img.ctypes.data, w, h, ch, img.strides[0], pr, len(prior), out, 65536,
+                         ctypes.byref(pa), ctypes.byref(apa))
+    if n < 0:
+        raise RuntimeError(f"ref_cnn_detect failed ({n})")
+    return [(d.x, d.y, d.w, d.h, d.score, d.scale, d.knn, d.num_detect) for d in out[:n]], pa, apa
+
+
+def merger(dets, threshold, delete=False):
+    """The reference Merger (cnn_detector_v3.cpp:2814-2936) on a list of (x, y, w, h, score, scale, knn, num_detect)."""
+    L = load()
+    inp = (RefDet * max(1, len(dets)))(*[RefDet(*d) for d in dets])
+    out = (RefDet * max(1, len(dets)))()
+    n = L.ref_merger(inp, len(dets), threshold, 1 if delete else 0, out, len(dets))
+    return [(d.x, d.y, d.w, d.h, d.score, d.scale, d.knn, d.num_detect) for d in out[:n]]
+
+
 def face_detect_fa(img, p, fast=False):
     """The reference's public Detect with facial analysis on: (x, y, w, h, score, gender, smile, glasses)."""
     L = load(fast)
@@ -136,8 +169,10 @@ def cntk_dump2binary(binary_file, dump_file):
     load().ref_cntk_dump2binary(binary_file.encode(), dump_file.encode())
 
 
-def detect_steps(img, p, with_levels=True):
-    """Replay of CNNDetector::Detect capturing gray, levels, response maps, raw and final detections."""
+def detect_steps(img, p, with_levels=True, resp_cap=None):
+    """Replay of CNNDetector::Detect capturing gray, levels, response maps, raw and final detections.
+    With `resp_cap` (floats for all response maps together, an upper bound) and no level images, the
+    reference runs once instead of once more to size its outputs."""
     L = load()
     h, w = img.shape[:2]
     ch = 1 if img.ndim == 2 else img.shape[2]
@@ -162,11 +197,21 @@ def detect_steps(img, p, with_levels=True):
         r["nf"] = nf
         return r
 
+    if resp_cap is not None and not with_levels:
+        r = run(0, int(resp_cap))
+        nl = r["nl"].value
+        if nl > cap or int(sum(int(r["rw"][i]) * int(r["rh"][i]) for i in range(nl))) > resp_cap:
+            raise RuntimeError("ref_detect_steps: response capacity too small")
+        return _steps_result(r, nl, with_levels)
     first = run(0, 0)
     nl = first["nl"].value
     lev_cap = int(sum(int(first["lw"][i]) * int(first["lh"][i]) for i in range(nl))) if with_levels else 0
     resp_cap = int(sum(int(first["rw"][i]) * int(first["rh"][i]) for i in range(nl)))
     r = run(lev_cap, resp_cap)
+    return _steps_result(r, nl, with_levels)
+
+
+def _steps_result(r, nl, with_levels):
     res = {"gray": r["gray"][: r["gw"].value * r["gh"].value].reshape(r["gh"].value, r["gw"].value), "levels": [], "resp": []}
     lo = ro = 0
     for i in range(nl):

@@ -424,4 +424,111 @@ int ref_merger(const ref_det* in, int n, float threshold, int del, ref_det* out,
     return m;
 }
 
+// ---- the internal CNNDetector class (cnn_detector_v3.h:82-453), driven directly ----
+
+// The same layout as ccnn_cnn_param / ccnn_cnn_advanced_param of include/ccnn_cnn.h.
+typedef struct {
+    int pipeline;
+    int max_image_width, max_image_height;
+    int min_obj_width, min_obj_height;
+    int max_obj_width, max_obj_height;
+    float scale_factor;
+    int min_neighbors;
+    int num_threads;
+} ref_cnn_param;
+
+typedef struct {
+    int detect_mode, detect_precision, packet_detection, gray_image_only, facial_analysis;
+    int equalize, reflection, type_check;
+    float treshold_1, treshold_2, treshold_3;
+    int adapt_min_neighbors, double_check, drop_detect, min_num_detect;
+    int device_info, cuda_device_id, cl_platform_id, cl_device_id, concurrent_kernels, num_cnn_copy;
+    int blur, img_resize, uniform_noise, merger_detect;
+    int index_output[4];
+} ref_cnn_advanced_param;
+
+static void to_ref_params(const ref_cnn_param* p, const ref_cnn_advanced_param* a, CNNDetector::Param* q, CNNDetector::AdvancedParam* b) {
+    q->pipeline = static_cast<CNNDetector::Pipeline>(p->pipeline);
+    q->max_image_size = Size(p->max_image_width, p->max_image_height);
+    q->min_obj_size = Size(p->min_obj_width, p->min_obj_height);
+    q->max_obj_size = Size(p->max_obj_width, p->max_obj_height);
+    q->scale_factor = p->scale_factor;
+    q->min_neighbors = p->min_neighbors;
+    q->num_threads = p->num_threads;
+    b->detect_mode = static_cast<CNNDetector::DetectMode>(a->detect_mode);
+    b->detect_precision = static_cast<CNNDetector::DetectPrecision>(a->detect_precision);
+    b->packet_detection = a->packet_detection != 0;
+    b->gray_image_only = a->gray_image_only != 0;
+    b->facial_analysis = a->facial_analysis != 0;
+    b->equalize = a->equalize != 0;
+    b->reflection = a->reflection != 0;
+    b->type_check = a->type_check;
+    b->treshold_1 = a->treshold_1;
+    b->treshold_2 = a->treshold_2;
+    b->treshold_3 = a->treshold_3;
+    b->adapt_min_neighbors = a->adapt_min_neighbors != 0;
+    b->double_check = a->double_check != 0;
+    b->drop_detect = a->drop_detect != 0;
+    b->min_num_detect = a->min_num_detect;
+    b->device_info = a->device_info != 0;
+    b->cuda_device_id = a->cuda_device_id;
+    b->cl_platform_id = a->cl_platform_id;
+    b->cl_device_id = a->cl_device_id;
+    b->concurrent_kernels = a->concurrent_kernels;
+    b->num_cnn_copy = a->num_cnn_copy;
+    b->blur = a->blur != 0;
+    b->img_resize = static_cast<CNNDetector::ImgResize>(a->img_resize);
+    b->uniform_noise = a->uniform_noise != 0;
+    b->merger_detect = a->merger_detect != 0;
+    for (int i = 0; i < 4; ++i) b->index_output[i] = a->index_output[i];
+}
+
+// CNNDetector(&param, &advanced_param) + Detect(detections, image) with `prior` already in the
+// vector; returns the detection count and, when given, the parameters the detector then reports.
+int ref_cnn_detect(const ref_cnn_param* p, const ref_cnn_advanced_param* a, const uint8_t* img, int w, int h, int ch, int step,
+                   const ref_det* prior, int n_prior, ref_det* out, int cap, ref_cnn_param* p_after, ref_cnn_advanced_param* a_after) {
+    std::lock_guard<std::mutex> lk(g_api_mutex);
+    CNNDetector::Param q;
+    CNNDetector::AdvancedParam b;
+    to_ref_params(p, a, &q, &b);
+    CNNDetector det(&q, &b);
+    if (det.isEmpty()) return -1;
+    std::vector<CNNDetector::Detection> dets;
+    for (int i = 0; i < n_prior; ++i) {
+        CNNDetector::Detection d(prior[i].x, prior[i].y, prior[i].w, prior[i].h, prior[i].score, prior[i].scale, prior[i].knn);
+        d.num_detect = prior[i].num_detect;
+        dets.push_back(d);
+    }
+    SIMD::Image_8u image(w, h, ch, const_cast<uint8_t*>(img), step);
+    const int r = det.Detect(dets, image);
+    if (r < 0) return r;
+    const int n = (int)dets.size();
+    for (int i = 0; i < n && i < cap; ++i) copy_det(&out[i], dets[i]);
+    if (p_after) {
+        const CNNDetector::Param g = det.getParam();
+        *p_after = *p;
+        p_after->pipeline = (int)g.pipeline;
+        p_after->max_image_width = g.max_image_size.width;
+        p_after->max_image_height = g.max_image_size.height;
+    }
+    if (a_after) {
+        const CNNDetector::AdvancedParam g = det.getAdvancedParam();
+        *a_after = *a;
+        a_after->packet_detection = g.packet_detection;
+        a_after->gray_image_only = g.gray_image_only;
+        a_after->facial_analysis = g.facial_analysis;
+        a_after->equalize = g.equalize;
+        a_after->reflection = g.reflection;
+        a_after->type_check = g.type_check;
+        a_after->adapt_min_neighbors = g.adapt_min_neighbors;
+        a_after->double_check = g.double_check;
+        a_after->drop_detect = g.drop_detect;
+        a_after->min_num_detect = g.min_num_detect;
+        a_after->blur = g.blur;
+        a_after->uniform_noise = g.uniform_noise;
+        a_after->merger_detect = g.merger_detect;
+    }
+    return n;
+}
+
 }  // extern "C"

@@ -11,7 +11,7 @@ if not torch.cuda.is_available():
 
 import compactcnncascade_b200 as ccnn  # noqa: E402
 from compactcnncascade_b200 import _capi  # noqa: E402
-from oracle import oracle as orc  # noqa: E402
+from oracle import ref  # noqa: E402
 
 
 def _params():
@@ -89,12 +89,16 @@ def test_gated_server_matches_gated_detector(mix):
     srv.close()
 
 
-def test_server_frame_matches_oracle(mix):
+def test_server_frame_matches_reference(mix):
+    """A served frame against the reference's own cascade (strict IEEE build of its sources)."""
+    if not ref.available():
+        pytest.skip("reference build oracle/_ref/libccnn_ref.so not present")
     srv = ccnn.FaceServer(_params())
     t = srv.submit(mix[0])
     faces, _ = srv.wait(t)
-    p = orc.params(max_w=640, max_h=480)
-    assert faces == orc.detect(np.ascontiguousarray(mix[0]), p)["final"]
+    img = np.ascontiguousarray(mix[0])
+    p = ref.params(max_w=img.shape[1], max_h=img.shape[0])
+    assert faces == ref.face_detect(img, p)
     srv.close()
 
 

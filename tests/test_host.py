@@ -18,7 +18,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared():
     names = []
-    for h in ("ccnn.h", "ccnn_inspect.h", "ccnn_server.h", "ccnn_gate.h"):
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not h.endswith(".h"):
+            continue
         src = open(os.path.join(ROOT, "include", h)).read()
         names += re.findall(r"CCNN_API\s+[\w\s\*]+?\b(ccnn_\w+)\s*\(", src)
     return sorted(set(names))
@@ -32,6 +34,23 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(L, n), n
     assert sorted(set(_capi.EXPORTED)) == names
     assert b"sm_100a" in L.ccnn_version()
+
+
+def test_cnn_detector_defaults_are_the_reference_defaults():
+    p, ap = _capi.CnnParam(), _capi.CnnAdvancedParam()
+    _capi.lib().ccnn_cnn_default_params(p, ap)
+    # CNNDetector::Param (cnn_detector_v3.h:114-123)
+    assert (p.pipeline, p.max_image_width, p.max_image_height) == (0, 1280, 720)
+    assert (p.min_obj_width, p.min_obj_height, p.max_obj_width, p.max_obj_height) == (48, 48, 0, 0)
+    assert abs(p.scale_factor - 1.2) < 1e-6 and p.min_neighbors == 2 and p.num_threads == 0
+    # CNNDetector::AdvancedParam (cnn_detector_v3.h:124-175)
+    assert (ap.detect_mode, ap.detect_precision, ap.packet_detection, ap.gray_image_only, ap.facial_analysis) == (1, 2, 0, 0, 0)
+    assert (ap.equalize, ap.reflection, ap.type_check) == (1, 1, 1)
+    assert (ap.treshold_1, ap.treshold_2, ap.treshold_3) == (0.0, 0.0, 0.0)
+    assert (ap.adapt_min_neighbors, ap.double_check, ap.drop_detect, ap.min_num_detect) == (0, 1, 1, 1)
+    assert (ap.device_info, ap.cuda_device_id, ap.cl_platform_id, ap.cl_device_id) == (0, 0, -1, -1)
+    assert (ap.concurrent_kernels, ap.num_cnn_copy, ap.blur, ap.img_resize, ap.uniform_noise, ap.merger_detect) == (3, 1, 0, 0, 0, 1)
+    assert list(ap.index_output) == [1, 0, 0, -1]
 
 
 def test_default_params_are_the_reference_defaults():
