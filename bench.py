@@ -320,6 +320,20 @@ def frame_bytes(levels, w, h):
     return 3 * w * h + 8 * w * h + sum(8 * a[0] * a[1] for a in levels) + sum(4 * a[3] * a[4] for a in levels)
 
 
+def committed_records():
+    """Longer measurements recorded once on a B200 and committed under profiles/: the serving sweep
+    (`bench.py --serving`) and the learned gate's held-out evaluation (`python -m
+    compactcnncascade_b200.gate --eval-only --report ...`). Empty when absent."""
+    out = {}
+    for key, name in (("serving_sweep", "serving_sweep_mixed_resolutions.json"), ("gate_heldout", "gate_heldout_eval_1080p.json")):
+        try:
+            with open(os.path.join(ROOT, "profiles", name)) as f:
+                out[key] = json.load(f)
+        except (OSError, ValueError):
+            pass
+    return out
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -352,7 +366,9 @@ def main():
     ap.add_argument("--batched-frames", type=int, default=8,
                     help="frames per batch of the batched-pyramid phase (3840x2160 and 4800x2400; 0: skip)")
     ap.add_argument("--serving", action="store_true",
-                    help="only the serving sweep: 10,000 mixed-resolution frames at 500, 1000, 2000, 4000 frames/s")
+                    help="only the serving sweep: 10,000 mixed-resolution frames per offered rate, plain and gated")
+    ap.add_argument("--serve-rates", default="500,1000,2000,4000,8000,16000", help="offered rates of the serving sweep, frames/s")
+    ap.add_argument("--serve-frames-sweep", type=int, default=10_000, help="frames per offered rate of the serving sweep")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -366,9 +382,15 @@ def main():
     if args.serving:
         if rank == 0:
             fr = serve_frames(4)
-            sweep = [run_serving(fr, r, 10_000, seed=int(r)) for r in (500.0, 1000.0, 2000.0, 4000.0)]
+            rates = [float(r) for r in args.serve_rates.split(",")]
+            sweep = [run_serving(fr, r, args.serve_frames_sweep, seed=int(r)) for r in rates]
+            from compactcnncascade_b200 import gate as gate_mod
+            gthr = gate_mod.load_meta().get("operating_threshold", 0.1)
+            gsweep = [run_serving(fr, r, args.serve_frames_sweep, seed=int(r), gate=(gate_mod.load(), gthr, args.gate_fallback))
+                      for r in rates]
             print(json.dumps({"metric": "serving loop p50/p99 ms and fps, mixed 640x480/1280x720/1920x1080/3840x2160 at 30/30/30/10 %",
-                              "unit": "ms", "data": "synthetic (seeded generator)", "sweep": sweep}), flush=True)
+                              "unit": "ms", "data": "synthetic (seeded generator)", "frames_per_rate": args.serve_frames_sweep,
+                              "sweep": sweep, "gated_threshold": gthr, "sweep_gated": gsweep}), flush=True)
         return
 
     from compactcnncascade_b200.replicas import rank_seeds
@@ -641,9 +663,14 @@ def main():
         line["gated"] = gated
     if batched:
         line["batched_pyramid"] = batched
+    rec = committed_records()
+    if gated and rec.get("gate_heldout"):
+        gated["heldout"] = rec["gate_heldout"]
     if serving:
         line["serving"] = dict(serving, note="serving loop (ccnn_server_*): Poisson arrivals of mixed 640x480/1280x720/"
                                              "1920x1080/3840x2160 frames at 30/30/30/10 %, latency = submit to result")
+    if serving and rec.get("serving_sweep"):
+        line["serving"]["sweep"] = rec["serving_sweep"]
     if serving_gated:
         line["serving"]["gated"] = dict(serving_gated, note="the same stream with the learned gate on in every resolution "
                                                             "class (weights trained at 1080p; recall measured at 1080p only)")

@@ -232,7 +232,7 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--pos-weight", type=float, default=40.0)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--thresholds", default="0.02,0.05,0.1,0.2,0.3")
+    ap.add_argument("--thresholds", default="0.02,0.05,0.1,0.2,0.3,0.4,0.5")
     ap.add_argument("--fallback", type=float, default=0.25)
     ap.add_argument("--out", default=WEIGHTS_1080P)
     ap.add_argument("--report", default=None, help="write the evaluation as JSON here")
@@ -253,6 +253,12 @@ def main(argv=None):
                     operating_threshold=_operating_point(ev, thr))
         print(f"operating threshold {meta['operating_threshold']}", flush=True)
         save(a.out, params, meta)
+        if a.report:
+            with open(a.report, "w") as f:
+                json.dump({"weights": os.path.basename(a.out), "eval_frames": a.eval_frames,
+                           "eval_seeds": meta["eval_seeds"], "fallback_fraction": a.fallback,
+                           "operating_threshold": meta["operating_threshold"], "eval": ev,
+                           "workload": meta.get("workload"), "reference": "plain cascade boxes matched at IoU >= 0.5"}, f, indent=1)
         return 0
     t0 = time.time()
     ds = collect(det, range(TRAIN_SEED0, TRAIN_SEED0 + a.train_frames))
