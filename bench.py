@@ -643,9 +643,8 @@ def main():
         "config": {"workload": WORKLOAD, "frames_per_step": B, "distinct_frames": len(frames),
                    "l2": f"inputs larger than L2: {len(frames)} distinct frames x {W * H * 3 / 1e6:.1f} MB cycled",
                    "parallelism": f"replicas x{world}", "levels": len(levels),
-                   "schedule": {"frame_slots": schedule[0], "window_ctas_per_sm": schedule[1],
-                                "source": "autotuner table (compactcnncascade_b200/schedules.json)"
-                                if autotune.lookup(p) else "defaults"},
+                   "schedule": dict(schedule, source="autotuner table (compactcnncascade_b200/schedules.json)"
+                                    if autotune.lookup(p) else "defaults"),
                    "stage1_candidates_last_frame": len(cands), "faces_per_frame": round(faces_total / (args.steps * B), 2)},
         "p50_ms": round(float(np.percentile(lat, 50)), 3),
         "p99_ms": round(float(np.percentile(lat, 99)), 3),

@@ -49,8 +49,8 @@ class FaceDetector:
     # ---- lifecycle ----
     def Init(self, param=None, models=None, schedule=None):
         """FaceDetector::Init (CompactCNNLibAPI_v2.cpp:373-407). Returns 0 or -1. `schedule`:
-        None (defaults), "auto" (the autotuner's entry for these parameters, when it has one) or
-        (frame_slots, window_ctas_per_sm)."""
+        None (defaults), "auto" (the autotuner's entry for these parameters, when it has one) or a
+        dict of schedule knobs (compactcnncascade_b200.autotune.KNOBS)."""
         if self._h is not None:
             self.Clear()
         self._param = param if param is not None else default_params()
@@ -65,9 +65,9 @@ class FaceDetector:
         self._h = h
         if schedule is not None:
             from . import autotune
-            sched = autotune.lookup(self._param) if schedule == "auto" else tuple(schedule)
+            sched = autotune.lookup(self._param) if schedule == "auto" else dict(schedule)
             if sched is not None:
-                autotune.set_schedule(self, *sched)
+                autotune.set_schedule(self, sched)
         return 0
 
     def Clear(self):

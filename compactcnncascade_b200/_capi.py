@@ -38,7 +38,7 @@ EXPORTED = [
     "ccnn_gate_labels", "ccnn_gate_features", "ccnn_gate_gradient", "ccnn_gate_train", "ccnn_server_set_gate",
     "ccnn_legacy_model_info", "ccnn_legacy_net_forward", "ccnn_set_schedule", "ccnn_get_schedule",
     "ccnn_measure_fp32_peak", "ccnn_cnn_default_params", "ccnn_cnn_create", "ccnn_cnn_detect", "ccnn_cnn_nms",
-    "ccnn_cnn_get_params", "ccnn_cnn_set_params",
+    "ccnn_cnn_get_params", "ccnn_cnn_set_params", "ccnn_set_schedule_ex", "ccnn_get_schedule_ex",
 ]
 
 
@@ -110,6 +110,12 @@ class CnnAdvancedParam(ctypes.Structure):
                                             "cuda_device_id", "cl_platform_id", "cl_device_id", "concurrent_kernels",
                                             "num_cnn_copy", "blur", "img_resize", "uniform_noise", "merger_detect")] + \
                [("index_output", ctypes.c_int * 4)]
+
+
+class Schedule(ctypes.Structure):
+    """ccnn_schedule (include/ccnn_inspect.h)."""
+    _fields_ = [("frame_slots", ctypes.c_int), ("window_ctas_per_sm", ctypes.c_int), ("front_blocks_per_sm", ctypes.c_int),
+                ("back_blocks_per_sm", ctypes.c_int)]
 
 
 class SynthFace(ctypes.Structure):
@@ -190,6 +196,8 @@ def lib():
         L.ccnn_legacy_model_info.argtypes = [ctypes.c_char_p, P(ci), ci]
         L.ccnn_set_schedule.argtypes = [vp, ci, ci]
         L.ccnn_get_schedule.argtypes = [vp, P(ci), P(ci)]
+        L.ccnn_set_schedule_ex.argtypes = [vp, P(Schedule)]
+        L.ccnn_get_schedule_ex.argtypes = [vp, P(Schedule)]
         L.ccnn_legacy_net_forward.argtypes = [ctypes.c_char_p, vp, ci, ci, ctypes.c_size_t, vp, ci, P(ci), P(ci), vp]
         L.ccnn_gate_stats.argtypes = [vp, P(ci), P(ci), P(ci), P(ci), P(ci)]
         L.ccnn_gate_labels.argtypes = [vp, vp, vp]

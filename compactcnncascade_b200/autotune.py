@@ -1,8 +1,16 @@
 """Schedule autotuner: for a frame size and detector settings, times the cascade on seeded synthetic
-frames (rendered on the device) under each candidate schedule -- frames in flight and resident
-stage-2/3 blocks per SM (include/ccnn_inspect.h, ccnn_set_schedule) -- and keeps the fastest in a
-JSON table keyed by the workload. FaceDetector.Init(..., schedule="auto") applies a table entry.
-Results never depend on the schedule; only throughput does.
+frames (rendered on the device) under candidate schedules and keeps the fastest in a JSON table
+keyed by the workload. FaceDetector.Init(..., schedule="auto") applies a table entry. Results never
+depend on the schedule; only throughput does.
+
+The knobs (include/ccnn_inspect.h, ccnn_schedule):
+  frame_slots          frames in flight, each with its own stream, buffers and captured graph
+  window_ctas_per_sm   resident blocks per SM of the persistent stage-2/3 window kernel
+  front_blocks_per_sm  register budget of the stage-1 front kernel (3: 80 registers, 4: 64)
+  back_blocks_per_sm   register budget of the stage-1 back kernel (3: 80 registers, 4: 64)
+
+The search is coordinate descent from the defaults: each knob in turn takes the value that times
+fastest with the others held, for two passes (a full product of the knobs would be 96 timings).
 
     python -m compactcnncascade_b200.autotune --width 1920 --height 1080
 """
@@ -15,8 +23,9 @@ import sys
 from . import _capi
 
 TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "schedules.json")
-SLOTS = (4, 8, 12, 16)
-WINDOW_CTAS = (2, 3, 4)
+KNOBS = (("frame_slots", (4, 8, 12, 16)), ("window_ctas_per_sm", (2, 3, 4)), ("front_blocks_per_sm", (3, 4)),
+         ("back_blocks_per_sm", (3, 4)))
+DEFAULTS = {"frame_slots": 8, "window_ctas_per_sm": 4, "front_blocks_per_sm": 3, "back_blocks_per_sm": 4}
 
 
 def key(width, height, scale_factor, min_face, max_face):
@@ -32,19 +41,23 @@ def load_table(path=TABLE):
 
 
 def lookup(p, path=TABLE):
-    """(frame_slots, window_ctas_per_sm) tuned for these parameters, or None."""
+    """The tuned schedule (knob -> value) for these parameters, or None."""
     e = load_table(path).get(key(p.max_image_width, p.max_image_height, p.scale_factor, p.min_face_height, p.max_face_height))
-    return (e["frame_slots"], e["window_ctas_per_sm"]) if e else None
+    if not e:
+        return None
+    return {k: e[k] for k, _ in KNOBS if k in e}
 
 
-def set_schedule(det, frame_slots, window_ctas_per_sm):
-    _capi.check(_capi.lib().ccnn_set_schedule(det._h, int(frame_slots), int(window_ctas_per_sm)), "ccnn_set_schedule")
+def set_schedule(det, schedule):
+    """Applies a schedule (dict of knobs; missing knobs keep their value) to a FaceDetector."""
+    s = _capi.Schedule(*[int(schedule.get(k, 0)) for k, _ in KNOBS])
+    _capi.check(_capi.lib().ccnn_set_schedule_ex(det._h, ctypes.byref(s)), "ccnn_set_schedule_ex")
 
 
 def get_schedule(det):
-    a, b = ctypes.c_int(), ctypes.c_int()
-    _capi.check(_capi.lib().ccnn_get_schedule(det._h, ctypes.byref(a), ctypes.byref(b)), "ccnn_get_schedule")
-    return a.value, b.value
+    s = _capi.Schedule()
+    _capi.check(_capi.lib().ccnn_get_schedule_ex(det._h, ctypes.byref(s)), "ccnn_get_schedule_ex")
+    return {k: getattr(s, k) for k, _ in KNOBS}
 
 
 def measure(det, frames, width, height, batch=64, steps=8, warmup=3):
@@ -69,8 +82,9 @@ def measure(det, frames, width, height, batch=64, steps=8, warmup=3):
 
 
 def tune(width, height, scale_factor=1.15, min_face=40, max_face=240, n_faces=20, min_patch=30, max_patch=300, distinct=16,
-         slots=SLOTS, window_ctas=WINDOW_CTAS, rounds=2):
-    """Times every candidate schedule `rounds` times (interleaved) and returns the table entry."""
+         knobs=KNOBS, passes=2, batch=64):
+    """Coordinate descent over the knobs; returns the table entry (the schedule, its frames/s and
+    every timing taken)."""
     import torch
     from . import FaceDetector, default_params, synth_frame_device
     p = default_params()
@@ -85,17 +99,28 @@ def tune(width, height, scale_factor=1.15, min_face=40, max_face=240, n_faces=20
         t = torch.empty((height, width, 3), dtype=torch.uint8, device="cuda")
         synth_frame_device(t.data_ptr(), width, height, 800_000 + s, n_faces, min_patch, max_patch)
         frames.append(t)
-    best = {}
-    for _ in range(rounds):
-        for sl in slots:
-            for wc in window_ctas:
-                set_schedule(det, sl, wc)
-                fps = measure(det, frames, width, height)
-                best[(sl, wc)] = max(best.get((sl, wc), 0.0), fps)
-    (sl, wc), fps = max(best.items(), key=lambda kv: kv[1])
+    timings = {}
+
+    def timed(sched):
+        name = "/".join(f"{sched[k]}" for k, _ in knobs)
+        set_schedule(det, sched)
+        fps = measure(det, frames, width, height, batch=batch)
+        timings[name] = round(max(timings.get(name, 0.0), fps), 1)
+        return fps
+
+    best = dict(DEFAULTS)
+    best_fps = timed(best)
+    for _ in range(passes):
+        for k, values in knobs:
+            for v in values:
+                if v == best[k]:
+                    continue
+                trial = dict(best, **{k: v})
+                fps = timed(trial)
+                if fps > best_fps:
+                    best, best_fps = trial, fps
     det.Clear()
-    return {"frame_slots": sl, "window_ctas_per_sm": wc, "frames_per_s": round(fps, 1),
-            "tried": {f"{a}x{b}": round(v, 1) for (a, b), v in sorted(best.items())}}
+    return dict(best, frames_per_s=round(best_fps, 1), knobs=[k for k, _ in knobs], tried=timings)
 
 
 def main(argv=None):
@@ -106,9 +131,13 @@ def main(argv=None):
     ap.add_argument("--min-face", type=int, default=40)
     ap.add_argument("--max-face", type=int, default=240)
     ap.add_argument("--faces", type=int, default=20)
+    ap.add_argument("--min-patch", type=int, default=30)
+    ap.add_argument("--max-patch", type=int, default=300)
+    ap.add_argument("--batch", type=int, default=64, help="frames per timed batch")
     ap.add_argument("--table", default=TABLE)
     a = ap.parse_args(argv)
-    entry = tune(a.width, a.height, a.scale_factor, a.min_face, a.max_face, n_faces=a.faces)
+    entry = tune(a.width, a.height, a.scale_factor, a.min_face, a.max_face, n_faces=a.faces, min_patch=a.min_patch,
+                 max_patch=a.max_patch, batch=a.batch)
     table = load_table(a.table)
     table[key(a.width, a.height, a.scale_factor, a.min_face, a.max_face)] = entry
     with open(a.table, "w") as f:

@@ -230,6 +230,17 @@ CCNN_API ccnn_status ccnn_get_schedule(ccnn_handle h, int* frame_slots, int* win
     return CCNN_OK;
 }
 
+CCNN_API ccnn_status ccnn_set_schedule_ex(ccnn_handle h, const ccnn_schedule* s) {
+    if (!h || !s) return CCNN_ERR_INVALID_ARG;
+    return h->det.set_schedule(s->frame_slots, s->window_ctas_per_sm, s->front_blocks_per_sm, s->back_blocks_per_sm);
+}
+
+CCNN_API ccnn_status ccnn_get_schedule_ex(ccnn_handle h, ccnn_schedule* s) {
+    if (!h || !s) return CCNN_ERR_INVALID_ARG;
+    h->det.get_schedule(&s->frame_slots, &s->window_ctas_per_sm, &s->front_blocks_per_sm, &s->back_blocks_per_sm);
+    return CCNN_OK;
+}
+
 CCNN_API ccnn_status ccnn_gate_set(ccnn_handle h, const float* params, int n_params, float threshold, float fallback_fraction) {
     if (!h) return CCNN_ERR_INVALID_ARG;
     return h->det.gate_set(params, n_params, threshold, fallback_fraction);

@@ -594,21 +594,26 @@ ccnn_status Detector::gate_set(const float* params, int n, float threshold, floa
     return CCNN_OK;
 }
 
-ccnn_status Detector::set_schedule(int frame_slots, int window_ctas_per_sm) {
+ccnn_status Detector::set_schedule(int frame_slots, int window_ctas_per_sm, int front_bpsm, int back_bpsm) {
     std::lock_guard<std::mutex> lk(mu_);
-    if (frame_slots < 0 || frame_slots > 64 || window_ctas_per_sm < 0 || window_ctas_per_sm > 4) {
-        set_error("schedule: 1-64 frame slots and 1-4 stage-2/3 blocks per SM (0 keeps the current value)");
+    if (frame_slots < 0 || frame_slots > 64 || window_ctas_per_sm < 0 || window_ctas_per_sm > 4 || (front_bpsm != 0 && (front_bpsm < 3 || front_bpsm > 4)) ||
+        (back_bpsm != 0 && (back_bpsm < 3 || back_bpsm > 4))) {
+        set_error("schedule: 1-64 frame slots, 1-4 stage-2/3 blocks per SM, 3-4 stage-1 blocks per SM (0 keeps the current value)");
         return CCNN_ERR_INVALID_ARG;
     }
     clear();
     if (frame_slots > 0) slots_.assign(frame_slots, Slot());
     if (window_ctas_per_sm > 0) window_ctas_per_sm_ = window_ctas_per_sm;
+    if (front_bpsm > 0) s1_sched_.front_blocks_per_sm = front_bpsm;
+    if (back_bpsm > 0) s1_sched_.back_blocks_per_sm = back_bpsm;
     return init();
 }
 
-void Detector::get_schedule(int* frame_slots, int* window_ctas_per_sm) const {
+void Detector::get_schedule(int* frame_slots, int* window_ctas_per_sm, int* front_bpsm, int* back_bpsm) const {
     *frame_slots = (int)slots_.size();
     *window_ctas_per_sm = window_ctas_per_sm_;
+    if (front_bpsm) *front_bpsm = s1_sched_.front_blocks_per_sm;
+    if (back_bpsm) *back_bpsm = s1_sched_.back_blocks_per_sm;
 }
 
 ccnn_status Detector::gate_disable() {
@@ -720,7 +725,7 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
     } else {
         CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
                                 gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr,
-                                gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}));
+                                gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}, s1_sched_));
     }
     CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                 (int)cand_cap_, s.st));
@@ -1243,7 +1248,8 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st,
                                  gated ? s.d_front_on : nullptr));
         CCNN_CUDA(cudaEventRecord(ev[2], s.st));
-        if (!legacy_) CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st, gated ? s.d_front_on : nullptr));
+        if (!legacy_)
+            CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st, gated ? s.d_front_on : nullptr, s1_sched_));
         CCNN_CUDA(cudaEventRecord(ev[3], s.st));
         if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
         if (legacy_) {  // the legacy network's three layers all count as the back entry
@@ -1251,7 +1257,8 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
             if (ls != CCNN_OK) return ls;
         } else
             CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
-                                         gated ? s.d_back_on : nullptr, gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}));
+                                         gated ? s.d_back_on : nullptr, gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{},
+                                         s1_sched_));
         CCNN_CUDA(cudaEventRecord(ev[4], s.st));
         CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                     (int)cand_cap_, s.st));

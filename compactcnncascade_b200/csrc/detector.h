@@ -109,8 +109,8 @@ class Detector {
     ccnn_status gate_disable();
     // schedule knobs an autotuner sets: frames in flight and resident stage-2/3 blocks per SM
     // (0 keeps the current value); the device state is rebuilt
-    ccnn_status set_schedule(int frame_slots, int window_ctas_per_sm);
-    void get_schedule(int* frame_slots, int* window_ctas_per_sm) const;
+    ccnn_status set_schedule(int frame_slots, int window_ctas_per_sm, int front_bpsm = 0, int back_bpsm = 0);
+    void get_schedule(int* frame_slots, int* window_ctas_per_sm, int* front_bpsm = nullptr, int* back_bpsm = nullptr) const;
     // training labels of the last frame (slot 0): uint8 [4][gh/16][gw/16], device memory
     ccnn_status gate_labels(uint8_t* d_labels, cudaStream_t st);
     // stage-1 tiles the gate let run in the last frame (slot 0), of all, and whether it fell back
@@ -172,6 +172,7 @@ class Detector {
     LegacyNet* d_lg_ = nullptr;
     ccnn_status enqueue_legacy_stage1(Slot& s, const Plan& p);
     int window_ctas_per_sm_ = 4;     // persistent stage-2/3 grid: this many blocks per SM
+    Stage1Sched s1_sched_{};         // stage-1 register budgets
     float* d_gate_ = nullptr;        // learned gate parameters (device memory)
     bool gate_on_ = false;
     float gate_thr_ = 0.5f, gate_amb_frac_ = 0.25f;

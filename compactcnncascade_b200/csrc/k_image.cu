@@ -8,6 +8,7 @@
 // and 128-bit stores; the staging buffer's row pitch is a multiple of 64 bytes so every
 // vector access is aligned. Rows whose width is not a multiple of 16 finish with scalar code.
 #include "kernels.h"
+#include "pyramid.cuh"
 #include "resample.cuh"
 
 namespace ccnn {
@@ -113,55 +114,7 @@ __global__ void __launch_bounds__(kPyrCols) pyramid_kernel(const __grid_constant
                                                            const uint8_t* __restrict__ front_on) {
     const int g = LT.first + blockIdx.x;
     const LevelDesc& L = LT.lv[find_level<&LevelDesc::pyr_base>(LT, g)];
-    const int local = g - L.pyr_base;
-    const int rb = local / L.pyr_wq;
-    const int cb = local - rb * L.pyr_wq;
-    if (front_on) {
-        // with the learned gate only the stage-1 front tiles that run read the level image: a block
-        // that none of them reads is left out (front tile (tx, ty) reads rows [32 ty, 32 ty + 35)
-        // and columns [64 tx, 64 tx + 68))
-        const int ty0 = max(0, (kPyrRows * rb - (2 * kK1TileY + 3) + 2 * kK1TileY) / (2 * kK1TileY));
-        const int ty1 = min((L.p1h + kK1TileY - 1) / kK1TileY - 1, (kPyrRows * rb + kPyrRows - 1) / (2 * kK1TileY));
-        const int tx0 = max(0, (kPyrCols * cb - (2 * kK1TileX + 4) + 2 * kK1TileX) / (2 * kK1TileX));
-        const int tx1 = min(L.k1_tiles_x - 1, (kPyrCols * cb + kPyrCols - 1) / (2 * kK1TileX));
-        bool need = false;
-        for (int ty = ty0; ty <= ty1 && !need; ++ty)
-            for (int tx = tx0; tx <= tx1; ++tx)
-                if (front_on[L.k1_base + ty * L.k1_tiles_x + tx]) {
-                    need = true;
-                    break;
-                }
-        if (!need) return;
-    }
-    const int x = cb * kPyrCols + threadIdx.x;
-    if (x >= L.img_pitch) return;
-    float* out = limg + L.img_off + x;
-    const int y0 = rb * kPyrRows;
-    const int y1 = y0 + kPyrRows < L.h ? y0 + kPyrRows : L.h;
-    if (x >= L.w) {
-        for (int y = y0; y < y1; ++y) out[(long long)y * L.img_pitch] = 0.f;
-        return;
-    }
-    if (L.mode == 0) {
-        for (int y = y0; y < y1; ++y) out[(long long)y * L.img_pitch] = __ldg(gray + (size_t)y * gpitch + x);
-        return;
-    }
-    const AxisSample sx = sample_col(x, L.sclx, gw);
-    if (L.mode == 1) {
-        for (int y = y0; y < y1; ++y)
-            out[(long long)y * L.img_pitch] = __ldg(gray + (size_t)sample_row(y, L.scly, gh).idx * gpitch + sx.idx);
-        return;
-    }
-#pragma unroll 4
-    for (int y = y0; y < y1; ++y) {
-        const AxisSample sy = sample_row(y, L.scly, gh);
-        uint32_t py = sy.idx;
-        if (py + 1 >= (uint32_t)gh) py--;  // bilinear keeps a row below
-        const float* r0 = gray + (size_t)py * gpitch + sx.idx;
-        const float top = fadd(fmul(__ldg(r0), sx.c), fmul(__ldg(r0 + 1), sx.f));
-        const float bot = fadd(fmul(__ldg(r0 + gpitch), sx.c), fmul(__ldg(r0 + gpitch + 1), sx.f));
-        out[(long long)y * L.img_pitch] = fadd(fmul(top, sy.c), fmul(bot, sy.f));
-    }
+    pyramid_block(L, g - L.pyr_base, gray, gpitch, gw, gh, limg, front_on);
 }
 
 cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* gray, int gpitch, int gw, int gh, float* limg,

@@ -8,16 +8,19 @@
 // front: one CTA per 32x16 tile of pooled L1 pixels of one level. The CTA stages its (67 x 35)
 //        input tile of the level image, runs the 4x4 conv + folded BN/LReLU + 2x2 max for the 4
 //        L1 maps and writes the 4 neighbour-map sums that L2 consumes (S1 arena).
-// back:  one CTA per 32x16 tile of response pixels. It stages the S1 tile (4 x 42 x 72) in shared
-//        memory, computes the 8 pooled L2 maps and their sums on the 35 x 20 halo tile, then every
-//        thread finishes two vertically adjacent response pixels: the 16 L3 maps (4w x 5h), the
-//        52 hidden neurons and the output neuron.
+// back:  one CTA per 32x16 tile of response pixels. It stages the S1 tile (4 x 42 x 72, two maps at
+//        a time) in shared memory, computes the 8 pooled L2 maps and their sums on the 35 x 20 halo
+//        tile, then every thread finishes two vertically adjacent response pixels: the 16 L3 maps
+//        (4w x 5h), the 52 hidden neurons and the output neuron.
+// Both kernels come in two register budgets (3 or 4 resident 256-thread blocks per SM), chosen per
+// workload by the schedule (Stage1Sched).
 // Packed f32x2 instructions run two identical chains of IEEE operations at once (two pixels, or
 // two maps that read the same input), so every value still sees the reference's roundings.
 // Every tile of every level is one block of the same grid; a block finds its level by binary
 // search over the level descriptors (kernel parameters), so a frame is two launches per group of
 // up to kParamLevels levels.
 #include "kernels.h"
+#include "pyramid.cuh"
 #include "resample.cuh"
 
 namespace ccnn {
@@ -43,44 +46,47 @@ struct FrontTile {
 };
 
 // Loads the (67 x 35) input tile of a front CTA from its level image. Rows that start 16-byte
-// aligned with a pitch of whole float4 groups are read as 17 float4 per row (columns past the
-// image width hold zeros or the caller's own padding; no stored pixel depends on them), other
-// images one float at a time.
+// aligned with a pitch of whole float4 groups are read as 34 float2 column pairs per row (the tile
+// starts at an even column, columns past the image width hold zeros or the caller's own padding; no
+// stored pixel depends on them); consecutive threads take consecutive pairs, so their stores into
+// the parity-split rows fall on consecutive words. Other images are read one float at a time.
+template <bool kCoherent>
 __device__ __forceinline__ void load_front_tile(FrontTile& T, const float* __restrict__ img, const LevelDesc& L, int ix0, int iy0) {
     if (L.img_vec) {
-        constexpr int kV = (kInW + 3) / 4;  // 17
-        for (int i = threadIdx.x; i < kInH * kV; i += blockDim.x) {
-            const int r = i / kV, c4 = i - r * kV;
-            const int x = ix0 + 4 * c4, y = iy0 + r;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (y < L.h && x < L.img_pitch) v = __ldg(reinterpret_cast<const float4*>(img + (long long)y * L.img_pitch + x));
-            T.put(r, 4 * c4, v.x);
-            T.put(r, 4 * c4 + 1, v.y);
-            T.put(r, 4 * c4 + 2, v.z);
-            if (4 * c4 + 3 < kInW) T.put(r, 4 * c4 + 3, v.w);
+        constexpr int kP = (kInW + 1) / 2;  // 34
+        for (int i = threadIdx.x; i < kInH * kP; i += blockDim.x) {
+            const int r = i / kP, j = i - r * kP;
+            const int x = ix0 + 2 * j, y = iy0 + r;
+            float2 v = make_float2(0.f, 0.f);
+            if (y < L.h && x < L.img_pitch) {
+                const float2* src = reinterpret_cast<const float2*>(img + (long long)y * L.img_pitch + x);
+                v = kCoherent ? __ldcg(src) : __ldg(src);
+            }
+            T.put(r, 2 * j, v.x);
+            if (2 * j + 1 < kInW) T.put(r, 2 * j + 1, v.y);
         }
     } else {
         for (int i = threadIdx.x; i < kInH * kInW; i += blockDim.x) {
             const int r = i / kInW, c = i - r * kInW;
             const int x = ix0 + c, y = iy0 + r;
-            T.put(r, c, (x < L.w && y < L.h) ? __ldg(img + (long long)y * L.img_pitch + x) : 0.f);
+            const float* src = img + (long long)y * L.img_pitch + x;
+            T.put(r, c, (x < L.w && y < L.h) ? (kCoherent ? __ldcg(src) : __ldg(src)) : 0.f);
         }
     }
 }
 
-__global__ void __launch_bounds__(256, 3) stage1_front_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ LevelTable LT,
-                                                              const float* __restrict__ limg, float* __restrict__ s1,
-                                                              const uint8_t* __restrict__ front_on) {
-    __shared__ FrontTile T;
-    const int g = LT.first + blockIdx.x;
-    if (front_on && !front_on[g]) return;  // gated off: no back tile reads this one
-    const LevelDesc& L = LT.lv[find_level<&LevelDesc::k1_base>(LT, g)];
-    const int t = g - L.k1_base;
+// Front tile t of level L: its (67 x 35) level-image tile staged in T, then the 4x4 conv + folded
+// BN/LReLU + 2x2 max of the 4 L1 maps for 32 x 16 pooled pixels (two vertically adjacent pixels a
+// thread) and the 4 neighbour-map sums written to the S1 arena. kCoherent: the level image was
+// written earlier in the same launch (read through L2, not the read-only path).
+template <bool kCoherent>
+__device__ __forceinline__ void front_tile(const Stage1W& W, FrontTile& T, const LevelDesc& L, int t, const float* __restrict__ limg,
+                                           float* __restrict__ s1) {
     const int px0 = (t % L.k1_tiles_x) * kK1TileX;
     const int py0 = (t / L.k1_tiles_x) * kK1TileY;
     const int ix0 = 2 * px0, iy0 = 2 * py0;
 
-    load_front_tile(T, limg + L.img_off, L, ix0, iy0);
+    load_front_tile<kCoherent>(T, limg + L.img_off, L, ix0, iy0);
     __syncthreads();
 
     const int qx = threadIdx.x & (kK1TileX - 1);
@@ -125,6 +131,18 @@ __global__ void __launch_bounds__(256, 3) stage1_front_kernel(const __grid_const
     }
 }
 
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) stage1_front_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ LevelTable LT,
+                                                              const float* __restrict__ limg, float* __restrict__ s1,
+                                                              const uint8_t* __restrict__ front_on) {
+    __shared__ FrontTile T;
+    const int g = LT.first + blockIdx.x;
+    if (front_on && !front_on[g]) return;  // gated off: no back tile reads this one
+    const LevelDesc& L = LT.lv[find_level<&LevelDesc::k1_base>(LT, g)];
+    front_tile<false>(W, T, L, g - L.k1_base, limg, s1);
+}
+
 constexpr int kP2TW = kK2TileX + 3;   // 35 pooled L2 columns (halo 3)
 constexpr int kP2TH = kK2TileY + 4;   // 20 pooled L2 rows (halo 4)
 constexpr int kS1TW = 2 * kP2TW + 2;  // 72
@@ -133,26 +151,80 @@ constexpr int kS1TWh = kS1TW / 2;     // 36 columns of each parity
 constexpr int kS2P = kP2TW + 1;       // 36: ts2 row pitch
 
 struct BackSmem {
-    float s1[4][kS1TH][kS1TW];    // column c stored at (c & 1) * kS1TWh + (c >> 1)
+    float s1[2][kS1TH][kS1TW];    // half of the S1 tile (maps 2h, 2h+1); column c at (c & 1) * kS1TWh + (c >> 1)
     float s2[8][kP2TH][kS2P];     // the 8 neighbour sums of the pooled L2 maps
 };
-constexpr int kBackSmemBytes = (int)sizeof(BackSmem);
+constexpr int kBackSmemBytes = (int)sizeof(BackSmem);  // 47,232 B: four blocks fit a SM
+constexpr int kP2Px = kP2TW * kP2TH;                    // 700 pooled L2 pixels of a tile
+constexpr int kP2Passes = (kP2Px + 255) / 256;          // 3
+
+// Pooled L2 pixel k of a tile: the 32 x 20 block first (a warp takes 32 consecutive columns of one
+// row, so its shared-memory reads and writes are conflict-free), then the 3 x 20 right edge.
+__device__ __forceinline__ void p2_pixel(int p, int* x, int* y) {
+    if (p < 32 * kP2TH) {
+        *x = p & 31;
+        *y = p >> 5;
+    } else {
+        const int q = p - 32 * kP2TH;
+        *x = 32 + q % 3;
+        *y = q / 3;
+    }
+}
+
+// S1 half h of a back tile (maps 2h and 2h+1) into S.s1 with 16-byte loads; columns past the plane
+// pitch and rows past p1h read as 0 (no valid response pixel depends on them)
+template <bool kCoherent>
+__device__ __forceinline__ void load_back_half(BackSmem& S, const float* __restrict__ s1, const LevelDesc& L, int sx0, int sy0, int h) {
+    const float* base = s1 + L.s1_off + (long long)(2 * h) * L.s1_plane;
+    constexpr int kV = kS1TW / 4;
+    for (int i = threadIdx.x; i < 2 * kS1TH * kV; i += blockDim.x) {
+        const int row = i / kV, c4 = i - row * kV;
+        const int m = row / kS1TH, rr = row - m * kS1TH;
+        const int x = sx0 + 4 * c4, y = sy0 + rr;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (y < L.p1h && x < L.s1_pitch) {
+            const float4* src = reinterpret_cast<const float4*>(base + m * L.s1_plane + (long long)y * L.s1_pitch + x);
+            v = kCoherent ? __ldcg(src) : __ldg(src);
+        }
+        *reinterpret_cast<float2*>(&S.s1[m][rr][2 * c4]) = make_float2(v.x, v.z);
+        *reinterpret_cast<float2*>(&S.s1[m][rr][kS1TWh + 2 * c4]) = make_float2(v.y, v.w);
+    }
+}
+
+// The pooled L2 maps (2i, 2i+1) at tile pixel (x, y), both from S1 map i (held as S.s1[i - 2h]):
+// 3x3 conv + BN/LReLU at the four positions of the 2x2 window, then their max
+__device__ __forceinline__ f2_t pool_l2_pair(const BackSmem& S, const Stage1W& W, int i, int il, int x, int y, f2_t nz) {
+    f2_t q[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(S.s1[il][2 * y + r][(c & 1) * kS1TWh + x + (c >> 1)]);
+    f2_t cv[4];
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        const int dy = d >> 1, dx = d & 1;
+        f2_t acc = f2_mul(q[dy][dx], f2_ld(W.k2p[i][0]), nz);
+#pragma unroll
+        for (int k = 1; k < 9; ++k) acc = f2_add(acc, f2_mul(q[dy + k / 3][dx + k % 3], f2_ld(W.k2p[i][k]), nz));
+        cv[d] = lrelu_bn2(acc, W.a2p[i], nz);
+    }
+    return f2_max4(cv[0], cv[1], cv[2], cv[3]);
+}
 
 // back: one CTA per 32 x 16 tile of response pixels.
-//   A: the S1 tile (4 x 42 x 72) is staged in shared memory with 16-byte loads;
-//   B: the 8 pooled L2 maps and their sums on the 35 x 20 halo tile (maps 2i and 2i+1 read the
-//      same S1 map i: one packed pair);
+//   A/B in two halves: the S1 maps 0-1 of the tile (2 x 42 x 72) are staged in shared memory with
+//      16-byte loads, the pooled L2 maps 0-3 computed on the 35 x 20 halo tile (maps 2i and 2i+1
+//      read the same S1 map i: one packed pair) and the neighbour sums 0-2 written; the two sums
+//      that also need maps 4-5 stay in registers while S1 maps 2-3 replace 0-1 and the second half
+//      finishes sums 3-7. Half the S1 tile in shared memory is what lets four blocks share a SM.
 //   C: every thread finishes two vertically adjacent response pixels, every operation packed over
 //      the pair: the 16 L3 maps (4w x 5h), the 52 hidden neurons and the output neuron.
-__global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ Stage1Dup D,
-                                                             const __grid_constant__ LevelTable LT, const float* __restrict__ s1,
-                                                             float* __restrict__ resp, int* __restrict__ counts, float thr,
-                                                             const uint8_t* __restrict__ back_on, const GateCells cells) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BackSmem& S = *reinterpret_cast<BackSmem*>(smem_raw);
-    const int g = LT.first + blockIdx.x;
-    const LevelDesc& L = LT.lv[find_level<&LevelDesc::k2_base>(LT, g)];
-    const int t = g - L.k2_base;
+// Back tile t of level L as above; g is its global back-tile index (the gate's tile index).
+// kCoherent: the S1 arena was written earlier in the same launch (read through L2).
+template <bool kCoherent>
+__device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, BackSmem& S, const LevelDesc& L, int t, int g,
+                                          const float* __restrict__ s1, float* __restrict__ resp, int* __restrict__ counts, float thr,
+                                          const uint8_t* __restrict__ back_on, const GateCells& cells) {
     const int ox0 = (t % L.k2_tiles_x) * kK2TileX;
     const int oy0 = (t / L.k2_tiles_x) * kK2TileY;
     if (back_on && !back_on[g]) {  // gated off: responses below any stage-1 threshold
@@ -163,58 +235,48 @@ __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_consta
         return;
     }
     const int sx0 = 2 * ox0, sy0 = 2 * oy0;
+    const f2_t nz = f2_ld(W.negzero);
 
-    // A: rows of 18 float4; columns past the plane pitch and rows past p1h read as 0 (no valid
-    // response pixel depends on them)
-    {
-        const float* base = s1 + L.s1_off;
-        constexpr int kV = kS1TW / 4;
-        for (int i = threadIdx.x; i < 4 * kS1TH * kV; i += blockDim.x) {
-            const int row = i / kV, c4 = i - row * kV;
-            const int m = row / kS1TH, rr = row - m * kS1TH;
-            const int x = sx0 + 4 * c4, y = sy0 + rr;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (y < L.p1h && x < L.s1_pitch)
-                v = __ldg(reinterpret_cast<const float4*>(base + m * L.s1_plane + (long long)y * L.s1_pitch + x));
-            *reinterpret_cast<float2*>(&S.s1[m][rr][2 * c4]) = make_float2(v.x, v.z);
-            *reinterpret_cast<float2*>(&S.s1[m][rr][kS1TWh + 2 * c4]) = make_float2(v.y, v.w);
+    // first half: pooled L2 maps 0-3, sums 0-2; (P2 + P3) and P3 of each pixel carried over
+    float carry23[kP2Passes], carry3[kP2Passes];
+    load_back_half<kCoherent>(S, s1, L, sx0, sy0, 0);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kP2Passes; ++k) {
+        const int p = threadIdx.x + 256 * k;
+        carry23[k] = carry3[k] = 0.f;
+        if (p < kP2Px) {
+            int x, y;
+            p2_pixel(p, &x, &y);
+            const f2_t a = pool_l2_pair(S, W, 0, 0, x, y, nz), b = pool_l2_pair(S, W, 1, 1, x, y, nz);
+            const float P0 = f2_lo(a), P1 = f2_hi(a), P2 = f2_lo(b), P3 = f2_hi(b);
+            const float s01 = fadd(P0, P1);
+            S.s2[0][y][x] = s01;
+            S.s2[1][y][x] = fadd(s01, P2);
+            S.s2[2][y][x] = fadd(fadd(P1, P2), P3);
+            carry23[k] = fadd(P2, P3);
+            carry3[k] = P3;
         }
     }
     __syncthreads();
-
-    const f2_t nz = f2_ld(W.negzero);
-    // B
-    for (int p = threadIdx.x; p < kP2TW * kP2TH; p += blockDim.x) {
-        const int x = p % kP2TW, y = p / kP2TW;
-        f2_t P[4];
+    // second half: pooled L2 maps 4-7, sums 3-7
+    load_back_half<kCoherent>(S, s1, L, sx0, sy0, 1);
+    __syncthreads();
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            f2_t q[4][4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(S.s1[i][2 * y + r][(c & 1) * kS1TWh + x + (c >> 1)]);
-            f2_t cv[4];
-#pragma unroll
-            for (int d = 0; d < 4; ++d) {
-                const int dy = d >> 1, dx = d & 1;
-                f2_t acc = f2_mul(q[dy][dx], f2_ld(W.k2p[i][0]), nz);
-#pragma unroll
-                for (int k = 1; k < 9; ++k) acc = f2_add(acc, f2_mul(q[dy + k / 3][dx + k % 3], f2_ld(W.k2p[i][k]), nz));
-                cv[d] = lrelu_bn2(acc, W.a2p[i], nz);
-            }
-            P[i] = f2_max4(cv[0], cv[1], cv[2], cv[3]);  // (map 2i, map 2i+1)
+    for (int k = 0; k < kP2Passes; ++k) {
+        const int p = threadIdx.x + 256 * k;
+        if (p < kP2Px) {
+            int x, y;
+            p2_pixel(p, &x, &y);
+            const f2_t a = pool_l2_pair(S, W, 2, 0, x, y, nz), b = pool_l2_pair(S, W, 3, 1, x, y, nz);
+            const float P4 = f2_lo(a), P5 = f2_hi(a), P6 = f2_lo(b), P7 = f2_hi(b);
+            S.s2[3][y][x] = fadd(carry23[k], P4);
+            S.s2[4][y][x] = fadd(fadd(carry3[k], P4), P5);
+            S.s2[5][y][x] = fadd(fadd(P4, P5), P6);
+            const float s67 = fadd(P6, P7);
+            S.s2[6][y][x] = fadd(fadd(P5, P6), P7);
+            S.s2[7][y][x] = s67;
         }
-        float Pm[8];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            Pm[2 * i] = f2_lo(P[i]);
-            Pm[2 * i + 1] = f2_hi(P[i]);
-        }
-        S.s2[0][y][x] = fadd(Pm[0], Pm[1]);
-#pragma unroll
-        for (int k = 1; k < 7; ++k) S.s2[k][y][x] = fadd(fadd(Pm[k - 1], Pm[k]), Pm[k + 1]);
-        S.s2[7][y][x] = fadd(Pm[6], Pm[7]);
     }
     __syncthreads();
 
@@ -305,6 +367,19 @@ __global__ void __launch_bounds__(256, 3) stage1_back_kernel(const __grid_consta
     }
 }
 
+template <int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) stage1_back_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ Stage1Dup D,
+                                                             const __grid_constant__ LevelTable LT, const float* __restrict__ s1,
+                                                             float* __restrict__ resp, int* __restrict__ counts, float thr,
+                                                             const uint8_t* __restrict__ back_on, const GateCells cells) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BackSmem& S = *reinterpret_cast<BackSmem*>(smem_raw);
+    const int g = LT.first + blockIdx.x;
+    const LevelDesc& L = LT.lv[find_level<&LevelDesc::k2_base>(LT, g)];
+    const int t = g - L.k2_base;
+    back_tile<false>(W, D, S, L, t, g, s1, resp, counts, thr, back_on, cells);
+}
+
 // Duplicated stage-1 parameters for the back kernel, derived from the packed weight block.
 static Stage1Dup make_dup(const Stage1W& W) {
     Stage1Dup D;
@@ -340,9 +415,7 @@ static Stage1Dup make_dup(const Stage1W& W) {
     return D;
 }
 
-cudaError_t stage1_setup() {
-    return cudaFuncSetAttribute(stage1_back_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBackSmemBytes);
-}
+
 
 // Launches KERNEL once per group of at most kParamLevels levels; tiles(L) is a level's block count
 // and base(L) its first global block.
@@ -363,25 +436,183 @@ static cudaError_t launch_grouped(const LevelDesc* levels, int n_levels, int Lev
 }
 
 cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st,
-                                const uint8_t* front_on) {
+                                const uint8_t* front_on, Stage1Sched sched) {
     return launch_grouped(
         levels, n_levels, &LevelDesc::k1_base, [](const LevelDesc& L) { return L.k1_tiles_x * ((L.p1h + kK1TileY - 1) / kK1TileY); },
-        [&](const LevelTable& T, int blocks) { stage1_front_kernel<<<blocks, 256, 0, st>>>(W, T, limg, s1, front_on); });
+        [&](const LevelTable& T, int blocks) {
+            if (sched.front_blocks_per_sm >= 4)
+                stage1_front_kernel<4><<<blocks, 256, 0, st>>>(W, T, limg, s1, front_on);
+            else
+                stage1_front_kernel<3><<<blocks, 256, 0, st>>>(W, T, limg, s1, front_on);
+        });
 }
 
 cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
-                               int* counts, float thr, const uint8_t* back_on, GateCells cells) {
+                               int* counts, float thr, const uint8_t* back_on, GateCells cells, Stage1Sched sched) {
     const Stage1Dup D = make_dup(W);
     return launch_grouped(
         levels, n_levels, &LevelDesc::k2_base, [](const LevelDesc& L) { return L.k2_tiles_x * ((L.oh + kK2TileY - 1) / kK2TileY); },
-        [&](const LevelTable& T, int blocks) { stage1_back_kernel<<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp, counts, thr, back_on, cells); });
+        [&](const LevelTable& T, int blocks) {
+            if (sched.back_blocks_per_sm >= 4)
+                stage1_back_kernel<4><<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp, counts, thr, back_on, cells);
+            else
+                stage1_back_kernel<3><<<blocks, 256, kBackSmemBytes, st>>>(W, D, T, s1, resp, counts, thr, back_on, cells);
+        });
 }
 
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
-                          cudaStream_t st, int* counts, float thr, const uint8_t* front_on, const uint8_t* back_on, GateCells cells) {
-    cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st, front_on);
+                          cudaStream_t st, int* counts, float thr, const uint8_t* front_on, const uint8_t* back_on, GateCells cells,
+                          Stage1Sched sched) {
+    cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st, front_on, sched);
     if (e != cudaSuccess) return e;
-    return launch_stage1_back(W, levels, n_levels, s1, resp, st, counts, thr, back_on, cells);
+    return launch_stage1_back(W, levels, n_levels, s1, resp, st, counts, thr, back_on, cells, sched);
+}
+
+// ---------------- batched form: one persistent launch over B frames ----------------
+//
+// Every pyramid block, front tile and back tile of every frame of a batch is one item of a device
+// work queue (an atomic counter); a persistent grid pops items in queue order until none are left.
+// Items of stage s of frame f wait until every item of stage s-1 of frame f has finished (a counter
+// per (frame, stage), polled with acquire loads by one thread and a bounded number of polls); the
+// diagonal queue order puts about one frame's worth of other items between a producer stage and its
+// consumer, so the polls almost never wait. Items are popped in queue order and only wait on
+// earlier items, so every wait ends whatever the number of resident blocks. Data written earlier in
+// the launch (level images, S1 planes) is read through L2 (ld.global.cg), never the read-only path.
+
+void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, int pyr_items, int front_items, int back_items, int gpitch,
+                       int gw, int gh, float thr) {
+    q->n_frames = n_frames;
+    q->n_levels = n_levels;
+    q->n_chunks = n_chunks;
+    q->gpitch = gpitch;
+    q->gw = gw;
+    q->gh = gh;
+    q->thr = thr;
+    q->stage_items[0] = pyr_items;
+    q->stage_items[1] = front_items;
+    q->stage_items[2] = back_items;
+    q->wait_limit = 1 << 22;  // x 256 ns of sleep: about a second before the launch gives up
+    int n = 0, first = 0;
+    for (int t = 0; t < n_frames + kBatchStages - 1; ++t)
+        for (int st = 0; st < kBatchStages; ++st) {
+            const int f = t - st;
+            if (f < 0 || f >= n_frames || q->stage_items[st] <= 0) continue;
+            q->seg_stage[n] = st;
+            q->seg_frame[n] = f;
+            q->seg_first[n] = first;
+            first += q->stage_items[st];
+            ++n;
+        }
+    q->seg_first[n] = first;
+    q->n_seg = n;
+    q->total = first;
+}
+
+// the level of item `g` of a stage: the last level whose first item (FIELD) is <= g
+template <int LevelDesc::*FIELD>
+__device__ __forceinline__ int find_level_global(const LevelDesc* __restrict__ lv, int n, int g) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (lv[mid].*FIELD <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+constexpr int kBatchSmem = (int)sizeof(BackSmem) > (int)sizeof(FrontTile) ? (int)sizeof(BackSmem) : (int)sizeof(FrontTile);
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) stage1_batch_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ Stage1Dup D,
+                                                              const __grid_constant__ BatchFrames F, const __grid_constant__ BatchQueue Q,
+                                                              const LevelDesc* __restrict__ levels, int* __restrict__ sync,
+                                                              int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_item;
+    __shared__ unsigned long long s_ready;  // bit 3f+s: stage s of frame f is known complete
+    if (threadIdx.x == 0) s_ready = 0ull;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&sync[0], 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= Q.total) break;
+        int sg = 0;
+        while (sg + 1 < Q.n_seg && Q.seg_first[sg + 1] <= item) ++sg;
+        const int stage = Q.seg_stage[sg], f = Q.seg_frame[sg], g = item - Q.seg_first[sg];
+        if (stage > 0) {
+            const int dep = kBatchStages * f + stage - 1;
+            if (!(s_ready & (1ull << dep))) {  // uniform: every thread reads the same word
+                if (threadIdx.x == 0) {
+                    const int need = Q.stage_items[stage - 1];
+                    int polls = 0;
+                    while (ld_acquire(&sync[1 + dep]) < need) {
+                        if (++polls > Q.wait_limit || ld_acquire(err) != 0) {
+                            atomicExch(err, 1);
+                            break;
+                        }
+                        __nanosleep(256);
+                    }
+                    __threadfence();
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) s_ready |= 1ull << dep;
+            }
+        }
+        if (stage == 0) {
+            if (g == 0)  // the back tiles of this frame count candidates into a zeroed table
+                for (int i = threadIdx.x; i < Q.n_chunks; i += blockDim.x) F.counts[f][i] = 0;
+            const LevelDesc& L = levels[find_level_global<&LevelDesc::pyr_base>(levels, Q.n_levels, g)];
+            pyramid_block(L, g - L.pyr_base, F.gray[f], Q.gpitch, Q.gw, Q.gh, F.limg[f], F.front_on[f]);
+        } else if (stage == 1) {
+            if (!F.front_on[f] || F.front_on[f][g]) {
+                const LevelDesc& L = levels[find_level_global<&LevelDesc::k1_base>(levels, Q.n_levels, g)];
+                front_tile<true>(W, *reinterpret_cast<FrontTile*>(smem_raw), L, g - L.k1_base, F.limg[f], F.s1[f]);
+            }
+        } else {
+            const LevelDesc& L = levels[find_level_global<&LevelDesc::k2_base>(levels, Q.n_levels, g)];
+            back_tile<true>(W, D, *reinterpret_cast<BackSmem*>(smem_raw), L, g - L.k2_base, g, F.s1[f], F.resp[f], F.counts[f], Q.thr,
+                            F.back_on[f], F.cells[f]);
+        }
+        __syncthreads();  // every thread is done with the item (and with the shared memory)
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&sync[1 + kBatchStages * f + stage], 1);
+        }
+    }
+}
+
+int stage1_batch_blocks_per_sm(int blocks_per_sm) {
+    int n = 0;
+    if (blocks_per_sm >= 4)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1_batch_kernel<4>, 256, kBatchSmem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1_batch_kernel<3>, 256, kBatchSmem);
+    return n > 0 ? n : 1;
+}
+
+cudaError_t launch_stage1_batch(const Stage1W& W, const BatchFrames& F, const BatchQueue& Q, const LevelDesc* d_levels, int* sync, int* err,
+                                int grid, cudaStream_t st, int blocks_per_sm) {
+    if (Q.total <= 0) return cudaSuccess;
+    const Stage1Dup D = make_dup(W);
+    grid = grid < Q.total ? grid : Q.total;
+    if (blocks_per_sm >= 4)
+        stage1_batch_kernel<4><<<grid, 256, kBatchSmem, st>>>(W, D, F, Q, d_levels, sync, err);
+    else
+        stage1_batch_kernel<3><<<grid, 256, kBatchSmem, st>>>(W, D, F, Q, d_levels, sync, err);
+    return cudaGetLastError();
+}
+
+cudaError_t stage1_setup() {
+    cudaError_t e = cudaFuncSetAttribute(stage1_back_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBackSmemBytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage1_back_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBackSmemBytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage1_batch_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBatchSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage1_batch_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBatchSmem);
+    return e;
 }
 
 }  // namespace ccnn

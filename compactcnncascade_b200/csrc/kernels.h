@@ -81,6 +81,47 @@ constexpr int kPyrCols = 256, kPyrRows = 8;
 cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* gray, int gpitch, int gw, int gh, float* limg,
                            cudaStream_t st,
                            const uint8_t* front_on = nullptr);
+// ---- batched form: one persistent launch runs the pyramid and stage 1 of B frames ----
+constexpr int kMaxBatch = 16;
+// per-frame buffers of the frames of one batch (frame f = entry f)
+struct BatchFrames {
+    const float* gray[kMaxBatch];
+    float* limg[kMaxBatch];
+    float* s1[kMaxBatch];
+    float* resp[kMaxBatch];
+    int* counts[kMaxBatch];
+    const uint8_t* front_on[kMaxBatch];  // the learned gate's tile activity, or null
+    const uint8_t* back_on[kMaxBatch];
+    GateCells cells[kMaxBatch];
+};
+// the work queue of a batch: segments of items, one per (stage, frame), in queue order; a stage's
+// items are its blocks in the per-frame kernels (pyramid blocks, front tiles, back tiles)
+constexpr int kBatchStages = 3;
+struct BatchQueue {
+    int n_frames, n_levels, n_chunks;
+    int gpitch, gw, gh;
+    float thr;
+    int stage_items[kBatchStages];  // items of one frame per stage
+    int n_seg, total;
+    int seg_stage[kBatchStages * kMaxBatch], seg_frame[kBatchStages * kMaxBatch], seg_first[kBatchStages * kMaxBatch + 1];
+    int wait_limit;                 // polls of a dependency before the launch reports an error
+};
+// builds the queue order: a diagonal wavefront over (stage, frame), so that stage s of frame f is
+// queued after stage s of frame f-1 and stage s-1 of frame f+1 (its producer is long done)
+void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, int pyr_items, int front_items, int back_items, int gpitch,
+                       int gw, int gh, float thr);
+// sync: 1 + kBatchStages * n_frames ints, zero before the launch (queue head, finished items per
+// (frame, stage)); err: set to 1 when a dependency wait gave up (results of the batch invalid)
+cudaError_t launch_stage1_batch(const Stage1W& W, const BatchFrames& F, const BatchQueue& Q, const LevelDesc* d_levels, int* sync, int* err,
+                                int grid, cudaStream_t st, int blocks_per_sm);
+// resident blocks of the persistent stage-1 kernel per SM (its grid is this times the SM count)
+int stage1_batch_blocks_per_sm(int blocks_per_sm);
+
+// register budget of the stage-1 kernels: resident 256-thread blocks per SM (3 or 4), a schedule knob
+struct Stage1Sched {
+    int front_blocks_per_sm = 3;
+    int back_blocks_per_sm = 4;
+};
 // stage-1 net over all levels; `levels` is a HOST array (the descriptors travel as kernel
 // parameters), level images at limg + img_off
 // counts (optional, zeroed by the caller): per candidate-scan chunk, responses > thr
@@ -88,15 +129,16 @@ cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* g
 // cell within one cell of it (in its level's octave) is written below every threshold
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
                           cudaStream_t st, int* counts = nullptr, float thr = 0.f, const uint8_t* front_on = nullptr,
-                          const uint8_t* back_on = nullptr, GateCells cells = GateCells{});
+                          const uint8_t* back_on = nullptr, GateCells cells = GateCells{}, Stage1Sched sched = Stage1Sched{});
 // front_on / back_on (optional): per-tile activity from the gate; inactive back tiles write
 // responses below every threshold
 cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st,
-                                const uint8_t* front_on = nullptr);
+                                const uint8_t* front_on = nullptr, Stage1Sched sched = Stage1Sched{});
 // dynamic shared memory of the stage-1 back kernel (set once per device before any launch)
 cudaError_t stage1_setup();
 cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
-                               int* counts = nullptr, float thr = 0.f, const uint8_t* back_on = nullptr, GateCells cells = GateCells{});
+                               int* counts = nullptr, float thr = 0.f, const uint8_t* back_on = nullptr, GateCells cells = GateCells{},
+                               Stage1Sched sched = Stage1Sched{});
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
                               const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st);
 // lg (optional): the legacy networks (device memory, [1] stage 2, [2] stage 3) replace N

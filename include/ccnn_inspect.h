@@ -119,6 +119,18 @@ CCNN_API ccnn_status ccnn_synth_frame_device(void* d_out, int width, int height,
 CCNN_API ccnn_status ccnn_set_schedule(ccnn_handle h, int frame_slots, int window_ctas_per_sm);
 CCNN_API ccnn_status ccnn_get_schedule(ccnn_handle h, int* frame_slots, int* window_ctas_per_sm);
 
+/* The full schedule: the two knobs above plus the register budget of the two stage-1 kernels
+ * (resident 256-thread blocks per SM, 3 or 4: more blocks hide more latency, fewer registers
+ * may spill). 0 keeps a value. Same rules as ccnn_set_schedule. */
+typedef struct {
+    int frame_slots;
+    int window_ctas_per_sm;
+    int front_blocks_per_sm;
+    int back_blocks_per_sm;
+} ccnn_schedule;
+CCNN_API ccnn_status ccnn_set_schedule_ex(ccnn_handle h, const ccnn_schedule* s);
+CCNN_API ccnn_status ccnn_get_schedule_ex(ccnn_handle h, ccnn_schedule* s);
+
 /* Legacy cascade networks (model format 1.0, the cnn4face{1,2,3}_new.bin family: tanh activations,
  * max or average pooling; reader SIMD::ConvNeuralNetwork::Init, src/CNNObjectDetector/cnn_simd.cpp:40-336,
  * forward pass Run_single_thread, cnn_simd.cpp:551-874, in the reference's plain-C++ build).

@@ -87,7 +87,8 @@ int main(int argc, char** argv) {
         g = detector.getParam();
         printf("param2 %d %.4f\n", g.min_face_height, g.scale_factor);
         print_faces("detect_param2", detector, img);
-        printf("clear %d %d\n", detector.Clear(), detector.isEmpty() ? 1 : 0);
+        const int crc = detector.Clear();
+        printf("clear %d %d\n", crc, detector.isEmpty() ? 1 : 0);
         FaceDetector::Face f[4];
         printf("detect_cleared %d\n", detector.Detect(f, img));
     }

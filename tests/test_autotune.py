@@ -12,8 +12,8 @@ def test_key_and_lookup(tmp_path):
     assert k == "1920x1080/sf1.15/min40/max240"
     path = tmp_path / "t.json"
     assert autotune.lookup(p, str(path)) is None  # no table
-    path.write_text(json.dumps({k: {"frame_slots": 12, "window_ctas_per_sm": 3}}))
-    assert autotune.lookup(p, str(path)) == (12, 3)
+    path.write_text(json.dumps({k: {"frame_slots": 12, "window_ctas_per_sm": 3, "back_blocks_per_sm": 4, "frames_per_s": 1.0}}))
+    assert autotune.lookup(p, str(path)) == {"frame_slots": 12, "window_ctas_per_sm": 3, "back_blocks_per_sm": 4}
     p.scale_factor = 1.05
     assert autotune.lookup(p, str(path)) is None
     path.write_text("not json")

@@ -1,4 +1,4 @@
-"""Schedules (ccnn_set_schedule) change throughput only: every schedule gives the same faces."""
+"""Schedules (ccnn_set_schedule_ex) change throughput only: every schedule gives the same faces."""
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -17,17 +17,19 @@ def test_results_do_not_depend_on_the_schedule():
     imgs = [ccnn.synth_frame(1280, 720, 60 + i, 10, 30, 300)[0] for i in range(5)]
     d = ccnn.FaceDetector()
     assert d.Init(p) == 0
-    assert autotune.get_schedule(d) == (8, 4)
+    assert autotune.get_schedule(d) == autotune.DEFAULTS
     want = d.DetectBatch(imgs)
     assert sum(len(f) for f in want) > 0
-    for sched in [(1, 1), (3, 2), (16, 3), (5, 4)]:
-        autotune.set_schedule(d, *sched)
-        assert autotune.get_schedule(d) == sched
+    names = [k for k, _ in autotune.KNOBS]
+    for sched in [(1, 1, 3, 3), (3, 2, 4, 4), (16, 3, 3, 4), (5, 4, 4, 3)]:
+        sd = dict(zip(names, sched))
+        autotune.set_schedule(d, sd)
+        assert autotune.get_schedule(d) == sd
         assert d.DetectBatch(imgs) == want
         assert [d.Detect(im) for im in imgs] == want
-    with pytest.raises(ccnn.CCNNError):
-        autotune.set_schedule(d, 65, 4)
-    with pytest.raises(ccnn.CCNNError):
-        autotune.set_schedule(d, 8, 5)
+    for bad in [{"frame_slots": 65}, {"window_ctas_per_sm": 5}, {"front_blocks_per_sm": 2}, {"back_blocks_per_sm": 5}]:
+        with pytest.raises(ccnn.CCNNError):
+            autotune.set_schedule(d, bad)
     d2 = ccnn.FaceDetector()
-    assert d2.Init(p, schedule=(2, 2)) == 0 and autotune.get_schedule(d2) == (2, 2)
+    assert d2.Init(p, schedule={"frame_slots": 2, "window_ctas_per_sm": 2}) == 0
+    assert autotune.get_schedule(d2) == dict(autotune.DEFAULTS, frame_slots=2, window_ctas_per_sm=2)
