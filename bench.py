@@ -131,13 +131,30 @@ def run_serving(frames_by_res, rate, n_frames, seed=1, gate=None):
 BATCHED = [((3840, 2160), 60, 20, 600), ((4800, 2400), 60, 20, 600)]
 
 
+def launches_per_frames(n_frames, n_levels, batch_frames, gated=False):
+    """Kernels the library launches for n_frames frames of one size: per frame gray, pyramid, stage-1
+    front and back (pyramid and stage 1 once per group of 32 levels), candidates, windows, replay
+    (+2 for the gate); in the batched form per group of batch_frames frames gray, one persistent
+    pyramid + stage-1 launch, candidates, windows, replay (+2 per frame for the gate), with leftover
+    frames per frame."""
+    groups = -(-n_levels // 32)
+    per_frame = 4 + 3 * groups + (2 if gated else 0)
+    if batch_frames and batch_frames >= 2:
+        full = n_frames // batch_frames
+        return full * (5 + (2 * batch_frames if gated else 0)) + (n_frames - full * batch_frames) * per_frame
+    return n_frames * per_frame
+
+
 def run_batched_pyramid(dev, args):
     """Scale 1.05, min face 20, no max face (the largest level is an upsampled 1.35x copy): 80+
-    pyramid levels of uneven sizes per frame, run as 8-frame pipelined batches of device-resident
-    frames (rendered on the device by the seeded generator). Device time from the library's events."""
+    pyramid levels of uneven sizes per frame, device-resident frames (rendered on the device by the
+    seeded generator) in 8-frame batches, device time from the library's events. Two forms: every
+    frame its own captured graph (8 frames in flight), and the batched form (groups of 8 frames one
+    graph each, the pyramid and stage 1 of all levels of all 8 frames in one persistent launch fed by
+    a device work queue, two groups in flight)."""
     import torch
     import compactcnncascade_b200 as ccnn
-    from compactcnncascade_b200 import _capi
+    from compactcnncascade_b200 import _capi, autotune
     L = _capi.lib()
     out = {}
     B = args.batched_frames
@@ -166,22 +183,41 @@ def run_batched_pyramid(dev, args):
                 raise SystemExit(f"ccnn_detect_device_batch failed: {_capi.last_error()}")
             return gms.value
 
-        for _ in range(max(3, args.warmup)):
-            step()
-        steps = max(3, args.steps // 4)
-        ms = sum(step() for _ in range(steps))
+        res = {}
+        n_levels = len(det.levels()) if det.levels() else 0
+        for form, sched in (("per_frame", {"frame_slots": B, "batch_frames": 0}),
+                            ("batched", {"frame_slots": 2 * B, "batch_frames": B})):
+            autotune.set_schedule(det, sched)
+            for _ in range(max(3, args.warmup)):
+                step()
+            ref_faces = [list(faces[j * cap: j * cap + nfaces[j]]) for j in range(B)]
+            steps = max(3, args.steps // 4)
+            ms = sum(step() for _ in range(steps))
+            if form == "batched":  # the batched form's faces equal the per-frame form's
+                res["faces_equal_per_frame"] = all(
+                    [(f.x, f.y, f.width, f.height, f.score) for f in faces[j * cap: j * cap + nfaces[j]]] ==
+                    [(f.x, f.y, f.width, f.height, f.score) for f in res["_pf_faces"][j]] for j in range(B))
+            else:
+                res["_pf_faces"] = ref_faces
+            n_levels = len(det.levels())
+            res[form] = {"frames_per_s": round(steps * B / (ms / 1e3), 1), "steps": steps,
+                         "launches_per_8_frames": launches_per_frames(8, n_levels, sched["batch_frames"])}
+        res.pop("_pf_faces", None)
+        autotune.set_schedule(det, {"frame_slots": B, "batch_frames": 0})
         lat = []
         for i in range(10):
             t0 = time.perf_counter()
             det.DetectDevice(frames[i % B].data_ptr(), w, h, 3, w * 3)
             lat.append((time.perf_counter() - t0) * 1e3)
-        out[f"{w}x{h}"] = {"frames_per_s": round(steps * B / (ms / 1e3), 1), "levels": len(det.levels()),
-                           "faces_per_frame": round(sum(nfaces[j] for j in range(B)) / B, 1),
-                           "p50_ms": round(float(np.percentile(lat[2:], 50)), 3), "batch": B, "steps": steps}
+        res.update({"frames_per_s": max(res["per_frame"]["frames_per_s"], res["batched"]["frames_per_s"]), "levels": n_levels,
+                    "faces_per_frame": round(sum(nfaces[j] for j in range(B)) / B, 1),
+                    "p50_ms": round(float(np.percentile(lat[2:], 50)), 3), "batch": B})
+        out[f"{w}x{h}"] = res
         det.Clear()
-    out["note"] = ("seeded frames with 60 face patches 20-600 px, scale 1.05, min face 20, no max face; all levels of a "
-                   "frame in one launch per kernel (level tables of at most 32 levels per launch), every frame's chain "
-                   "a CUDA graph, 8 frames in flight; device-resident frames, device time from CUDA events")
+    out["note"] = ("seeded frames with 60 face patches 20-600 px, scale 1.05, min face 20, no max face; device-resident frames, "
+                   "device time from CUDA events. per_frame: every frame's chain one CUDA graph (pyramid and stage 1 in level "
+                   "tables of at most 32 levels a launch), 8 frames in flight. batched: 8 frames one graph, the pyramid and stage 1 "
+                   "of all levels of all 8 frames in one persistent launch fed by a device work queue, two 8-frame groups in flight")
     return out
 
 
@@ -654,7 +690,7 @@ def main():
                 "bound_note": "host frames cross PCIe: h2d_gbs is the upload rate this throughput implies",
                 "h2d_bytes_per_step": B * W * H * 3,
                 "d2h_bytes_per_step": B * (4 + 1024 * 20)},
-        "gpu_launches": len(KERNELS) * args.steps * B,
+        "gpu_launches": args.steps * launches_per_frames(B, len(levels), schedule.get("batch_frames", 0)),
         "roofline": roofline,
         "wall_value": round(frames_timed / wall_dev, 2),
     }

@@ -115,7 +115,7 @@ class CnnAdvancedParam(ctypes.Structure):
 class Schedule(ctypes.Structure):
     """ccnn_schedule (include/ccnn_inspect.h)."""
     _fields_ = [("frame_slots", ctypes.c_int), ("window_ctas_per_sm", ctypes.c_int), ("front_blocks_per_sm", ctypes.c_int),
-                ("back_blocks_per_sm", ctypes.c_int)]
+                ("back_blocks_per_sm", ctypes.c_int), ("batch_frames", ctypes.c_int), ("batch_blocks_per_sm", ctypes.c_int)]
 
 
 class SynthFace(ctypes.Structure):

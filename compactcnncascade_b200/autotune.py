@@ -8,6 +8,9 @@ The knobs (include/ccnn_inspect.h, ccnn_schedule):
   window_ctas_per_sm   resident blocks per SM of the persistent stage-2/3 window kernel
   front_blocks_per_sm  register budget of the stage-1 front kernel (3: 80 registers, 4: 64)
   back_blocks_per_sm   register budget of the stage-1 back kernel (3: 80 registers, 4: 64)
+  batch_frames         frames per batched graph (0: every frame its own graph); the batched form
+                       runs the pyramid and stage 1 of a whole group in one persistent launch
+  batch_blocks_per_sm  register budget of that persistent kernel (3 or 4)
 
 The search is coordinate descent from the defaults: each knob in turn takes the value that times
 fastest with the others held, for two passes (a full product of the knobs would be 96 timings).
@@ -24,8 +27,9 @@ from . import _capi
 
 TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "schedules.json")
 KNOBS = (("frame_slots", (4, 8, 12, 16)), ("window_ctas_per_sm", (2, 3, 4)), ("front_blocks_per_sm", (3, 4)),
-         ("back_blocks_per_sm", (3, 4)))
-DEFAULTS = {"frame_slots": 8, "window_ctas_per_sm": 4, "front_blocks_per_sm": 3, "back_blocks_per_sm": 4}
+         ("back_blocks_per_sm", (3, 4)), ("batch_frames", (0, 2, 4, 8)), ("batch_blocks_per_sm", (3, 4)))
+DEFAULTS = {"frame_slots": 8, "window_ctas_per_sm": 4, "front_blocks_per_sm": 3, "back_blocks_per_sm": 4, "batch_frames": 0,
+            "batch_blocks_per_sm": 3}
 
 
 def key(width, height, scale_factor, min_face, max_face):
@@ -50,7 +54,7 @@ def lookup(p, path=TABLE):
 
 def set_schedule(det, schedule):
     """Applies a schedule (dict of knobs; missing knobs keep their value) to a FaceDetector."""
-    s = _capi.Schedule(*[int(schedule.get(k, 0)) for k, _ in KNOBS])
+    s = _capi.Schedule(*[int(schedule.get(k, -1 if k == "batch_frames" else 0)) for k, _ in KNOBS])
     _capi.check(_capi.lib().ccnn_set_schedule_ex(det._h, ctypes.byref(s)), "ccnn_set_schedule_ex")
 
 
@@ -116,6 +120,8 @@ def tune(width, height, scale_factor=1.15, min_face=40, max_face=240, n_faces=20
                 if v == best[k]:
                     continue
                 trial = dict(best, **{k: v})
+                if trial["batch_frames"] > trial["frame_slots"]:
+                    continue
                 fps = timed(trial)
                 if fps > best_fps:
                     best, best_fps = trial, fps

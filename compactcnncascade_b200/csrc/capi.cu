@@ -232,12 +232,14 @@ CCNN_API ccnn_status ccnn_get_schedule(ccnn_handle h, int* frame_slots, int* win
 
 CCNN_API ccnn_status ccnn_set_schedule_ex(ccnn_handle h, const ccnn_schedule* s) {
     if (!h || !s) return CCNN_ERR_INVALID_ARG;
-    return h->det.set_schedule(s->frame_slots, s->window_ctas_per_sm, s->front_blocks_per_sm, s->back_blocks_per_sm);
+    return h->det.set_schedule(s->frame_slots, s->window_ctas_per_sm, s->front_blocks_per_sm, s->back_blocks_per_sm, s->batch_frames,
+                               s->batch_blocks_per_sm);
 }
 
 CCNN_API ccnn_status ccnn_get_schedule_ex(ccnn_handle h, ccnn_schedule* s) {
     if (!h || !s) return CCNN_ERR_INVALID_ARG;
-    h->det.get_schedule(&s->frame_slots, &s->window_ctas_per_sm, &s->front_blocks_per_sm, &s->back_blocks_per_sm);
+    h->det.get_schedule(&s->frame_slots, &s->window_ctas_per_sm, &s->front_blocks_per_sm, &s->back_blocks_per_sm, &s->batch_frames,
+                        &s->batch_blocks_per_sm);
     return CCNN_OK;
 }
 

@@ -135,6 +135,7 @@ void Detector::free_slot(Slot& s) {
 void Detector::clear() {
     if (!inited_) return;
     cudaSetDevice(device_);
+    free_batches();
     for (auto& s : slots_) {
         if (s.st) cudaStreamSynchronize(s.st);
         free_slot(s);
@@ -360,6 +361,7 @@ ccnn_status Detector::init() {
     CCNN_CUDA(stage1_setup());
     CCNN_CUDA(facial_setup());
 
+    sm_count_ = prop.multiProcessorCount;
     inited_ = true;
     ++init_gen_;
     for (auto& s : slots_) {
@@ -368,6 +370,11 @@ ccnn_status Detector::init() {
             clear();
             return st;
         }
+    }
+    ccnn_status bs = alloc_batches();
+    if (bs != CCNN_OK) {
+        clear();
+        return bs;
     }
     return CCNN_OK;
 }
@@ -594,11 +601,15 @@ ccnn_status Detector::gate_set(const float* params, int n, float threshold, floa
     return CCNN_OK;
 }
 
-ccnn_status Detector::set_schedule(int frame_slots, int window_ctas_per_sm, int front_bpsm, int back_bpsm) {
+ccnn_status Detector::set_schedule(int frame_slots, int window_ctas_per_sm, int front_bpsm, int back_bpsm, int batch_frames, int batch_bpsm) {
     std::lock_guard<std::mutex> lk(mu_);
+    const int slots = frame_slots > 0 ? frame_slots : (int)slots_.size();
+    const int batch = batch_frames >= 0 ? batch_frames : batch_frames_;
     if (frame_slots < 0 || frame_slots > 64 || window_ctas_per_sm < 0 || window_ctas_per_sm > 4 || (front_bpsm != 0 && (front_bpsm < 3 || front_bpsm > 4)) ||
-        (back_bpsm != 0 && (back_bpsm < 3 || back_bpsm > 4))) {
-        set_error("schedule: 1-64 frame slots, 1-4 stage-2/3 blocks per SM, 3-4 stage-1 blocks per SM (0 keeps the current value)");
+        (back_bpsm != 0 && (back_bpsm < 3 || back_bpsm > 4)) || (batch_bpsm != 0 && (batch_bpsm < 3 || batch_bpsm > 4)) || batch > kMaxBatch ||
+        batch == 1 || (batch > 1 && slots < batch)) {
+        set_error("schedule: 1-64 frame slots, 1-4 stage-2/3 blocks per SM, 3-4 stage-1 blocks per SM, batches of 0 or 2-16 frames and "
+                  "at least as many frame slots as frames per batch (0 keeps the current value)");
         return CCNN_ERR_INVALID_ARG;
     }
     clear();
@@ -606,14 +617,18 @@ ccnn_status Detector::set_schedule(int frame_slots, int window_ctas_per_sm, int 
     if (window_ctas_per_sm > 0) window_ctas_per_sm_ = window_ctas_per_sm;
     if (front_bpsm > 0) s1_sched_.front_blocks_per_sm = front_bpsm;
     if (back_bpsm > 0) s1_sched_.back_blocks_per_sm = back_bpsm;
+    if (batch_frames >= 0) batch_frames_ = batch_frames;
+    if (batch_bpsm > 0) batch_bpsm_ = batch_bpsm;
     return init();
 }
 
-void Detector::get_schedule(int* frame_slots, int* window_ctas_per_sm, int* front_bpsm, int* back_bpsm) const {
+void Detector::get_schedule(int* frame_slots, int* window_ctas_per_sm, int* front_bpsm, int* back_bpsm, int* batch_frames, int* batch_bpsm) const {
     *frame_slots = (int)slots_.size();
     *window_ctas_per_sm = window_ctas_per_sm_;
     if (front_bpsm) *front_bpsm = s1_sched_.front_blocks_per_sm;
     if (back_bpsm) *back_bpsm = s1_sched_.back_blocks_per_sm;
+    if (batch_frames) *batch_frames = batch_frames_;
+    if (batch_bpsm) *batch_bpsm = batch_bpsm_;
 }
 
 ccnn_status Detector::gate_disable() {
@@ -1018,7 +1033,65 @@ ccnn_status Detector::detect_batch(const ccnn_image* imgs, int n_img, bool devic
         CCNN_CUDA(cudaEventRecord(t0, slots_[0].st));
         for (int k = 1; k < n_sl; ++k) CCNN_CUDA(cudaStreamWaitEvent(slots_[k].st, t0, 0));
     }
-    for (int i = 0; i < n_img; ++i) {
+    // batched form: groups of batch_frames_ frames of one plan, each group one graph, the batch
+    // contexts in turn (the next group is uploaded while the previous one runs); what is left over
+    // (fewer frames than a group, or frames the batched form does not cover) runs frame by frame
+    int first_single = 0;
+    const int B = batch_frames_;
+    if (B >= 2 && n_img >= B && inited_ && !batches_.empty()) {
+        bool same = true;
+        for (int i = 1; i < n_img && same; ++i)
+            same = imgs[i].cols == imgs[0].cols && imgs[i].rows == imgs[0].rows && imgs[i].channels == imgs[0].channels;
+        const Plan* p0 = nullptr;
+        bool empty = false;
+        if (same) {
+            // admission of the first frame settles the detector's state (re-initialisation, level count)
+            ccnn_status st = prepare_frame(imgs[0], &p0, &empty);
+            if (st != CCNN_OK) return st;
+        }
+        if (same && !empty && inited_ && !batches_.empty() && batch_usable(*p0)) {
+            const int n_full = n_img / B;
+            const int n_ctx = (int)batches_.size();
+            for (int g = 0; g < n_full; ++g) {
+                BatchCtx& c = batches_[g % n_ctx];
+                if (c.pending_first >= 0) {
+                    ccnn_status st = collect_batch(c, B, faces, cap_per, n_faces, &worst);
+                    if (st != CCNN_OK) return st;
+                }
+                for (int f = 0; f < B; ++f) {
+                    const Plan* pf = nullptr;
+                    ccnn_status st = prepare_frame(imgs[g * B + f], &pf, &empty);
+                    if (st != CCNN_OK) return st;
+                    if (pf != p0 || empty) {
+                        set_error("internal: frames of one size gave different pyramid plans");
+                        return CCNN_ERR_CUDA;
+                    }
+                }
+                if (device_input) {
+                    cudaStream_t cst = slots_[c.first_slot].st;
+                    if (ordered_gen != init_gen_) {
+                        CCNN_CUDA(cudaEventRecord(order_ev_, cudaStreamLegacy));
+                        std::fill(waited.begin(), waited.end(), 0);
+                        ordered_gen = init_gen_;
+                    }
+                    if (!waited[c.first_slot]) {
+                        CCNN_CUDA(cudaStreamWaitEvent(cst, order_ev_, 0));
+                        waited[c.first_slot] = 1;
+                    }
+                }
+                ccnn_status st = launch_batch(c, *p0, imgs + (size_t)g * B, B, device_input);
+                if (st != CCNN_OK) return st;
+                c.pending_first = g * B;
+            }
+            for (auto& c : batches_)
+                if (c.pending_first >= 0) {
+                    ccnn_status st = collect_batch(c, B, faces, cap_per, n_faces, &worst);
+                    if (st != CCNN_OK) return st;
+                }
+            first_single = n_full * B;
+        }
+    }
+    for (int i = first_single; i < n_img; ++i) {
         const int k = i % n_sl;
         Slot& s = slots_[k];
         if (pending[k] >= 0) {
@@ -1374,6 +1447,206 @@ ccnn_status Detector::inspect_raw(ccnn_detection* out, int cap, int* n) {
         out[i].knn = d[i].knn;
         out[i].num_detect = d[i].num_detect;
     }
+    return CCNN_OK;
+}
+
+// ---------------- batched form: groups of B frames in one graph ----------------
+
+ccnn_status Detector::alloc_batches() {
+    batches_.clear();
+    const int B = batch_frames_;
+    if (B < 2 || (int)slots_.size() < B) return CCNN_OK;
+    const int n_ctx = (int)slots_.size() / B;
+    batches_.assign(n_ctx, BatchCtx());
+    const long long face_cap = std::max<long long>(cand_cap_, kHostFaces);
+    for (int k = 0; k < n_ctx; ++k) {
+        BatchCtx& c = batches_[k];
+        c.first_slot = k * B;
+        CCNN_CUDA(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+        CCNN_CUDA(cudaMalloc(&c.d_sync, sizeof(int) * (2 + kBatchStages * B)));
+        CCNN_CUDA(cudaMalloc(&c.d_rargs, sizeof(ReplayArgs) * B));
+        CCNN_CUDA(cudaMalloc(&c.d_src, sizeof(FrameSrc) * B));
+        CCNN_CUDA(cudaMallocHost(&c.h_src, sizeof(FrameSrc) * B));
+        CCNN_CUDA(cudaMalloc(&c.d_faces, sizeof(FaceOut) * face_cap * B));
+        CCNN_CUDA(cudaMalloc(&c.d_nf, sizeof(int) * B));
+        CCNN_CUDA(cudaMallocHost(&c.h_faces, sizeof(FaceOut) * kGraphFaces * B));
+        CCNN_CUDA(cudaMallocHost(&c.h_nf, sizeof(int) * (B + 1)));
+    }
+    return CCNN_OK;
+}
+
+void Detector::free_batches() {
+    for (auto& c : batches_) {
+        if (c.done) cudaEventSynchronize(c.done);
+        if (c.exec) cudaGraphExecDestroy(c.exec);
+        cudaFree(c.d_sync);
+        cudaFree(c.d_rargs);
+        cudaFree(c.d_src);
+        cudaFreeHost(c.h_src);
+        cudaFree(c.d_faces);
+        cudaFree(c.d_nf);
+        cudaFreeHost(c.h_faces);
+        cudaFreeHost(c.h_nf);
+        if (c.done) cudaEventDestroy(c.done);
+    }
+    batches_.clear();
+}
+
+// The batched form covers the CNTK cascade on frames at their own resolution (no input downscale),
+// without facial analysis; other configurations run every frame as its own graph.
+bool Detector::batch_usable(const Plan& p) const {
+    return !batches_.empty() && !legacy_ && !d_lnet_ && !p.downscale && p.n_levels > 0 && (p.ch == 1 || p.ch == 3 || p.ch == 4);
+}
+
+// The graph of a batch: gray of every frame in one launch, the learned gate per frame (when on),
+// the pyramid and stage 1 of every level of every frame in one persistent launch, the candidates of
+// every frame in one launch, the stage-2/3 windows of every frame's candidates in one persistent
+// launch, every frame's replay in one launch (a block each), then the results to the host.
+ccnn_status Detector::enqueue_batch_kernels(BatchCtx& c, const Plan& p, int B) {
+    cudaStream_t st = slots_[c.first_slot].st;
+    const bool gated = gate_on_ && slots_[c.first_slot].gate.prob && p.gw >= 32 && p.gh >= 32;
+    BatchFrames F{};
+    BatchCands C{};
+    WinBatch WB{};
+    WB.n_frames = B;
+    for (int f = 0; f < B; ++f) {
+        Slot& s = slots_[c.first_slot + f];
+        F.gray[f] = s.d_gray;
+        F.limg[f] = s.d_limg;
+        F.s1[f] = s.d_s1;
+        F.resp[f] = s.d_resp;
+        F.counts[f] = s.d_counts;
+        F.front_on[f] = gated ? s.d_front_on : nullptr;
+        F.back_on[f] = gated ? s.d_back_on : nullptr;
+        F.cells[f] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{};
+        C.cands[f] = s.d_cands;
+        C.ncand[f] = s.d_ncand;
+        WB.gray[f] = s.d_gray;
+        WB.cands[f] = s.d_cands;
+        WB.ncand[f] = s.d_ncand;
+        WB.out[f] = s.d_win;
+    }
+    const int gpitch = slots_[c.first_slot].gray_pitch;
+    CCNN_CUDA(cudaMemsetAsync(c.d_sync, 0, sizeof(int) * (2 + kBatchStages * B), st));
+    CCNN_CUDA(launch_gray_batch(c.d_src, B, p.in_w, p.in_h, p.ch, F, gpitch, st));
+    if (gated)
+        for (int f = 0; f < B; ++f) {
+            Slot& s = slots_[c.first_slot + f];
+            CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_, gate_amb_frac_,
+                                  s.d_back_on, s.d_front_on, st));
+        }
+    const LevelDesc& last = p.levels[p.n_levels - 1];
+    const int pyr_items = last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows);
+    BatchQueue Q;
+    build_batch_queue(&Q, B, p.n_levels, (int)p.chunks.size(), pyr_items, p.k1_tiles, p.k2_tiles, gpitch, p.gw, p.gh, cfg_.thr1);
+    const int grid = sm_count_ * stage1_batch_blocks_per_sm(batch_bpsm_);
+    int* sync = c.d_sync;
+    int* err = c.d_sync + 1 + kBatchStages * B;
+    CCNN_CUDA(launch_stage1_batch(w1_, F, Q, p.d_levels, sync, err, grid, st, batch_bpsm_));
+    CCNN_CUDA(launch_cand_write_batch(p.d_chunks, (int)p.chunks.size(), p.d_levels, F, C, B, cfg_.thr1, (int)cand_cap_, st));
+    if (detect_enabled_) CCNN_CUDA(launch_window_batch(*wn_, WB, gpitch, p.gw, p.gh, p.d_levels, cfg_, window_grid_, st));
+    CCNN_CUDA(launch_replay_batch(c.d_rargs, B, st));
+    const long long face_cap = std::max<long long>(cand_cap_, kHostFaces);
+    CCNN_CUDA(cudaMemcpyAsync(c.h_nf, c.d_nf, sizeof(int) * B, cudaMemcpyDeviceToHost, st));
+    CCNN_CUDA(cudaMemcpyAsync(c.h_nf + B, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CCNN_CUDA(cudaMemcpy2DAsync(c.h_faces, sizeof(FaceOut) * kGraphFaces, c.d_faces, sizeof(FaceOut) * face_cap, sizeof(FaceOut) * kGraphFaces, B,
+                                cudaMemcpyDeviceToHost, st));
+    return CCNN_OK;
+}
+
+ccnn_status Detector::launch_batch(BatchCtx& c, const Plan& p, const ccnn_image* imgs, int B, bool device_input) {
+    cudaStream_t st = slots_[c.first_slot].st;
+    const bool gated = gate_on_ && slots_[c.first_slot].gate.prob && p.gw >= 32 && p.gh >= 32;
+    if (c.exec_plan != &p || c.exec_gated != gated) {
+        if (c.exec) {
+            cudaGraphExecDestroy(c.exec);
+            c.exec = nullptr;
+        }
+        // per-frame replay arguments of this plan (device memory the replay kernel reads)
+        const long long face_cap = std::max<long long>(cand_cap_, kHostFaces);
+        std::vector<ReplayArgs> ra(B);
+        for (int f = 0; f < B; ++f) {
+            ra[f] = replay_args(slots_[c.first_slot + f], p);
+            ra[f].faces = c.d_faces + (size_t)f * face_cap;
+            ra[f].face_cap = (int)face_cap;
+            ra[f].n_faces = c.d_nf + f;
+        }
+        CCNN_CUDA(cudaMemcpyAsync(c.d_rargs, ra.data(), sizeof(ReplayArgs) * B, cudaMemcpyHostToDevice, st));
+        CCNN_CUDA(cudaStreamSynchronize(st));
+        cudaGraph_t g;
+        CCNN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        ccnn_status es = enqueue_batch_kernels(c, p, B);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (es != CCNN_OK) return es;
+        CCNN_CUDA(ce);
+        ce = cudaGraphInstantiate(&c.exec, g, 0);
+        cudaGraphDestroy(g);
+        CCNN_CUDA(ce);
+        c.exec_plan = &p;
+        c.exec_gated = gated;
+    }
+    // sources: aligned device frames are read where they are; others are packed into the slot
+    for (int f = 0; f < B; ++f) {
+        const ccnn_image& img = imgs[f];
+        Slot& s = slots_[c.first_slot + f];
+        const bool in_place = device_input && !((uintptr_t)img.data & 63) && !(img.step & 63) && img.step <= (size_t)INT32_MAX;
+        if (in_place) {
+            c.h_src[f].data = img.data;
+            c.h_src[f].pitch = (int)img.step;
+        } else {
+            const size_t row = (size_t)img.cols * img.channels;
+            const cudaMemcpyKind kind = device_input ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+            if (img.step == p.in_pitch)
+                CCNN_CUDA(cudaMemcpyAsync(s.d_in, img.data, p.in_pitch * (size_t)(img.rows - 1) + row, kind, st));
+            else
+                CCNN_CUDA(cudaMemcpy2DAsync(s.d_in, p.in_pitch, img.data, img.step, row, img.rows, kind, st));
+            c.h_src[f].data = s.d_in;
+            c.h_src[f].pitch = (int)p.in_pitch;
+        }
+        c.h_src[f].pad = 0;
+        s.last_in_place = in_place;
+        s.last_plan = &p;
+    }
+    CCNN_CUDA(cudaMemcpyAsync(c.d_src, c.h_src, sizeof(FrameSrc) * B, cudaMemcpyHostToDevice, st));
+    CCNN_CUDA(cudaGraphLaunch(c.exec, st));
+    CCNN_CUDA(cudaEventRecord(c.done, st));
+    CCNN_CUDA(cudaEventRecord(slots_[c.first_slot].done, st));
+    return CCNN_OK;
+}
+
+ccnn_status Detector::collect_batch(BatchCtx& c, int B, ccnn_face* faces, int cap_per, int* n_faces, ccnn_status* worst) {
+    CCNN_CUDA(cudaEventSynchronize(c.done));
+    CCNN_CUDA(cudaGetLastError());
+    if (c.h_nf[B] != 0) {
+        set_error("batched stage 1: a dependency wait gave up (results of the batch discarded)");
+        return CCNN_ERR_CUDA;
+    }
+    const long long face_cap = std::max<long long>(cand_cap_, kHostFaces);
+    for (int f = 0; f < B; ++f) {
+        const int img = c.pending_first + f;
+        const int nf = c.h_nf[f];
+        const int take = std::min(nf, cap_per);
+        const FaceOut* src = c.h_faces + (size_t)f * kGraphFaces;
+        if (take > kGraphFaces) {
+            c.h_extra.resize(take);
+            CCNN_CUDA(cudaMemcpy(c.h_extra.data(), c.d_faces + (size_t)f * face_cap, sizeof(FaceOut) * take, cudaMemcpyDeviceToHost));
+            src = c.h_extra.data();
+        }
+        ccnn_face* out = faces + (size_t)img * cap_per;
+        for (int i = 0; i < take; ++i) {
+            out[i].x = src[i].x;
+            out[i].y = src[i].y;
+            out[i].width = src[i].w;
+            out[i].height = src[i].h;
+            out[i].score = src[i].score;
+            out[i].gender = src[i].gender;
+            out[i].smile = src[i].smile;
+            out[i].glasses = src[i].glasses;
+        }
+        n_faces[img] = nf;
+        if (nf > cap_per) *worst = CCNN_TRUNCATED;
+    }
+    c.pending_first = -1;
     return CCNN_OK;
 }
 

@@ -78,6 +78,27 @@ struct Slot {
     std::vector<FaceOut> h_extra;     // faces beyond the pinned buffer's kHostFaces
 };
 
+// A batch context: B consecutive frame slots whose frames run as one captured graph (batched gray,
+// one persistent launch for the pyramid and stage 1 of every frame, batched candidate write, windows
+// and replay), with the group's sources and results in its own buffers.
+struct BatchCtx {
+    int first_slot = 0;
+    cudaEvent_t done = nullptr;
+    int* d_sync = nullptr;        // queue head, finished items per (frame, stage), error flag
+    ReplayArgs* d_rargs = nullptr;
+    FrameSrc* d_src = nullptr;
+    FrameSrc* h_src = nullptr;    // pinned
+    FaceOut* d_faces = nullptr;   // B x face capacity
+    int* d_nf = nullptr;          // B face counts
+    FaceOut* h_faces = nullptr;   // pinned, B x kGraphFaces
+    int* h_nf = nullptr;          // pinned, B face counts and the error flag
+    cudaGraphExec_t exec = nullptr;
+    const Plan* exec_plan = nullptr;
+    bool exec_gated = false;
+    int pending_first = -1;       // index in the caller's image array of the frames in flight
+    std::vector<FaceOut> h_extra;
+};
+
 class Detector {
    public:
     static constexpr int kSlots = 8;
@@ -109,8 +130,10 @@ class Detector {
     ccnn_status gate_disable();
     // schedule knobs an autotuner sets: frames in flight and resident stage-2/3 blocks per SM
     // (0 keeps the current value); the device state is rebuilt
-    ccnn_status set_schedule(int frame_slots, int window_ctas_per_sm, int front_bpsm = 0, int back_bpsm = 0);
-    void get_schedule(int* frame_slots, int* window_ctas_per_sm, int* front_bpsm = nullptr, int* back_bpsm = nullptr) const;
+    ccnn_status set_schedule(int frame_slots, int window_ctas_per_sm, int front_bpsm = 0, int back_bpsm = 0, int batch_frames = -1,
+                             int batch_bpsm = 0);
+    void get_schedule(int* frame_slots, int* window_ctas_per_sm, int* front_bpsm = nullptr, int* back_bpsm = nullptr,
+                      int* batch_frames = nullptr, int* batch_bpsm = nullptr) const;
     // training labels of the last frame (slot 0): uint8 [4][gh/16][gw/16], device memory
     ccnn_status gate_labels(uint8_t* d_labels, cudaStream_t st);
     // stage-1 tiles the gate let run in the last frame (slot 0), of all, and whether it fell back
@@ -173,6 +196,16 @@ class Detector {
     ccnn_status enqueue_legacy_stage1(Slot& s, const Plan& p);
     int window_ctas_per_sm_ = 4;     // persistent stage-2/3 grid: this many blocks per SM
     Stage1Sched s1_sched_{};         // stage-1 register budgets
+    int batch_frames_ = 0;           // frames per batched launch (0: every frame its own graph)
+    int batch_bpsm_ = 3;             // register budget of the persistent batched stage-1 kernel
+    std::vector<BatchCtx> batches_;
+    int sm_count_ = 0;
+    ccnn_status alloc_batches();
+    void free_batches();
+    ccnn_status enqueue_batch_kernels(BatchCtx& c, const Plan& p, int B);
+    ccnn_status launch_batch(BatchCtx& c, const Plan& p, const ccnn_image* imgs, int B, bool device_input);
+    ccnn_status collect_batch(BatchCtx& c, int B, ccnn_face* faces, int cap_per, int* n_faces, ccnn_status* worst);
+    bool batch_usable(const Plan& p) const;
     float* d_gate_ = nullptr;        // learned gate parameters (device memory)
     bool gate_on_ = false;
     float gate_thr_ = 0.5f, gate_amb_frac_ = 0.25f;

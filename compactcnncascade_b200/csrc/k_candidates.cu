@@ -53,19 +53,19 @@ __device__ __forceinline__ int block_sum(int v, int* warp_tot) {
     return t;
 }
 
-__global__ void __launch_bounds__(kChunkThreads) cand_write_kernel(const int4* __restrict__ chunks, int n_chunks,
-                                                                   const LevelDesc* __restrict__ levels, const float* __restrict__ resp,
-                                                                   float thr, const int* __restrict__ counts, Candidate* __restrict__ out,
-                                                                   int* __restrict__ n_out, int cap) {
+// the hits of chunk `c` of a frame's scan, written in raster order after those of earlier chunks
+__device__ __forceinline__ void cand_write_chunk(const int4* __restrict__ chunks, int n_chunks, const LevelDesc* __restrict__ levels,
+                                                 const float* __restrict__ resp, float thr, const int* __restrict__ counts,
+                                                 Candidate* __restrict__ out, int* __restrict__ n_out, int cap, int c) {
     __shared__ int wt[32];
     __shared__ int tot;
     // offset of this chunk = sum of the counts of the chunks visited before it
     int part = 0;
-    for (int i = threadIdx.x; i < (int)blockIdx.x; i += blockDim.x) part += counts[i];
+    for (int i = threadIdx.x; i < c; i += blockDim.x) part += counts[i];
     int off = block_sum(part, wt);
-    if (blockIdx.x == n_chunks - 1 && threadIdx.x == 0) *n_out = min(off + counts[blockIdx.x], cap);
+    if (c == n_chunks - 1 && threadIdx.x == 0) *n_out = min(off + counts[c], cap);
 
-    const int4 ck = chunks[blockIdx.x];
+    const int4 ck = chunks[c];
     const LevelDesc L = levels[ck.x];
     for (int b0 = 0; b0 < ck.z; b0 += blockDim.x) {
         const int i = b0 + threadIdx.x;
@@ -88,6 +88,35 @@ __global__ void __launch_bounds__(kChunkThreads) cand_write_kernel(const int4* _
         }
         off += tot;
     }
+}
+
+__global__ void __launch_bounds__(kChunkThreads) cand_write_kernel(const int4* __restrict__ chunks, int n_chunks,
+                                                                   const LevelDesc* __restrict__ levels, const float* __restrict__ resp,
+                                                                   float thr, const int* __restrict__ counts, Candidate* __restrict__ out,
+                                                                   int* __restrict__ n_out, int cap) {
+    cand_write_chunk(chunks, n_chunks, levels, resp, thr, counts, out, n_out, cap, blockIdx.x);
+}
+
+// the frames of a batch: blockIdx.y is the frame
+__global__ void __launch_bounds__(kChunkThreads) cand_write_batch_kernel(const int4* __restrict__ chunks, int n_chunks,
+                                                                         const LevelDesc* __restrict__ levels,
+                                                                         const __grid_constant__ BatchFrames F,
+                                                                         const __grid_constant__ BatchCands C, float thr, int cap) {
+    const int f = blockIdx.y;
+    cand_write_chunk(chunks, n_chunks, levels, F.resp[f], thr, F.counts[f], C.cands[f], C.ncand[f], cap, blockIdx.x);
+}
+
+cudaError_t launch_cand_write_batch(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const BatchFrames& F, const BatchCands& C,
+                                    int n_frames, float thr, int cap, cudaStream_t st) {
+    if (n_chunks <= 0) {
+        for (int f = 0; f < n_frames; ++f) {
+            const cudaError_t e = cudaMemsetAsync(C.ncand[f], 0, sizeof(int), st);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+    cand_write_batch_kernel<<<dim3(n_chunks, n_frames), kChunkThreads, 0, st>>>(d_chunks, n_chunks, d_levels, F, C, thr, cap);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,

@@ -17,11 +17,11 @@ __device__ __forceinline__ float gray_bgr(uint32_t b, uint32_t g, uint32_t r) {
     return fadd(fadd(fmul(0.114f, (float)b), fmul(0.587f, (float)g)), fmul(0.299f, (float)r));
 }
 
+// 16 pixels of a row (item = row x 16-pixel chunk), 128-bit loads and stores
 template <int CH>
-__global__ void __launch_bounds__(256) gray_kernel(const uint8_t* __restrict__ src, int spitch, int w, int h,
-                                                   float* __restrict__ dst, int dpitch) {
+__device__ __forceinline__ void gray_chunk(const uint8_t* __restrict__ src, int spitch, int w, int h, float* __restrict__ dst, int dpitch,
+                                           int item) {
     const int chunks = (w + 15) >> 4;  // 16-pixel chunks per row; one chunk per thread
-    const int item = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = item / chunks;
     const int x0 = (item - y * chunks) * 16;
     if (y >= h) return;
@@ -49,6 +49,33 @@ __global__ void __launch_bounds__(256) gray_kernel(const uint8_t* __restrict__ s
             out[x] = (CH == 1) ? (float)p[0] : gray_bgr(p[0], p[1], p[2]);
         }
     }
+}
+
+template <int CH>
+__global__ void __launch_bounds__(256) gray_kernel(const uint8_t* __restrict__ src, int spitch, int w, int h,
+                                                   float* __restrict__ dst, int dpitch) {
+    gray_chunk<CH>(src, spitch, w, h, dst, dpitch, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// the frames of a batch: blockIdx.y is the frame; sources (64-byte aligned base and pitch) from a
+// device table the host fills before every launch
+template <int CH>
+__global__ void __launch_bounds__(256) gray_batch_kernel(const FrameSrc* __restrict__ src, int w, int h, const __grid_constant__ BatchFrames F,
+                                                         int dpitch) {
+    const FrameSrc fs = src[blockIdx.y];
+    gray_chunk<CH>(fs.data, fs.pitch, w, h, const_cast<float*>(F.gray[blockIdx.y]), dpitch, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+cudaError_t launch_gray_batch(const FrameSrc* d_src, int n_frames, int w, int h, int ch, const BatchFrames& F, int dpitch, cudaStream_t st) {
+    const long long items = (long long)h * ((w + 15) / 16);
+    dim3 grid((unsigned)((items + 255) / 256), (unsigned)n_frames);
+    switch (ch) {
+        case 1: gray_batch_kernel<1><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
+        case 3: gray_batch_kernel<3><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
+        case 4: gray_batch_kernel<4><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 const void* gray_kernel_fn(int ch) {

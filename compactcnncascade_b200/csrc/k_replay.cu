@@ -177,7 +177,7 @@ constexpr int kBitWords = kBitMax / 32;
 constexpr int kOwnVerdict = -kBitMax - 1;  // the candidate's own stage-2/3 verdict
 constexpr int kOwnScore = -kBitMax - 2;    // the candidate's stage-1 score (detection disabled)
 
-__global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) {
+__device__ __forceinline__ void replay_body(const ReplayArgs& a) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ int s_lvl_start[kMaxLevels + 1];
     __shared__ int s_nD, s_nS;
@@ -721,10 +721,29 @@ cudaError_t launch_nms(const Det* in, int n, uint8_t* checked, Det* out, int* n_
     return cudaGetLastError();
 }
 
-cudaError_t replay_setup() { return cudaFuncSetAttribute(replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReplaySmemBytes); }
+__global__ void __launch_bounds__(kRT, 1) replay_kernel(const ReplayArgs a) { replay_body(a); }
+
+// the frames of a batch: block f replays args[f]
+__global__ void __launch_bounds__(kRT, 1) replay_batch_kernel(const ReplayArgs* __restrict__ args) {
+    __shared__ ReplayArgs s_args;
+    if (threadIdx.x == 0) s_args = args[blockIdx.x];
+    __syncthreads();
+    replay_body(s_args);
+}
+
+cudaError_t replay_setup() {
+    cudaError_t e = cudaFuncSetAttribute(replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReplaySmemBytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(replay_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReplaySmemBytes);
+    return e;
+}
 
 cudaError_t launch_replay(const ReplayArgs& a, cudaStream_t st) {
     replay_kernel<<<1, kRT, kReplaySmemBytes, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_replay_batch(const ReplayArgs* d_args, int n_frames, cudaStream_t st) {
+    replay_batch_kernel<<<n_frames, kRT, kReplaySmemBytes, st>>>(d_args);
     return cudaGetLastError();
 }
 

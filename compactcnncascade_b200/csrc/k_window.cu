@@ -340,57 +340,103 @@ __device__ void prepare_window(const WinArgs& a, WindowSmem& S, const Candidate&
 // candidate one after the other, doubling the kernel's latency. Inside an item, stage 3 runs only
 // when stage 2 does not end the check (the reference's early exits, cnn_detector_v3.cpp:1698-1706);
 // otherwise its slot keeps (max -10, count 0), exactly what the reference leaves behind.
+// One work item: window `mod` of candidate ci, stage 2 then (unless an early exit ends the check)
+// stage 3, the (max, count) pair of each written to a.out.
+template <bool kLegacy>
+__device__ __forceinline__ void window_item(const WindowNets& N, const WinArgs& a, WindowSmem& S, int ci, int mod) {
+    const CascadeConfig& C = a.cfg;
+    const Candidate cd = a.cands[ci];
+    const LevelDesc& L = a.levels[cd.level];
+    const int mn = (C.adapt_min_neighbors && L.scale > 0.7f && C.min_neighbors > 1) ? C.min_neighbors - 1 : C.min_neighbors;
+    prepare_window(a, S, cd, L.inv_scale, mod);
+    WinOut r[2];
+    r[1].max = -10.f;
+    r[1].knn = 0;
+    for (int stage = 0; stage < 2; ++stage) {
+        if constexpr (kLegacy)
+            legacy_window_net(a.lg[1 + stage], S, stage == 0 ? 0 : (C.reflection ? 1 : 2));
+        else if (stage == 0)
+            window_net(N.s2, S, 0);
+        else
+            window_net(N.s3, S, C.reflection ? 1 : 2);
+        // every thread reduces the 16 responses itself (no extra barrier needed)
+        const float thr = stage == 0 ? C.thr2 : C.thr3;
+        float mx = -10.f;
+        int kc = 0;
+#pragma unroll
+        for (int o = 0; o < kOutN; ++o) {
+            const float d = S.out[o];
+            mx = (mx < d) ? d : mx;  // MAX(max_score, d) (cnn_detector_v3.cpp:1667-1683)
+            if (d > thr) kc++;
+        }
+        r[stage].max = mx;
+        r[stage].knn = kc;
+        if (stage == 0) {
+            const bool stop = (C.type_check == 0 && kc >= mn) || (C.type_check > 0 && kc <= 0) || (C.type_check == 2 && kc < mn);
+            if (stop) break;
+        }
+    }
+    if (threadIdx.x == 0) {
+        a.out[(size_t)ci * 4 + 2 * mod] = r[0];
+        a.out[(size_t)ci * 4 + 2 * mod + 1] = r[1];
+    }
+    __syncthreads();
+}
+
 template <bool kLegacy>
 __global__ void __launch_bounds__(kWT, 4) window_kernel(const __grid_constant__ WindowNets N, const WinArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WindowSmem& S = *reinterpret_cast<WindowSmem*>(smem_raw);
     const int n = *a.n_cand;
-    const CascadeConfig& C = a.cfg;
-    const int per_cand = C.double_check ? 2 : 1;
+    const int per_cand = a.cfg.double_check ? 2 : 1;
     const int total = n * per_cand;
     for (int it = blockIdx.x; it < total; it += gridDim.x) {
         const int ci = it / per_cand;
-        const int mod = it - ci * per_cand;
-        const Candidate cd = a.cands[ci];
-        const LevelDesc& L = a.levels[cd.level];
-        const int mn = (C.adapt_min_neighbors && L.scale > 0.7f && C.min_neighbors > 1) ? C.min_neighbors - 1 : C.min_neighbors;
-        prepare_window(a, S, cd, L.inv_scale, mod);
-        WinOut r[2];
-        r[1].max = -10.f;
-        r[1].knn = 0;
-        for (int stage = 0; stage < 2; ++stage) {
-            if constexpr (kLegacy)
-                legacy_window_net(a.lg[1 + stage], S, stage == 0 ? 0 : (C.reflection ? 1 : 2));
-            else if (stage == 0)
-                window_net(N.s2, S, 0);
-            else
-                window_net(N.s3, S, C.reflection ? 1 : 2);
-            // every thread reduces the 16 responses itself (no extra barrier needed)
-            const float thr = stage == 0 ? C.thr2 : C.thr3;
-            float mx = -10.f;
-            int kc = 0;
-#pragma unroll
-            for (int o = 0; o < kOutN; ++o) {
-                const float d = S.out[o];
-                mx = (mx < d) ? d : mx;  // MAX(max_score, d) (cnn_detector_v3.cpp:1667-1683)
-                if (d > thr) kc++;
-            }
-            r[stage].max = mx;
-            r[stage].knn = kc;
-            if (stage == 0) {
-                const bool stop = (C.type_check == 0 && kc >= mn) || (C.type_check > 0 && kc <= 0) || (C.type_check == 2 && kc < mn);
-                if (stop) break;
-            }
-        }
-        if (threadIdx.x == 0) {
-            a.out[(size_t)ci * 4 + 2 * mod] = r[0];
-            a.out[(size_t)ci * 4 + 2 * mod + 1] = r[1];
-        }
-        __syncthreads();
+        window_item<kLegacy>(N, a, S, ci, it - ci * per_cand);
+    }
+}
+
+// The candidates of every frame of a batch as one persistent item list (frame by frame); the
+// per-frame gray image, candidates and outputs come from B, the rest from `base`.
+__global__ void __launch_bounds__(kWT, 4) window_batch_kernel(const __grid_constant__ WindowNets N, const WinArgs base,
+                                                              const __grid_constant__ WinBatch B) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WindowSmem& S = *reinterpret_cast<WindowSmem*>(smem_raw);
+    __shared__ int s_pre[kMaxBatch + 1];
+    if (threadIdx.x == 0) {
+        s_pre[0] = 0;
+        for (int f = 0; f < B.n_frames; ++f) s_pre[f + 1] = s_pre[f] + *B.ncand[f];
+    }
+    __syncthreads();
+    const int per_cand = base.cfg.double_check ? 2 : 1;
+    const int total = s_pre[B.n_frames] * per_cand;
+    for (int it = blockIdx.x; it < total; it += gridDim.x) {
+        const int c = it / per_cand;
+        int f = 0;
+        while (s_pre[f + 1] <= c) ++f;
+        WinArgs a = base;
+        a.gray = B.gray[f];
+        a.cands = B.cands[f];
+        a.n_cand = B.ncand[f];
+        a.out = B.out[f];
+        window_item<false>(N, a, S, c - s_pre[f], it - c * per_cand);
     }
 }
 
 int window_smem_bytes() { return (int)sizeof(WindowSmem); }
+
+cudaError_t launch_window_batch(const WindowNets& N, const WinBatch& B, int gpitch, int gw, int gh, const LevelDesc* levels,
+                                const CascadeConfig& cfg, int grid, cudaStream_t st) {
+    WinArgs a{};
+    a.gpitch = gpitch;
+    a.gw = gw;
+    a.gh = gh;
+    a.levels = levels;
+    a.cfg = cfg;
+    a.lg = nullptr;
+    window_batch_kernel<<<grid, kWT, sizeof(WindowSmem), st>>>(N, a, B);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
                           const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st, const LegacyNet* lg) {

@@ -106,6 +106,31 @@ struct BatchQueue {
     int seg_stage[kBatchStages * kMaxBatch], seg_frame[kBatchStages * kMaxBatch], seg_first[kBatchStages * kMaxBatch + 1];
     int wait_limit;                 // polls of a dependency before the launch reports an error
 };
+// source of one frame of a batch (device memory, 64-byte aligned base and pitch)
+struct FrameSrc {
+    const uint8_t* data;
+    int pitch;
+    int pad;
+};
+cudaError_t launch_gray_batch(const FrameSrc* d_src, int n_frames, int w, int h, int ch, const BatchFrames& F, int dpitch, cudaStream_t st);
+// per-frame outputs of the candidate, window and replay stages of a batch
+struct BatchCands {
+    Candidate* cands[kMaxBatch];
+    int* ncand[kMaxBatch];
+};
+cudaError_t launch_cand_write_batch(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const BatchFrames& F, const BatchCands& C,
+                                    int n_frames, float thr, int cap, cudaStream_t st);
+struct WinBatch {
+    const float* gray[kMaxBatch];
+    const Candidate* cands[kMaxBatch];
+    const int* ncand[kMaxBatch];
+    WinOut* out[kMaxBatch];
+    int n_frames;
+};
+cudaError_t launch_window_batch(const WindowNets& N, const WinBatch& B, int gpitch, int gw, int gh, const LevelDesc* levels,
+                                const CascadeConfig& cfg, int grid, cudaStream_t st);
+// the replay of every frame of a batch: block f runs args[f] (device memory)
+cudaError_t launch_replay_batch(const ReplayArgs* d_args, int n_frames, cudaStream_t st);
 // builds the queue order: a diagonal wavefront over (stage, frame), so that stage s of frame f is
 // queued after stage s of frame f-1 and stage s-1 of frame f+1 (its producer is long done)
 void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, int pyr_items, int front_items, int back_items, int gpitch,

@@ -119,14 +119,22 @@ CCNN_API ccnn_status ccnn_synth_frame_device(void* d_out, int width, int height,
 CCNN_API ccnn_status ccnn_set_schedule(ccnn_handle h, int frame_slots, int window_ctas_per_sm);
 CCNN_API ccnn_status ccnn_get_schedule(ccnn_handle h, int* frame_slots, int* window_ctas_per_sm);
 
-/* The full schedule: the two knobs above plus the register budget of the two stage-1 kernels
+/* The full schedule: the two knobs above, the register budget of the two stage-1 kernels
  * (resident 256-thread blocks per SM, 3 or 4: more blocks hide more latency, fewer registers
- * may spill). 0 keeps a value. Same rules as ccnn_set_schedule. */
+ * may spill), and the batched form: batch_frames > 1 runs groups of that many frames of one size
+ * through ccnn_detect_batch / ccnn_detect_device_batch as one graph each (the pyramid and stage 1
+ * of every level of every frame of the group in one persistent launch fed by a device work queue,
+ * then the candidates, windows and replays of the group in one launch each); frame_slots must be at
+ * least batch_frames, and frame_slots / batch_frames groups are in flight. batch_blocks_per_sm is
+ * the persistent kernel's register budget (3 or 4). 0 keeps a value (batch_frames: -1 keeps it, 0
+ * turns the batched form off). Same rules as ccnn_set_schedule. */
 typedef struct {
     int frame_slots;
     int window_ctas_per_sm;
     int front_blocks_per_sm;
     int back_blocks_per_sm;
+    int batch_frames;
+    int batch_blocks_per_sm;
 } ccnn_schedule;
 CCNN_API ccnn_status ccnn_set_schedule_ex(ccnn_handle h, const ccnn_schedule* s);
 CCNN_API ccnn_status ccnn_get_schedule_ex(ccnn_handle h, ccnn_schedule* s);
