@@ -39,6 +39,7 @@ EXPORTED = [
     "ccnn_legacy_model_info", "ccnn_legacy_net_forward", "ccnn_set_schedule", "ccnn_get_schedule",
     "ccnn_measure_fp32_peak", "ccnn_cnn_default_params", "ccnn_cnn_create", "ccnn_cnn_detect", "ccnn_cnn_nms",
     "ccnn_cnn_get_params", "ccnn_cnn_set_params", "ccnn_set_schedule_ex", "ccnn_get_schedule_ex",
+    "ccnn_sort_permutation_device",
 ]
 
 
@@ -171,6 +172,7 @@ def lib():
         L.ccnn_inspect_candidates.argtypes = [vp, P(CandidateInfo), ci, P(ci)]
         L.ccnn_inspect_raw_detections.argtypes = [vp, P(Detection), ci, P(ci)]
         L.ccnn_sort_permutation.argtypes = [vp, ci, vp]
+        L.ccnn_sort_permutation_device.argtypes = [vp, ci, vp]
         L.ccnn_detect_device_batch.argtypes = [vp, P(Image), ci, P(Face), ci, P(ci), P(ctypes.c_float)]
         L.ccnn_profile_last_frame.argtypes = [vp, ci, P(ctypes.c_float), ci]
         L.ccnn_plan_levels.argtypes = [P(Params), ci, ci, ci, P(LevelInfo), ci, P(ci)]

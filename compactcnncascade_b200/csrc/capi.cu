@@ -412,6 +412,11 @@ CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm
     return CCNN_OK;
 }
 
+CCNN_API ccnn_status ccnn_sort_permutation_device(const float* scales, int n, int* perm) {
+    if (n < 0 || (n > 0 && (!scales || !perm))) return CCNN_ERR_INVALID_ARG;
+    return ccnn::cuda_status(ccnn::sort_permutation_device(scales, n, perm), "block-wide sort");
+}
+
 }  // extern "C"
 
 // Exhaustive check of the packed reciprocal used by the rational tanh against the IEEE reciprocal.

@@ -21,6 +21,8 @@
 // dependent decisions with one ballot over the bit words per candidate. Levels with more than
 // kBitMax candidates take the direct route (warp 0 tests the appended boxes 32 at a time). The sort
 // permutes (scale, index) keys, and the clustering runs in warp 0.
+#include <vector>
+
 #include "kernels.h"
 #include "replay.cuh"
 #include "window_common.cuh"
@@ -57,6 +59,19 @@ struct MergeTest {
     int X[4], Y[4];
 };
 
+// fl(a / b) > t for a >= 0, b > 0 and t > 0 (normal floats), without the division: the rounded
+// quotient exceeds t exactly when the real one lies above the midpoint between t and the next float,
+// or on it when the tie rounds to that next float (t's last significand bit is 1). mid * b carries at
+// most 25 + 24 significant bits, so the double product and comparison are exact.
+__device__ __forceinline__ bool quot_gt(float a, float b, float t) {
+    const double mid = 0.5 * ((double)t + (double)nextafterf(t, __int_as_float(0x7f800000)));
+    const double prod = mid * (double)b;
+    const double aa = (double)a;
+    if (aa > prod) return true;
+    if (aa < prod) return false;
+    return (__float_as_uint(t) & 1u) != 0u;
+}
+
 __device__ __forceinline__ MergeTest merge_test(const Det& a, const Det& b, float threshold) {
     MergeTest t;
     t.hit = false;
@@ -70,15 +85,23 @@ __device__ __forceinline__ MergeTest merge_test(const Det& a, const Det& b, floa
     sort4(Y);
     const float su = (float)((X[3] - X[0]) * (Y[3] - Y[0]));
     const float si = (float)((X[2] - X[1]) * (Y[2] - Y[1]));
-    const float r1 = fdiv(si, S1), r2 = fdiv(si, S2), r3 = fdiv(si, su);
-    float ratio = r1 > r2 ? r2 : r1;
     const int CX1 = X[0] + ((X[3] - X[0]) >> 1);
     const int CY1 = Y[0] + ((Y[3] - Y[0]) >> 1);
     const int CX2 = X[1] + ((X[2] - X[1]) >> 1);
     const int CY2 = Y[1] + ((Y[2] - Y[1]) >> 1);
     const int thrC = imin(X[3] - X[0], X[2] - X[1]) >> 1;
-    if (r3 > fmul(0.75f, threshold) && (r1 < r2 ? r2 : r1) > 0.7f && abs(CX1 - CX2) < thrC && abs(CY1 - CY2) < thrC) ratio = 1.f;
-    t.hit = ratio > threshold;
+    const bool centred = abs(CX1 - CX2) < thrC && abs(CY1 - CY2) < thrC;
+    if (S1 > 0.f && S2 > 0.f && su > 0.f && si >= 0.f && threshold > 0.f) {
+        // r1 = si / S1, r2 = si / S2, r3 = si / su as the reference rounds them, compared without
+        // dividing: min(r1, r2) > threshold is both > threshold, max(r1, r2) > 0.7 is either
+        const bool over = centred && quot_gt(si, su, fmul(0.75f, threshold)) && (quot_gt(si, S1, 0.7f) || quot_gt(si, S2, 0.7f));
+        t.hit = over ? (1.f > threshold) : (quot_gt(si, S1, threshold) && quot_gt(si, S2, threshold));
+    } else {
+        const float r1 = fdiv(si, S1), r2 = fdiv(si, S2), r3 = fdiv(si, su);
+        float ratio = r1 > r2 ? r2 : r1;
+        if (r3 > fmul(0.75f, threshold) && (r1 < r2 ? r2 : r1) > 0.7f && centred) ratio = 1.f;
+        t.hit = ratio > threshold;
+    }
     t.s1_gt_s2 = S1 > S2;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -301,135 +324,157 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
                 //      levels first, then S in order) has drop type 1;
                 //   T: boxes appended by the survivors' pass: survivor i overlaps (> 0.5) a box of T
                 //      (a copy), or its stage-2/3 verdict accepts it (or detection is disabled).
-                const bool thread_item = tid < m;  // candidate i = tid (m <= 256: warps 0..7)
-                const int i = tid;
-                int code = -1, acc = 0;
-                if (thread_item) {
-                    code = first_dec[g + i];
-                    acc = C.detect_enabled ? res[g + i].accepted : 1;
-                    if (acc && a.attr && a.attr[g + i].x) acc = 0;  // facial analysis dropped it
-                }
-                if (tid < kBitWords) {
-                    s_S[tid] = 0u;
-                    s_T[tid] = 0u;
-                }
-                __syncthreads();
-                bool inS = false;
-                for (int round = 0; round <= m; ++round) {
-                    bool in = false;
-                    if (thread_item) {
-                        if (code >= 0) {
-                            in = (code & 1) == 0;
+                // Warp 0 runs both fixed points alone (lane l holds candidates l, l + 32, ...): a round
+                // is one ballot per word, with no block-wide barrier.
+                if (warp == 0) {
+                    const bool check = C.detect_enabled != 0;
+                    auto a1 = [&](int i, int w) { return s_a1[i * W + w]; };
+                    auto a2 = [&](int i, int w) { return s_a2[i * W + w]; };
+                    auto code_of = [&](int i) { return first_dec[g + i]; };
+                    auto acc_of = [&](int i) {
+                        int acc = C.detect_enabled ? res[g + i].accepted : 1;
+                        if (acc && a.attr && a.attr[g + i].x) acc = 0;  // facial analysis dropped it
+                        return acc;
+                    };
+                    // first decisive box of the level among set X: its bit word and drop type
+                    auto in_scan = [&](int i) {
+                        const int code = code_of(i);
+                        if (code >= 0) return (code & 1) == 0;
+                        for (int w = 0; w < W; ++w) {
+                            const uint32_t hit = (a1(i, w) | a2(i, w)) & s_S[w];
+                            if (hit) return ((a1(i, w) >> (__ffs(hit) - 1)) & 1u) != 0u;
+                        }
+                        return false;
+                    };
+                    if (lane < kBitWords) {
+                        s_S[lane] = 0u;
+                        s_T[lane] = 0u;
+                    }
+                    __syncwarp();
+                    for (int round = 0; round <= m; ++round) {
+                        uint32_t nw[kBitWords];
+                        bool changed = false;
+#pragma unroll
+                        for (int q = 0; q < kBitWords; ++q) {
+                            const int i = lane + 32 * q;
+                            nw[q] = __ballot_sync(0xffffffffu, q < W && i < m && in_scan(i));
+                            changed |= q < W && nw[q] != s_S[q];
+                        }
+                        __syncwarp();
+#pragma unroll
+                        for (int q = 0; q < kBitWords; ++q)
+                            if (lane == q && q < W) s_S[q] = nw[q];
+                        __syncwarp();
+                        if (!changed) break;
+                    }
+                    // survivors: not decided by the scan
+                    auto survivor = [&](int i) {
+                        if (code_of(i) >= 0) return false;
+                        for (int w = 0; w < W; ++w)
+                            if ((a1(i, w) | a2(i, w)) & s_S[w]) return false;
+                        return true;
+                    };
+                    uint32_t surv_w[kBitWords];
+#pragma unroll
+                    for (int q = 0; q < kBitWords; ++q) {
+                        const int i = lane + 32 * q;
+                        surv_w[q] = __ballot_sync(0xffffffffu, q < W && i < m && survivor(i));
+                    }
+                    for (int round = 0; round <= m; ++round) {
+                        uint32_t nw[kBitWords];
+                        bool changed = false;
+#pragma unroll
+                        for (int q = 0; q < kBitWords; ++q) {
+                            const int i = lane + 32 * q;
+                            bool in = false;
+                            if (q < W && i < m && ((surv_w[q] >> lane) & 1u)) {
+                                in = acc_of(i) != 0;
+                                if (check)
+                                    for (int w = 0; w < W && !in; ++w) in = (a1(i, w) & s_T[w]) != 0u;
+                            }
+                            nw[q] = __ballot_sync(0xffffffffu, in);
+                            changed |= q < W && nw[q] != s_T[q];
+                        }
+                        __syncwarp();
+#pragma unroll
+                        for (int q = 0; q < kBitWords; ++q)
+                            if (lane == q && q < W) s_T[q] = nw[q];
+                        __syncwarp();
+                        if (!changed) break;
+                    }
+                    // D index (scan appends in candidate order, then the survivors' appends) and the
+                    // source of each box's score/knn
+                    int nScan = 0, nSurv = 0;
+                    for (int w = 0; w < W; ++w) {
+                        nScan += __popc(s_S[w]);
+                        nSurv += __popc(s_T[w]);
+                    }
+                    for (int i = lane; i < m; i += 32) {
+                        const uint32_t below = (1u << (i & 31)) - 1u;
+                        const int code = code_of(i);
+                        int dst = -1, src = 0;
+                        if ((s_S[i >> 5] >> (i & 31)) & 1u) {
+                            int r = 0;
+                            for (int w = 0; w < (i >> 5); ++w) r += __popc(s_S[w]);
+                            dst = nD + r + __popc(s_S[i >> 5] & below);
+                            if (code >= 0) {
+                                src = code >> 1;
+                            } else {
+                                for (int w = 0; w < W; ++w) {
+                                    const uint32_t hit = (a1(i, w) | a2(i, w)) & s_S[w];
+                                    if (hit) {
+                                        src = -1 - (32 * w + __ffs(hit) - 1);
+                                        break;
+                                    }
+                                }
+                            }
+                        } else if ((s_T[i >> 5] >> (i & 31)) & 1u) {
+                            int r = 0;
+                            for (int w = 0; w < (i >> 5); ++w) r += __popc(s_T[w]);
+                            dst = nD + nScan + r + __popc(s_T[i >> 5] & below);
+                            src = C.detect_enabled ? kOwnVerdict : kOwnScore;
+                            if (check)
+                                for (int w = 0; w < W; ++w) {
+                                    const uint32_t hit = a1(i, w) & s_T[w];
+                                    if (hit) {
+                                        src = -1 - (32 * w + __ffs(hit) - 1);
+                                        break;
+                                    }
+                                }
+                        }
+                        s_didx[i] = dst;
+                        s_src[i] = src;
+                    }
+                    __syncwarp();
+                    // the boxes: rect of the candidate, score/knn from the end of its copy chain
+                    for (int i = lane; i < m; i += 32) {
+                        if (s_didx[i] < 0) continue;
+                        int r = i, src = s_src[i];
+                        while (src < 0 && src > kOwnVerdict) {  // a box of this level: follow it
+                            r = -1 - src;
+                            src = s_src[r];
+                        }
+                        float sc;
+                        int kn;
+                        if (src >= 0) {
+                            sc = D[src].score;
+                            kn = D[src].knn;
+                        } else if (src == kOwnVerdict) {
+                            sc = res[g + r].score;
+                            kn = res[g + r].knn;
                         } else {
-                            for (int w = 0; w < W; ++w) {
-                                const uint32_t hit = (s_a1[i * W + w] | s_a2[i * W + w]) & s_S[w];
-                                if (hit) {
-                                    in = (s_a1[i * W + w] >> (__ffs(hit) - 1)) & 1u;
-                                    break;
-                                }
-                            }
+                            sc = cands[g + r].score;
+                            kn = 0;
                         }
+                        const Det nr = cand_rect(cands[g + i], inv_scale, scale, C.pat_w, C.pat_h);
+                        D[s_didx[i]] = make_det(nr.x, nr.y, nr.w, nr.h, sc, scale, kn);
+                        // facial data travels with a candidate's own accepted box, not with copies
+                        if (a.fa_scratch) a.fa_scratch[s_didx[i]] = (s_src[i] == kOwnVerdict) ? g + i : -1;
                     }
-                    const uint32_t word = __ballot_sync(0xffffffffu, in);
-                    __syncthreads();  // every thread has read the previous round's S
-                    const bool changed = (lane == 0 && warp < W && s_S[warp] != word);
-                    if (lane == 0 && warp < W) s_S[warp] = word;
-                    inS = in;
-                    if (!__syncthreads_or(changed)) break;
-                }
-                // survivors: not decided by the scan
-                bool surv_i = false;
-                if (thread_item && code < 0) {
-                    surv_i = true;
-                    for (int w = 0; w < W; ++w)
-                        if ((s_a1[i * W + w] | s_a2[i * W + w]) & s_S[w]) {
-                            surv_i = false;
-                            break;
-                        }
-                }
-                const bool check = C.detect_enabled != 0;
-                for (int round = 0; round <= m; ++round) {
-                    bool in = false;
-                    if (surv_i) {
-                        in = acc != 0;
-                        if (check)
-                            for (int w = 0; w < W && !in; ++w) in = (s_a1[i * W + w] & s_T[w]) != 0u;
-                    }
-                    const uint32_t word = __ballot_sync(0xffffffffu, in);
-                    __syncthreads();
-                    const bool changed = (lane == 0 && warp < W && s_T[warp] != word);
-                    if (lane == 0 && warp < W) s_T[warp] = word;
-                    if (!__syncthreads_or(changed)) break;
-                }
-                // D index (scan appends in candidate order, then the survivors' appends) and the
-                // source of each box's score/knn
-                int nScan = 0, nSurv = 0;
-                for (int w = 0; w < W; ++w) {
-                    nScan += __popc(s_S[w]);
-                    nSurv += __popc(s_T[w]);
-                }
-                if (thread_item) {
-                    const uint32_t below = (1u << (i & 31)) - 1u;
-                    int dst = -1, src = 0;
-                    if (inS) {
-                        int r = 0;
-                        for (int w = 0; w < (i >> 5); ++w) r += __popc(s_S[w]);
-                        dst = nD + r + __popc(s_S[i >> 5] & below);
-                        if (code >= 0) {
-                            src = code >> 1;
-                        } else {
-                            for (int w = 0; w < W; ++w) {
-                                const uint32_t hit = (s_a1[i * W + w] | s_a2[i * W + w]) & s_S[w];
-                                if (hit) {
-                                    src = -1 - (32 * w + __ffs(hit) - 1);
-                                    break;
-                                }
-                            }
-                        }
-                    } else if ((s_T[i >> 5] >> (i & 31)) & 1u) {
-                        int r = 0;
-                        for (int w = 0; w < (i >> 5); ++w) r += __popc(s_T[w]);
-                        dst = nD + nScan + r + __popc(s_T[i >> 5] & below);
-                        src = C.detect_enabled ? kOwnVerdict : kOwnScore;
-                        if (check)
-                            for (int w = 0; w < W; ++w) {
-                                const uint32_t hit = s_a1[i * W + w] & s_T[w];
-                                if (hit) {
-                                    src = -1 - (32 * w + __ffs(hit) - 1);
-                                    break;
-                                }
-                            }
-                    }
-                    s_didx[i] = dst;
-                    s_src[i] = src;
+                    if (lane == 0) s_nD = nD + nScan + nSurv;
                 }
                 __syncthreads();
-                // the boxes: rect of the candidate, score/knn from the end of its copy chain
-                if (thread_item && s_didx[i] >= 0) {
-                    int r = i, src = s_src[i];
-                    while (src < 0 && src > kOwnVerdict) {  // a box of this level: follow it
-                        r = -1 - src;
-                        src = s_src[r];
-                    }
-                    float sc;
-                    int kn;
-                    if (src >= 0) {
-                        sc = D[src].score;
-                        kn = D[src].knn;
-                    } else if (src == kOwnVerdict) {
-                        sc = res[g + r].score;
-                        kn = res[g + r].knn;
-                    } else {
-                        sc = cands[g + r].score;
-                        kn = 0;
-                    }
-                    const Det nr = cand_rect(cands[g + i], inv_scale, scale, C.pat_w, C.pat_h);
-                    D[s_didx[i]] = make_det(nr.x, nr.y, nr.w, nr.h, sc, scale, kn);
-                    // facial data travels with a candidate's own accepted box, not with copies
-                    if (a.fa_scratch) a.fa_scratch[s_didx[i]] = (s_src[i] == kOwnVerdict) ? g + i : -1;
-                }
-                nD += nScan + nSurv;
-                __syncthreads();
+                nD = s_nD;
                 continue;
             }
             if (warp == 0) {
@@ -542,8 +587,15 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
     ScaleKey* K = fits ? reinterpret_cast<ScaleKey*>(sm) : reinterpret_cast<ScaleKey*>(a.M);
     for (int i = tid; i < nD; i += kRT) K[i] = ScaleKey{D[nD - 1 - i].scale, i};
     __syncthreads();
-    if (nD > 16 && tid == 0) introsort_scale_desc(K, nD);  // n <= 16: insertion sort of a sorted list
-    __syncthreads();
+    // n <= 16: insertion sort of a sorted list. The block-wide sort keeps its segment lists in the
+    // bit-matrix words (free after the level loop) and its leaves in the survivors' scratch.
+    constexpr int kSortSegs = (kBitMax * kBitWords) / 3;
+    if (nD > 16 && nD / 17 <= kSortSegs) {
+        introsort_scale_desc_block(K, nD, reinterpret_cast<int*>(s_a1), reinterpret_cast<int*>(s_a2), kSortSegs, a.survivors);
+    } else {
+        if (nD > 16 && tid == 0) introsort_scale_desc(K, nD);
+        __syncthreads();
+    }
     for (int i = tid; i < nD; i += kRT) {
         R[i] = D[nD - 1 - K[i].idx];
         if (a.fa_scratch) a.fa_scratch[a.face_cap + i] = a.fa_scratch[nD - 1 - K[i].idx];
@@ -729,6 +781,42 @@ __global__ void __launch_bounds__(kRT, 1) replay_batch_kernel(const ReplayArgs* 
     if (threadIdx.x == 0) s_args = args[blockIdx.x];
     __syncthreads();
     replay_body(s_args);
+}
+
+// The block-wide sort of n (scale, index) keys (device memory) and its permutation, for tests.
+__global__ void __launch_bounds__(kRT, 1) sort_check_kernel(ScaleKey* K, int n, int* leaves, int* perm) {
+    constexpr int kSegs = (kBitMax * kBitWords) / 3;
+    __shared__ int seg_a[3 * kSegs], seg_b[3 * kSegs];
+    if (n > 16 && n / 17 <= kSegs) {
+        introsort_scale_desc_block(K, n, seg_a, seg_b, kSegs, leaves);
+    } else {
+        if (threadIdx.x == 0) {
+            if (n > 16) introsort_scale_desc(K, n);
+            else insertion_sort(K, 0, n);
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = K[i].idx;
+}
+
+cudaError_t sort_permutation_device(const float* scales, int n, int* perm) {
+    std::vector<ScaleKey> k(n);
+    for (int i = 0; i < n; ++i) k[i] = ScaleKey{scales[i], i};
+    ScaleKey* d_k = nullptr;
+    int *d_leaves = nullptr, *d_perm = nullptr;
+    cudaError_t e = cudaMalloc(&d_k, sizeof(ScaleKey) * (n + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_leaves, sizeof(int) * (n + 2));
+    if (e == cudaSuccess) e = cudaMalloc(&d_perm, sizeof(int) * (n + 1));
+    if (e == cudaSuccess && n > 0) e = cudaMemcpy(d_k, k.data(), sizeof(ScaleKey) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        sort_check_kernel<<<1, kRT>>>(d_k, n, d_leaves, d_perm);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && n > 0) e = cudaMemcpy(perm, d_perm, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d_k);
+    cudaFree(d_leaves);
+    cudaFree(d_perm);
+    return e;
 }
 
 cudaError_t replay_setup() {

@@ -184,6 +184,9 @@ cudaError_t launch_facial(const LandmarkNet* d_net, const float* gray, int gpitc
 constexpr int kReplaySmemBytes = 200 * 1024;
 cudaError_t replay_setup();
 cudaError_t launch_replay(const ReplayArgs& a, cudaStream_t st);
+// the replay kernel's block-wide sort on n keys (synchronous; for tests): perm[i] = input index of
+// the i-th key after sorting by scale, descending, in libstdc++ std::sort's order of ties
+cudaError_t sort_permutation_device(const float* scales, int n, int* perm);
 // CNNDetector::Detect with detections already in the caller's vector (cnn_detector_v3.cpp:2753-2806):
 // [prior, new clusters] through the min_num_detect filter (applied to the priors here; the clusters
 // come filtered) and Merger(0.2, del), then the optional rescale; scratch holds 2 * (n_prior + n_new)

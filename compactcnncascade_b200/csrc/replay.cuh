@@ -243,4 +243,74 @@ CCNN_HD void introsort_scale_desc(T* v, int n) {
     }
 }
 
+#if defined(__CUDACC__)
+// The same introsort by the whole block. The partitions of one recursion depth touch disjoint
+// segments, so each round partitions every segment longer than the threshold at once (a thread a
+// segment, the reference's steps within it); the heapsort fallback is per segment too. The final
+// insertion sort of the reference never moves an element across a partition cut (everything before
+// a cut has a scale >= the pivot >= everything after it, and the insertion stops at the first element
+// that is not smaller), so it is the same as an insertion sort of each leaf segment, run in parallel.
+// seg_a / seg_b: 3 * max_segs ints each (shared memory); leaves: n ints of scratch (any memory);
+// n must be > 16 and n / 17 <= max_segs. Every thread of the block calls it.
+template <class T>
+__device__ void introsort_scale_desc_block(T* v, int n, int* seg_a, int* seg_b, int max_segs, int* leaves) {
+    const int kThreshold = 16;
+    __shared__ int s_cur, s_next, s_leaves;
+    if (threadIdx.x == 0) {
+        seg_a[0] = 0;
+        seg_a[1] = n;
+        seg_a[2] = 2 * floor_log2(n);
+        s_cur = 1;
+        s_leaves = 0;
+    }
+    __syncthreads();
+    int* cur = seg_a;
+    int* nxt = seg_b;
+    for (;;) {
+        const int ncur = s_cur;
+        if (ncur == 0) break;
+        __syncthreads();
+        if (threadIdx.x == 0) s_next = 0;
+        __syncthreads();
+        for (int k = threadIdx.x; k < ncur; k += blockDim.x) {
+            const int first = cur[3 * k], last = cur[3 * k + 1];
+            int depth = cur[3 * k + 2];
+            if (depth == 0) {
+                heap_sort_el(v + first, last - first);
+                continue;
+            }
+            --depth;
+            const int mid = first + (last - first) / 2;
+            median_to_first(&v[first], &v[first + 1], &v[mid], &v[last - 1]);
+            const int cut = unguarded_partition(v, first + 1, last, first);
+            const int lo[2] = {first, cut}, hi[2] = {cut, last};
+            for (int c = 0; c < 2; ++c) {
+                const int len = hi[c] - lo[c];
+                if (len > kThreshold) {
+                    const int slot = atomicAdd(&s_next, 1);
+                    if (slot < max_segs) {
+                        nxt[3 * slot] = lo[c];
+                        nxt[3 * slot + 1] = hi[c];
+                        nxt[3 * slot + 2] = depth;
+                    }
+                } else if (len > 1) {
+                    const int slot = atomicAdd(&s_leaves, 1);
+                    leaves[2 * slot] = lo[c];
+                    leaves[2 * slot + 1] = hi[c];
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_cur = s_next < max_segs ? s_next : max_segs;
+        int* t = cur;
+        cur = nxt;
+        nxt = t;
+        __syncthreads();
+    }
+    const int nleaf = s_leaves;
+    for (int k = threadIdx.x; k < nleaf; k += blockDim.x) insertion_sort(v, leaves[2 * k], leaves[2 * k + 1]);
+    __syncthreads();
+}
+#endif
+
 }  // namespace ccnn

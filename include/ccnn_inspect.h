@@ -154,6 +154,10 @@ CCNN_API ccnn_status ccnn_legacy_net_forward(const char* model_path, const float
 /* The permutation the detector's device sort applies to detections with the given scales
  * (perm[i] = input index placed at slot i); equals std::sort with comp(a, b) = b < a. */
 CCNN_API ccnn_status ccnn_sort_permutation(const float* scales, int n, int* perm);
+/* The same permutation computed on the device by the replay kernel's block-wide sort (partition
+ * rounds in parallel, leaf insertion sorts in parallel); scales and perm are host memory, synchronous.
+ * No reference counterpart: it exists so tests can compare the block-wide form with std::sort. */
+CCNN_API ccnn_status ccnn_sort_permutation_device(const float* scales, int n, int* perm);
 
 #ifdef __cplusplus
 }
