@@ -8,7 +8,8 @@ The knobs (include/ccnn_inspect.h, ccnn_schedule):
   window_ctas_per_sm   resident blocks per SM of the persistent stage-2/3 window kernel
   front_blocks_per_sm  register budget of the stage-1 front kernel (3: 80 registers, 4: 64)
   back_blocks_per_sm   register budget of the stage-1 back kernel (3: 80 registers, 4: 64)
-  batch_frames         frames per batched graph (0: every frame its own graph); the batched form
+  batch_frames         frames per batched graph (0: every frame its own graph; 1: the same with the
+                       pyramid and stage 1 of all levels in one persistent launch); the batched form
                        runs the pyramid and stage 1 of a whole group in one persistent launch
   batch_blocks_per_sm  register budget of that persistent kernel (3 or 4)
 
@@ -27,7 +28,7 @@ from . import _capi
 
 TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "schedules.json")
 KNOBS = (("frame_slots", (4, 8, 12, 16)), ("window_ctas_per_sm", (2, 3, 4)), ("front_blocks_per_sm", (3, 4)),
-         ("back_blocks_per_sm", (3, 4)), ("batch_frames", (0, 2, 4, 8)), ("batch_blocks_per_sm", (3, 4)))
+         ("back_blocks_per_sm", (3, 4)), ("batch_frames", (0, 1, 2, 4, 8)), ("batch_blocks_per_sm", (3, 4)))
 DEFAULTS = {"frame_slots": 8, "window_ctas_per_sm": 4, "front_blocks_per_sm": 3, "back_blocks_per_sm": 4, "batch_frames": 0,
             "batch_blocks_per_sm": 3}
 

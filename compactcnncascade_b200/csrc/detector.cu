@@ -126,6 +126,7 @@ void Detector::free_slot(Slot& s) {
     cudaFree(s.d_mk);
     cudaFree(s.d_nmk);
     cudaFreeHost(s.h_nfaces);
+    cudaFree(s.d_sync1);
     cudaFreeHost(s.h_faces);
     if (s.done) cudaEventDestroy(s.done);
     if (s.st) cudaStreamDestroy(s.st);
@@ -440,7 +441,9 @@ ccnn_status Detector::alloc_slot(Slot& s) {
         CCNN_CUDA(cudaMalloc(&s.d_attr, sizeof(int4) * cand_cap_));
         CCNN_CUDA(cudaMalloc(&s.d_fa, sizeof(int) * 5 * cand_cap_));
     }
-    CCNN_CUDA(cudaMallocHost(&s.h_nfaces, sizeof(int)));
+    CCNN_CUDA(cudaMallocHost(&s.h_nfaces, 2 * sizeof(int)));
+    s.h_nfaces[1] = 0;
+    CCNN_CUDA(cudaMalloc(&s.d_sync1, sizeof(int) * (2 + kBatchStages)));
     CCNN_CUDA(cudaMallocHost(&s.h_faces, sizeof(FaceOut) * kHostFaces));
     CCNN_CUDA(cudaMemsetAsync(s.d_ncand, 0, sizeof(int), s.st));
     CCNN_CUDA(cudaMemsetAsync(s.d_nraw, 0, sizeof(int), s.st));
@@ -607,8 +610,8 @@ ccnn_status Detector::set_schedule(int frame_slots, int window_ctas_per_sm, int 
     const int batch = batch_frames >= 0 ? batch_frames : batch_frames_;
     if (frame_slots < 0 || frame_slots > 64 || window_ctas_per_sm < 0 || window_ctas_per_sm > 4 || (front_bpsm != 0 && (front_bpsm < 3 || front_bpsm > 4)) ||
         (back_bpsm != 0 && (back_bpsm < 3 || back_bpsm > 4)) || (batch_bpsm != 0 && (batch_bpsm < 3 || batch_bpsm > 4)) || batch > kMaxBatch ||
-        batch == 1 || (batch > 1 && slots < batch)) {
-        set_error("schedule: 1-64 frame slots, 1-4 stage-2/3 blocks per SM, 3-4 stage-1 blocks per SM, batches of 0 or 2-16 frames and "
+        (batch > 1 && slots < batch)) {
+        set_error("schedule: 1-64 frame slots, 1-4 stage-2/3 blocks per SM, 3-4 stage-1 blocks per SM, batches of 0-16 frames and "
                   "at least as many frame slots as frames per batch (0 keeps the current value)");
         return CCNN_ERR_INVALID_ARG;
     }
@@ -731,16 +734,41 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
         CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_, gate_amb_frac_,
                               s.d_back_on, s.d_front_on, s.st));
     }
-    CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st, gated ? s.d_front_on : nullptr));
-    // the back kernel counts each chunk's candidates as it writes the responses
-    if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
-    if (legacy_) {
-        const ccnn_status ls = enqueue_legacy_stage1(s, p);
-        if (ls != CCNN_OK) return ls;
+    const bool single = single_launch_stage1() && p.n_levels > 0;
+    if (single) {
+        // the pyramid and stage 1 of every level in one persistent launch (the batched form's kernel
+        // on one frame): what the reference's level atlas (packet mode) is for
+        BatchFrames F{};
+        F.gray[0] = s.d_gray;
+        F.limg[0] = s.d_limg;
+        F.s1[0] = s.d_s1;
+        F.resp[0] = s.d_resp;
+        F.counts[0] = s.d_counts;
+        F.front_on[0] = gated ? s.d_front_on : nullptr;
+        F.back_on[0] = gated ? s.d_back_on : nullptr;
+        F.cells[0] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{};
+        const LevelDesc& last = p.levels[p.n_levels - 1];
+        BatchQueue Q;
+        build_batch_queue(&Q, 1, p.n_levels, (int)p.chunks.size(), last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows),
+                          p.k1_tiles, p.k2_tiles, s.gray_pitch, p.gw, p.gh, cfg_.thr1);
+        CCNN_CUDA(cudaMemsetAsync(s.d_sync1, 0, sizeof(int) * (2 + kBatchStages), s.st));
+        CCNN_CUDA(launch_stage1_batch(w1_, F, Q, p.d_levels, s.d_sync1, s.d_sync1 + 1 + kBatchStages,
+                                      sm_count_ * stage1_batch_blocks_per_sm(batch_bpsm_), s.st, batch_bpsm_));
+        CCNN_CUDA(cudaMemcpyAsync(s.h_nfaces + 1, s.d_sync1 + 1 + kBatchStages, sizeof(int), cudaMemcpyDeviceToHost, s.st));
     } else {
-        CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
-                                gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr,
-                                gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}, s1_sched_));
+        CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st, gated ? s.d_front_on : nullptr));
+        // the back kernel counts each chunk's candidates as it writes the responses
+        if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
+    }
+    if (!single) {
+        if (legacy_) {
+            const ccnn_status ls = enqueue_legacy_stage1(s, p);
+            if (ls != CCNN_OK) return ls;
+        } else {
+            CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
+                                    gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr,
+                                    gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}, s1_sched_));
+        }
     }
     CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
                                 (int)cand_cap_, s.st));
@@ -854,6 +882,11 @@ ccnn_status Detector::enqueue(Slot& s, const Plan& p, const ccnn_image& img, boo
 ccnn_status Detector::collect_raw(Slot& s, int cap, int* n, const FaceOut** src) {
     CCNN_CUDA(cudaEventSynchronize(s.done));
     CCNN_CUDA(cudaGetLastError());
+    if (s.h_nfaces[1] != 0) {
+        s.h_nfaces[1] = 0;
+        set_error("single-launch stage 1: a dependency wait gave up (the frame's results are invalid)");
+        return CCNN_ERR_CUDA;
+    }
     const int nf = *s.h_nfaces;
     *n = nf;
     const int take = std::min(nf, cap);
@@ -1494,6 +1527,16 @@ void Detector::free_batches() {
 
 // The batched form covers the CNTK cascade on frames at their own resolution (no input downscale),
 // without facial analysis; other configurations run every frame as its own graph.
+// One persistent launch for the pyramid and stage 1 of a frame: the schedule's batch_frames == 1,
+// or AdvancedParam::packet_detection on a GPU pipeline (the reference's CUDA build keeps packet mode
+// only there, cnn_detector_v3.cpp:67-84; precision `def` turns it off, :922-925). CNTK cascade only.
+bool Detector::single_launch_stage1() const {
+    if (legacy_) return false;
+    const bool packet = has_cnn_ && cnn_ap_.packet_detection && cnn_p_.pipeline != CCNN_PIPELINE_CPU &&
+                        cnn_ap_.detect_precision != CCNN_PRECISION_DEF;
+    return batch_frames_ == 1 || packet;
+}
+
 bool Detector::batch_usable(const Plan& p) const {
     return !batches_.empty() && !legacy_ && !d_lnet_ && !p.downscale && p.n_levels > 0 && (p.ch == 1 || p.ch == 3 || p.ch == 4);
 }

@@ -58,7 +58,8 @@ struct Slot {
     int* d_nraw = nullptr;
     FaceOut* d_faces = nullptr;
     int* d_nfaces = nullptr;
-    int* h_nfaces = nullptr;   // pinned
+    int* h_nfaces = nullptr;   // pinned: face count, then the single-launch stage 1's error flag
+    int* d_sync1 = nullptr;    // single-launch stage 1: queue head, finished items per stage, error flag
     FaceOut* h_faces = nullptr;  // pinned, kHostFaces entries
     GateScratch gate{};          // learned gate: features, activations, probabilities (when enabled)
     uint8_t* d_front_on = nullptr;  // learned gate: stage-1 tile activity
@@ -196,7 +197,9 @@ class Detector {
     ccnn_status enqueue_legacy_stage1(Slot& s, const Plan& p);
     int window_ctas_per_sm_ = 4;     // persistent stage-2/3 grid: this many blocks per SM
     Stage1Sched s1_sched_{};         // stage-1 register budgets
-    int batch_frames_ = 0;           // frames per batched launch (0: every frame its own graph)
+    int batch_frames_ = 0;           // frames per batched launch (0: every frame its own graph; 1: every frame
+                                     // its own graph with the pyramid and stage 1 in one persistent launch)
+    bool single_launch_stage1() const;
     int batch_bpsm_ = 3;             // register budget of the persistent batched stage-1 kernel
     std::vector<BatchCtx> batches_;
     int sm_count_ = 0;

@@ -119,3 +119,24 @@ def test_batched_largest_frames_equal_per_frame():
     autotune.set_schedule(d, {"frame_slots": 2, "batch_frames": 2})
     assert _device_batch(d, frames, w, h) == want
     d.Clear()
+
+
+def test_single_launch_stage1_equals_per_frame():
+    """batch_frames = 1 (and packet mode of the CNNDetector API): every frame keeps its own graph, with
+    the pyramid and stage 1 of all its levels in one persistent launch."""
+    from compactcnncascade_b200 import gate
+    for (w, h, mn, mx, sf, nf, lo, hi) in [(1280, 720, 40, 240, 1.15, 10, 30, 300), (1920, 1080, 20, 0, 1.05, 30, 20, 600)]:
+        imgs = [ccnn.synth_frame(w, h, 8000 + i, nf, lo, hi)[0] for i in range(3)]
+        d = ccnn.FaceDetector()
+        assert d.Init(_params(w, h, min_face=mn, max_face=mx, sf=sf)) == 0
+        want = [d.Detect(im) for im in imgs]
+        autotune.set_schedule(d, {"batch_frames": 1})
+        assert [d.Detect(im) for im in imgs] == want
+        assert d.DetectBatch(imgs) == want
+        if sf == 1.15:
+            d.setGate(gate.load(), 0.1, 0.25)
+            gated = [d.Detect(im) for im in imgs]
+            autotune.set_schedule(d, {"batch_frames": 0})
+            d.setGate(gate.load(), 0.1, 0.25)
+            assert [d.Detect(im) for im in imgs] == gated
+        d.Clear()
