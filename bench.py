@@ -184,7 +184,6 @@ def run_batched_pyramid(dev, args):
             return gms.value
 
         res = {}
-        n_levels = len(det.levels()) if det.levels() else 0
         for form, sched in (("per_frame", {"frame_slots": B, "batch_frames": 0}),
                             ("batched", {"frame_slots": 2 * B, "batch_frames": B})):
             autotune.set_schedule(det, sched)
@@ -401,6 +400,9 @@ def main():
     ap.add_argument("--gate-fallback", type=float, default=0.25, help="ambiguous-cell fraction that falls back to the full scan")
     ap.add_argument("--batched-frames", type=int, default=8,
                     help="frames per batch of the batched-pyramid phase (3840x2160 and 4800x2400; 0: skip)")
+    ap.add_argument("--schedule", default="auto",
+                    help="schedule of the main phases: 'auto' (the autotuner's table entry), 'default', or knob=value,... "
+                         "(compactcnncascade_b200.autotune.KNOBS) on top of the defaults")
     ap.add_argument("--serving", action="store_true",
                     help="only the serving sweep: 10,000 mixed-resolution frames per offered rate, plain and gated")
     ap.add_argument("--serve-rates", default="500,1000,2000,4000,8000,16000", help="offered rates of the serving sweep, frames/s")
@@ -457,9 +459,14 @@ def main():
     p.detect_mode = 1
     p.cuda_device_id = dev
     det = ccnn.FaceDetector()
-    if det.Init(p, schedule="auto") != 0:  # the autotuner's schedule for this workload, when tuned
-        raise SystemExit(f"detector init failed: {_capi.last_error()}")
     from compactcnncascade_b200 import autotune
+    if args.schedule in ("auto", "default"):
+        sched_arg, sched_src = (args.schedule if args.schedule == "auto" else None), None
+    else:
+        sched_arg = dict((k, int(v)) for k, v in (kv.split("=") for kv in args.schedule.split(",")))
+        sched_src = f"command line ({args.schedule})"
+    if det.Init(p, schedule=sched_arg) != 0:  # the autotuner's schedule for this workload, when tuned
+        raise SystemExit(f"detector init failed: {_capi.last_error()}")
     schedule = autotune.get_schedule(det)
     L = _capi.lib()
 
@@ -546,9 +553,10 @@ def main():
     lat = np.array(lat[min(5, len(lat) - 1):])
 
     # ---- per-kernel profile of the last frame (CUDA events around each kernel) ----
-    kms = (ctypes.c_float * len(KERNELS))()
-    L.ccnn_profile_last_frame(det._h, args.profile_iters, kms, len(KERNELS))
+    kms = (ctypes.c_float * (len(KERNELS) + 2))()
+    L.ccnn_profile_last_frame(det._h, args.profile_iters, kms, len(KERNELS) + 2)
     kernel_ms = {KERNELS[i]: float(kms[i]) for i in range(len(KERNELS))}
+    single_launch_ms = float(kms[len(KERNELS) + 1])
     levels = det.levels()
     cands = det.candidates()
     work = algorithmic_work(levels, W, H)
@@ -587,6 +595,12 @@ def main():
                       "frac": round(value / world * fb_frame / (hbm_peak * 1e9), 5),
                       "note": "whole-frame algorithmic bytes (BGR read, gray write+read, each level write+read, response maps) "
                               "x frames/s"},
+        "single_launch_stage1": ({"ms": round(single_launch_ms, 4),
+                                  "achieved": round((work["stage1_front"][0] + work["stage1_back"][0]) / (single_launch_ms * 1e-3) / 1e12, 3),
+                                  "frac": round((work["stage1_front"][0] + work["stage1_back"][0]) / (single_launch_ms * 1e-3) / 1e12 / fp32_peak, 4),
+                                  "note": "the pyramid and stage 1 of the frame as one persistent launch (the batched form's kernel on one "
+                                          "frame): front + back fp32 lane operations / its event time, same ceiling"}
+                                 if single_launch_ms > 0 else None),
         "latency_kernel": {"kernel": "replay_merge", "ms": round(kernel_ms["replay_merge"], 4),
                            "note": "one block per frame (sequential reference semantics); it overlaps other frames' kernels in "
                                    "the slot pipeline, so it sets single-frame latency rather than throughput"},
@@ -679,8 +693,8 @@ def main():
         "config": {"workload": WORKLOAD, "frames_per_step": B, "distinct_frames": len(frames),
                    "l2": f"inputs larger than L2: {len(frames)} distinct frames x {W * H * 3 / 1e6:.1f} MB cycled",
                    "parallelism": f"replicas x{world}", "levels": len(levels),
-                   "schedule": dict(schedule, source="autotuner table (compactcnncascade_b200/schedules.json)"
-                                    if autotune.lookup(p) else "defaults"),
+                   "schedule": dict(schedule, source=sched_src or ("autotuner table (compactcnncascade_b200/schedules.json)"
+                                                                   if (args.schedule == "auto" and autotune.lookup(p)) else "defaults")),
                    "stage1_candidates_last_frame": len(cands), "faces_per_frame": round(faces_total / (args.steps * B), 2)},
         "p50_ms": round(float(np.percentile(lat, 50)), 3),
         "p99_ms": round(float(np.percentile(lat, 99)), 3),

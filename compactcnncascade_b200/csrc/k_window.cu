@@ -383,8 +383,10 @@ __device__ __forceinline__ void window_item(const WindowNets& N, const WinArgs& 
     __syncthreads();
 }
 
-template <bool kLegacy>
-__global__ void __launch_bounds__(kWT, 4) window_kernel(const __grid_constant__ WindowNets N, const WinArgs a) {
+// kMinBlocks: the register budget (4 resident blocks a SM: 64 registers; 2: up to 128, no spills),
+// matched to the schedule's resident blocks
+template <bool kLegacy, int kMinBlocks>
+__global__ void __launch_bounds__(kWT, kMinBlocks) window_kernel(const __grid_constant__ WindowNets N, const WinArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WindowSmem& S = *reinterpret_cast<WindowSmem*>(smem_raw);
     const int n = *a.n_cand;
@@ -398,7 +400,8 @@ __global__ void __launch_bounds__(kWT, 4) window_kernel(const __grid_constant__ 
 
 // The candidates of every frame of a batch as one persistent item list (frame by frame); the
 // per-frame gray image, candidates and outputs come from B, the rest from `base`.
-__global__ void __launch_bounds__(kWT, 4) window_batch_kernel(const __grid_constant__ WindowNets N, const WinArgs base,
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kWT, kMinBlocks) window_batch_kernel(const __grid_constant__ WindowNets N, const WinArgs base,
                                                               const __grid_constant__ WinBatch B) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WindowSmem& S = *reinterpret_cast<WindowSmem*>(smem_raw);
@@ -426,7 +429,7 @@ __global__ void __launch_bounds__(kWT, 4) window_batch_kernel(const __grid_const
 int window_smem_bytes() { return (int)sizeof(WindowSmem); }
 
 cudaError_t launch_window_batch(const WindowNets& N, const WinBatch& B, int gpitch, int gw, int gh, const LevelDesc* levels,
-                                const CascadeConfig& cfg, int grid, cudaStream_t st) {
+                                const CascadeConfig& cfg, int grid, cudaStream_t st, int ctas_per_sm) {
     WinArgs a{};
     a.gpitch = gpitch;
     a.gw = gw;
@@ -434,12 +437,16 @@ cudaError_t launch_window_batch(const WindowNets& N, const WinBatch& B, int gpit
     a.levels = levels;
     a.cfg = cfg;
     a.lg = nullptr;
-    window_batch_kernel<<<grid, kWT, sizeof(WindowSmem), st>>>(N, a, B);
+    if (ctas_per_sm <= 2)
+        window_batch_kernel<2><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a, B);
+    else
+        window_batch_kernel<4><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a, B);
     return cudaGetLastError();
 }
 
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
-                          const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st, const LegacyNet* lg) {
+                          const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st, const LegacyNet* lg,
+                          int ctas_per_sm) {
     static_assert(sizeof(WindowSmem) + 64 <= 48 * 1024, "window kernel shared memory must stay under the default 48 KB");
     WinArgs a;
     a.gray = gray;
@@ -453,9 +460,11 @@ cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, in
     a.cfg = cfg;
     a.lg = lg;
     if (lg)
-        window_kernel<true><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
+        window_kernel<true, 4><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
+    else if (ctas_per_sm <= 2)
+        window_kernel<false, 2><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
     else
-        window_kernel<false><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
+        window_kernel<false, 4><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
     return cudaGetLastError();
 }
 

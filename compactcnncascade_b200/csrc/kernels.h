@@ -128,7 +128,7 @@ struct WinBatch {
     int n_frames;
 };
 cudaError_t launch_window_batch(const WindowNets& N, const WinBatch& B, int gpitch, int gw, int gh, const LevelDesc* levels,
-                                const CascadeConfig& cfg, int grid, cudaStream_t st);
+                                const CascadeConfig& cfg, int grid, cudaStream_t st, int ctas_per_sm = 4);
 // the replay of every frame of a batch: block f runs args[f] (device memory)
 cudaError_t launch_replay_batch(const ReplayArgs* d_args, int n_frames, cudaStream_t st);
 // builds the queue order: a diagonal wavefront over (stage, frame), so that stage s of frame f is
@@ -167,9 +167,10 @@ cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
                               const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st);
 // lg (optional): the legacy networks (device memory, [1] stage 2, [2] stage 3) replace N
+// ctas_per_sm: resident blocks a SM the grid was sized for; 2 or fewer selects the 128-register build
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
                           const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st,
-                          const LegacyNet* lg = nullptr);
+                          const LegacyNet* lg = nullptr, int ctas_per_sm = 4);
 // one legacy (format 1.0) network on a w x h image (pitch floats): scratch holds its pooled L1 and
 // L2 maps; counts (optional) gets each scan chunk's responses above thr
 cudaError_t launch_legacy_forward(const LegacyNet* d_net, const LegacyNet& h_net, const float* img, int pitch, int w, int h, float* scratch,

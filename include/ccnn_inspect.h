@@ -89,8 +89,11 @@ CCNN_API ccnn_status ccnn_plan_levels(const ccnn_params* p, int cols, int rows, 
                                       int* n_levels);
 
 /* Re-runs the handle's last frame `iters` times (CCNN_ERR_UNSUPPORTED when that frame was read in
- * place from device memory) and writes the mean duration (ms, CUDA events) of each kernel of the chain: [0] gray, [1] pyramid, [2] stage-1 front, [3] stage-1 back (which also
- * counts the candidates), [4] candidate write, [5] stage-2/3 windows, [6] replay/sort/merge. */
+ * place from device memory) and writes the mean duration (ms, CUDA events) of each kernel of the
+ * chain: [0] gray, [1] pyramid, [2] stage-1 front, [3] stage-1 back (which also counts the
+ * candidates), [4] candidate write, [5] stage-2/3 windows, [6] replay/sort/merge, [7] the learned gate
+ * (when on), [8] the pyramid and stage 1 as one persistent launch (the batched form's kernel on this
+ * frame). n_kernels entries are written. */
 CCNN_API ccnn_status ccnn_profile_last_frame(ccnn_handle h, int iters, float* kernel_ms, int n_kernels);
 
 /* Compares, on the current device, the packed reciprocal the kernels use in the rational tanh with the
