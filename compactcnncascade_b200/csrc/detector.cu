@@ -734,10 +734,11 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
         CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_, gate_amb_frac_,
                               s.d_back_on, s.d_front_on, s.st));
     }
-    const bool single = single_launch_stage1() && p.n_levels > 0;
+    const bool single = single_launch_stage1() && p.n_levels > 0 && p.n_levels <= kMaxBatchLevels;
     if (single) {
-        // the pyramid and stage 1 of every level in one persistent launch (the batched form's kernel
-        // on one frame): what the reference's level atlas (packet mode) is for
+        // the pyramid of every level in one launch (no level-count limit), then stage 1 of every level
+        // in one persistent launch (the batched form's kernels on one frame): what the reference's
+        // level atlas (packet mode) is for
         BatchFrames F{};
         F.gray[0] = s.d_gray;
         F.limg[0] = s.d_limg;
@@ -748,9 +749,10 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
         F.back_on[0] = gated ? s.d_back_on : nullptr;
         F.cells[0] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{};
         const LevelDesc& last = p.levels[p.n_levels - 1];
+        CCNN_CUDA(launch_pyramid_batch(F, p.d_levels, p.n_levels, (int)p.chunks.size(),
+                                       last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows), 1, s.gray_pitch, p.gw, p.gh, s.st));
         BatchQueue Q;
-        build_batch_queue(&Q, 1, p.n_levels, (int)p.chunks.size(), last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows),
-                          p.k1_tiles, p.k2_tiles, s.gray_pitch, p.gw, p.gh, cfg_.thr1);
+        build_batch_queue(&Q, 1, p.n_levels, (int)p.chunks.size(), p.k1_tiles, p.k2_tiles, cfg_.thr1);
         CCNN_CUDA(cudaMemsetAsync(s.d_sync1, 0, sizeof(int) * (2 + kBatchStages), s.st));
         CCNN_CUDA(launch_stage1_batch(w1_, F, Q, p.d_levels, s.d_sync1, s.d_sync1 + 1 + kBatchStages,
                                       sm_count_ * stage1_batch_blocks_per_sm(batch_bpsm_), s.st, batch_bpsm_));
@@ -1396,7 +1398,7 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     // entry K + 1: the pyramid and stage 1 of the frame as one persistent launch (the batched form's
     // kernel on this frame), measured the same way
     double single = 0.0;
-    if (n_ms > K + 1 && !legacy_ && p.n_levels > 0) {
+    if (n_ms > K + 1 && !legacy_ && p.n_levels > 0 && p.n_levels <= kMaxBatchLevels) {
         BatchFrames F{};
         F.gray[0] = s.d_gray;
         F.limg[0] = s.d_limg;
@@ -1407,12 +1409,13 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         F.back_on[0] = gated ? s.d_back_on : nullptr;
         F.cells[0] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{};
         const LevelDesc& last = p.levels[p.n_levels - 1];
+        const int pyr_items = last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows);
         BatchQueue Q;
-        build_batch_queue(&Q, 1, p.n_levels, (int)p.chunks.size(), last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows),
-                          p.k1_tiles, p.k2_tiles, s.gray_pitch, p.gw, p.gh, cfg_.thr1);
+        build_batch_queue(&Q, 1, p.n_levels, (int)p.chunks.size(), p.k1_tiles, p.k2_tiles, cfg_.thr1);
         const int grid = sm_count_ * stage1_batch_blocks_per_sm(batch_bpsm_);
         for (int it = 0; it < iters; ++it) {
             CCNN_CUDA(cudaMemsetAsync(s.d_sync1, 0, sizeof(int) * (2 + kBatchStages), s.st));
+            CCNN_CUDA(launch_pyramid_batch(F, p.d_levels, p.n_levels, (int)p.chunks.size(), pyr_items, 1, s.gray_pitch, p.gw, p.gh, s.st));
             CCNN_CUDA(cudaEventRecord(ev[0], s.st));
             CCNN_CUDA(launch_stage1_batch(w1_, F, Q, p.d_levels, s.d_sync1, s.d_sync1 + 1 + kBatchStages, grid, s.st, batch_bpsm_));
             CCNN_CUDA(cudaEventRecord(ev[1], s.st));
@@ -1573,13 +1576,15 @@ bool Detector::single_launch_stage1() const {
 }
 
 bool Detector::batch_usable(const Plan& p) const {
-    return !batches_.empty() && !legacy_ && !d_lnet_ && !p.downscale && p.n_levels > 0 && (p.ch == 1 || p.ch == 3 || p.ch == 4);
+    return !batches_.empty() && !legacy_ && !d_lnet_ && !p.downscale && p.n_levels > 0 && p.n_levels <= kMaxBatchLevels &&
+           (p.ch == 1 || p.ch == 3 || p.ch == 4);
 }
 
-// The graph of a batch: gray of every frame in one launch, the learned gate per frame (when on),
-// the pyramid and stage 1 of every level of every frame in one persistent launch, the candidates of
-// every frame in one launch, the stage-2/3 windows of every frame's candidates in one persistent
-// launch, every frame's replay in one launch (a block each), then the results to the host.
+// The graph of a batch: gray of every frame in one launch, the learned gate per frame (when on), the
+// pyramid of every level of every frame in one launch, stage 1 of every level of every frame in one
+// persistent launch fed by a device work queue, the candidates of every frame in one launch, the
+// stage-2/3 windows of every frame's candidates in one persistent launch, every frame's replay in one
+// launch (a block each), then the results to the host.
 ccnn_status Detector::enqueue_batch_kernels(BatchCtx& c, const Plan& p, int B) {
     cudaStream_t st = slots_[c.first_slot].st;
     const bool gated = gate_on_ && slots_[c.first_slot].gate.prob && p.gw >= 32 && p.gh >= 32;
@@ -1615,8 +1620,9 @@ ccnn_status Detector::enqueue_batch_kernels(BatchCtx& c, const Plan& p, int B) {
         }
     const LevelDesc& last = p.levels[p.n_levels - 1];
     const int pyr_items = last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows);
+    CCNN_CUDA(launch_pyramid_batch(F, p.d_levels, p.n_levels, (int)p.chunks.size(), pyr_items, B, gpitch, p.gw, p.gh, st));
     BatchQueue Q;
-    build_batch_queue(&Q, B, p.n_levels, (int)p.chunks.size(), pyr_items, p.k1_tiles, p.k2_tiles, gpitch, p.gw, p.gh, cfg_.thr1);
+    build_batch_queue(&Q, B, p.n_levels, (int)p.chunks.size(), p.k1_tiles, p.k2_tiles, cfg_.thr1);
     const int grid = sm_count_ * stage1_batch_blocks_per_sm(batch_bpsm_);
     int* sync = c.d_sync;
     int* err = c.d_sync + 1 + kBatchStages * B;

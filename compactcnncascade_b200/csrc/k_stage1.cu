@@ -46,24 +46,26 @@ struct FrontTile {
 };
 
 // Loads the (67 x 35) input tile of a front CTA from its level image. Rows that start 16-byte
-// aligned with a pitch of whole float4 groups are read as 34 float2 column pairs per row (the tile
-// starts at an even column, columns past the image width hold zeros or the caller's own padding; no
-// stored pixel depends on them); consecutive threads take consecutive pairs, so their stores into
-// the parity-split rows fall on consecutive words. Other images are read one float at a time.
+// aligned with a pitch of whole float4 groups are read as 17 float4 per row (columns past the
+// image width hold zeros or the caller's own padding; no stored pixel depends on them), other
+// images one float at a time. kCoherent: the image was written earlier in the same launch (read
+// through L2, never the read-only path).
 template <bool kCoherent>
 __device__ __forceinline__ void load_front_tile(FrontTile& T, const float* __restrict__ img, const LevelDesc& L, int ix0, int iy0) {
     if (L.img_vec) {
-        constexpr int kP = (kInW + 1) / 2;  // 34
-        for (int i = threadIdx.x; i < kInH * kP; i += blockDim.x) {
-            const int r = i / kP, j = i - r * kP;
-            const int x = ix0 + 2 * j, y = iy0 + r;
-            float2 v = make_float2(0.f, 0.f);
+        constexpr int kV = (kInW + 3) / 4;  // 17
+        for (int i = threadIdx.x; i < kInH * kV; i += blockDim.x) {
+            const int r = i / kV, c4 = i - r * kV;
+            const int x = ix0 + 4 * c4, y = iy0 + r;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
             if (y < L.h && x < L.img_pitch) {
-                const float2* src = reinterpret_cast<const float2*>(img + (long long)y * L.img_pitch + x);
+                const float4* src = reinterpret_cast<const float4*>(img + (long long)y * L.img_pitch + x);
                 v = kCoherent ? __ldcg(src) : __ldg(src);
             }
-            T.put(r, 2 * j, v.x);
-            if (2 * j + 1 < kInW) T.put(r, 2 * j + 1, v.y);
+            T.put(r, 4 * c4, v.x);
+            T.put(r, 4 * c4 + 1, v.y);
+            T.put(r, 4 * c4 + 2, v.z);
+            if (4 * c4 + 3 < kInW) T.put(r, 4 * c4 + 3, v.w);
         }
     } else {
         for (int i = threadIdx.x; i < kInH * kInW; i += blockDim.x) {
@@ -470,27 +472,24 @@ cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_level
 
 // ---------------- batched form: one persistent launch over B frames ----------------
 //
-// Every pyramid block, front tile and back tile of every frame of a batch is one item of a device
-// work queue (an atomic counter); a persistent grid pops items in queue order until none are left.
-// Items of stage s of frame f wait until every item of stage s-1 of frame f has finished (a counter
-// per (frame, stage), polled with acquire loads by one thread and a bounded number of polls); the
-// diagonal queue order puts about one frame's worth of other items between a producer stage and its
-// consumer, so the polls almost never wait. Items are popped in queue order and only wait on
-// earlier items, so every wait ends whatever the number of resident blocks. Data written earlier in
-// the launch (level images, S1 planes) is read through L2 (ld.global.cg), never the read-only path.
+// Every front tile and back tile of every level of every frame of a batch is one item of a device
+// work queue (an atomic counter); a persistent grid takes items in queue order until none are left,
+// claiming its next item while it works on the current one. Items of the back stage of frame f wait
+// until every front item of frame f has finished (a counter per (frame, stage), polled with acquire
+// loads by one thread, a bounded number of times); the diagonal queue order puts about one frame's
+// worth of other items between a frame's front tiles and its back tiles, so the polls almost never
+// wait. An item only waits on items queued before it, and a block holds at most the item it works on
+// and the one it claimed after it, so every wait ends whatever the number of resident blocks. The
+// level images come from the batched pyramid launch before; the S1 planes are written earlier in the
+// same launch and are read through L2 (ld.global.cg), never the read-only path.
 
-void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, int pyr_items, int front_items, int back_items, int gpitch,
-                       int gw, int gh, float thr) {
+void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, int front_items, int back_items, float thr) {
     q->n_frames = n_frames;
     q->n_levels = n_levels;
     q->n_chunks = n_chunks;
-    q->gpitch = gpitch;
-    q->gw = gw;
-    q->gh = gh;
     q->thr = thr;
-    q->stage_items[0] = pyr_items;
-    q->stage_items[1] = front_items;
-    q->stage_items[2] = back_items;
+    q->stage_items[0] = front_items;
+    q->stage_items[1] = back_items;
     q->wait_limit = 1 << 22;  // x 256 ns of sleep: about a second before the launch gives up
     int n = 0, first = 0;
     for (int t = 0; t < n_frames + kBatchStages - 1; ++t)
@@ -508,17 +507,6 @@ void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, 
     q->total = first;
 }
 
-// the level of item `g` of a stage: the last level whose first item (FIELD) is <= g
-template <int LevelDesc::*FIELD>
-__device__ __forceinline__ int find_level_global(const LevelDesc* __restrict__ lv, int n, int g) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (lv[mid].*FIELD <= g) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
 __device__ __forceinline__ int ld_acquire(const int* p) {
     int v;
     asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -534,13 +522,22 @@ __global__ void __launch_bounds__(256, kMinBlocks) stage1_batch_kernel(const __g
                                                               int* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item;
-    __shared__ unsigned long long s_ready;  // bit 3f+s: stage s of frame f is known complete
-    if (threadIdx.x == 0) s_ready = 0ull;
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&sync[0], 1);
-        __syncthreads();
-        const int item = s_item;
-        if (item >= Q.total) break;
+    __shared__ unsigned long long s_ready;  // bit 2f+s: stage s of frame f is known complete
+    __shared__ int s_base[kBatchStages][kMaxBatchLevels];  // first front / back item of each level
+    const int nl = Q.n_levels < kMaxBatchLevels ? Q.n_levels : kMaxBatchLevels;
+    for (int l = threadIdx.x; l < nl; l += blockDim.x) {
+        s_base[0][l] = levels[l].k1_base;
+        s_base[1][l] = levels[l].k2_base;
+    }
+    if (threadIdx.x == 0) {
+        s_ready = 0ull;
+        s_item = atomicAdd(&sync[0], 1);
+    }
+    __syncthreads();
+    int item = s_item;
+    while (item < Q.total) {
+        int next = 0;
+        if (threadIdx.x == 0) next = atomicAdd(&sync[0], 1);  // the next item, claimed while this one runs
         int sg = 0;
         while (sg + 1 < Q.n_seg && Q.seg_first[sg + 1] <= item) ++sg;
         const int stage = Q.seg_stage[sg], f = Q.seg_frame[sg], g = item - Q.seg_first[sg];
@@ -563,18 +560,17 @@ __global__ void __launch_bounds__(256, kMinBlocks) stage1_batch_kernel(const __g
                 if (threadIdx.x == 0) s_ready |= 1ull << dep;
             }
         }
+        // the level of the item: the last level whose first item is <= g
+        int lo = 0, hi = nl - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_base[stage][mid] <= g) lo = mid; else hi = mid - 1;
+        }
+        const LevelDesc& L = levels[lo];
         if (stage == 0) {
-            if (g == 0)  // the back tiles of this frame count candidates into a zeroed table
-                for (int i = threadIdx.x; i < Q.n_chunks; i += blockDim.x) F.counts[f][i] = 0;
-            const LevelDesc& L = levels[find_level_global<&LevelDesc::pyr_base>(levels, Q.n_levels, g)];
-            pyramid_block(L, g - L.pyr_base, F.gray[f], Q.gpitch, Q.gw, Q.gh, F.limg[f], F.front_on[f]);
-        } else if (stage == 1) {
-            if (!F.front_on[f] || F.front_on[f][g]) {
-                const LevelDesc& L = levels[find_level_global<&LevelDesc::k1_base>(levels, Q.n_levels, g)];
-                front_tile<true>(W, *reinterpret_cast<FrontTile*>(smem_raw), L, g - L.k1_base, F.limg[f], F.s1[f]);
-            }
+            if (!F.front_on[f] || F.front_on[f][g])
+                front_tile<false>(W, *reinterpret_cast<FrontTile*>(smem_raw), L, g - L.k1_base, F.limg[f], F.s1[f]);
         } else {
-            const LevelDesc& L = levels[find_level_global<&LevelDesc::k2_base>(levels, Q.n_levels, g)];
             back_tile<true>(W, D, *reinterpret_cast<BackSmem*>(smem_raw), L, g - L.k2_base, g, F.s1[f], F.resp[f], F.counts[f], Q.thr,
                             F.back_on[f], F.cells[f]);
         }
@@ -582,8 +578,34 @@ __global__ void __launch_bounds__(256, kMinBlocks) stage1_batch_kernel(const __g
         if (threadIdx.x == 0) {
             __threadfence();
             atomicAdd(&sync[1 + kBatchStages * f + stage], 1);
+            s_item = next;
         }
+        __syncthreads();
+        item = s_item;
     }
+}
+
+// The batched pyramid: blockIdx.y is the frame, every level of it in one grid (level bases searched
+// in global memory, no level-count limit); block 0 of a frame also zeroes its candidate counts.
+__global__ void __launch_bounds__(kPyrCols) pyramid_batch_kernel(const __grid_constant__ BatchFrames F, const LevelDesc* __restrict__ levels,
+                                                                 int n_levels, int n_chunks, int gpitch, int gw, int gh) {
+    const int f = blockIdx.y, g = blockIdx.x;
+    if (g == 0)
+        for (int i = threadIdx.x; i < n_chunks; i += blockDim.x) F.counts[f][i] = 0;
+    int lo = 0, hi = n_levels - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (levels[mid].pyr_base <= g) lo = mid; else hi = mid - 1;
+    }
+    const LevelDesc& L = levels[lo];
+    pyramid_block(L, g - L.pyr_base, F.gray[f], gpitch, gw, gh, F.limg[f], F.front_on[f]);
+}
+
+cudaError_t launch_pyramid_batch(const BatchFrames& F, const LevelDesc* d_levels, int n_levels, int n_chunks, int pyr_items, int n_frames,
+                                 int gpitch, int gw, int gh, cudaStream_t st) {
+    if (pyr_items <= 0) return cudaSuccess;
+    pyramid_batch_kernel<<<dim3(pyr_items, n_frames), kPyrCols, 0, st>>>(F, d_levels, n_levels, n_chunks, gpitch, gw, gh);
+    return cudaGetLastError();
 }
 
 int stage1_batch_blocks_per_sm(int blocks_per_sm) {
@@ -598,6 +620,7 @@ int stage1_batch_blocks_per_sm(int blocks_per_sm) {
 cudaError_t launch_stage1_batch(const Stage1W& W, const BatchFrames& F, const BatchQueue& Q, const LevelDesc* d_levels, int* sync, int* err,
                                 int grid, cudaStream_t st, int blocks_per_sm) {
     if (Q.total <= 0) return cudaSuccess;
+    if (Q.n_levels > kMaxBatchLevels) return cudaErrorInvalidValue;
     const Stage1Dup D = make_dup(W);
     grid = grid < Q.total ? grid : Q.total;
     if (blocks_per_sm >= 4)

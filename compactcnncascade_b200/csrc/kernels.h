@@ -94,18 +94,35 @@ struct BatchFrames {
     const uint8_t* back_on[kMaxBatch];
     GateCells cells[kMaxBatch];
 };
-// the work queue of a batch: segments of items, one per (stage, frame), in queue order; a stage's
-// items are its blocks in the per-frame kernels (pyramid blocks, front tiles, back tiles)
-constexpr int kBatchStages = 3;
+// the work queue of a batch: segments of items, one per (stage, frame), in queue order; the items of
+// a stage are its blocks in the per-frame kernels (stage 0 front tiles, stage 1 back tiles)
+constexpr int kBatchStages = 2;
 struct BatchQueue {
     int n_frames, n_levels, n_chunks;
-    int gpitch, gw, gh;
     float thr;
     int stage_items[kBatchStages];  // items of one frame per stage
     int n_seg, total;
     int seg_stage[kBatchStages * kMaxBatch], seg_frame[kBatchStages * kMaxBatch], seg_first[kBatchStages * kMaxBatch + 1];
     int wait_limit;                 // polls of a dependency before the launch reports an error
 };
+// builds the queue order: a diagonal wavefront over (stage, frame), so that the back tiles of frame f
+// are queued after the front tiles of frame f+1 (their producer is long done)
+void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, int front_items, int back_items, float thr);
+// sync: 1 + kBatchStages * n_frames ints, zero before the launch (queue head, finished items per
+// (frame, stage)); err: set to 1 when a dependency wait gave up (results of the batch invalid).
+// The level images must exist (launch_pyramid_batch) and the candidate counts be zero.
+cudaError_t launch_stage1_batch(const Stage1W& W, const BatchFrames& F, const BatchQueue& Q, const LevelDesc* d_levels, int* sync, int* err,
+                                int grid, cudaStream_t st, int blocks_per_sm);
+// levels of a pyramid the persistent stage-1 kernel takes (their first items live in shared memory);
+// deeper pyramids run the per-level kernels
+constexpr int kMaxBatchLevels = 256;
+// resident blocks of the persistent stage-1 kernel per SM (its grid is this times the SM count)
+int stage1_batch_blocks_per_sm(int blocks_per_sm);
+// every level image of every frame of a batch in one launch (no level-count limit), and the frames'
+// candidate counts zeroed
+cudaError_t launch_pyramid_batch(const BatchFrames& F, const LevelDesc* d_levels, int n_levels, int n_chunks, int pyr_items, int n_frames,
+                                 int gpitch, int gw, int gh, cudaStream_t st);
+
 // source of one frame of a batch (device memory, 64-byte aligned base and pitch)
 struct FrameSrc {
     const uint8_t* data;
@@ -131,16 +148,6 @@ cudaError_t launch_window_batch(const WindowNets& N, const WinBatch& B, int gpit
                                 const CascadeConfig& cfg, int grid, cudaStream_t st, int ctas_per_sm = 4);
 // the replay of every frame of a batch: block f runs args[f] (device memory)
 cudaError_t launch_replay_batch(const ReplayArgs* d_args, int n_frames, cudaStream_t st);
-// builds the queue order: a diagonal wavefront over (stage, frame), so that stage s of frame f is
-// queued after stage s of frame f-1 and stage s-1 of frame f+1 (its producer is long done)
-void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, int pyr_items, int front_items, int back_items, int gpitch,
-                       int gw, int gh, float thr);
-// sync: 1 + kBatchStages * n_frames ints, zero before the launch (queue head, finished items per
-// (frame, stage)); err: set to 1 when a dependency wait gave up (results of the batch invalid)
-cudaError_t launch_stage1_batch(const Stage1W& W, const BatchFrames& F, const BatchQueue& Q, const LevelDesc* d_levels, int* sync, int* err,
-                                int grid, cudaStream_t st, int blocks_per_sm);
-// resident blocks of the persistent stage-1 kernel per SM (its grid is this times the SM count)
-int stage1_batch_blocks_per_sm(int blocks_per_sm);
 
 // register budget of the stage-1 kernels: resident 256-thread blocks per SM (3 or 4), a schedule knob
 struct Stage1Sched {
