@@ -20,7 +20,10 @@
 // pairs: all warps evaluate them into bit matrices first, and warp 0 then replays the order-
 // dependent decisions with one ballot over the bit words per candidate. Levels with more than
 // kBitMax candidates take the direct route (warp 0 tests the appended boxes 32 at a time). The sort
-// permutes (scale, index) keys, and the clustering runs in warp 0.
+// permutes (scale, index) keys. The first clustering pass runs per group of boxes that cannot
+// interact (a warp a group), the second on bit matrices of its pair tests; lists too long for the
+// shared scratch take one warp through the reference's loop.
+#include <climits>
 #include <vector>
 
 #include "kernels.h"
@@ -192,6 +195,267 @@ __device__ int merger_warp(const Det* in, int n, uint8_t* checked, Det* out, flo
     return nout;
 }
 
+// ---- the first merge by independent groups ----
+// Merger(0.5, false) grows a cluster box as the bounding box of the boxes it absorbed, and a box
+// only merges into a cluster box it overlaps. Split the boxes into groups whose bounding boxes do not
+// overlap each other (the overlap relation closed under bounding boxes): no cluster box of one group
+// can then overlap a box of another, so each group runs the reference's loop on its own and the
+// clusters, listed by their first box, come out in the order of the single loop.
+
+// concurrent union-find in shared memory: parent[x] <= x, roots have parent[x] == x. Linking CASes
+// the larger root onto the smaller and retries from the value found (the hooking of Jaiganesh and
+// Burtscher's ECL-CC, SC'18); roots only ever move to a smaller index, so a compression write, even
+// a late one, still points at an ancestor.
+__device__ __forceinline__ int uf_root(volatile int* parent, int x) {
+    int cur = parent[x];
+    if (cur != x) {
+        int prev = x, next;
+        while (cur > (next = parent[cur])) {
+            parent[prev] = next;
+            prev = cur;
+            cur = next;
+        }
+    }
+    return cur;
+}
+
+__device__ __forceinline__ bool uf_hook(volatile int* parent, int a, int b) {
+    int ra = uf_root(parent, a), rb = uf_root(parent, b);
+    while (ra != rb) {
+        if (ra < rb) {
+            const int t = ra;
+            ra = rb;
+            rb = t;
+        }
+        const int old = atomicCAS(const_cast<int*>(parent + ra), ra, rb);
+        if (old == ra) return true;
+        ra = old;
+    }
+    return false;
+}
+
+// The reference's loop over the boxes of group r (parent[j] == r) by one warp, as merger_warp does
+// for the whole list; seed_box[i1] / seed_of[j]: the merged box of the cluster that box i1 starts,
+// the first box of the cluster that absorbed box j.
+__device__ void merge_group_warp(const Det* in, int n, const int* parent, int r, uint8_t* checked, Det* seed_box, int* seed_of) {
+    const int lane = threadIdx.x & 31;
+    for (int cb = r & ~31; cb < n; cb += 32) {
+        const int jj = cb + lane;
+        unsigned mm = __ballot_sync(0xffffffffu, jj < n && jj >= r && parent[jj] == r);
+        while (mm) {
+            const int i1 = cb + __ffs(mm) - 1;
+            mm &= mm - 1;
+            if (checked[i1]) continue;
+            Det nmax = in[i1], nmin = in[i1];
+            for (int base = i1 + 1; base < n; base += 32) {
+                const int j = base + lane;
+                bool live = j < n && parent[j] == r && !checked[j];
+                if (!__any_sync(0xffffffffu, live)) continue;
+                const Det e = live ? in[j] : nmax;
+                int start = 0;
+                while (true) {
+                    const MergeTest mt = merge_test(nmax, e, 0.5f);
+                    const unsigned m = __ballot_sync(0xffffffffu, live && lane >= start && mt.hit);
+                    if (!m) break;
+                    const int f = __ffs(m) - 1;
+                    const Det ef = in[base + f];
+                    int X[4] = {nmax.x, nmax.x2, ef.x, ef.x2};
+                    int Y[4] = {nmax.y, nmax.y2, ef.y, ef.y2};
+                    sort4(X);
+                    sort4(Y);
+                    nmax.x = imin(nmax.x, X[0]);
+                    nmax.y = imin(nmax.y, Y[0]);
+                    nmax.x2 = imax(nmax.x2, X[3]);
+                    nmax.y2 = imax(nmax.y2, Y[3]);
+                    nmin.x = imax(nmin.x, X[1]);
+                    nmin.y = imax(nmin.y, Y[1]);
+                    nmin.x2 = imin(nmin.x2, X[2]);
+                    nmin.y2 = imin(nmin.y2, Y[2]);
+                    nmax.score = (nmax.score < ef.score) ? ef.score : nmax.score;
+                    nmax.knn = imax(nmax.knn, ef.knn);
+                    nmax.scale = (nmax.scale > ef.scale) ? ef.scale : nmax.scale;
+                    nmax.num_detect++;
+                    if (lane == f) {
+                        checked[j] = 1;
+                        live = false;
+                        seed_of[j] = i1;
+                    }
+                    start = f + 1;
+                }
+                __syncwarp();
+            }
+            Det rr = nmax;
+            rr.x = (nmin.x + nmax.x) >> 1;
+            rr.y = (nmin.y + nmax.y) >> 1;
+            rr.x2 = (nmin.x2 + nmax.x2) >> 1;
+            rr.y2 = (nmin.y2 + nmax.y2) >> 1;
+            rr.w = rr.x2 - rr.x;
+            rr.h = rr.y2 - rr.y;
+            if (lane == 0) {
+                seed_of[i1] = i1;
+                seed_box[i1] = rr;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Merger(0.5, false) of n <= kGroupMax sorted boxes by the whole block; returns the cluster count
+// (every thread). out: the clusters in reference order; seed_box: n Det of scratch; clus (optional):
+// cluster of every box; ws_a / ws_b: 4n / 3n ints of shared memory.
+constexpr int kGroupMax = 512;
+__device__ int first_merge_groups(const Det* in, int n, uint8_t* checked, Det* out, Det* seed_box, int* clus, int* ws_a, int* ws_b) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    volatile int* parent = ws_a;
+    int* bx0 = ws_a + n;
+    int* by0 = ws_a + 2 * n;
+    int* bx1 = ws_a + 3 * n;
+    int* by1 = ws_b;
+    int* seed_of = ws_b + n;
+    int* rank_of = ws_b + 2 * n;
+    __shared__ int s_groups;
+    for (int j = tid; j < n; j += blockDim.x) {
+        parent[j] = j;
+        checked[j] = 0;
+    }
+    __syncthreads();
+    // boxes that overlap or touch share a group
+    for (int i = warp; i < n; i += nwarps) {
+        const Det bi = in[i];
+        const int ax0 = imin(bi.x, bi.x2), ax1 = imax(bi.x, bi.x2), ay0 = imin(bi.y, bi.y2), ay1 = imax(bi.y, bi.y2);
+        for (int j = i + 1 + lane; j < n; j += 32) {
+            const Det bj = in[j];
+            if (ax0 <= imax(bj.x, bj.x2) && imin(bj.x, bj.x2) <= ax1 && ay0 <= imax(bj.y, bj.y2) && imin(bj.y, bj.y2) <= ay1)
+                uf_hook(parent, i, j);
+        }
+    }
+    __syncthreads();
+    // groups whose bounding boxes overlap or touch are joined until none do
+    for (;;) {
+        for (int j = tid; j < n; j += blockDim.x) {
+            int v = parent[j];
+            while (v != parent[v]) v = parent[v];
+            parent[j] = v;  // only this thread writes parent[j] in this pass
+            bx0[j] = by0[j] = INT_MAX;
+            bx1[j] = by1[j] = INT_MIN;
+        }
+        __syncthreads();
+        for (int j = tid; j < n; j += blockDim.x) {
+            const Det b = in[j];
+            const int g = parent[j];
+            atomicMin(&bx0[g], imin(b.x, b.x2));
+            atomicMin(&by0[g], imin(b.y, b.y2));
+            atomicMax(&bx1[g], imax(b.x, b.x2));
+            atomicMax(&by1[g], imax(b.y, b.y2));
+        }
+        __syncthreads();
+        bool linked = false;
+        for (int i = warp; i < n; i += nwarps) {
+            if (parent[i] != i) continue;
+            for (int j = i + 1 + lane; j < n; j += 32)
+                if (parent[j] == j && bx0[i] <= bx1[j] && bx0[j] <= bx1[i] && by0[i] <= by1[j] && by0[j] <= by1[i])
+                    linked |= uf_hook(parent, i, j);
+        }
+        if (!__syncthreads_or(linked)) break;
+    }
+    // a pass without links left every parent a root: group g = the root; warp w takes the groups
+    // w, w + nwarps, ... in order of their roots
+    int ord = 0;
+    for (int cb = 0; cb < n; cb += 32) {
+        const int j = cb + lane;
+        unsigned rm = __ballot_sync(0xffffffffu, j < n && parent[j] == j);
+        while (rm) {
+            const int g = cb + __ffs(rm) - 1;
+            rm &= rm - 1;
+            if (ord++ % nwarps == warp) merge_group_warp(in, n, const_cast<const int*>(ws_a), g, checked, seed_box, seed_of);
+        }
+    }
+    __syncthreads();
+    // clusters ranked by their first box
+    if (warp == 0) {
+        int w = 0;
+        for (int cb = 0; cb < n; cb += 32) {
+            const int j = cb + lane;
+            const bool s = j < n && seed_of[j] == j;
+            const unsigned m = __ballot_sync(0xffffffffu, s);
+            if (s) rank_of[j] = w + __popc(m & ((1u << lane) - 1u));
+            w += __popc(m);
+        }
+        if (lane == 0) s_groups = w;
+    }
+    __syncthreads();
+    const int nM = s_groups;
+    for (int j = tid; j < n; j += blockDim.x) {
+        const int s = seed_of[j];
+        if (s == j) out[rank_of[j]] = seed_box[j];
+        if (clus) clus[j] = rank_of[s];
+    }
+    __syncthreads();
+    return nM;
+}
+
+// Merger(0.2, true) of n <= 256 boxes by the whole block. With deletion a box never grows, so each
+// pair test depends on the two boxes only: bit j of word w of row i (j = 32w + bit > i) is set in
+// `take` when box i deletes box j (the test hits and box i is larger), in `drop` when box j deletes
+// box i. The reference's loop then runs on bit sets in warp 0: a box not yet deleted deletes its live
+// `take` boxes up to its first live `drop` box, and is itself dropped if there is one.
+// take / drop: n * ceil(n / 32) words each. Returns the output count (every thread).
+__device__ int second_merge_bits(const Det* in, int n, Det* out, int* src, uint32_t* take, uint32_t* drop) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int W = (n + 31) >> 5;
+    __shared__ int s_out;
+    for (int it = warp; it < n * W; it += nwarps) {
+        const int i = it / W, w = it - i * W;
+        const int j = 32 * w + lane;
+        bool hit = false, gt = false;
+        if (j > i && j < n) {
+            const MergeTest mt = merge_test(in[i], in[j], 0.2f);
+            hit = mt.hit;
+            gt = mt.s1_gt_s2;
+        }
+        const uint32_t bt = __ballot_sync(0xffffffffu, hit && gt), bd = __ballot_sync(0xffffffffu, hit && !gt);
+        if (lane == 0) {
+            take[it] = bt;
+            drop[it] = bd;
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t del = 0u;  // lane w < W: the deleted boxes of word w
+        int nout = 0;
+        for (int i = 0; i < n; ++i) {
+            if ((__shfl_sync(0xffffffffu, del, i >> 5) >> (i & 31)) & 1u) continue;
+            const uint32_t t = lane < W ? take[i * W + lane] & ~del : 0u;
+            const uint32_t d = lane < W ? drop[i * W + lane] & ~del : 0u;
+            const unsigned dm = __ballot_sync(0xffffffffu, d != 0u);
+            if (dm) {
+                const int wf = __ffs(dm) - 1;
+                const uint32_t first = __shfl_sync(0xffffffffu, d, wf);
+                if (lane < wf) del |= t;
+                else if (lane == wf) del |= t & ((1u << (__ffs(first) - 1)) - 1u);
+                continue;
+            }
+            del |= t;
+            if (lane == 0) {
+                const Det b = in[i];
+                Det rr = b;
+                rr.x = (b.x + b.x) >> 1;
+                rr.y = (b.y + b.y) >> 1;
+                rr.x2 = (b.x2 + b.x2) >> 1;
+                rr.y2 = (b.y2 + b.y2) >> 1;
+                rr.w = rr.x2 - rr.x;
+                rr.h = rr.y2 - rr.y;
+                out[nout] = rr;
+                if (src) src[nout] = i;
+            }
+            nout++;
+        }
+        if (lane == 0) s_out = nout;
+    }
+    __syncthreads();
+    return s_out;
+}
+
 constexpr int kMaxLevels = 1024;
 
 
@@ -297,6 +561,30 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
             }
             const int m = e - g;
             const int W = (m + 31) >> 5;
+            // box of candidate i of the level: its rect, score/knn from the end of its copy chain;
+            // facial data travels with a candidate's own accepted box, not with copies
+            auto emit_box = [&](int i) {
+                int r = i, src = s_src[i];
+                while (src < 0 && src > kOwnVerdict) {  // a box of this level: follow it
+                    r = -1 - src;
+                    src = s_src[r];
+                }
+                float sc;
+                int kn;
+                if (src >= 0) {
+                    sc = D[src].score;
+                    kn = D[src].knn;
+                } else if (src == kOwnVerdict) {
+                    sc = res[g + r].score;
+                    kn = res[g + r].knn;
+                } else {
+                    sc = cands[g + r].score;
+                    kn = 0;
+                }
+                const Det nr = cand_rect(cands[g + i], inv_scale, scale, C.pat_w, C.pat_h);
+                D[s_didx[i]] = make_det(nr.x, nr.y, nr.w, nr.h, sc, scale, kn);
+                if (a.fa_scratch) a.fa_scratch[s_didx[i]] = (s_src[i] == kOwnVerdict) ? g + i : -1;
+            };
             if (m <= kBitMax) {
                 // candidate-pair tests of this level, one ballot per (row i, word w)
                 for (int it = warp; it < m * W; it += kRT / 32) {
@@ -315,166 +603,184 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
                 }
             }
             __syncthreads();
-            if (m <= kBitMax) {
-                // The order-dependent decisions of the level as fixed points over candidate sets (bit
-                // j of word w = candidate 32w + j). Candidate i's decision depends only on candidates
-                // j < i, so after t rounds the first t candidates are final, and a round that changes
-                // nothing has reached the unique solution, which is the sequential one.
-                //   S: boxes appended during the scan: the first decisive box of candidate i (earlier
-                //      levels first, then S in order) has drop type 1;
-                //   T: boxes appended by the survivors' pass: survivor i overlaps (> 0.5) a box of T
-                //      (a copy), or its stage-2/3 verdict accepts it (or detection is disabled).
-                // Warp 0 runs both fixed points alone (lane l holds candidates l, l + 32, ...): a round
-                // is one ballot per word, with no block-wide barrier.
+            // The order-dependent decisions of the level as fixed points over candidate sets (bit j of
+            // word w = candidate 32w + j). Candidate i's decision depends only on candidates j < i, so
+            // after t rounds the first t candidates are final, and a round that changes nothing has
+            // reached the unique solution, which is the sequential one.
+            //   S: boxes appended during the scan: the first decisive box of candidate i (earlier
+            //      levels first, then S in order) has drop type 1;
+            //   T: boxes appended by the survivors' pass: survivor i overlaps (> 0.5) a box of T
+            //      (a copy), or its stage-2/3 verdict accepts it (or detection is disabled).
+            const bool check = C.detect_enabled != 0;
+            if (m <= 32) {
+                // one word: warp 0 alone, candidate i = lane, its rows and decisions in registers;
+                // a round is one ballot
                 if (warp == 0) {
-                    const bool check = C.detect_enabled != 0;
-                    auto a1 = [&](int i, int w) { return s_a1[i * W + w]; };
-                    auto a2 = [&](int i, int w) { return s_a2[i * W + w]; };
-                    auto code_of = [&](int i) { return first_dec[g + i]; };
-                    auto acc_of = [&](int i) {
-                        int acc = C.detect_enabled ? res[g + i].accepted : 1;
+                    const int i = lane;
+                    const bool valid = i < m;
+                    int code = -1, acc = 0;
+                    uint32_t r1 = 0u, r2 = 0u;
+                    if (valid) {
+                        code = first_dec[g + i];
+                        acc = C.detect_enabled ? res[g + i].accepted : 1;
                         if (acc && a.attr && a.attr[g + i].x) acc = 0;  // facial analysis dropped it
-                        return acc;
-                    };
-                    // first decisive box of the level among set X: its bit word and drop type
-                    auto in_scan = [&](int i) {
-                        const int code = code_of(i);
-                        if (code >= 0) return (code & 1) == 0;
-                        for (int w = 0; w < W; ++w) {
-                            const uint32_t hit = (a1(i, w) | a2(i, w)) & s_S[w];
-                            if (hit) return ((a1(i, w) >> (__ffs(hit) - 1)) & 1u) != 0u;
-                        }
-                        return false;
-                    };
-                    if (lane < kBitWords) {
-                        s_S[lane] = 0u;
-                        s_T[lane] = 0u;
+                        r1 = s_a1[i];
+                        r2 = s_a2[i];
                     }
-                    __syncwarp();
+                    uint32_t S = 0u;
                     for (int round = 0; round <= m; ++round) {
-                        uint32_t nw[kBitWords];
-                        bool changed = false;
-#pragma unroll
-                        for (int q = 0; q < kBitWords; ++q) {
-                            const int i = lane + 32 * q;
-                            nw[q] = __ballot_sync(0xffffffffu, q < W && i < m && in_scan(i));
-                            changed |= q < W && nw[q] != s_S[q];
+                        bool in = false;
+                        if (valid) {
+                            if (code >= 0) {
+                                in = (code & 1) == 0;
+                            } else {
+                                const uint32_t hit = (r1 | r2) & S;
+                                if (hit) in = ((r1 >> (__ffs(hit) - 1)) & 1u) != 0u;
+                            }
                         }
-                        __syncwarp();
-#pragma unroll
-                        for (int q = 0; q < kBitWords; ++q)
-                            if (lane == q && q < W) s_S[q] = nw[q];
-                        __syncwarp();
-                        if (!changed) break;
+                        const uint32_t nS = __ballot_sync(0xffffffffu, in);
+                        if (nS == S) break;
+                        S = nS;
                     }
                     // survivors: not decided by the scan
-                    auto survivor = [&](int i) {
-                        if (code_of(i) >= 0) return false;
-                        for (int w = 0; w < W; ++w)
-                            if ((a1(i, w) | a2(i, w)) & s_S[w]) return false;
-                        return true;
-                    };
-                    uint32_t surv_w[kBitWords];
-#pragma unroll
-                    for (int q = 0; q < kBitWords; ++q) {
-                        const int i = lane + 32 * q;
-                        surv_w[q] = __ballot_sync(0xffffffffu, q < W && i < m && survivor(i));
-                    }
+                    const bool surv_i = valid && code < 0 && ((r1 | r2) & S) == 0u;
+                    uint32_t T = 0u;
                     for (int round = 0; round <= m; ++round) {
-                        uint32_t nw[kBitWords];
-                        bool changed = false;
-#pragma unroll
-                        for (int q = 0; q < kBitWords; ++q) {
-                            const int i = lane + 32 * q;
-                            bool in = false;
-                            if (q < W && i < m && ((surv_w[q] >> lane) & 1u)) {
-                                in = acc_of(i) != 0;
-                                if (check)
-                                    for (int w = 0; w < W && !in; ++w) in = (a1(i, w) & s_T[w]) != 0u;
-                            }
-                            nw[q] = __ballot_sync(0xffffffffu, in);
-                            changed |= q < W && nw[q] != s_T[q];
-                        }
-                        __syncwarp();
-#pragma unroll
-                        for (int q = 0; q < kBitWords; ++q)
-                            if (lane == q && q < W) s_T[q] = nw[q];
-                        __syncwarp();
-                        if (!changed) break;
+                        const bool in = surv_i && (acc != 0 || (check && (r1 & T) != 0u));
+                        const uint32_t nT = __ballot_sync(0xffffffffu, in);
+                        if (nT == T) break;
+                        T = nT;
                     }
                     // D index (scan appends in candidate order, then the survivors' appends) and the
                     // source of each box's score/knn
-                    int nScan = 0, nSurv = 0;
-                    for (int w = 0; w < W; ++w) {
-                        nScan += __popc(s_S[w]);
-                        nSurv += __popc(s_T[w]);
-                    }
-                    for (int i = lane; i < m; i += 32) {
-                        const uint32_t below = (1u << (i & 31)) - 1u;
-                        const int code = code_of(i);
+                    const int nScan = __popc(S);
+                    const uint32_t below = (1u << i) - 1u;
+                    if (valid) {
                         int dst = -1, src = 0;
-                        if ((s_S[i >> 5] >> (i & 31)) & 1u) {
-                            int r = 0;
-                            for (int w = 0; w < (i >> 5); ++w) r += __popc(s_S[w]);
-                            dst = nD + r + __popc(s_S[i >> 5] & below);
-                            if (code >= 0) {
-                                src = code >> 1;
-                            } else {
-                                for (int w = 0; w < W; ++w) {
-                                    const uint32_t hit = (a1(i, w) | a2(i, w)) & s_S[w];
-                                    if (hit) {
-                                        src = -1 - (32 * w + __ffs(hit) - 1);
-                                        break;
-                                    }
-                                }
-                            }
-                        } else if ((s_T[i >> 5] >> (i & 31)) & 1u) {
-                            int r = 0;
-                            for (int w = 0; w < (i >> 5); ++w) r += __popc(s_T[w]);
-                            dst = nD + nScan + r + __popc(s_T[i >> 5] & below);
+                        if ((S >> i) & 1u) {
+                            dst = nD + __popc(S & below);
+                            src = code >= 0 ? (code >> 1) : -1 - (__ffs((r1 | r2) & S) - 1);
+                        } else if ((T >> i) & 1u) {
+                            dst = nD + nScan + __popc(T & below);
                             src = C.detect_enabled ? kOwnVerdict : kOwnScore;
-                            if (check)
-                                for (int w = 0; w < W; ++w) {
-                                    const uint32_t hit = a1(i, w) & s_T[w];
-                                    if (hit) {
-                                        src = -1 - (32 * w + __ffs(hit) - 1);
-                                        break;
-                                    }
-                                }
+                            if (check && (r1 & T)) src = -1 - (__ffs(r1 & T) - 1);
                         }
                         s_didx[i] = dst;
                         s_src[i] = src;
                     }
                     __syncwarp();
-                    // the boxes: rect of the candidate, score/knn from the end of its copy chain
-                    for (int i = lane; i < m; i += 32) {
-                        if (s_didx[i] < 0) continue;
-                        int r = i, src = s_src[i];
-                        while (src < 0 && src > kOwnVerdict) {  // a box of this level: follow it
-                            r = -1 - src;
-                            src = s_src[r];
-                        }
-                        float sc;
-                        int kn;
-                        if (src >= 0) {
-                            sc = D[src].score;
-                            kn = D[src].knn;
-                        } else if (src == kOwnVerdict) {
-                            sc = res[g + r].score;
-                            kn = res[g + r].knn;
-                        } else {
-                            sc = cands[g + r].score;
-                            kn = 0;
-                        }
-                        const Det nr = cand_rect(cands[g + i], inv_scale, scale, C.pat_w, C.pat_h);
-                        D[s_didx[i]] = make_det(nr.x, nr.y, nr.w, nr.h, sc, scale, kn);
-                        // facial data travels with a candidate's own accepted box, not with copies
-                        if (a.fa_scratch) a.fa_scratch[s_didx[i]] = (s_src[i] == kOwnVerdict) ? g + i : -1;
-                    }
-                    if (lane == 0) s_nD = nD + nScan + nSurv;
+                    if (valid && s_didx[i] >= 0) emit_box(i);
+                    if (lane == 0) s_nD = nD + nScan + __popc(T);
                 }
                 __syncthreads();
                 nD = s_nD;
+                continue;
+            }
+            if (m <= kBitMax) {
+                // several words: a thread a candidate (m <= 256: warps 0..7), block-wide rounds
+                const bool thread_item = tid < m;
+                const int i = tid;
+                int code = -1, acc = 0;
+                if (thread_item) {
+                    code = first_dec[g + i];
+                    acc = C.detect_enabled ? res[g + i].accepted : 1;
+                    if (acc && a.attr && a.attr[g + i].x) acc = 0;  // facial analysis dropped it
+                }
+                if (tid < kBitWords) {
+                    s_S[tid] = 0u;
+                    s_T[tid] = 0u;
+                }
+                __syncthreads();
+                bool inS = false;
+                for (int round = 0; round <= m; ++round) {
+                    bool in = false;
+                    if (thread_item) {
+                        if (code >= 0) {
+                            in = (code & 1) == 0;
+                        } else {
+                            for (int w = 0; w < W; ++w) {
+                                const uint32_t hit = (s_a1[i * W + w] | s_a2[i * W + w]) & s_S[w];
+                                if (hit) {
+                                    in = (s_a1[i * W + w] >> (__ffs(hit) - 1)) & 1u;
+                                    break;
+                                }
+                            }
+                        }
+                    }
+                    const uint32_t word = __ballot_sync(0xffffffffu, in);
+                    __syncthreads();  // every thread has read the previous round's S
+                    const bool changed = (lane == 0 && warp < W && s_S[warp] != word);
+                    if (lane == 0 && warp < W) s_S[warp] = word;
+                    inS = in;
+                    if (!__syncthreads_or(changed)) break;
+                }
+                // survivors: not decided by the scan
+                bool surv_i = false;
+                if (thread_item && code < 0) {
+                    surv_i = true;
+                    for (int w = 0; w < W; ++w)
+                        if ((s_a1[i * W + w] | s_a2[i * W + w]) & s_S[w]) {
+                            surv_i = false;
+                            break;
+                        }
+                }
+                for (int round = 0; round <= m; ++round) {
+                    bool in = false;
+                    if (surv_i) {
+                        in = acc != 0;
+                        if (check)
+                            for (int w = 0; w < W && !in; ++w) in = (s_a1[i * W + w] & s_T[w]) != 0u;
+                    }
+                    const uint32_t word = __ballot_sync(0xffffffffu, in);
+                    __syncthreads();
+                    const bool changed = (lane == 0 && warp < W && s_T[warp] != word);
+                    if (lane == 0 && warp < W) s_T[warp] = word;
+                    if (!__syncthreads_or(changed)) break;
+                }
+                int nScan = 0, nSurv = 0;
+                for (int w = 0; w < W; ++w) {
+                    nScan += __popc(s_S[w]);
+                    nSurv += __popc(s_T[w]);
+                }
+                if (thread_item) {
+                    const uint32_t below = (1u << (i & 31)) - 1u;
+                    int dst = -1, src = 0;
+                    if (inS) {
+                        int r = 0;
+                        for (int w = 0; w < (i >> 5); ++w) r += __popc(s_S[w]);
+                        dst = nD + r + __popc(s_S[i >> 5] & below);
+                        if (code >= 0) {
+                            src = code >> 1;
+                        } else {
+                            for (int w = 0; w < W; ++w) {
+                                const uint32_t hit = (s_a1[i * W + w] | s_a2[i * W + w]) & s_S[w];
+                                if (hit) {
+                                    src = -1 - (32 * w + __ffs(hit) - 1);
+                                    break;
+                                }
+                            }
+                        }
+                    } else if ((s_T[i >> 5] >> (i & 31)) & 1u) {
+                        int r = 0;
+                        for (int w = 0; w < (i >> 5); ++w) r += __popc(s_T[w]);
+                        dst = nD + nScan + r + __popc(s_T[i >> 5] & below);
+                        src = C.detect_enabled ? kOwnVerdict : kOwnScore;
+                        if (check)
+                            for (int w = 0; w < W; ++w) {
+                                const uint32_t hit = s_a1[i * W + w] & s_T[w];
+                                if (hit) {
+                                    src = -1 - (32 * w + __ffs(hit) - 1);
+                                    break;
+                                }
+                            }
+                    }
+                    s_didx[i] = dst;
+                    s_src[i] = src;
+                }
+                __syncthreads();
+                if (thread_item && s_didx[i] >= 0) emit_box(i);
+                nD += nScan + nSurv;
+                __syncthreads();
                 continue;
             }
             if (warp == 0) {
@@ -602,28 +908,41 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
     }
     __syncthreads();
 
-    // post-processing in warp 0
-    if (warp != 0) return;
-    if (lane == 0) {
+    // post-processing: the two merges by the whole block where their scratch fits in the bit-matrix
+    // words (free after the level loop and the sort), else in warp 0
+    __shared__ int s_nM;
+    if (tid == 0) {
         *a.n_raw = nD;
         if (a.n_m_out) *a.n_m_out = 0;
     }
-    __syncwarp();
     int nF = 0;
     const Det* fin = R;
-    if (nD > 0) {
-        int* fa = a.fa_scratch;
-        const int cap = a.face_cap;
-        int* clus = fa ? fa + 2 * cap : nullptr;  // cluster of every sorted box
-        int* keepmap = fa ? fa + 3 * cap : nullptr;  // first-merge cluster of every kept box
-        int* fsrc = fa ? fa + 4 * cap : nullptr;     // kept box of every final box
-        if (C.merger_detect) {
-            int nM = merger_warp(R, nD, checked, M, 0.5f, false, clus);
-            if (keepmap)
-                for (int k = lane; k < nM; k += 32) keepmap[k] = k;
-            __syncwarp();
-            if (C.min_num_detect > 1) {
-                // stable erase of clusters with fewer than min_num_detect merges
+    int* fa = a.fa_scratch;
+    const int cap = a.face_cap;
+    int* clus = fa ? fa + 2 * cap : nullptr;     // cluster of every sorted box
+    int* keepmap = fa ? fa + 3 * cap : nullptr;  // first-merge cluster of every kept box
+    int* fsrc = fa ? fa + 4 * cap : nullptr;     // kept box of every final box
+    uint32_t* ws_a = reinterpret_cast<uint32_t*>(s_a1);
+    uint32_t* ws_b = reinterpret_cast<uint32_t*>(s_a2);
+    if (nD > 0 && C.merger_detect) {
+        int nM;
+        if (nD <= kGroupMax) {
+            // F is scratch here (the first box of every cluster's merged box) until the second merge
+            nM = first_merge_groups(R, nD, checked, M, F, clus, reinterpret_cast<int*>(ws_a), reinterpret_cast<int*>(ws_b));
+        } else {
+            if (warp == 0) {
+                const int k = merger_warp(R, nD, checked, M, 0.5f, false, clus);
+                if (lane == 0) s_nM = k;
+            }
+            __syncthreads();
+            nM = s_nM;
+        }
+        if (keepmap)
+            for (int k = tid; k < nM; k += kRT) keepmap[k] = k;
+        __syncthreads();
+        if (C.min_num_detect > 1) {
+            // stable erase of clusters with fewer than min_num_detect merges
+            if (warp == 0) {
                 int w = 0;
                 for (int base = 0; base < nM; base += 32) {
                     const int kk = base + lane;
@@ -639,32 +958,41 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
                     __syncwarp();
                     w += __popc(m);
                 }
-                nM = w;
+                if (lane == 0) s_nM = w;
             }
-            if (a.m_out) {
-                for (int k = lane; k < nM; k += 32) a.m_out[k] = M[k];
-                if (lane == 0) *a.n_m_out = nM;
-                __syncwarp();
-            }
-            if (nM > 0) {
-                nF = merger_warp(M, nM, checked, F, 0.2f, true, nullptr, fsrc);
-                fin = F;
-            } else {
-                nF = 0;
-            }
-        } else {
-            if (fa)
-                for (int k = lane; k < nD; k += 32) {
-                    clus[k] = k;
-                    keepmap[k] = k;
-                    fsrc[k] = k;
-                }
-            __syncwarp();
-            nF = nD;
-            fin = R;
+            __syncthreads();
+            nM = s_nM;
         }
+        if (a.m_out) {
+            for (int k = tid; k < nM; k += kRT) a.m_out[k] = M[k];
+            if (tid == 0) *a.n_m_out = nM;
+        }
+        if (nM > 0) {
+            if (nM <= kBitMax) {
+                nF = second_merge_bits(M, nM, F, fsrc, ws_a, ws_b);
+            } else {
+                __syncthreads();
+                if (warp == 0) {
+                    const int k = merger_warp(M, nM, checked, F, 0.2f, true, nullptr, fsrc);
+                    if (lane == 0) s_nM = k;
+                }
+                __syncthreads();
+                nF = s_nM;
+            }
+            fin = F;
+        }
+    } else if (nD > 0) {
+        if (fa)
+            for (int k = tid; k < nD; k += kRT) {
+                clus[k] = k;
+                keepmap[k] = k;
+                fsrc[k] = k;
+            }
+        nF = nD;
+        fin = R;
     }
-    for (int i = lane; i < nF && i < a.face_cap; i += 32) {
+    __syncthreads();
+    for (int i = tid; i < nF && i < a.face_cap; i += kRT) {
         const Det d = fin[i];
         FaceOut f;
         if (C.rescale_output) {
@@ -721,7 +1049,7 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
         }
         a.faces[i] = f;
     }
-    if (lane == 0) *a.n_faces = nF;
+    if (tid == 0) *a.n_faces = nF;
 }
 
 // Detect with the caller's detections in front (cnn_detector_v3.cpp:2753-2806), one warp: the
