@@ -11,10 +11,11 @@ The knobs (include/ccnn_inspect.h, ccnn_schedule):
   batch_frames         frames per batched graph (0: every frame its own graph; 1: the same with the
                        pyramid and stage 1 of all levels in one persistent launch); the batched form
                        runs the pyramid and stage 1 of a whole group in one persistent launch
-  batch_blocks_per_sm  register budget of that persistent kernel (3 or 4)
+  batch_blocks_per_sm  resident blocks per SM of that persistent kernel (its grid; 4: 64 registers,
+                       1-3: 80; fewer leave SMs to other frames' kernels)
 
 The search is coordinate descent from the defaults: each knob in turn takes the value that times
-fastest with the others held, for two passes (a full product of the knobs would be 96 timings).
+fastest with the others held, for two passes (a full product of the knobs would be 960 timings).
 
     python -m compactcnncascade_b200.autotune --width 1920 --height 1080
 """
@@ -28,7 +29,7 @@ from . import _capi
 
 TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "schedules.json")
 KNOBS = (("frame_slots", (4, 8, 12, 16)), ("window_ctas_per_sm", (2, 3, 4)), ("front_blocks_per_sm", (3, 4)),
-         ("back_blocks_per_sm", (3, 4)), ("batch_frames", (0, 1, 2, 4, 8)), ("batch_blocks_per_sm", (3, 4)))
+         ("back_blocks_per_sm", (3, 4)), ("batch_frames", (0, 1, 2, 4, 8)), ("batch_blocks_per_sm", (1, 2, 3, 4)))
 DEFAULTS = {"frame_slots": 8, "window_ctas_per_sm": 4, "front_blocks_per_sm": 3, "back_blocks_per_sm": 4, "batch_frames": 0,
             "batch_blocks_per_sm": 3}
 

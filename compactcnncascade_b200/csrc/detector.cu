@@ -609,10 +609,11 @@ ccnn_status Detector::set_schedule(int frame_slots, int window_ctas_per_sm, int 
     const int slots = frame_slots > 0 ? frame_slots : (int)slots_.size();
     const int batch = batch_frames >= 0 ? batch_frames : batch_frames_;
     if (frame_slots < 0 || frame_slots > 64 || window_ctas_per_sm < 0 || window_ctas_per_sm > 4 || (front_bpsm != 0 && (front_bpsm < 3 || front_bpsm > 4)) ||
-        (back_bpsm != 0 && (back_bpsm < 3 || back_bpsm > 4)) || (batch_bpsm != 0 && (batch_bpsm < 3 || batch_bpsm > 4)) || batch > kMaxBatch ||
+        (back_bpsm != 0 && (back_bpsm < 3 || back_bpsm > 4)) || (batch_bpsm != 0 && (batch_bpsm < 1 || batch_bpsm > 4)) || batch > kMaxBatch ||
         (batch > 1 && slots < batch)) {
-        set_error("schedule: 1-64 frame slots, 1-4 stage-2/3 blocks per SM, 3-4 stage-1 blocks per SM, batches of 0-16 frames and "
-                  "at least as many frame slots as frames per batch (0 keeps the current value)");
+        set_error("schedule: 1-64 frame slots, 1-4 stage-2/3 blocks per SM, 3-4 stage-1 blocks per SM, batches of 0-16 frames, "
+                  "1-4 persistent stage-1 blocks per SM and at least as many frame slots as frames per batch (0 keeps the "
+                  "current value)");
         return CCNN_ERR_INVALID_ARG;
     }
     clear();

@@ -200,7 +200,7 @@ class Detector {
     int batch_frames_ = 0;           // frames per batched launch (0: every frame its own graph; 1: every frame
                                      // its own graph with the pyramid and stage 1 in one persistent launch)
     bool single_launch_stage1() const;
-    int batch_bpsm_ = 3;             // register budget of the persistent batched stage-1 kernel
+    int batch_bpsm_ = 3;             // resident blocks per SM (grid) of the persistent stage-1 kernel
     std::vector<BatchCtx> batches_;
     int sm_count_ = 0;
     ccnn_status alloc_batches();

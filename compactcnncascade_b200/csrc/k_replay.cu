@@ -512,6 +512,13 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
         F = a.F;
         checked = a.checked;
     }
+    // With drop_detect, the candidate-pair tests of every level (bit j of word w of candidate i's row:
+    // drop_test(candidate i, box of candidate 32w + j of the same level) == 1 / == 2) are evaluated
+    // for all levels at once before the level loop, where the rows (kBitWords words per candidate)
+    // fit in shared memory beside the working set; the loop then only reads them.
+    const bool pre_rows = fits && C.drop_detect && ((121LL * n + 15) & ~15LL) + 8LL * kBitWords * n <= kReplaySmemBytes;
+    uint32_t* P1 = pre_rows ? reinterpret_cast<uint32_t*>(sm + ((121LL * n + 15) & ~15LL)) : nullptr;
+    uint32_t* P2 = pre_rows ? P1 + (size_t)kBitWords * n : nullptr;
     for (int l = tid; l <= nl; l += kRT) s_lvl_start[l] = 0;
     __syncthreads();
     // verdicts and per-level candidate counts (candidates are grouped by level, smallest first)
@@ -530,6 +537,34 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
         s_nD = 0;
     }
     __syncthreads();
+    if (pre_rows) {
+        // a warp a candidate row, one ballot a word
+        for (int c = warp; c < n; c += kRT / 32) {
+            const Candidate cd = cands[c];
+            const int k = nl - 1 - cd.level;
+            const int g = s_lvl_start[k], m = s_lvl_start[k + 1] - g, i = c - g;
+            if (m > kBitMax) continue;
+            const LevelDesc& Lc = a.levels[cd.level];
+            const Det nr = cand_rect(cd, Lc.inv_scale, Lc.scale, C.pat_w, C.pat_h);
+            const Det ex = rect_shrink(nr, 0.7f);
+            for (int w = 0; w < ((i + 31) >> 5); ++w) {
+                const int j = 32 * w + lane;
+                int t = 0;
+                if (j < i) t = drop_test(nr, ex, cand_rect(cands[g + j], Lc.inv_scale, Lc.scale, C.pat_w, C.pat_h));
+                const uint32_t b1 = __ballot_sync(0xffffffffu, t == 1), b2 = __ballot_sync(0xffffffffu, t == 2);
+                if (lane == 0) {
+                    P1[(size_t)c * kBitWords + w] = b1;
+                    P2[(size_t)c * kBitWords + w] = b2;
+                }
+            }
+            // words at and past the candidate's own index stay 0
+            if (lane < kBitWords && lane >= ((i + 31) >> 5)) {
+                P1[(size_t)c * kBitWords + lane] = 0u;
+                P2[(size_t)c * kBitWords + lane] = 0u;
+            }
+        }
+        __syncthreads();
+    }
 
     int nD = 0;
     for (int k = 0; k < nl; ++k) {
@@ -585,7 +620,15 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
                 D[s_didx[i]] = make_det(nr.x, nr.y, nr.w, nr.h, sc, scale, kn);
                 if (a.fa_scratch) a.fa_scratch[s_didx[i]] = (s_src[i] == kOwnVerdict) ? g + i : -1;
             };
-            if (m <= kBitMax) {
+            if (pre_rows) {
+                // the level's rows, evaluated before the loop (levels of up to 32 read them in warp 0)
+                if (m > 32 && m <= kBitMax)
+                    for (int it = tid; it < m * W; it += kRT) {
+                        const int i = it / W, w = it - i * W;
+                        s_a1[it] = P1[(size_t)(g + i) * kBitWords + w];
+                        s_a2[it] = P2[(size_t)(g + i) * kBitWords + w];
+                    }
+            } else if (m <= kBitMax) {
                 // candidate-pair tests of this level, one ballot per (row i, word w)
                 for (int it = warp; it < m * W; it += kRT / 32) {
                     const int i = it / W, w = it - i * W;
@@ -624,8 +667,8 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
                         code = first_dec[g + i];
                         acc = C.detect_enabled ? res[g + i].accepted : 1;
                         if (acc && a.attr && a.attr[g + i].x) acc = 0;  // facial analysis dropped it
-                        r1 = s_a1[i];
-                        r2 = s_a2[i];
+                        r1 = pre_rows ? P1[(size_t)(g + i) * kBitWords] : s_a1[i];
+                        r2 = pre_rows ? P2[(size_t)(g + i) * kBitWords] : s_a2[i];
                     }
                     uint32_t S = 0u;
                     for (int round = 0; round <= m; ++round) {
@@ -894,10 +937,11 @@ __device__ __forceinline__ void replay_body(const ReplayArgs& a) {
     for (int i = tid; i < nD; i += kRT) K[i] = ScaleKey{D[nD - 1 - i].scale, i};
     __syncthreads();
     // n <= 16: insertion sort of a sorted list. The block-wide sort keeps its segment lists in the
-    // bit-matrix words (free after the level loop) and its leaves in the survivors' scratch.
+    // bit-matrix words (free after the level loop) and its partitions' stop lists in the scan and
+    // survivor scratch (also free).
     constexpr int kSortSegs = (kBitMax * kBitWords) / 3;
     if (nD > 16 && nD / 17 <= kSortSegs) {
-        introsort_scale_desc_block(K, nD, reinterpret_cast<int*>(s_a1), reinterpret_cast<int*>(s_a2), kSortSegs, a.survivors);
+        introsort_scale_desc_block(K, nD, reinterpret_cast<int*>(s_a1), reinterpret_cast<int*>(s_a2), kSortSegs, first_dec, surv);
     } else {
         if (nD > 16 && tid == 0) introsort_scale_desc(K, nD);
         __syncthreads();
@@ -1112,11 +1156,11 @@ __global__ void __launch_bounds__(kRT, 1) replay_batch_kernel(const ReplayArgs* 
 }
 
 // The block-wide sort of n (scale, index) keys (device memory) and its permutation, for tests.
-__global__ void __launch_bounds__(kRT, 1) sort_check_kernel(ScaleKey* K, int n, int* leaves, int* perm) {
+__global__ void __launch_bounds__(kRT, 1) sort_check_kernel(ScaleKey* K, int n, int* scratch, int* perm) {
     constexpr int kSegs = (kBitMax * kBitWords) / 3;
     __shared__ int seg_a[3 * kSegs], seg_b[3 * kSegs];
     if (n > 16 && n / 17 <= kSegs) {
-        introsort_scale_desc_block(K, n, seg_a, seg_b, kSegs, leaves);
+        introsort_scale_desc_block(K, n, seg_a, seg_b, kSegs, scratch, scratch + n);
     } else {
         if (threadIdx.x == 0) {
             if (n > 16) introsort_scale_desc(K, n);
@@ -1133,7 +1177,7 @@ cudaError_t sort_permutation_device(const float* scales, int n, int* perm) {
     ScaleKey* d_k = nullptr;
     int *d_leaves = nullptr, *d_perm = nullptr;
     cudaError_t e = cudaMalloc(&d_k, sizeof(ScaleKey) * (n + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_leaves, sizeof(int) * (n + 2));
+    if (e == cudaSuccess) e = cudaMalloc(&d_leaves, sizeof(int) * (2 * n + 2));
     if (e == cudaSuccess) e = cudaMalloc(&d_perm, sizeof(int) * (n + 1));
     if (e == cudaSuccess && n > 0) e = cudaMemcpy(d_k, k.data(), sizeof(ScaleKey) * n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {

@@ -608,12 +608,14 @@ cudaError_t launch_pyramid_batch(const BatchFrames& F, const LevelDesc* d_levels
     return cudaGetLastError();
 }
 
+// resident blocks per SM of the persistent kernel: the schedule's count (1-4), at most what fits
 int stage1_batch_blocks_per_sm(int blocks_per_sm) {
     int n = 0;
     if (blocks_per_sm >= 4)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1_batch_kernel<4>, 256, kBatchSmem);
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1_batch_kernel<3>, 256, kBatchSmem);
+    if (blocks_per_sm >= 1 && blocks_per_sm < n) n = blocks_per_sm;
     return n > 0 ? n : 1;
 }
 

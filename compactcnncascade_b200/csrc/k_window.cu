@@ -283,52 +283,80 @@ __device__ void prepare_window(const WinArgs& a, WindowSmem& S, const Candidate&
     const int rx = S.geo[0], ry = S.geo[1], rcols = S.geo[2], rrows = S.geo[3];
     const bool copy = (rcols == kCropW && rrows == kCropH);  // FastImageResize copies equal sizes
     const uint32_t sclx = fp_step(max(rcols, 1), kCropW), scly = fp_step(max(rrows, 1), kCropH);
-    for (int p = threadIdx.x; p < kCropW * kCropH; p += kWT) {
-        const int ix = p % kCropW, iy = p / kCropW;
-        int sx, sy;
-        if (copy) {
-            sx = ix;
-            sy = iy;
-        } else {
-            sx = (int)sample_col(ix, sclx, rcols).idx;
-            sy = (int)sample_row(iy, scly, rrows).idx;
+    // every load of the thread's pixels is issued before the first is used (the gray frame is read
+    // from L2, so the loads overlap instead of queueing one latency each); the byte values stay in
+    // registers until the equalisation table is known
+    constexpr int kPx = kCropW * kCropH;
+    constexpr int kPerThread = (kPx + kWT - 1) / kWT;
+    float v[kPerThread];
+#pragma unroll
+    for (int k = 0; k < kPerThread; ++k) {
+        const int p = threadIdx.x + k * kWT;
+        v[k] = 0.f;
+        if (p < kPx) {
+            const int ix = p % kCropW, iy = p / kCropW;
+            int sx, sy;
+            if (copy) {
+                sx = ix;
+                sy = iy;
+            } else {
+                sx = (int)sample_col(ix, sclx, rcols).idx;
+                sy = (int)sample_row(iy, scly, rrows).idx;
+            }
+            // memory guard only: valid candidates always sample inside the frame
+            const int gx = min(max(rx + sx, 0), a.gw - 1), gy = min(max(ry + sy, 0), a.gh - 1);
+            v[k] = a.gray[(size_t)gy * a.gpitch + gx];
         }
-        // memory guard only: valid candidates always sample inside the frame
-        const int gx = min(max(rx + sx, 0), a.gw - 1), gy = min(max(ry + sy, 0), a.gh - 1);
-        const float v = a.gray[(size_t)gy * a.gpitch + gx];
-        const uint8_t u = (uint8_t)__float2int_rz(fadd(v, 0.5f));
-        S.crop[iy][ix] = u;
-        if (a.cfg.equalize) atomicAdd(&S.hist[u], 1);
+    }
+    const bool eq = a.cfg.equalize != 0;
+    uint32_t u[(kPerThread + 3) / 4];  // the bytes, four to a register
+#pragma unroll
+    for (int k = 0; k < (kPerThread + 3) / 4; ++k) u[k] = 0u;
+#pragma unroll
+    for (int k = 0; k < kPerThread; ++k) {
+        const int p = threadIdx.x + k * kWT;
+        const uint32_t b = (uint8_t)__float2int_rz(fadd(v[k], 0.5f));
+        u[k >> 2] |= b << (8 * (k & 3));
+        if (p < kPx) {
+            if (eq)
+                atomicAdd(&S.hist[b], 1);
+            else
+                S.crop[p / kCropW][p % kCropW] = (uint8_t)b;
+        }
     }
     __syncthreads();
-    if (!a.cfg.equalize) return;
+    if (!eq) return;
     // cumulative histogram (256 bins, one per thread): shuffle scan + warp totals
     {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        int v = S.hist[threadIdx.x];
+        int c = S.hist[threadIdx.x];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int y2 = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane >= o) v += y2;
+            int y2 = __shfl_up_sync(0xffffffffu, c, o);
+            if (lane >= o) c += y2;
         }
         __shared__ int wsum[8];
-        if (lane == 31) wsum[wid] = v;
+        if (lane == 31) wsum[wid] = c;
         __syncthreads();
         int add = 0;
         for (int w = 0; w < wid; ++w) add += wsum[w];
-        S.lut[threadIdx.x] = v + add;  // cf_hist
+        S.lut[threadIdx.x] = c + add;  // cf_hist
         __syncthreads();
     }
     const float bmin = (float)S.lut[0], bmax = (float)S.lut[255];
-    if (bmin == bmax) return;  // the reference leaves the window unchanged
-    const float delt = fdiv(255.f, fsub(bmax, bmin));
-    const int lv = (int)fadd(fmul(fsub((float)S.lut[threadIdx.x], bmin), delt), 0.5f);
-    __syncthreads();
-    S.lut[threadIdx.x] = lv;
-    __syncthreads();
-    for (int p = threadIdx.x; p < kCropW * kCropH; p += kWT) {
-        const int ix = p % kCropW, iy = p / kCropW;
-        S.crop[iy][ix] = (uint8_t)S.lut[S.crop[iy][ix]];
+    if (bmin != bmax) {
+        const float delt = fdiv(255.f, fsub(bmax, bmin));
+        const int lv = (int)fadd(fmul(fsub((float)S.lut[threadIdx.x], bmin), delt), 0.5f);
+        __syncthreads();
+        S.lut[threadIdx.x] = lv;
+        __syncthreads();
+    }
+    // the equalised bytes (the reference leaves the window unchanged when every pixel is equal)
+#pragma unroll
+    for (int k = 0; k < kPerThread; ++k) {
+        const int p = threadIdx.x + k * kWT;
+        const uint32_t b = (u[k >> 2] >> (8 * (k & 3))) & 0xffu;
+        if (p < kPx) S.crop[p / kCropW][p % kCropW] = (uint8_t)(bmin != bmax ? S.lut[b] : b);
     }
     __syncthreads();
 }

@@ -244,24 +244,91 @@ CCNN_HD void introsort_scale_desc(T* v, int n) {
 }
 
 #if defined(__CUDACC__)
-// The same introsort by the whole block. The partitions of one recursion depth touch disjoint
-// segments, so each round partitions every segment longer than the threshold at once (a thread a
-// segment, the reference's steps within it); the heapsort fallback is per segment too. The final
-// insertion sort of the reference never moves an element across a partition cut (everything before
-// a cut has a scale >= the pivot >= everything after it, and the insertion stops at the first element
-// that is not smaller), so it is the same as an insertion sort of each leaf segment, run in parallel.
-// seg_a / seg_b: 3 * max_segs ints each (shared memory); leaves: n ints of scratch (any memory);
-// n must be > 16 and n / 17 <= max_segs. Every thread of the block calls it.
+// unguarded_partition(v, piv + 1, hi, piv) by one warp. The left pointer stops at the elements that
+// do not compare before the pivot, the right one at those the pivot does not compare before; a
+// pointer only ever examines positions the other has not swapped yet, except at the crossing. So with
+// L_k / R_k the k-th stop of each pointer on the values as they are now (left ascending from piv + 1,
+// right descending from hi - 1), the partition swaps (L_k, R_k) for every k before the first k* with
+// L_k* >= R_k* (or no stop left), and returns the left pointer's last stop: L_k*, or R_(k*-1) where
+// the left pointer runs into the swapped region first. lbuf / rbuf: scratch of hi - piv ints each.
 template <class T>
-__device__ void introsort_scale_desc_block(T* v, int n, int* seg_a, int* seg_b, int max_segs, int* leaves) {
+__device__ int warp_partition(T* v, int piv, int hi, int* lbuf, int* rbuf) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const T p = v[piv];
+    int nL = 0, nR = 0;
+    for (int base = piv + 1; base < hi; base += 32) {
+        const int i = base + lane;
+        const bool f = i < hi && !comp_scale_desc(v[i], p);
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        if (f) lbuf[nL + __popc(m & lt)] = i;
+        nL += __popc(m);
+    }
+    for (int base = hi - 1; base >= piv; base -= 32) {
+        const int j = base - lane;
+        const bool g = j >= piv && !comp_scale_desc(p, v[j]);
+        const unsigned m = __ballot_sync(0xffffffffu, g);
+        if (g) rbuf[nR + __popc(m & lt)] = j;
+        nR += __popc(m);
+    }
+    __syncwarp();
+    int ks = 0;
+    for (int kb = 0;; kb += 32) {
+        const int k = kb + lane;
+        const bool stop = k >= nL || k >= nR || lbuf[k] >= rbuf[k];
+        const unsigned m = __ballot_sync(0xffffffffu, stop);
+        if (m) {
+            ks = kb + __ffs(m) - 1;
+            break;
+        }
+    }
+    // the swapped pairs are disjoint: L_j < R_j for j < k*, both lists strictly monotone
+    for (int k = lane; k < ks; k += 32) swap_el(&v[lbuf[k]], &v[rbuf[k]]);
+    int cut = ks < nL ? lbuf[ks] : hi;
+    if (ks > 0 && rbuf[ks - 1] < cut) cut = rbuf[ks - 1];
+    __syncwarp();
+    return cut;
+}
+
+// insertion_sort(v, lo, hi) by one warp (hi - lo <= 32): the insertion sort never moves an element
+// past an equal one, so it is the stable sort, and every element's place is its rank.
+template <class T>
+__device__ void warp_stable_sort(T* v, int lo, int hi) {
+    const int lane = threadIdx.x & 31;
+    const int len = hi - lo;
+    T val;
+    int r = 0;
+    if (lane < len) {
+        val = v[lo + lane];
+        for (int q = 0; q < len; ++q) {
+            const T o = v[lo + q];
+            if (comp_scale_desc(o, val) || (q < lane && !comp_scale_desc(val, o))) ++r;
+        }
+    }
+    __syncwarp();
+    if (lane < len) v[lo + r] = val;
+    __syncwarp();
+}
+
+// The same introsort by the whole block. The partitions of one recursion depth touch disjoint
+// segments, so each round partitions every segment longer than the threshold at once (a warp a
+// segment, the partition itself parallel as above; the heapsort fallback by one lane). The final
+// insertion sort of the reference never moves an element across a partition cut (everything before a
+// cut has a scale >= the pivot >= everything after it, and the insertion stops at the first element
+// that is not smaller), so it is the same as an insertion sort of each leaf segment, which the warp
+// that splits a leaf off runs at once. seg_a / seg_b: 3 * max_segs ints each (shared memory);
+// lbuf / rbuf: n ints each of scratch (any memory); n must be > 16 and n / 17 <= max_segs. Every
+// thread of the block calls it.
+template <class T>
+__device__ void introsort_scale_desc_block(T* v, int n, int* seg_a, int* seg_b, int max_segs, int* lbuf, int* rbuf) {
     const int kThreshold = 16;
-    __shared__ int s_cur, s_next, s_leaves;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    __shared__ int s_cur, s_next;
     if (threadIdx.x == 0) {
         seg_a[0] = 0;
         seg_a[1] = n;
         seg_a[2] = 2 * floor_log2(n);
         s_cur = 1;
-        s_leaves = 0;
     }
     __syncthreads();
     int* cur = seg_a;
@@ -272,31 +339,33 @@ __device__ void introsort_scale_desc_block(T* v, int n, int* seg_a, int* seg_b, 
         __syncthreads();
         if (threadIdx.x == 0) s_next = 0;
         __syncthreads();
-        for (int k = threadIdx.x; k < ncur; k += blockDim.x) {
+        for (int k = warp; k < ncur; k += nwarps) {
             const int first = cur[3 * k], last = cur[3 * k + 1];
             int depth = cur[3 * k + 2];
             if (depth == 0) {
-                heap_sort_el(v + first, last - first);
+                if (lane == 0) heap_sort_el(v + first, last - first);
+                __syncwarp();
                 continue;
             }
             --depth;
             const int mid = first + (last - first) / 2;
-            median_to_first(&v[first], &v[first + 1], &v[mid], &v[last - 1]);
-            const int cut = unguarded_partition(v, first + 1, last, first);
+            if (lane == 0) median_to_first(&v[first], &v[first + 1], &v[mid], &v[last - 1]);
+            __syncwarp();
+            const int cut = warp_partition(v, first, last, lbuf + first, rbuf + first);
             const int lo[2] = {first, cut}, hi[2] = {cut, last};
             for (int c = 0; c < 2; ++c) {
                 const int len = hi[c] - lo[c];
                 if (len > kThreshold) {
-                    const int slot = atomicAdd(&s_next, 1);
-                    if (slot < max_segs) {
-                        nxt[3 * slot] = lo[c];
-                        nxt[3 * slot + 1] = hi[c];
-                        nxt[3 * slot + 2] = depth;
+                    if (lane == 0) {
+                        const int slot = atomicAdd(&s_next, 1);
+                        if (slot < max_segs) {
+                            nxt[3 * slot] = lo[c];
+                            nxt[3 * slot + 1] = hi[c];
+                            nxt[3 * slot + 2] = depth;
+                        }
                     }
                 } else if (len > 1) {
-                    const int slot = atomicAdd(&s_leaves, 1);
-                    leaves[2 * slot] = lo[c];
-                    leaves[2 * slot + 1] = hi[c];
+                    warp_stable_sort(v, lo[c], hi[c]);
                 }
             }
         }
@@ -307,9 +376,6 @@ __device__ void introsort_scale_desc_block(T* v, int n, int* seg_a, int* seg_b, 
         nxt = t;
         __syncthreads();
     }
-    const int nleaf = s_leaves;
-    for (int k = threadIdx.x; k < nleaf; k += blockDim.x) insertion_sort(v, leaves[2 * k], leaves[2 * k + 1]);
-    __syncthreads();
 }
 #endif
 

@@ -129,8 +129,9 @@ CCNN_API ccnn_status ccnn_get_schedule(ccnn_handle h, int* frame_slots, int* win
  * of every level of every frame of the group in one persistent launch fed by a device work queue,
  * then the candidates, windows and replays of the group in one launch each); frame_slots must be at
  * least batch_frames, and frame_slots / batch_frames groups are in flight. batch_blocks_per_sm is
- * the persistent kernel's register budget (3 or 4). 0 keeps a value (batch_frames: -1 keeps it, 0
- * turns the batched form off). Same rules as ccnn_set_schedule. */
+ * the persistent kernel's resident blocks per SM (its grid, 1-4; 4 selects the 64-register build,
+ * 1-3 the 80-register one; fewer blocks leave SMs to other frames' kernels). 0 keeps a value
+ * (batch_frames: -1 keeps it, 0 turns the batched form off). Same rules as ccnn_set_schedule. */
 typedef struct {
     int frame_slots;
     int window_ctas_per_sm;

@@ -36,7 +36,7 @@ def _device_batch(det, frames, w, h, steps=None, cap=512):
     return [[(f.x, f.y, f.width, f.height, f.score) for f in faces[i * cap: i * cap + nf[i]]] for i in range(n)]
 
 
-@pytest.mark.parametrize("batch,slots,bpsm", [(2, 4, 3), (4, 8, 4), (8, 8, 3), (8, 16, 4)])
+@pytest.mark.parametrize("batch,slots,bpsm", [(2, 4, 3), (4, 8, 4), (8, 8, 3), (8, 16, 4), (4, 8, 1)])
 def test_batched_host_frames_equal_per_frame(batch, slots, bpsm):
     w, h = 1280, 720
     imgs = [ccnn.synth_frame(w, h, 5000 + i, 10, 30, 300)[0] for i in range(11)]  # leftovers after the last full group
