@@ -507,13 +507,16 @@ def main():
     for s in range(args.warmup):
         device_step(s)
     barrier()
+    # NVTX ranges name the timed regions for profilers (ncu --nvtx --nvtx-include "plain/")
     with ClockSampler(dev) as clk:
         t0 = time.perf_counter()
         gpu_ms = 0.0
         faces_total = 0
+        torch.cuda.nvtx.range_push("plain")
         for s in range(args.steps):
             gpu_ms += device_step(args.warmup + s)
             faces_total += sum(nf[j] for j in range(B))
+        torch.cuda.nvtx.range_pop()
         barrier()
         wall_dev = time.perf_counter() - t0
     clocks = clk.summary()
@@ -627,8 +630,10 @@ def main():
         barrier()
         with ClockSampler(dev) as gclk:
             g_ms = 0.0
+            torch.cuda.nvtx.range_push("gated")
             for s in range(args.steps):
                 g_ms += device_step(args.warmup + s)
+            torch.cuda.nvtx.range_pop()
             barrier()
         g_wall_e2e = None
         for s in range(args.warmup):
