@@ -132,16 +132,19 @@ BATCHED = [((3840, 2160), 60, 20, 600), ((4800, 2400), 60, 20, 600)]
 
 
 def launches_per_frames(n_frames, n_levels, batch_frames, gated=False):
-    """Kernels the library launches for n_frames frames of one size: per frame gray, pyramid, stage-1
-    front and back (pyramid and stage 1 once per group of 32 levels), candidates, windows, replay
-    (+2 for the gate); in the batched form per group of batch_frames frames gray, one persistent
-    pyramid + stage-1 launch, candidates, windows, replay (+2 per frame for the gate), with leftover
-    frames per frame."""
+    """Kernels the library launches for n_frames frames of one size. Per frame: gray, stage-1 front and
+    back once per group of 32 levels (the front kernel resamples the pyramid levels itself),
+    candidates, windows, replay; with batch_frames == 1 stage 1 is one persistent launch instead. In
+    the batched form, per group of batch_frames frames: gray, the count reset, one persistent
+    pyramid + stage-1 launch, candidates, windows, replay; leftover frames run per frame. The learned
+    gate adds its inference and one mask launch per group of 32 levels to every frame."""
     groups = -(-n_levels // 32)
-    per_frame = 4 + 3 * groups + (2 if gated else 0)
+    gate = (1 + groups) if gated else 0
+    per_frame = (5 if batch_frames == 1 else 4 + 2 * groups) + gate
     if batch_frames and batch_frames >= 2:
         full = n_frames // batch_frames
-        return full * (5 + (2 * batch_frames if gated else 0)) + (n_frames - full * batch_frames) * per_frame
+        leftover = (n_frames - full * batch_frames) * (4 + 2 * groups + gate)
+        return full * (6 + batch_frames * gate) + leftover
     return n_frames * per_frame
 
 
@@ -214,8 +217,9 @@ def run_batched_pyramid(dev, args):
         out[f"{w}x{h}"] = res
         det.Clear()
     out["note"] = ("seeded frames with 60 face patches 20-600 px, scale 1.05, min face 20, no max face; device-resident frames, "
-                   "device time from CUDA events. per_frame: every frame's chain one CUDA graph (pyramid and stage 1 in level "
-                   "tables of at most 32 levels a launch), 8 frames in flight. batched: 8 frames one graph, the pyramid and stage 1 "
+                   "device time from CUDA events. per_frame: every frame's chain one CUDA graph (stage 1, whose front kernel "
+                   "resamples the pyramid levels, in level tables of at most 32 levels a launch), 8 frames in flight. batched: 8 "
+                   "frames one graph, the pyramid and stage 1 "
                    "of all levels of all 8 frames in one persistent launch fed by a device work queue, two 8-frame groups in flight")
     return out
 
@@ -320,8 +324,9 @@ def algorithmic_work(levels, gw, gh):
             per response pixel:   16 L3 maps x (20 mul + 19 add + 5)
                                   + 52 hidden x (4 mul + 4 add + 1 slope + 13 tanh + 2 scale + 2 out)
                                   + 8 output ops
-    bytes: front reads each level image once and writes 4 S1 planes (16 B per pooled L1 pixel);
-    back reads the S1 planes and writes the response maps (4 B per response pixel)."""
+    bytes: front reads the gray samples of each level pixel (4 B per level pixel; it resamples the
+    level tiles from the gray frame, no level image is stored) and writes 4 S1 planes (16 B per
+    pooled L1 pixel); back reads the S1 planes and writes the response maps (4 B per response pixel)."""
     ops_front = ops_back = 0
     by_front = 0
     by_back = 0
@@ -351,8 +356,11 @@ def dram_traffic():
 
 
 def frame_bytes(levels, w, h):
-    """Algorithmic bytes of a frame: BGR read, gray write+read, each level write+read, response maps."""
-    return 3 * w * h + 8 * w * h + sum(8 * a[0] * a[1] for a in levels) + sum(4 * a[3] * a[4] for a in levels)
+    """Algorithmic bytes of a frame: BGR read, gray write, the gray samples of every level pixel read by
+    the stage-1 front kernel, the S1 planes written and read (4 planes of pooled L1 pixels), the
+    response maps written and read."""
+    s1 = sum(((a[0] - 3) >> 1) * ((a[1] - 3) >> 1) for a in levels)
+    return 3 * w * h + 4 * w * h + sum(4 * a[0] * a[1] for a in levels) + 32 * s1 + sum(8 * a[3] * a[4] for a in levels)
 
 
 def committed_records():
@@ -596,7 +604,7 @@ def main():
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback 6650 GB/s"},
         "frame_hbm": {"bytes_per_frame": fb_frame, "achieved": round(value / world * fb_frame / 1e9, 2), "unit": "GB/s",
                       "frac": round(value / world * fb_frame / (hbm_peak * 1e9), 5),
-                      "note": "whole-frame algorithmic bytes (BGR read, gray write+read, each level write+read, response maps) "
+                      "note": "whole-frame algorithmic bytes (BGR read, gray write, gray samples of every level pixel, S1 planes and response maps written and read) "
                               "x frames/s"},
         "single_launch_stage1": ({"ms": round(single_launch_ms, 4),
                                   "achieved": round((work["stage1_front"][0] + work["stage1_back"][0]) / (single_launch_ms * 1e-3) / 1e12, 3),

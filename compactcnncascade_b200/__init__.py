@@ -148,6 +148,16 @@ class FaceDetector:
         _capi.check(_capi.lib().ccnn_gate_stats(self._h, *[ctypes.byref(x) for x in v]), "ccnn_gate_stats")
         return tuple(x.value for x in v)
 
+    def gateProbabilities(self):
+        """The learned gate's probabilities of the last frame, shape (4, rows // 16, cols // 16)."""
+        n = ctypes.c_int()
+        _capi.check(_capi.lib().ccnn_gate_probabilities(self._h, None, 0, ctypes.byref(n)), "ccnn_gate_probabilities")
+        out = np.empty(n.value, np.float32)
+        _capi.check(_capi.lib().ccnn_gate_probabilities(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n.value,
+                                                        ctypes.byref(n)), "ccnn_gate_probabilities")
+        _, gw, gh, _ = self.grayDevice()
+        return out.reshape(4, (gh // 8) // 2, (gw // 8) // 2)
+
     def grayDevice(self):
         """(device pointer, cols, rows, step in bytes) of the last frame's fp32 gray image."""
         ptr, w, h, step = ctypes.c_void_p(), ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()

@@ -5,7 +5,8 @@ depend on the schedule; only throughput does.
 
 The knobs (include/ccnn_inspect.h, ccnn_schedule):
   frame_slots          frames in flight, each with its own stream, buffers and captured graph
-  window_ctas_per_sm   resident blocks per SM of the persistent stage-2/3 window kernel
+  window_ctas_per_sm   resident blocks per SM of the persistent stage-2/3 window kernel (5, 6: builds
+                       with 48 and 40 registers a thread)
   front_blocks_per_sm  register budget of the stage-1 front kernel (3: 80 registers, 4: 64)
   back_blocks_per_sm   register budget of the stage-1 back kernel (3: 80 registers, 4: 64)
   batch_frames         frames per batched graph (0: every frame its own graph; 1: the same with the
@@ -28,7 +29,7 @@ import sys
 from . import _capi
 
 TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "schedules.json")
-KNOBS = (("frame_slots", (4, 8, 12, 16)), ("window_ctas_per_sm", (2, 3, 4)), ("front_blocks_per_sm", (3, 4)),
+KNOBS = (("frame_slots", (4, 8, 12, 16)), ("window_ctas_per_sm", (2, 3, 4, 5, 6)), ("front_blocks_per_sm", (3, 4)),
          ("back_blocks_per_sm", (3, 4)), ("batch_frames", (0, 1, 2, 4, 8)), ("batch_blocks_per_sm", (1, 2, 3, 4)))
 DEFAULTS = {"frame_slots": 8, "window_ctas_per_sm": 4, "front_blocks_per_sm": 3, "back_blocks_per_sm": 4, "batch_frames": 0,
             "batch_blocks_per_sm": 3}

@@ -258,6 +258,11 @@ CCNN_API ccnn_status ccnn_gate_stats(ccnn_handle h, int* front_run, int* front_t
     return h->det.gate_stats(front_run, front_total, back_run, back_total, fallback);
 }
 
+CCNN_API ccnn_status ccnn_gate_probabilities(ccnn_handle h, float* out, int capacity, int* n) {
+    if (!h || !n || capacity < 0) return CCNN_ERR_INVALID_ARG;
+    return h->det.gate_probabilities(out, capacity, n);
+}
+
 CCNN_API ccnn_status ccnn_gate_labels(ccnn_handle h, unsigned char* d_labels, void* stream) {
     if (!h || !d_labels) return CCNN_ERR_INVALID_ARG;
     return h->det.gate_labels(d_labels, (cudaStream_t)stream);

@@ -102,6 +102,7 @@ void Detector::free_slot(Slot& s) {
     s.d_fa = nullptr;
     cudaFree(s.gate.ambiguous);  // the bitmaps share its allocation
     cudaFree(s.gate.prob);
+    cudaFree(s.gate.feat);
     cudaFree(s.d_front_on);
     cudaFree(s.d_back_on);
     s.gate = GateScratch{};
@@ -360,6 +361,7 @@ ccnn_status Detector::init() {
     facial_grid_ = prop.multiProcessorCount;  // one 118 KB-shared-memory block per SM
     CCNN_CUDA(replay_setup());
     CCNN_CUDA(stage1_setup());
+    CCNN_CUDA(window_setup());
     CCNN_CUDA(facial_setup());
 
     sm_count_ = prop.multiProcessorCount;
@@ -404,6 +406,10 @@ ccnn_status Detector::estimate_bytes(const ccnn_params& p, const char* const* mo
     return CCNN_OK;
 }
 
+// the level arena: only the legacy network reads stored level images (the CNTK stage-1 front kernel
+// resamples its tiles from the gray frame)
+long long Detector::limg_floats() const { return legacy_ ? std::max(4LL, img_cap_) : 4LL; }
+
 ccnn_status Detector::alloc_slot(Slot& s) {
     CCNN_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
     CCNN_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
@@ -411,7 +417,7 @@ ccnn_status Detector::alloc_slot(Slot& s) {
     CCNN_CUDA(cudaMalloc(&s.d_in, s.in_pitch * max_h_));
     s.gray_pitch = (int)round_up(max_w_, 16);
     CCNN_CUDA(cudaMalloc(&s.d_gray, sizeof(float) * (size_t)s.gray_pitch * max_h_));
-    CCNN_CUDA(cudaMalloc(&s.d_limg, sizeof(float) * std::max(4LL, img_cap_)));
+    CCNN_CUDA(cudaMalloc(&s.d_limg, sizeof(float) * limg_floats()));
     CCNN_CUDA(cudaMalloc(&s.d_s1, sizeof(float) * std::max(1LL, s1_cap_)));
     CCNN_CUDA(cudaMalloc(&s.d_resp, sizeof(float) * std::max(1LL, resp_cap_)));
     CCNN_CUDA(cudaMalloc(&s.d_counts, sizeof(int) * chunk_cap_));
@@ -569,6 +575,7 @@ ccnn_status Detector::alloc_gate(Slot& s) {
     s.gate.ambiguous = (int*)words;
     s.gate.bits = (uint32_t*)words + 1;
     CCNN_CUDA(cudaMalloc(&s.gate.prob, sizeof(float) * std::max<size_t>(1, kGK * cells)));
+    CCNN_CUDA(cudaMalloc(&s.gate.feat, sizeof(__half) * std::max<size_t>(1, w8 * h8)));
     CCNN_CUDA(cudaMalloc(&s.d_front_on, std::max(1, k1_cap_)));
     CCNN_CUDA(cudaMalloc(&s.d_back_on, std::max(1, k2_cap_)));
     return CCNN_OK;
@@ -608,10 +615,10 @@ ccnn_status Detector::set_schedule(int frame_slots, int window_ctas_per_sm, int 
     std::lock_guard<std::mutex> lk(mu_);
     const int slots = frame_slots > 0 ? frame_slots : (int)slots_.size();
     const int batch = batch_frames >= 0 ? batch_frames : batch_frames_;
-    if (frame_slots < 0 || frame_slots > 64 || window_ctas_per_sm < 0 || window_ctas_per_sm > 4 || (front_bpsm != 0 && (front_bpsm < 3 || front_bpsm > 4)) ||
+    if (frame_slots < 0 || frame_slots > 64 || window_ctas_per_sm < 0 || window_ctas_per_sm > 6 || (front_bpsm != 0 && (front_bpsm < 3 || front_bpsm > 4)) ||
         (back_bpsm != 0 && (back_bpsm < 3 || back_bpsm > 4)) || (batch_bpsm != 0 && (batch_bpsm < 1 || batch_bpsm > 4)) || batch > kMaxBatch ||
         (batch > 1 && slots < batch)) {
-        set_error("schedule: 1-64 frame slots, 1-4 stage-2/3 blocks per SM, 3-4 stage-1 blocks per SM, batches of 0-16 frames, "
+        set_error("schedule: 1-64 frame slots, 1-6 stage-2/3 blocks per SM, 3-4 stage-1 blocks per SM, batches of 0-16 frames, "
                   "1-4 persistent stage-1 blocks per SM and at least as many frame slots as frames per batch (0 keeps the "
                   "current value)");
         return CCNN_ERR_INVALID_ARG;
@@ -695,6 +702,26 @@ ccnn_status Detector::gate_stats(int* front_run, int* front_total, int* back_run
     return CCNN_OK;
 }
 
+ccnn_status Detector::gate_probabilities(float* out, int cap, int* n) {
+    std::lock_guard<std::mutex> lk(mu_);
+    Slot& s = slots_[0];
+    if (!inited_ || !s.last_plan) {
+        set_error("no frame has been processed");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    const Plan& p = *s.last_plan;
+    if (!gate_on_ || !s.gate.prob || p.gw < 32 || p.gh < 32) {
+        set_error("the last frame ran without the learned gate");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    cudaSetDevice(device_);
+    CCNN_CUDA(cudaStreamSynchronize(s.st));
+    const int total = kGK * ((p.gw / 8) / 2) * ((p.gh / 8) / 2);
+    *n = total;
+    if (out && cap > 0) CCNN_CUDA(cudaMemcpy(out, s.gate.prob, sizeof(float) * std::min(cap, total), cudaMemcpyDeviceToHost));
+    return cap < total ? CCNN_TRUNCATED : CCNN_OK;
+}
+
 ReplayArgs Detector::replay_args(Slot& s, const Plan& p) const {
     ReplayArgs a;
     a.cands = s.d_cands;
@@ -723,35 +750,37 @@ ReplayArgs Detector::replay_args(Slot& s, const Plan& p) const {
 }
 
 ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
+    // the learned gate decides which stage-1 tiles run, and so which parts of the pyramid are read;
+    // the gray launch also writes its input features
+    const bool gated = gate_on_ && s.gate.prob && p.gw >= 32 && p.gh >= 32;
+    s.gray_feat = (gated && !p.downscale) ? s.gate.feat : nullptr;
     cudaError_t e;
     if (p.downscale)
         e = launch_gray_u8_resized(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, s.d_gray, s.gray_pitch, p.gw, p.gh, s.st);
     else
-        e = launch_gray(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st);
+        e = launch_gray(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st, s.gray_feat);
     CCNN_CUDA(e);
-    // the learned gate decides which stage-1 tiles run, and so which parts of the pyramid are read
-    const bool gated = gate_on_ && s.gate.prob && p.gw >= 32 && p.gh >= 32;
     if (gated) {
-        CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_, gate_amb_frac_,
-                              s.d_back_on, s.d_front_on, s.st));
+        CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.gray_feat != nullptr, p.levels.data(), p.n_levels, s.gate,
+                              gate_thr_, gate_amb_frac_, s.d_back_on, s.d_front_on, s.st));
     }
     const bool single = single_launch_stage1() && p.n_levels > 0 && p.n_levels <= kMaxBatchLevels;
     if (single) {
-        // the pyramid of every level in one launch (no level-count limit), then stage 1 of every level
-        // in one persistent launch (the batched form's kernels on one frame): what the reference's
+        // the pyramid and stage 1 of every level in one persistent launch (the batched form's kernel on
+        // one frame; front tiles resample their level tiles from the gray frame): what the reference's
         // level atlas (packet mode) is for
         BatchFrames F{};
         F.gray[0] = s.d_gray;
-        F.limg[0] = s.d_limg;
+        F.gpitch = s.gray_pitch;
+        F.gw = p.gw;
+        F.gh = p.gh;
         F.s1[0] = s.d_s1;
         F.resp[0] = s.d_resp;
         F.counts[0] = s.d_counts;
         F.front_on[0] = gated ? s.d_front_on : nullptr;
         F.back_on[0] = gated ? s.d_back_on : nullptr;
         F.cells[0] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{};
-        const LevelDesc& last = p.levels[p.n_levels - 1];
-        CCNN_CUDA(launch_pyramid_batch(F, p.d_levels, p.n_levels, (int)p.chunks.size(),
-                                       last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows), 1, s.gray_pitch, p.gw, p.gh, s.st));
+        if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
         BatchQueue Q;
         build_batch_queue(&Q, 1, p.n_levels, (int)p.chunks.size(), p.k1_tiles, p.k2_tiles, cfg_.thr1);
         CCNN_CUDA(cudaMemsetAsync(s.d_sync1, 0, sizeof(int) * (2 + kBatchStages), s.st));
@@ -759,7 +788,9 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
                                       sm_count_ * stage1_batch_blocks_per_sm(batch_bpsm_), s.st, batch_bpsm_));
         CCNN_CUDA(cudaMemcpyAsync(s.h_nfaces + 1, s.d_sync1 + 1 + kBatchStages, sizeof(int), cudaMemcpyDeviceToHost, s.st));
     } else {
-        CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st, gated ? s.d_front_on : nullptr));
+        // the legacy network reads stored level images; the CNTK front kernel resamples its tiles from
+        // the gray frame itself
+        if (legacy_) CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
         // the back kernel counts each chunk's candidates as it writes the responses
         if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
     }
@@ -768,9 +799,10 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
             const ccnn_status ls = enqueue_legacy_stage1(s, p);
             if (ls != CCNN_OK) return ls;
         } else {
-            CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
+            CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, nullptr, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
                                     gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr,
-                                    gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}, s1_sched_));
+                                    gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}, s1_sched_,
+                                    GrayRef{s.d_gray, s.gray_pitch, p.gw, p.gh}));
         }
     }
     CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
@@ -802,7 +834,8 @@ ccnn_status Detector::enqueue_legacy_stage1(Slot& s, const Plan& p) {
 static cudaError_t retarget_gray(Slot& s, const Plan& p, const uint8_t* src, int spitch) {
     int w = p.in_w, h = p.in_h, dpitch = s.gray_pitch;
     float* dst = s.d_gray;
-    void* args[6] = {&src, &spitch, &w, &h, &dst, &dpitch};
+    __half* feat = s.gray_feat;
+    void* args[7] = {&src, &spitch, &w, &h, &dst, &dpitch, &feat};
     cudaKernelNodeParams kp = s.gray_kp;
     kp.kernelParams = args;
     kp.extra = nullptr;
@@ -838,7 +871,7 @@ ccnn_status Detector::enqueue(Slot& s, const Plan& p, const ccnn_image& img, boo
             CCNN_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
             std::vector<cudaGraphNode_t> nodes(nn);
             if (nn) CCNN_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
-            const void* fn = gray_kernel_fn(p.ch);
+            const void* fn = gray_kernel_fn(p.ch, s.gray_feat != nullptr);
             for (cudaGraphNode_t nd : nodes) {
                 cudaGraphNodeType t;
                 CCNN_CUDA(cudaGraphNodeGetType(nd, &t));
@@ -1033,11 +1066,12 @@ size_t Detector::slot_bytes() const {
     const size_t in = (size_t)round_up((long long)max_w_ * 4, 64) * max_h_;
     const size_t gray = sizeof(float) * (size_t)round_up(max_w_, 16) * max_h_;
     const size_t per_cand = sizeof(Candidate) + sizeof(CandResult) + 4 * sizeof(WinOut) + 5 * sizeof(Det) + 2 * sizeof(int) + 1;
-    size_t per_slot = in + gray + sizeof(float) * (size_t)(std::max(4LL, img_cap_) + std::max(1LL, s1_cap_) + std::max(1LL, resp_cap_)) +
+    size_t per_slot = in + gray + sizeof(float) * (size_t)(limg_floats() + std::max(1LL, s1_cap_) + std::max(1LL, resp_cap_)) +
                       sizeof(int) * chunk_cap_ + per_cand * (size_t)cand_cap_ + sizeof(FaceOut) * std::max<long long>(cand_cap_, kHostFaces);
     if (gate_on_) {
         const size_t cells = ((size_t)max_w_ / 16) * ((size_t)max_h_ / 16);
         per_slot += sizeof(uint32_t) * (1 + (size_t)gate_bitmap_words(max_w_, max_h_)) + sizeof(float) * std::max<size_t>(1, kGK * cells) +
+                    sizeof(__half) * std::max<size_t>(1, ((size_t)max_w_ / 8) * ((size_t)max_h_ / 8)) +
                     (size_t)std::max(1, k1_cap_) + (size_t)std::max(1, k2_cap_);
     }
     if (h_lnet_) per_slot += (sizeof(int4) + 5 * sizeof(int)) * (size_t)cand_cap_;
@@ -1323,7 +1357,8 @@ ccnn_status Detector::stage1_forward(const float* d_img, int w, int h, size_t st
 }
 
 // Re-runs the last frame's kernel chain on slot 0 `iters` times with an event between every
-// two kernels; ms[k] gets the mean duration of kernel k: gray, pyramid, stage-1 front, stage-1
+// two kernels; ms[k] gets the mean duration of kernel k: gray, pyramid (legacy family only: the CNTK
+// front kernel resamples the levels itself, so this entry is the empty gap), stage-1 front, stage-1
 // back (with the candidate count and the memset of the counts before it), candidate write,
 // stage-2/3 windows, replay; ms[7] the learned gate; ms[8] the pyramid and stage 1 as one
 // persistent launch.
@@ -1349,21 +1384,22 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     const ReplayArgs a = replay_args(s, p);
     for (int it = 0; it < iters; ++it) {
         CCNN_CUDA(cudaEventRecord(ev[0], s.st));
+        __half* feat = (gated && !p.downscale) ? s.gate.feat : nullptr;
         if (p.downscale)
             CCNN_CUDA(launch_gray_u8_resized(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, s.d_gray, s.gray_pitch, p.gw, p.gh, s.st));
         else
-            CCNN_CUDA(launch_gray(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st));
+            CCNN_CUDA(launch_gray(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st, feat));
         CCNN_CUDA(cudaEventRecord(ev[1], s.st));
         if (gated) {
-            CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_,
+            CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, feat != nullptr, p.levels.data(), p.n_levels, s.gate, gate_thr_,
                                   gate_amb_frac_, s.d_back_on, s.d_front_on, s.st));
         }
         CCNN_CUDA(cudaEventRecord(ev[K + 1], s.st));
-        CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st,
-                                 gated ? s.d_front_on : nullptr));
+        if (legacy_) CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
         CCNN_CUDA(cudaEventRecord(ev[2], s.st));
         if (!legacy_)
-            CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, s.d_limg, s.d_s1, s.st, gated ? s.d_front_on : nullptr, s1_sched_));
+            CCNN_CUDA(launch_stage1_front(w1_, p.levels.data(), p.n_levels, nullptr, s.d_s1, s.st, gated ? s.d_front_on : nullptr, s1_sched_,
+                                          GrayRef{s.d_gray, s.gray_pitch, p.gw, p.gh}));
         CCNN_CUDA(cudaEventRecord(ev[3], s.st));
         if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
         if (legacy_) {  // the legacy network's three layers all count as the back entry
@@ -1402,21 +1438,21 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
     if (n_ms > K + 1 && !legacy_ && p.n_levels > 0 && p.n_levels <= kMaxBatchLevels) {
         BatchFrames F{};
         F.gray[0] = s.d_gray;
-        F.limg[0] = s.d_limg;
+        F.gpitch = s.gray_pitch;
+        F.gw = p.gw;
+        F.gh = p.gh;
         F.s1[0] = s.d_s1;
         F.resp[0] = s.d_resp;
         F.counts[0] = s.d_counts;
         F.front_on[0] = gated ? s.d_front_on : nullptr;
         F.back_on[0] = gated ? s.d_back_on : nullptr;
         F.cells[0] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{};
-        const LevelDesc& last = p.levels[p.n_levels - 1];
-        const int pyr_items = last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows);
         BatchQueue Q;
         build_batch_queue(&Q, 1, p.n_levels, (int)p.chunks.size(), p.k1_tiles, p.k2_tiles, cfg_.thr1);
         const int grid = sm_count_ * stage1_batch_blocks_per_sm(batch_bpsm_);
         for (int it = 0; it < iters; ++it) {
             CCNN_CUDA(cudaMemsetAsync(s.d_sync1, 0, sizeof(int) * (2 + kBatchStages), s.st));
-            CCNN_CUDA(launch_pyramid_batch(F, p.d_levels, p.n_levels, (int)p.chunks.size(), pyr_items, 1, s.gray_pitch, p.gw, p.gh, s.st));
+            if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
             CCNN_CUDA(cudaEventRecord(ev[0], s.st));
             CCNN_CUDA(launch_stage1_batch(w1_, F, Q, p.d_levels, s.d_sync1, s.d_sync1 + 1 + kBatchStages, grid, s.st, batch_bpsm_));
             CCNN_CUDA(cudaEventRecord(ev[1], s.st));
@@ -1582,8 +1618,8 @@ bool Detector::batch_usable(const Plan& p) const {
 }
 
 // The graph of a batch: gray of every frame in one launch, the learned gate per frame (when on), the
-// pyramid of every level of every frame in one launch, stage 1 of every level of every frame in one
-// persistent launch fed by a device work queue, the candidates of every frame in one launch, the
+// pyramid and stage 1 of every level of every frame in one persistent launch fed by a device work
+// queue (front items resample their level tiles from the gray frames), the candidates of every frame in one launch, the
 // stage-2/3 windows of every frame's candidates in one persistent launch, every frame's replay in one
 // launch (a block each), then the results to the host.
 ccnn_status Detector::enqueue_batch_kernels(BatchCtx& c, const Plan& p, int B) {
@@ -1596,7 +1632,7 @@ ccnn_status Detector::enqueue_batch_kernels(BatchCtx& c, const Plan& p, int B) {
     for (int f = 0; f < B; ++f) {
         Slot& s = slots_[c.first_slot + f];
         F.gray[f] = s.d_gray;
-        F.limg[f] = s.d_limg;
+        F.feat[f] = gated ? s.gate.feat : nullptr;
         F.s1[f] = s.d_s1;
         F.resp[f] = s.d_resp;
         F.counts[f] = s.d_counts;
@@ -1611,17 +1647,18 @@ ccnn_status Detector::enqueue_batch_kernels(BatchCtx& c, const Plan& p, int B) {
         WB.out[f] = s.d_win;
     }
     const int gpitch = slots_[c.first_slot].gray_pitch;
+    F.gpitch = gpitch;
+    F.gw = p.gw;
+    F.gh = p.gh;
     CCNN_CUDA(cudaMemsetAsync(c.d_sync, 0, sizeof(int) * (2 + kBatchStages * B), st));
     CCNN_CUDA(launch_gray_batch(c.d_src, B, p.in_w, p.in_h, p.ch, F, gpitch, st));
     if (gated)
         for (int f = 0; f < B; ++f) {
             Slot& s = slots_[c.first_slot + f];
-            CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, p.levels.data(), p.n_levels, s.gate, gate_thr_, gate_amb_frac_,
-                                  s.d_back_on, s.d_front_on, st));
+            CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, true, p.levels.data(), p.n_levels, s.gate, gate_thr_,
+                                  gate_amb_frac_, s.d_back_on, s.d_front_on, st));
         }
-    const LevelDesc& last = p.levels[p.n_levels - 1];
-    const int pyr_items = last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows);
-    CCNN_CUDA(launch_pyramid_batch(F, p.d_levels, p.n_levels, (int)p.chunks.size(), pyr_items, B, gpitch, p.gw, p.gh, st));
+    CCNN_CUDA(launch_counts_zero_batch(F, (int)p.chunks.size(), B, st));
     BatchQueue Q;
     build_batch_queue(&Q, B, p.n_levels, (int)p.chunks.size(), p.k1_tiles, p.k2_tiles, cfg_.thr1);
     const int grid = sm_count_ * stage1_batch_blocks_per_sm(batch_bpsm_);

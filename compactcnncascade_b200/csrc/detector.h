@@ -43,7 +43,7 @@ struct Slot {
     size_t in_pitch = 0;
     float* d_gray = nullptr;
     int gray_pitch = 0;  // floats
-    float* d_limg = nullptr;  // level arena: every level image of the frame
+    float* d_limg = nullptr;  // level arena: every level image of the frame (legacy family only)
     float* d_s1 = nullptr;
     float* d_resp = nullptr;
     int* d_counts = nullptr;
@@ -73,6 +73,7 @@ struct Slot {
     cudaGraph_t graph = nullptr;          // kept while `exec` lives: its gray-kernel node is updated per frame
     cudaGraphNode_t gray_node = nullptr;  // the gray conversion, retargeted at a device frame read in place
     cudaKernelNodeParams gray_kp{};
+    __half* gray_feat = nullptr;          // the gate features the captured gray node writes, or null
     bool gray_in_place = false;           // the node currently reads the caller's frame
     bool last_in_place = false;           // the last frame was not copied into d_in
     const Plan* last_plan = nullptr;  // plan of the last frame run on this slot
@@ -139,6 +140,7 @@ class Detector {
     ccnn_status gate_labels(uint8_t* d_labels, cudaStream_t st);
     // stage-1 tiles the gate let run in the last frame (slot 0), of all, and whether it fell back
     ccnn_status gate_stats(int* front_run, int* front_total, int* back_run, int* back_total, int* fallback);
+    ccnn_status gate_probabilities(float* out, int cap, int* n);
 
     // Non-blocking use of one slot by a single scheduling thread (the serving loop): launch a
     // host frame on slot k, test for completion, fetch the faces. Frames must have the size the
@@ -149,6 +151,7 @@ class Detector {
     ccnn_status fetch(int k, ccnn_face* faces, int cap, int* n);
     // device bytes held by the frame slots
     size_t slot_bytes() const;
+    long long limg_floats() const;
     // the device bytes create() would allocate for these arguments, computed on the host without
     // touching the device (so that a caller can make room before allocating)
     static ccnn_status estimate_bytes(const ccnn_params& p, const char* const* model_paths, int n_slots, bool colour_input,

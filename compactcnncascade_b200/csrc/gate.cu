@@ -257,13 +257,14 @@ inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t);
 namespace {
 
 // One launch for the whole network on a frame: each block computes a tile of kIX x kIY a2 pixels
-// (kIX/2 x kIY/2 cells) from the gray frame, with the same fp16 storage points as the training
-// forward (f, a1 and a2 rounded to binary16), writes the octave probabilities and sets the
-// cell's bit in the per-octave row bitmaps when the probability reaches the threshold.
+// (kIX/2 x kIY/2 cells) from the frame's binary16 input features (written by the gray-conversion
+// launch, or by gate_features_kernel), with the same fp16 storage points as the training forward
+// (f, a1 and a2 rounded to binary16), writes the octave probabilities and sets the cell's bit in the
+// per-octave row bitmaps when the probability reaches the threshold.
 constexpr int kIX = 16, kIY = 8;
 constexpr int kFX = kIX + 4, kFY = kIY + 4, kAX = kIX + 2, kAY = kIY + 2;
 
-__global__ void __launch_bounds__(256) gate_infer_kernel(const float* __restrict__ P, const float* __restrict__ gray, int gpitch, int w8, int h8,
+__global__ void __launch_bounds__(256) gate_infer_kernel(const float* __restrict__ P, const __half* __restrict__ feat, int w8, int h8,
                                                          float thr, float amb_lo, uint32_t* __restrict__ bits, int wwords,
                                                          float* __restrict__ prob, int* __restrict__ ambiguous) {
     __shared__ float sp[kGateParams];
@@ -277,23 +278,8 @@ __global__ void __launch_bounds__(256) gate_infer_kernel(const float* __restrict
     if (tid == 0) samb = 0;
     if (tid < kFX * kFY) {
         const int fx = x0 - 2 + tid % kFX, fy = y0 - 2 + tid / kFX;
-        float v = 0.f;  // zero padding of the first convolution
-        if (fx >= 0 && fx < w8 && fy >= 0 && fy < h8) {
-            // the detector's gray rows are 64-byte aligned with a pitch of 16 floats: 16-byte loads,
-            // summed in the same order as gate_features_kernel
-            float4 q[16];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                const float4* row = reinterpret_cast<const float4*>(gray + (size_t)(8 * fy + r) * gpitch + 8 * fx);
-                q[2 * r] = __ldg(row);
-                q[2 * r + 1] = __ldg(row + 1);
-            }
-            float s = 0.f;
-#pragma unroll
-            for (int r = 0; r < 16; ++r) s = (((s + q[r].x) + q[r].y) + q[r].z) + q[r].w;
-            v = (s * (1.f / 64.f) - 128.f) * (1.f / 64.f);
-        }
-        sf[tid / kFX][tid % kFX] = __float2half(v);
+        // zero padding of the first convolution
+        sf[tid / kFX][tid % kFX] = (fx >= 0 && fx < w8 && fy >= 0 && fy < h8) ? feat[(size_t)fy * w8 + fx] : __float2half(0.f);
     }
     __syncthreads();
     if (tid < kAX * kAY) {
@@ -313,22 +299,32 @@ __global__ void __launch_bounds__(256) gate_infer_kernel(const float* __restrict
     }
     __syncthreads();
     {
-        // two threads per a2 pixel, four output maps each
-        const int px = tid & (kIX * kIY - 1), half = tid / (kIX * kIY);
-        const int ix = px % kIX, iy = px / kIX;
+        // warp co computes output map co; lane l four a2 pixels of column l % 16 (rows 4 (l / 16) ..
+        // + 3), the map's 72 weights held in registers; every output sums its (ci, tap) products in
+        // the training forward's order
+        static_assert(kIX == 16 && kIY == 8 && kGC == 8, "one warp per map, 16 columns x 2 row groups of 4");
+        const int co = tid >> 5, lane = tid & 31;
+        const int ix = lane & 15, iy0 = (lane >> 4) * 4;
+        float wt[kGC * 9];
+#pragma unroll
+        for (int k = 0; k < kGC * 9; ++k) wt[k] = sp[kW2 + co * kGC * 9 + k];
         float z[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) z[j] = sp[kB2 + 4 * half + j];
+        for (int j = 0; j < 4; ++j) z[j] = sp[kB2 + co];
 #pragma unroll
-        for (int ci = 0; ci < kGC; ++ci)
+        for (int ci = 0; ci < kGC; ++ci) {
+            float v[6][3];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                const float v = __half2float(sa1[ci][iy + k / 3][ix + k % 3]);
+            for (int r = 0; r < 6; ++r)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) z[j] += sp[kW2 + ((4 * half + j) * kGC + ci) * 9 + k] * v;
-            }
+                for (int c = 0; c < 3; ++c) v[r][c] = __half2float(sa1[ci][iy0 + r][ix + c]);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) sa2[4 * half + j][iy][ix] = __float2half(lrelu(z[j]));
+            for (int k = 0; k < 9; ++k)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) z[j] += wt[ci * 9 + k] * v[j + k / 3][k % 3];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) sa2[co][iy0 + j][ix] = __float2half(lrelu(z[j]));
     }
     __syncthreads();
     const int w16 = w8 / 2, h16 = h8 / 2;
@@ -443,14 +439,15 @@ int gate_bitmap_words(int gw, int gh) {
     return kGK * h16 * ((w16 + 31) / 32);
 }
 
-cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, int gw, int gh, const LevelDesc* levels, int n_levels, GateScratch sc,
-                        float thr, float amb_frac, uint8_t* back_on, uint8_t* front_on, cudaStream_t st) {
+cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, int gw, int gh, bool feat_ready, const LevelDesc* levels,
+                        int n_levels, GateScratch sc, float thr, float amb_frac, uint8_t* back_on, uint8_t* front_on, cudaStream_t st) {
     const int w8 = gw / 8, h8 = gh / 8, w16 = w8 / 2, h16 = h8 / 2;
     const int wwords = (w16 + 31) / 32;
     // the ambiguous-cell counter and the bitmaps right behind it are one zeroed range
     cudaError_t e = cudaMemsetAsync(sc.ambiguous, 0, sizeof(uint32_t) * ((size_t)gate_bitmap_words(gw, gh) + 1), st);
     if (e != cudaSuccess) return e;
-    gate_infer_kernel<<<dim3((w8 + kIX - 1) / kIX, (h8 + kIY - 1) / kIY), 256, 0, st>>>(d_params, gray, gpitch, w8, h8, thr, 0.25f * thr, sc.bits,
+    if (!feat_ready) gate_features_kernel<<<dim3(blocks(w8, 128), h8), 128, 0, st>>>(gray, gpitch, w8, h8, sc.feat);
+    gate_infer_kernel<<<dim3((w8 + kIX - 1) / kIX, (h8 + kIY - 1) / kIY), 256, 0, st>>>(d_params, sc.feat, w8, h8, thr, 0.25f * thr, sc.bits,
                                                                                        wwords, sc.prob, sc.ambiguous);
     const int amb_limit = gate_cells(sc, gw, gh, amb_frac).amb_limit;
     const int n_words = gate_bitmap_words(gw, gh);

@@ -8,38 +8,12 @@
 // The scan space is cut into chunks that never straddle two levels (host-built chunk table,
 // chunks in visiting order). The stage-1 back kernel counts each chunk's hits as it writes the
 // responses; this kernel gives each chunk its offset (sum of the counts of earlier chunks) and
-// writes its hits in order using a ballot/popc prefix inside each warp and a warp-total scan
-// across the block.
+// writes its hits in order, ranked by warp ballots and per-(round, warp) counts.
 #include "kernels.h"
 
 namespace ccnn {
 
 constexpr int kChunkThreads = 256;
-
-// Exclusive prefix of a 0/1 predicate across the block: warp ballot + popc inside a warp,
-// then a shuffle scan over the (<= 32) warp totals. Returns the rank; *total gets the count.
-__device__ __forceinline__ int block_pred_rank(int pred, int* warp_tot, int* total) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const unsigned m = __ballot_sync(0xffffffffu, pred);
-    const int rank = __popc(m & ((1u << lane) - 1u));
-    if (lane == 0) warp_tot[wid] = __popc(m);
-    __syncthreads();
-    if (wid == 0) {
-        const int nw = blockDim.x >> 5;
-        int t = lane < nw ? warp_tot[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, t, o);
-            if (lane >= o) t += y;
-        }
-        if (lane < nw) warp_tot[lane] = t;  // inclusive
-        if (lane == nw - 1) *total = t;
-    }
-    __syncthreads();
-    const int r = (wid ? warp_tot[wid - 1] : 0) + rank;
-    __syncthreads();
-    return r;
-}
 
 __device__ __forceinline__ int block_sum(int v, int* warp_tot) {
 #pragma unroll
@@ -53,40 +27,62 @@ __device__ __forceinline__ int block_sum(int v, int* warp_tot) {
     return t;
 }
 
-// the hits of chunk `c` of a frame's scan, written in raster order after those of earlier chunks
+// the hits of chunk `c` of a frame's scan, written in raster order after those of earlier chunks.
+// A chunk the stage-1 kernel counted no hit in writes nothing (only the last chunk, which stores the
+// frame's total, still sums the counts). The others load all their responses at once (round k of
+// thread t holds element 256 k + t), rank every hit by ballots (one count per (round, warp) in
+// shared memory, one barrier) and write it at the chunk's offset plus its rank.
+constexpr int kChunkRounds = kCandChunk / kChunkThreads;  // 8
+static_assert(kChunkRounds * kChunkThreads == kCandChunk, "a chunk is whole rounds of the block");
+
 __device__ __forceinline__ void cand_write_chunk(const int4* __restrict__ chunks, int n_chunks, const LevelDesc* __restrict__ levels,
                                                  const float* __restrict__ resp, float thr, const int* __restrict__ counts,
                                                  Candidate* __restrict__ out, int* __restrict__ n_out, int cap, int c) {
     __shared__ int wt[32];
-    __shared__ int tot;
+    __shared__ int rw[kChunkRounds * (kChunkThreads / 32)];
+    const int hits = counts[c];  // uniform over the block
+    const bool last = c == n_chunks - 1;
+    if (hits == 0 && !last) return;
     // offset of this chunk = sum of the counts of the chunks visited before it
     int part = 0;
     for (int i = threadIdx.x; i < c; i += blockDim.x) part += counts[i];
-    int off = block_sum(part, wt);
-    if (c == n_chunks - 1 && threadIdx.x == 0) *n_out = min(off + counts[c], cap);
+    const int off = block_sum(part, wt);
+    if (last && threadIdx.x == 0) *n_out = min(off + hits, cap);
+    if (hits == 0) return;
 
     const int4 ck = chunks[c];
-    const LevelDesc L = levels[ck.x];
-    for (int b0 = 0; b0 < ck.z; b0 += blockDim.x) {
-        const int i = b0 + threadIdx.x;
-        float r = 0.f;
-        int hit = 0;
-        if (i < ck.z) {
-            r = resp[L.resp_off + ck.y + i];
-            hit = r > thr ? 1 : 0;
+    const LevelDesc& L = levels[ck.x];
+    const float* src = resp + L.resp_off + ck.y;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float r[kChunkRounds];
+#pragma unroll
+    for (int k = 0; k < kChunkRounds; ++k) {
+        const int i = k * kChunkThreads + threadIdx.x;
+        r[k] = i < ck.z ? src[i] : thr;  // thr itself is never a hit
+    }
+    unsigned m[kChunkRounds];
+#pragma unroll
+    for (int k = 0; k < kChunkRounds; ++k) {
+        m[k] = __ballot_sync(0xffffffffu, r[k] > thr);
+        if (lane == 0) rw[k * (kChunkThreads / 32) + wid] = __popc(m[k]);
+    }
+    __syncthreads();
+    const int ow = L.ow;
+#pragma unroll
+    for (int k = 0; k < kChunkRounds; ++k) {
+        if (!(r[k] > thr)) continue;
+        int pos = off + __popc(m[k] & ((1u << lane) - 1u));
+        for (int q = 0; q < k * (kChunkThreads / 32) + wid; ++q) pos += rw[q];
+        if (pos < cap) {
+            const int e = ck.y + k * kChunkThreads + threadIdx.x;
+            const int j = e / ow, ii = e - j * ow;
+            Candidate cd;
+            cd.level = ck.x;
+            cd.px = ii * 4;
+            cd.py = j * 4;
+            cd.score = r[k];
+            out[pos] = cd;
         }
-        const int pos = block_pred_rank(hit, wt, &tot);
-        if (hit && off + pos < cap) {
-            const int e = ck.y + i;
-            const int j = e / L.ow, ii = e - j * L.ow;
-            Candidate c;
-            c.level = ck.x;
-            c.px = ii * 4;
-            c.py = j * 4;
-            c.score = r;
-            out[off + pos] = c;
-        }
-        off += tot;
     }
 }
 

@@ -7,6 +7,7 @@
 // Each thread converts 16 consecutive pixels of one row with 128-bit loads (1, 3 or 4 x uint4)
 // and 128-bit stores; the staging buffer's row pitch is a multiple of 64 bytes so every
 // vector access is aligned. Rows whose width is not a multiple of 16 finish with scalar code.
+// With the learned gate on, the same launch also writes the gate's 1/8-resolution input features.
 #include "kernels.h"
 #include "pyramid.cuh"
 #include "resample.cuh"
@@ -17,86 +18,129 @@ __device__ __forceinline__ float gray_bgr(uint32_t b, uint32_t g, uint32_t r) {
     return fadd(fadd(fmul(0.114f, (float)b), fmul(0.587f, (float)g)), fmul(0.299f, (float)r));
 }
 
-// 16 pixels of a row (item = row x 16-pixel chunk), 128-bit loads and stores
-template <int CH>
-__device__ __forceinline__ void gray_chunk(const uint8_t* __restrict__ src, int spitch, int w, int h, float* __restrict__ dst, int dpitch,
-                                           int item) {
-    const int chunks = (w + 15) >> 4;  // 16-pixel chunks per row; one chunk per thread
-    const int y = item / chunks;
-    const int x0 = (item - y * chunks) * 16;
-    if (y >= h) return;
-    const uint8_t* row = src + (size_t)y * spitch;
-    float* out = dst + (size_t)y * dpitch;
-    if (x0 + 16 <= w) {
-        uint8_t px[16 * CH];
-        const uint4* vsrc = reinterpret_cast<const uint4*>(row + (size_t)x0 * CH);
+// One block converts 8 rows (a warp each) x 32 chunks of 16 pixels (a lane each): 128-bit loads
+// and stores, a warp's accesses walking one row. kFeat (the learned gate is on): the block also keeps
+// its rows in shared memory and writes the gate's input features of its 8x8 cells, each the sum of
+// the cell's 64 gray values in row-major order from 0 (the order the gate's training forward uses,
+// gate.cu), (sum / 64 - 128) / 64 in binary16; only cells wholly inside the frame (W/8 x H/8) get one.
+constexpr int kGrayRows = 8, kGrayChunks = 32;
+constexpr int kCellPitch = 9;  // floats per 8-pixel cell row in shared memory (padded: conflict-free sums)
+
+template <int CH, bool kFeat>
+__device__ __forceinline__ void gray_block(const uint8_t* __restrict__ src, int spitch, int w, int h, float* __restrict__ dst, int dpitch,
+                                           __half* __restrict__ feat, int bx, int by) {
+    __shared__ float keep[kFeat ? kGrayRows : 1][kFeat ? 2 * kGrayChunks * kCellPitch : 1];
+    const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
+    const int x0 = (bx * kGrayChunks + lane) * 16;
+    const int y = by * kGrayRows + r;
+    if (y < h && x0 < w) {
+        const uint8_t* row = src + (size_t)y * spitch;
+        float* out = dst + (size_t)y * dpitch;
+        // pixel k of the chunk: cell 2 * lane + k / 8, position k % 8
+        auto keep_px = [&](int k, float v) {
+            if constexpr (kFeat) keep[r][(2 * lane + (k >> 3)) * kCellPitch + (k & 7)] = v;
+        };
+        if (x0 + 16 <= w) {
+            uint8_t px[16 * CH];
+            const uint4* vsrc = reinterpret_cast<const uint4*>(row + (size_t)x0 * CH);
 #pragma unroll
-        for (int v = 0; v < CH; ++v) *reinterpret_cast<uint4*>(px + 16 * v) = __ldg(vsrc + v);
-        float g[16];
+            for (int v = 0; v < CH; ++v) *reinterpret_cast<uint4*>(px + 16 * v) = __ldg(vsrc + v);
+            float g[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            if (CH == 1)
-                g[i] = (float)px[i];
-            else
-                g[i] = gray_bgr(px[i * CH + 0], px[i * CH + 1], px[i * CH + 2]);
+            for (int i = 0; i < 16; ++i) {
+                if (CH == 1)
+                    g[i] = (float)px[i];
+                else
+                    g[i] = gray_bgr(px[i * CH + 0], px[i * CH + 1], px[i * CH + 2]);
+                keep_px(i, g[i]);
+            }
+            float4* vdst = reinterpret_cast<float4*>(out + x0);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) vdst[v] = make_float4(g[4 * v], g[4 * v + 1], g[4 * v + 2], g[4 * v + 3]);
+        } else {
+            for (int x = x0; x < w; ++x) {
+                const uint8_t* p = row + (size_t)x * CH;
+                const float v = (CH == 1) ? (float)p[0] : gray_bgr(p[0], p[1], p[2]);
+                out[x] = v;
+                keep_px(x - x0, v);
+            }
         }
-        float4* vdst = reinterpret_cast<float4*>(out + x0);
+    }
+    if constexpr (kFeat) {
+        __syncthreads();
+        const int w8 = w / 8, h8 = h / 8;
+        const int cx = bx * 2 * kGrayChunks + threadIdx.x;
+        if (threadIdx.x < 2 * kGrayChunks && cx < w8 && by < h8) {
+            float sum = 0.f;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) vdst[v] = make_float4(g[4 * v], g[4 * v + 1], g[4 * v + 2], g[4 * v + 3]);
-    } else {
-        for (int x = x0; x < w; ++x) {
-            const uint8_t* p = row + (size_t)x * CH;
-            out[x] = (CH == 1) ? (float)p[0] : gray_bgr(p[0], p[1], p[2]);
+            for (int rr = 0; rr < kGrayRows; ++rr)
+#pragma unroll
+                for (int c = 0; c < 8; ++c) sum = fadd(sum, keep[rr][threadIdx.x * kCellPitch + c]);
+            feat[(size_t)by * w8 + cx] = __float2half(fmul(fsub(fmul(sum, 1.f / 64.f), 128.f), 1.f / 64.f));
         }
     }
 }
 
-template <int CH>
+template <int CH, bool kFeat>
 __global__ void __launch_bounds__(256) gray_kernel(const uint8_t* __restrict__ src, int spitch, int w, int h,
-                                                   float* __restrict__ dst, int dpitch) {
-    gray_chunk<CH>(src, spitch, w, h, dst, dpitch, blockIdx.x * blockDim.x + threadIdx.x);
+                                                   float* __restrict__ dst, int dpitch, __half* __restrict__ feat) {
+    gray_block<CH, kFeat>(src, spitch, w, h, dst, dpitch, feat, blockIdx.x, blockIdx.y);
 }
 
-// the frames of a batch: blockIdx.y is the frame; sources (64-byte aligned base and pitch) from a
+static dim3 gray_grid(int w, int h, int frames = 1) {
+    const int chunks = (w + 15) / 16;
+    return dim3((unsigned)((chunks + kGrayChunks - 1) / kGrayChunks), (unsigned)((h + kGrayRows - 1) / kGrayRows), (unsigned)frames);
+}
+
+// the frames of a batch: blockIdx.z is the frame; sources (64-byte aligned base and pitch) from a
 // device table the host fills before every launch
-template <int CH>
+template <int CH, bool kFeat>
 __global__ void __launch_bounds__(256) gray_batch_kernel(const FrameSrc* __restrict__ src, int w, int h, const __grid_constant__ BatchFrames F,
                                                          int dpitch) {
-    const FrameSrc fs = src[blockIdx.y];
-    gray_chunk<CH>(fs.data, fs.pitch, w, h, const_cast<float*>(F.gray[blockIdx.y]), dpitch, blockIdx.x * blockDim.x + threadIdx.x);
+    const FrameSrc fs = src[blockIdx.z];
+    gray_block<CH, kFeat>(fs.data, fs.pitch, w, h, const_cast<float*>(F.gray[blockIdx.z]), dpitch, F.feat[blockIdx.z], blockIdx.x, blockIdx.y);
 }
 
 cudaError_t launch_gray_batch(const FrameSrc* d_src, int n_frames, int w, int h, int ch, const BatchFrames& F, int dpitch, cudaStream_t st) {
-    const long long items = (long long)h * ((w + 15) / 16);
-    dim3 grid((unsigned)((items + 255) / 256), (unsigned)n_frames);
-    switch (ch) {
-        case 1: gray_batch_kernel<1><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
-        case 3: gray_batch_kernel<3><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
-        case 4: gray_batch_kernel<4><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
+    const dim3 grid = gray_grid(w, h, n_frames);
+    const bool feat = F.feat[0] != nullptr;
+    switch (ch * 2 + (feat ? 1 : 0)) {
+        case 2: gray_batch_kernel<1, false><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
+        case 3: gray_batch_kernel<1, true><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
+        case 6: gray_batch_kernel<3, false><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
+        case 7: gray_batch_kernel<3, true><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
+        case 8: gray_batch_kernel<4, false><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
+        case 9: gray_batch_kernel<4, true><<<grid, 256, 0, st>>>(d_src, w, h, F, dpitch); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
-const void* gray_kernel_fn(int ch) {
+template <int CH>
+static const void* gray_fn(bool feat) {
+    return feat ? reinterpret_cast<const void*>(gray_kernel<CH, true>) : reinterpret_cast<const void*>(gray_kernel<CH, false>);
+}
+
+const void* gray_kernel_fn(int ch, bool feat) {
     switch (ch) {
-        case 1: return reinterpret_cast<const void*>(gray_kernel<1>);
-        case 3: return reinterpret_cast<const void*>(gray_kernel<3>);
-        case 4: return reinterpret_cast<const void*>(gray_kernel<4>);
+        case 1: return gray_fn<1>(feat);
+        case 3: return gray_fn<3>(feat);
+        case 4: return gray_fn<4>(feat);
     }
     return nullptr;
 }
 
-cudaError_t launch_gray(const uint8_t* src, int spitch, int w, int h, int ch, float* dst, int dpitch, cudaStream_t st) {
+cudaError_t launch_gray(const uint8_t* src, int spitch, int w, int h, int ch, float* dst, int dpitch, cudaStream_t st, __half* feat) {
     if ((spitch & 63) || (dpitch & 15) || (reinterpret_cast<uintptr_t>(src) & 63) || (reinterpret_cast<uintptr_t>(dst) & 63))
         return cudaErrorMisalignedAddress;  // the staging buffers are allocated 64-byte aligned
-    dim3 block(256);
-    const long long items = (long long)h * ((w + 15) / 16);
-    dim3 grid((unsigned)((items + 255) / 256));
-    switch (ch) {
-        case 1: gray_kernel<1><<<grid, block, 0, st>>>(src, spitch, w, h, dst, dpitch); break;
-        case 3: gray_kernel<3><<<grid, block, 0, st>>>(src, spitch, w, h, dst, dpitch); break;
-        case 4: gray_kernel<4><<<grid, block, 0, st>>>(src, spitch, w, h, dst, dpitch); break;
+    const dim3 grid = gray_grid(w, h);
+    switch (ch * 2 + (feat ? 1 : 0)) {
+        case 2: gray_kernel<1, false><<<grid, 256, 0, st>>>(src, spitch, w, h, dst, dpitch, feat); break;
+        case 3: gray_kernel<1, true><<<grid, 256, 0, st>>>(src, spitch, w, h, dst, dpitch, feat); break;
+        case 6: gray_kernel<3, false><<<grid, 256, 0, st>>>(src, spitch, w, h, dst, dpitch, feat); break;
+        case 7: gray_kernel<3, true><<<grid, 256, 0, st>>>(src, spitch, w, h, dst, dpitch, feat); break;
+        case 8: gray_kernel<4, false><<<grid, 256, 0, st>>>(src, spitch, w, h, dst, dpitch, feat); break;
+        case 9: gray_kernel<4, true><<<grid, 256, 0, st>>>(src, spitch, w, h, dst, dpitch, feat); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

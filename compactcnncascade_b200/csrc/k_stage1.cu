@@ -5,9 +5,11 @@
 // add/add2 (:916-950), conv_3x3 (:36-91), conv_5x4 (:158-187), lrelu_bn (:623-645),
 // mulCN_add_tanhW (:646-672), mulC/mulC1_add (:952-984), tanhW (:673-690).
 //
-// front: one CTA per 32x16 tile of pooled L1 pixels of one level. The CTA stages its (67 x 35)
-//        input tile of the level image, runs the 4x4 conv + folded BN/LReLU + 2x2 max for the 4
-//        L1 maps and writes the 4 neighbour-map sums that L2 consumes (S1 arena).
+// front: one CTA per 32x16 tile of pooled L1 pixels of one level. The CTA resamples its (67 x 35)
+//        input tile of the level image straight from the gray frame (the pyramid is never stored;
+//        a stored image is read instead where the caller gives one), runs the 4x4 conv + folded
+//        BN/LReLU + 2x2 max for the 4 L1 maps and writes the 4 neighbour-map sums that L2 consumes
+//        (S1 arena).
 // back:  one CTA per 32x16 tile of response pixels. It stages the S1 tile (4 x 42 x 72, two maps at
 //        a time) in shared memory, computes the 8 pooled L2 maps and their sums on the 35 x 20 halo
 //        tile, then every thread finishes two vertically adjacent response pixels: the 16 L3 maps
@@ -77,19 +79,67 @@ __device__ __forceinline__ void load_front_tile(FrontTile& T, const float* __res
     }
 }
 
-// Front tile t of level L: its (67 x 35) level-image tile staged in T, then the 4x4 conv + folded
+// The front tile straight from the gray frame: every level pixel of the (67 x 35) tile resampled the
+// way the pyramid kernel writes it (copy, nearest neighbour, or bilinear on the 12-bit fixed-point
+// steps; RunCPUDetect, cnn_detector_v3.cpp:2090-2104, with ImageResizer, image_resize.cpp:46-122,
+// 393-541), so the level image is never stored. Thread (g, c) takes tile column c < 64 (its column
+// sample in registers) and rows g, g + 4, ... of it, so a warp reads 32 neighbouring columns of the
+// same gray rows; columns 64-66 follow, one sample a thread. Pixels outside the level read as 0, like
+// the zero columns past a stored level image's width. The gray frame was written by an earlier
+// launch (read-only path).
+struct FrontSmem {
+    FrontTile T;
+};
+
+// level pixel (x, y) = tile (c, r) from its column sample sx
+__device__ __forceinline__ float resample_px(const GrayRef& G, const LevelDesc& L, const AxisSample& sx, int x, int y) {
+    if (x >= L.w || y >= L.h) return 0.f;
+    if (L.mode == 0) return __ldg(G.p + (size_t)y * G.pitch + x);
+    const AxisSample sy = sample_row(y, L.scly, G.h);
+    if (L.mode == 1) return __ldg(G.p + (size_t)sy.idx * G.pitch + sx.idx);
+    uint32_t py = sy.idx;
+    if (py + 1 >= (uint32_t)G.h) py--;  // bilinear keeps a row below
+    const float* r0 = G.p + (size_t)py * G.pitch + sx.idx;
+    const float top = fadd(fmul(__ldg(r0), sx.c), fmul(__ldg(r0 + 1), sx.f));
+    const float bot = fadd(fmul(__ldg(r0 + G.pitch), sx.c), fmul(__ldg(r0 + G.pitch + 1), sx.f));
+    return fadd(fmul(top, sy.c), fmul(bot, sy.f));
+}
+
+__device__ __forceinline__ void resample_front_tile(FrontSmem& S, const GrayRef& G, const LevelDesc& L, int ix0, int iy0) {
+    static_assert(kInW == 67 && kInH == 35, "64 + 3 columns, 35 rows in 4 row groups");
+    {
+        const int c = threadIdx.x & 63, g = threadIdx.x >> 6;
+        const AxisSample sx = sample_col(ix0 + c, L.sclx, G.w);
+#pragma unroll
+        for (int k = 0; k < (kInH + 3) / 4; ++k) {
+            const int r = g + 4 * k;
+            if (r < kInH) S.T.put(r, c, resample_px(G, L, sx, ix0 + c, iy0 + r));
+        }
+    }
+    if (threadIdx.x < 3 * kInH) {
+        const int c = 64 + threadIdx.x % 3, r = threadIdx.x / 3;
+        S.T.put(r, c, resample_px(G, L, sample_col(ix0 + c, L.sclx, G.w), ix0 + c, iy0 + r));
+    }
+}
+
+// Front tile t of level L: its (67 x 35) level-image tile staged in S.T (resampled from the gray
+// frame G when kFromGray, else read from the stored level images limg), then the 4x4 conv + folded
 // BN/LReLU + 2x2 max of the 4 L1 maps for 32 x 16 pooled pixels (two vertically adjacent pixels a
-// thread) and the 4 neighbour-map sums written to the S1 arena. kCoherent: the level image was
+// thread) and the 4 neighbour-map sums written to the S1 arena. kCoherent: a stored level image was
 // written earlier in the same launch (read through L2, not the read-only path).
-template <bool kCoherent>
-__device__ __forceinline__ void front_tile(const Stage1W& W, FrontTile& T, const LevelDesc& L, int t, const float* __restrict__ limg,
-                                           float* __restrict__ s1) {
+template <bool kFromGray, bool kCoherent>
+__device__ __forceinline__ void front_tile(const Stage1W& W, FrontSmem& S, const LevelDesc& L, int t, const float* __restrict__ limg,
+                                           const GrayRef& G, float* __restrict__ s1) {
     const int px0 = (t % L.k1_tiles_x) * kK1TileX;
     const int py0 = (t / L.k1_tiles_x) * kK1TileY;
     const int ix0 = 2 * px0, iy0 = 2 * py0;
 
-    load_front_tile<kCoherent>(T, limg + L.img_off, L, ix0, iy0);
+    if constexpr (kFromGray)
+        resample_front_tile(S, G, L, ix0, iy0);
+    else
+        load_front_tile<kCoherent>(S.T, limg + L.img_off, L, ix0, iy0);
     __syncthreads();
+    const FrontTile& T = S.T;
 
     const int qx = threadIdx.x & (kK1TileX - 1);
     const int qy = (threadIdx.x >> 5) * 2;
@@ -134,15 +184,17 @@ __device__ __forceinline__ void front_tile(const Stage1W& W, FrontTile& T, const
 }
 
 
-template <int kMinBlocks>
+// kFromGray: level tiles resampled from the gray frame G (the detection path), else read from the
+// stored level images limg (a caller's own level image)
+template <bool kFromGray, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) stage1_front_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ LevelTable LT,
-                                                              const float* __restrict__ limg, float* __restrict__ s1,
+                                                              const float* __restrict__ limg, const GrayRef G, float* __restrict__ s1,
                                                               const uint8_t* __restrict__ front_on) {
-    __shared__ FrontTile T;
+    __shared__ FrontSmem S;
     const int g = LT.first + blockIdx.x;
     if (front_on && !front_on[g]) return;  // gated off: no back tile reads this one
     const LevelDesc& L = LT.lv[find_level<&LevelDesc::k1_base>(LT, g)];
-    front_tile<false>(W, T, L, g - L.k1_base, limg, s1);
+    front_tile<kFromGray, false>(W, S, L, g - L.k1_base, limg, G, s1);
 }
 
 constexpr int kP2TW = kK2TileX + 3;   // 35 pooled L2 columns (halo 3)
@@ -284,6 +336,25 @@ __device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, 
 
     // C: pixels (x, y) and (x, y + 1)
     const int x = threadIdx.x & (kK2TileX - 1), y = (threadIdx.x / kK2TileX) * 2;
+    if (cells.bits && *cells.ambiguous <= cells.amb_limit) {
+        // learned gate, per warp (its 32 x 2 response pixels): when no likely cell of the level's
+        // octave lies within one cell of any of their window centres, every candidate among them
+        // would be dropped below, so the warp writes the skip marker instead of computing them
+        const int gy = oy0 + y;  // warp-uniform
+        const int gx1 = min(ox0 + kK2TileX, L.ow) - 1, gy1 = min(gy + 1, L.oh - 1);
+        const int cx0 = (int)((4.f * ox0 + 11.5f) * L.inv_scale) / 16, cx1 = (int)((4.f * gx1 + 11.5f) * L.inv_scale) / 16;
+        const int cy0 = (int)((4.f * gy + 13.5f) * L.inv_scale) / 16, cy1 = (int)((4.f * gy1 + 13.5f) * L.inv_scale) / 16;
+        const uint32_t* B = cells.bits + (long long)min(L.octave, kGK - 1) * cells.h16 * cells.wwords;
+        if (gy >= L.oh || !gate_any_bit(B, cells.wwords, max(0, cx0 - 1), min(cells.w16 - 1, cx1 + 1), max(0, cy0 - 1),
+                                       min(cells.h16 - 1, cy1 + 1))) {
+            const int gx = ox0 + x;
+            if (gx < L.ow) {
+                if (gy < L.oh) resp[L.resp_off + (long long)gy * L.ow + gx] = -1e30f;
+                if (gy + 1 < L.oh) resp[L.resp_off + (long long)(gy + 1) * L.ow + gx] = -1e30f;
+            }
+            return;
+        }
+    }
     // L3 maps (2k, 2k+1) of the pixel pair, both from neighbour-sum map k; conv_5x4 keeps one
     // partial sum per kernel row, added in row order
     auto l3_pair = [&](int k, f2_t* m0, f2_t* m1) {
@@ -438,14 +509,15 @@ static cudaError_t launch_grouped(const LevelDesc* levels, int n_levels, int Lev
 }
 
 cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st,
-                                const uint8_t* front_on, Stage1Sched sched) {
+                                const uint8_t* front_on, Stage1Sched sched, GrayRef gray) {
     return launch_grouped(
         levels, n_levels, &LevelDesc::k1_base, [](const LevelDesc& L) { return L.k1_tiles_x * ((L.p1h + kK1TileY - 1) / kK1TileY); },
         [&](const LevelTable& T, int blocks) {
-            if (sched.front_blocks_per_sm >= 4)
-                stage1_front_kernel<4><<<blocks, 256, 0, st>>>(W, T, limg, s1, front_on);
+            const bool four = sched.front_blocks_per_sm >= 4;
+            if (gray.p)
+                (four ? stage1_front_kernel<true, 4> : stage1_front_kernel<true, 3>)<<<blocks, 256, 0, st>>>(W, T, limg, gray, s1, front_on);
             else
-                stage1_front_kernel<3><<<blocks, 256, 0, st>>>(W, T, limg, s1, front_on);
+                (four ? stage1_front_kernel<false, 4> : stage1_front_kernel<false, 3>)<<<blocks, 256, 0, st>>>(W, T, limg, gray, s1, front_on);
         });
 }
 
@@ -464,8 +536,8 @@ cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_
 
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
                           cudaStream_t st, int* counts, float thr, const uint8_t* front_on, const uint8_t* back_on, GateCells cells,
-                          Stage1Sched sched) {
-    cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st, front_on, sched);
+                          Stage1Sched sched, GrayRef gray) {
+    cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st, front_on, sched, gray);
     if (e != cudaSuccess) return e;
     return launch_stage1_back(W, levels, n_levels, s1, resp, st, counts, thr, back_on, cells, sched);
 }
@@ -513,7 +585,7 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
     return v;
 }
 
-constexpr int kBatchSmem = (int)sizeof(BackSmem) > (int)sizeof(FrontTile) ? (int)sizeof(BackSmem) : (int)sizeof(FrontTile);
+constexpr int kBatchSmem = (int)sizeof(BackSmem) > (int)sizeof(FrontSmem) ? (int)sizeof(BackSmem) : (int)sizeof(FrontSmem);
 
 template <int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) stage1_batch_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ Stage1Dup D,
@@ -569,7 +641,8 @@ __global__ void __launch_bounds__(256, kMinBlocks) stage1_batch_kernel(const __g
         const LevelDesc& L = levels[lo];
         if (stage == 0) {
             if (!F.front_on[f] || F.front_on[f][g])
-                front_tile<false>(W, *reinterpret_cast<FrontTile*>(smem_raw), L, g - L.k1_base, F.limg[f], F.s1[f]);
+                front_tile<true, false>(W, *reinterpret_cast<FrontSmem*>(smem_raw), L, g - L.k1_base, nullptr,
+                                  GrayRef{F.gray[f], F.gpitch, F.gw, F.gh}, F.s1[f]);
         } else {
             back_tile<true>(W, D, *reinterpret_cast<BackSmem*>(smem_raw), L, g - L.k2_base, g, F.s1[f], F.resp[f], F.counts[f], Q.thr,
                             F.back_on[f], F.cells[f]);
@@ -585,26 +658,16 @@ __global__ void __launch_bounds__(256, kMinBlocks) stage1_batch_kernel(const __g
     }
 }
 
-// The batched pyramid: blockIdx.y is the frame, every level of it in one grid (level bases searched
-// in global memory, no level-count limit); block 0 of a frame also zeroes its candidate counts.
-__global__ void __launch_bounds__(kPyrCols) pyramid_batch_kernel(const __grid_constant__ BatchFrames F, const LevelDesc* __restrict__ levels,
-                                                                 int n_levels, int n_chunks, int gpitch, int gw, int gh) {
-    const int f = blockIdx.y, g = blockIdx.x;
-    if (g == 0)
-        for (int i = threadIdx.x; i < n_chunks; i += blockDim.x) F.counts[f][i] = 0;
-    int lo = 0, hi = n_levels - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (levels[mid].pyr_base <= g) lo = mid; else hi = mid - 1;
-    }
-    const LevelDesc& L = levels[lo];
-    pyramid_block(L, g - L.pyr_base, F.gray[f], gpitch, gw, gh, F.limg[f], F.front_on[f]);
+// The candidate counts of every frame of a batch zeroed (blockIdx.x is the frame), before the
+// persistent stage-1 launch counts into them.
+__global__ void __launch_bounds__(256) counts_zero_batch_kernel(const __grid_constant__ BatchFrames F, int n_chunks) {
+    int* c = F.counts[blockIdx.x];
+    for (int i = threadIdx.x; i < n_chunks; i += blockDim.x) c[i] = 0;
 }
 
-cudaError_t launch_pyramid_batch(const BatchFrames& F, const LevelDesc* d_levels, int n_levels, int n_chunks, int pyr_items, int n_frames,
-                                 int gpitch, int gw, int gh, cudaStream_t st) {
-    if (pyr_items <= 0) return cudaSuccess;
-    pyramid_batch_kernel<<<dim3(pyr_items, n_frames), kPyrCols, 0, st>>>(F, d_levels, n_levels, n_chunks, gpitch, gw, gh);
+cudaError_t launch_counts_zero_batch(const BatchFrames& F, int n_chunks, int n_frames, cudaStream_t st) {
+    if (n_chunks <= 0 || n_frames <= 0) return cudaSuccess;
+    counts_zero_batch_kernel<<<n_frames, 256, 0, st>>>(F, n_chunks);
     return cudaGetLastError();
 }
 

@@ -411,8 +411,8 @@ __device__ __forceinline__ void window_item(const WindowNets& N, const WinArgs& 
     __syncthreads();
 }
 
-// kMinBlocks: the register budget (4 resident blocks a SM: 64 registers; 2: up to 128, no spills),
-// matched to the schedule's resident blocks
+// kMinBlocks: the register budget (2 resident blocks a SM: up to 128 registers, no spills; 4: 64;
+// 5: 48; 6: 40, more spilled), matched to the schedule's resident blocks
 template <bool kLegacy, int kMinBlocks>
 __global__ void __launch_bounds__(kWT, kMinBlocks) window_kernel(const __grid_constant__ WindowNets N, const WinArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -491,9 +491,21 @@ cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, in
         window_kernel<true, 4><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
     else if (ctas_per_sm <= 2)
         window_kernel<false, 2><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
+    else if (ctas_per_sm == 5)
+        window_kernel<false, 5><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
+    else if (ctas_per_sm >= 6)
+        window_kernel<false, 6><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
     else
         window_kernel<false, 4><<<grid, kWT, sizeof(WindowSmem), st>>>(N, a);
     return cudaGetLastError();
+}
+
+// five or six resident window blocks need most of a SM's 228 KB as shared memory
+cudaError_t window_setup() {
+    cudaError_t e = cudaFuncSetAttribute(window_kernel<false, 5>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(window_kernel<false, 6>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    return e;
 }
 
 }  // namespace ccnn

@@ -50,9 +50,12 @@ struct ReplayArgs {
     int* n_m_out;
 };
 
-// the gray kernel instantiation for `ch` channels (to find its node in a captured graph)
-const void* gray_kernel_fn(int ch);
-cudaError_t launch_gray(const uint8_t* src, int spitch, int w, int h, int ch, float* dst, int dpitch, cudaStream_t st);
+// the gray kernel instantiation for `ch` channels, with or without the gate features (to find its
+// node in a captured graph)
+const void* gray_kernel_fn(int ch, bool feat);
+// feat (optional): the learned gate's binary16 input features (W/8 x H/8) written by the same launch
+cudaError_t launch_gray(const uint8_t* src, int spitch, int w, int h, int ch, float* dst, int dpitch, cudaStream_t st,
+                        __half* feat = nullptr);
 cudaError_t launch_gray_u8_resized(const uint8_t* src, int spitch, int sw, int sh, float* dst, int dpitch, int dw, int dh,
                                    cudaStream_t st);
 cudaError_t launch_resize_f32(const float* src, int spitch, int sw, int sh, float* dst, int dpitch, int dw, int dh, int type,
@@ -64,14 +67,17 @@ struct GateScratch {
     int* ambiguous;  // cells with a probability in [thr / 4, thr); the bitmaps follow it
     uint32_t* bits;  // per octave, per cell row: one bit per cell at or above the threshold
     float* prob;     // kGK x (W/16 x H/16) probabilities
+    __half* feat;    // W/8 x H/8 binary16 input features
 };
 // words of the octave row bitmaps for a gw x gh gray frame
 int gate_bitmap_words(int gw, int gh);
 // the gate network on the frame's gray image, then the stage-1 tile activity of every level
 // the cell bitmaps of a gated frame for the stage-1 back kernel
 GateCells gate_cells(GateScratch sc, int gw, int gh, float amb_frac);
-cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, int gw, int gh, const LevelDesc* levels, int n_levels, GateScratch sc,
-                        float thr, float amb_frac, uint8_t* back_on, uint8_t* front_on, cudaStream_t st);
+// feat_ready: sc.feat already holds the frame's features (the gray launch wrote them); otherwise they
+// are computed from `gray` first
+cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, int gw, int gh, bool feat_ready, const LevelDesc* levels,
+                        int n_levels, GateScratch sc, float thr, float amb_frac, uint8_t* back_on, uint8_t* front_on, cudaStream_t st);
 cudaError_t launch_gate_labels(const Candidate* cands, const CandResult* res, const int* ncand, int cap, const LevelDesc* d_levels, int gw, int gh,
                                uint8_t* labels, cudaStream_t st);
 
@@ -83,10 +89,12 @@ cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* g
                            const uint8_t* front_on = nullptr);
 // ---- batched form: one persistent launch runs the pyramid and stage 1 of B frames ----
 constexpr int kMaxBatch = 16;
-// per-frame buffers of the frames of one batch (frame f = entry f)
+// per-frame buffers of the frames of one batch (frame f = entry f); the gray frames share one size
+// and pitch
 struct BatchFrames {
     const float* gray[kMaxBatch];
-    float* limg[kMaxBatch];
+    __half* feat[kMaxBatch];  // the learned gate's input features (written by the gray launch), or null
+    int gpitch, gw, gh;
     float* s1[kMaxBatch];
     float* resp[kMaxBatch];
     int* counts[kMaxBatch];
@@ -110,7 +118,8 @@ struct BatchQueue {
 void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, int front_items, int back_items, float thr);
 // sync: 1 + kBatchStages * n_frames ints, zero before the launch (queue head, finished items per
 // (frame, stage)); err: set to 1 when a dependency wait gave up (results of the batch invalid).
-// The level images must exist (launch_pyramid_batch) and the candidate counts be zero.
+// Front items resample their level tiles from the gray frames (the pyramid is never stored); the
+// candidate counts must be zero (launch_counts_zero_batch).
 cudaError_t launch_stage1_batch(const Stage1W& W, const BatchFrames& F, const BatchQueue& Q, const LevelDesc* d_levels, int* sync, int* err,
                                 int grid, cudaStream_t st, int blocks_per_sm);
 // levels of a pyramid the persistent stage-1 kernel takes (their first items live in shared memory);
@@ -118,10 +127,8 @@ cudaError_t launch_stage1_batch(const Stage1W& W, const BatchFrames& F, const Ba
 constexpr int kMaxBatchLevels = 256;
 // resident blocks of the persistent stage-1 kernel per SM (its grid is this times the SM count)
 int stage1_batch_blocks_per_sm(int blocks_per_sm);
-// every level image of every frame of a batch in one launch (no level-count limit), and the frames'
-// candidate counts zeroed
-cudaError_t launch_pyramid_batch(const BatchFrames& F, const LevelDesc* d_levels, int n_levels, int n_chunks, int pyr_items, int n_frames,
-                                 int gpitch, int gw, int gh, cudaStream_t st);
+// the candidate counts of every frame of a batch zeroed, in one launch
+cudaError_t launch_counts_zero_batch(const BatchFrames& F, int n_chunks, int n_frames, cudaStream_t st);
 
 // source of one frame of a batch (device memory, 64-byte aligned base and pitch)
 struct FrameSrc {
@@ -154,18 +161,25 @@ struct Stage1Sched {
     int front_blocks_per_sm = 3;
     int back_blocks_per_sm = 4;
 };
+// the frame's gray image as the stage-1 front kernel resamples each level tile from it; p == nullptr:
+// the level images are stored (limg + img_off) and read instead
+struct GrayRef {
+    const float* p;
+    int pitch, w, h;
+};
 // stage-1 net over all levels; `levels` is a HOST array (the descriptors travel as kernel
-// parameters), level images at limg + img_off
+// parameters); level tiles resampled from `gray`, or read from limg + img_off when gray.p is null
 // counts (optional, zeroed by the caller): per candidate-scan chunk, responses > thr
 // cells (optional): the gate's cell bitmaps; a response above thr whose window centre has no likely
 // cell within one cell of it (in its level's octave) is written below every threshold
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
                           cudaStream_t st, int* counts = nullptr, float thr = 0.f, const uint8_t* front_on = nullptr,
-                          const uint8_t* back_on = nullptr, GateCells cells = GateCells{}, Stage1Sched sched = Stage1Sched{});
+                          const uint8_t* back_on = nullptr, GateCells cells = GateCells{}, Stage1Sched sched = Stage1Sched{},
+                          GrayRef gray = GrayRef{});
 // front_on / back_on (optional): per-tile activity from the gate; inactive back tiles write
 // responses below every threshold
 cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st,
-                                const uint8_t* front_on = nullptr, Stage1Sched sched = Stage1Sched{});
+                                const uint8_t* front_on = nullptr, Stage1Sched sched = Stage1Sched{}, GrayRef gray = GrayRef{});
 // dynamic shared memory of the stage-1 back kernel (set once per device before any launch)
 cudaError_t stage1_setup();
 cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
@@ -174,7 +188,9 @@ cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_
 cudaError_t launch_cand_write(const int4* d_chunks, int n_chunks, const LevelDesc* d_levels, const float* resp, float thr,
                               const int* counts, Candidate* out, int* n_out, int cap, cudaStream_t st);
 // lg (optional): the legacy networks (device memory, [1] stage 2, [2] stage 3) replace N
-// ctas_per_sm: resident blocks a SM the grid was sized for; 2 or fewer selects the 128-register build
+// ctas_per_sm: resident blocks a SM the grid was sized for (1-6); 2 or fewer selects the
+// 128-register build, 5 and 6 the 48- and 40-register ones
+cudaError_t window_setup();
 cudaError_t launch_window(const WindowNets& N, const float* gray, int gpitch, int gw, int gh, const Candidate* cands, const int* n_cand,
                           const LevelDesc* levels, WinOut* out, const CascadeConfig& cfg, int grid, cudaStream_t st,
                           const LegacyNet* lg = nullptr, int ctas_per_sm = 4);

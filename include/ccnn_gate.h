@@ -43,6 +43,11 @@ CCNN_API ccnn_status ccnn_gate_disable(ccnn_handle h);
  * gate off every tile runs. */
 CCNN_API ccnn_status ccnn_gate_stats(ccnn_handle h, int* front_run, int* front_total, int* back_run, int* back_total, int* fallback);
 
+/* The gate's probabilities for the handle's last frame (run with the gate on): 4 octaves x
+ * (rows/16) x (cols/16) floats in host memory, octave-major, cell rows in order. *n gets the count;
+ * returns CCNN_TRUNCATED when capacity is smaller (the first `capacity` are written). */
+CCNN_API ccnn_status ccnn_gate_probabilities(ccnn_handle h, float* out, int capacity, int* n);
+
 /* Training labels from the handle's last frame (run with the gate off): 1 at the (octave, cell) of
  * the window centre of every candidate that stage 3 accepted, else 0; d_labels is device memory of
  * 4 x (rows/16) x (cols/16) bytes for the frame's gray size, written on `stream`. */

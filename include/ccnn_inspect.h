@@ -90,7 +90,8 @@ CCNN_API ccnn_status ccnn_plan_levels(const ccnn_params* p, int cols, int rows, 
 
 /* Re-runs the handle's last frame `iters` times (CCNN_ERR_UNSUPPORTED when that frame was read in
  * place from device memory) and writes the mean duration (ms, CUDA events) of each kernel of the
- * chain: [0] gray, [1] pyramid, [2] stage-1 front, [3] stage-1 back (which also counts the
+ * chain: [0] gray, [1] pyramid (the legacy family only; the CNTK stage-1 front kernel resamples the
+ * levels from the gray frame itself, so this entry is an empty gap), [2] stage-1 front, [3] stage-1 back (which also counts the
  * candidates), [4] candidate write, [5] stage-2/3 windows, [6] replay/sort/merge, [7] the learned gate
  * (when on), [8] the pyramid and stage 1 as one persistent launch (the batched form's kernel on this
  * frame). n_kernels entries are written. */
@@ -116,7 +117,7 @@ CCNN_API ccnn_status ccnn_synth_frame_device(void* d_out, int width, int height,
 
 /* Schedule of a handle, as the autotuner (compactcnncascade_b200/autotune.py) picks it per frame size:
  * frames in flight (1-64, default 8) and resident blocks per SM of the persistent stage-2/3 window
- * kernel (1-4, default 4); 0 keeps a value. Rebuilds the handle's device state (as a re-Init does).
+ * kernel (1-6, default 4; 5 and 6 select builds with fewer registers a thread); 0 keeps a value. Rebuilds the handle's device state (as a re-Init does).
  * Results do not depend on the schedule. No reference counterpart (the reference has no GPU
  * schedule to tune). */
 CCNN_API ccnn_status ccnn_set_schedule(ccnn_handle h, int frame_slots, int window_ctas_per_sm);

@@ -62,6 +62,31 @@ def test_features_are_normalised_8x8_means():
     assert np.allclose(feat.cpu().numpy().astype(np.float64), want, atol=2e-3)
 
 
+@pytest.mark.parametrize("w,h", [(1920, 1080), (333, 211), (640, 480)])
+def test_detector_probabilities_follow_the_network(w, h):
+    """The features the gray-conversion launch writes for the gate inside the frame's graph give the
+    probabilities of the network restated in float64 on the features of the standalone feature
+    kernel (fp16 storage points; fp32 accumulation order differs)."""
+    p = ccnn.default_params()
+    p.max_image_width, p.max_image_height = w, h
+    p.min_face_height, p.max_face_height, p.scale_factor = 40, 240, 1.15
+    d = ccnn.FaceDetector()
+    assert d.Init(p) == 0
+    params = gate.load() if os.path.exists(gate.WEIGHTS_1080P) else gate.init_params(3)
+    d.setGate(params, 0.5, 1.0)
+    imgs = [ccnn.synth_frame(w, h, 60 + k, 5, 30, max(31, min(w, h) // 2))[0] for k in range(3)]
+    d.DetectBatch(imgs[:2])
+    d.Detect(imgs[2])
+    got = d.gateProbabilities()
+    gptr, gw, gh, step = d.grayDevice()
+    feat = torch.empty((gh // 8, gw // 8), dtype=torch.float16, device="cuda")
+    ccnn._capi.check(ccnn._capi.lib().ccnn_gate_features(gptr, gw, gh, step, feat.data_ptr(), None), "features")
+    torch.cuda.synchronize()
+    want = gate_ref.forward(params.astype(np.float64), feat.cpu().numpy()[None].astype(np.float64), fp16=True)[0]
+    assert got.shape == want.shape
+    assert np.abs(got - want).max() <= 2e-3
+
+
 @pytest.mark.parametrize("seed", [21, 22])
 def test_gate_fully_on_is_the_plain_cascade(seed):
     d = _det()

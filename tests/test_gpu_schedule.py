@@ -21,13 +21,14 @@ def test_results_do_not_depend_on_the_schedule():
     want = d.DetectBatch(imgs)
     assert sum(len(f) for f in want) > 0
     names = [k for k, _ in autotune.KNOBS]
-    for sched in [(1, 1, 3, 3, 0, 3), (3, 2, 4, 4, 2, 4), (16, 3, 3, 4, 4, 3), (5, 4, 4, 3, 5, 3), (2, 2, 3, 4, 1, 4)]:
+    for sched in [(1, 1, 3, 3, 0, 3), (3, 2, 4, 4, 2, 4), (16, 3, 3, 4, 4, 3), (5, 4, 4, 3, 5, 3), (2, 2, 3, 4, 1, 4), (12, 5, 4, 4, 0, 3),
+                  (8, 6, 3, 4, 0, 3)]:
         sd = dict(zip(names, sched))
         autotune.set_schedule(d, sd)
         assert autotune.get_schedule(d) == sd
         assert d.DetectBatch(imgs) == want
         assert [d.Detect(im) for im in imgs] == want
-    for bad in [{"frame_slots": 65}, {"window_ctas_per_sm": 5}, {"front_blocks_per_sm": 2}, {"back_blocks_per_sm": 5},
+    for bad in [{"frame_slots": 65}, {"window_ctas_per_sm": 7}, {"front_blocks_per_sm": 2}, {"back_blocks_per_sm": 5},
                 {"batch_frames": 17}, {"frame_slots": 4, "batch_frames": 8}, {"batch_blocks_per_sm": 5}]:
         with pytest.raises(ccnn.CCNNError):
             autotune.set_schedule(d, bad)
