@@ -139,6 +139,10 @@ class FaceDetector:
         _capi.check(_capi.lib().ccnn_gate_set(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), p.size, float(threshold),
                                               float(fallback_fraction)), "ccnn_gate_set")
 
+    def setGateMargin(self, pixels):
+        """Pixels (0-64, default 16) around a candidate's window centre the gate searches for a likely cell."""
+        _capi.check(_capi.lib().ccnn_gate_set_margin(self._h, int(pixels)), "ccnn_gate_set_margin")
+
     def disableGate(self):
         _capi.check(_capi.lib().ccnn_gate_disable(self._h), "ccnn_gate_disable")
 
@@ -274,11 +278,13 @@ class FaceServer:
         except Exception:
             pass
 
-    def set_gate(self, params, threshold=0.5, fallback_fraction=0.25):
-        """The learned gate (FaceDetector.setGate) for every resolution class; before the first submit."""
+    def set_gate(self, params, threshold=0.5, fallback_fraction=0.25, margin=16):
+        """The learned gate (FaceDetector.setGate, setGateMargin) for every resolution class; before the
+        first submit."""
         p = np.ascontiguousarray(params, np.float32)
         _capi.check(_capi.lib().ccnn_server_set_gate(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), p.size,
                                                      float(threshold), float(fallback_fraction)), "ccnn_server_set_gate")
+        _capi.check(_capi.lib().ccnn_server_set_gate_margin(self._h, int(margin)), "ccnn_server_set_gate_margin")
 
     def submit(self, img):
         """Queues a uint8 HxW / HxWxC frame; returns its ticket, or None when the queue is full."""

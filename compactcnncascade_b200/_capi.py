@@ -34,8 +34,8 @@ EXPORTED = [
     "ccnn_sort_permutation", "ccnn_detect_device_batch", "ccnn_profile_last_frame", "ccnn_plan_levels", "ccnn_stage1_forward_static",
     "ccnn_server_create", "ccnn_server_destroy", "ccnn_server_submit", "ccnn_server_poll", "ccnn_server_wait",
     "ccnn_server_stats_get", "ccnn_host_alloc", "ccnn_host_free", "ccnn_cntk_dump_to_binary",
-    "ccnn_check_reciprocal", "ccnn_synth_frame_device", "ccnn_gate_set", "ccnn_gate_disable", "ccnn_gate_stats", "ccnn_gate_probabilities",
-    "ccnn_gate_labels", "ccnn_gate_features", "ccnn_gate_gradient", "ccnn_gate_train", "ccnn_server_set_gate",
+    "ccnn_check_reciprocal", "ccnn_synth_frame_device", "ccnn_gate_set", "ccnn_gate_disable", "ccnn_gate_stats", "ccnn_gate_probabilities", "ccnn_gate_set_margin",
+    "ccnn_gate_labels", "ccnn_gate_features", "ccnn_gate_gradient", "ccnn_gate_train", "ccnn_server_set_gate", "ccnn_server_set_gate_margin",
     "ccnn_legacy_model_info", "ccnn_legacy_net_forward", "ccnn_set_schedule", "ccnn_get_schedule",
     "ccnn_measure_fp32_peak", "ccnn_cnn_default_params", "ccnn_cnn_create", "ccnn_cnn_detect", "ccnn_cnn_nms",
     "ccnn_cnn_get_params", "ccnn_cnn_set_params", "ccnn_set_schedule_ex", "ccnn_get_schedule_ex",
@@ -195,6 +195,7 @@ def lib():
         L.ccnn_gate_set.argtypes = [vp, fp, ci, ctypes.c_float, ctypes.c_float]
         L.ccnn_gate_disable.argtypes = [vp]
         L.ccnn_server_set_gate.argtypes = [vp, fp, ci, ctypes.c_float, ctypes.c_float]
+        L.ccnn_server_set_gate_margin.argtypes = [vp, ci]
         L.ccnn_legacy_model_info.argtypes = [ctypes.c_char_p, P(ci), ci]
         L.ccnn_set_schedule.argtypes = [vp, ci, ci]
         L.ccnn_get_schedule.argtypes = [vp, P(ci), P(ci)]
@@ -203,6 +204,7 @@ def lib():
         L.ccnn_legacy_net_forward.argtypes = [ctypes.c_char_p, vp, ci, ci, ctypes.c_size_t, vp, ci, P(ci), P(ci), vp]
         L.ccnn_gate_stats.argtypes = [vp, P(ci), P(ci), P(ci), P(ci), P(ci)]
         L.ccnn_gate_probabilities.argtypes = [vp, P(ctypes.c_float), ci, P(ci)]
+        L.ccnn_gate_set_margin.argtypes = [vp, ci]
         L.ccnn_gate_labels.argtypes = [vp, vp, vp]
         L.ccnn_gate_features.argtypes = [vp, ci, ci, ctypes.c_size_t, vp, vp]
         L.ccnn_gate_gradient.argtypes = [vp, vp, vp, ci, ci, ci, ctypes.c_float, fp, fp]

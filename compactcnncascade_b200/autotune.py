@@ -18,7 +18,7 @@ The knobs (include/ccnn_inspect.h, ccnn_schedule):
 The search is coordinate descent from the defaults: each knob in turn takes the value that times
 fastest with the others held, for two passes (a full product of the knobs would be 960 timings).
 
-    python -m compactcnncascade_b200.autotune --width 1920 --height 1080
+    python -m compactcnncascade_b200.autotune --width 1920 --height 1080 [--gate]
 """
 import argparse
 import ctypes
@@ -35,8 +35,10 @@ DEFAULTS = {"frame_slots": 8, "window_ctas_per_sm": 4, "front_blocks_per_sm": 3,
             "batch_blocks_per_sm": 3}
 
 
-def key(width, height, scale_factor, min_face, max_face):
-    return f"{width}x{height}/sf{scale_factor:g}/min{min_face}/max{max_face}"
+def key(width, height, scale_factor, min_face, max_face, gated=False):
+    """Table key of a workload; the learned gate changes which kernels dominate, so a gated detector
+    has entries of its own."""
+    return f"{width}x{height}/sf{scale_factor:g}/min{min_face}/max{max_face}" + ("/gate" if gated else "")
 
 
 def load_table(path=TABLE):
@@ -47,9 +49,10 @@ def load_table(path=TABLE):
         return {}
 
 
-def lookup(p, path=TABLE):
-    """The tuned schedule (knob -> value) for these parameters, or None."""
-    e = load_table(path).get(key(p.max_image_width, p.max_image_height, p.scale_factor, p.min_face_height, p.max_face_height))
+def lookup(p, path=TABLE, gated=False):
+    """The tuned schedule (knob -> value) for these parameters (with the learned gate on, when
+    gated), or None."""
+    e = load_table(path).get(key(p.max_image_width, p.max_image_height, p.scale_factor, p.min_face_height, p.max_face_height, gated))
     if not e:
         return None
     return {k: e[k] for k, _ in KNOBS if k in e}
@@ -89,9 +92,10 @@ def measure(det, frames, width, height, batch=64, steps=8, warmup=3):
 
 
 def tune(width, height, scale_factor=1.15, min_face=40, max_face=240, n_faces=20, min_patch=30, max_patch=300, distinct=16,
-         knobs=KNOBS, passes=2, batch=64):
+         knobs=KNOBS, passes=2, batch=64, gate=None):
     """Coordinate descent over the knobs; returns the table entry (the schedule, its frames/s and
-    every timing taken)."""
+    every timing taken). gate: (parameters, threshold, margin in pixels) of the learned gate to time
+    with, or None."""
     import torch
     from . import FaceDetector, default_params, synth_frame_device
     p = default_params()
@@ -101,6 +105,9 @@ def tune(width, height, scale_factor=1.15, min_face=40, max_face=240, n_faces=20
     det = FaceDetector()
     if det.Init(p) != 0:
         raise RuntimeError(_capi.last_error())
+    if gate is not None:
+        det.setGate(gate[0], gate[1])
+        det.setGateMargin(gate[2] if len(gate) > 2 else 16)
     frames = []
     for s in range(distinct):
         t = torch.empty((height, width, 3), dtype=torch.uint8, device="cuda")
@@ -129,7 +136,11 @@ def tune(width, height, scale_factor=1.15, min_face=40, max_face=240, n_faces=20
                 if fps > best_fps:
                     best, best_fps = trial, fps
     det.Clear()
-    return dict(best, frames_per_s=round(best_fps, 1), knobs=[k for k, _ in knobs], tried=timings)
+    entry = dict(best, frames_per_s=round(best_fps, 1), knobs=[k for k, _ in knobs], tried=timings)
+    if gate is not None:
+        entry["gate_threshold"] = gate[1]
+        entry["gate_margin"] = gate[2] if len(gate) > 2 else 16
+    return entry
 
 
 def main(argv=None):
@@ -144,11 +155,17 @@ def main(argv=None):
     ap.add_argument("--max-patch", type=int, default=300)
     ap.add_argument("--batch", type=int, default=64, help="frames per timed batch")
     ap.add_argument("--table", default=TABLE)
+    ap.add_argument("--gate", action="store_true", help="tune with the shipped learned gate at its operating threshold")
     a = ap.parse_args(argv)
+    gate = None
+    if a.gate:
+        from . import gate as gate_mod
+        meta = gate_mod.load_meta()
+        gate = (gate_mod.load(), meta.get("operating_threshold", 0.1), meta.get("operating_margin", 16))
     entry = tune(a.width, a.height, a.scale_factor, a.min_face, a.max_face, n_faces=a.faces, min_patch=a.min_patch,
-                 max_patch=a.max_patch, batch=a.batch)
+                 max_patch=a.max_patch, batch=a.batch, gate=gate)
     table = load_table(a.table)
-    table[key(a.width, a.height, a.scale_factor, a.min_face, a.max_face)] = entry
+    table[key(a.width, a.height, a.scale_factor, a.min_face, a.max_face, gate is not None)] = entry
     with open(a.table, "w") as f:
         json.dump(table, f, indent=1, sort_keys=True)
     print(json.dumps(entry), flush=True)

@@ -258,6 +258,11 @@ CCNN_API ccnn_status ccnn_gate_stats(ccnn_handle h, int* front_run, int* front_t
     return h->det.gate_stats(front_run, front_total, back_run, back_total, fallback);
 }
 
+CCNN_API ccnn_status ccnn_gate_set_margin(ccnn_handle h, int pixels) {
+    if (!h) return CCNN_ERR_INVALID_ARG;
+    return h->det.gate_set_margin(pixels);
+}
+
 CCNN_API ccnn_status ccnn_gate_probabilities(ccnn_handle h, float* out, int capacity, int* n) {
     if (!h || !n || capacity < 0) return CCNN_ERR_INVALID_ARG;
     return h->det.gate_probabilities(out, capacity, n);

@@ -243,12 +243,18 @@ struct LevelDesc {
 };
 
 // The learned gate's per-octave cell bitmaps as the stage-1 back kernel reads them: bits == nullptr
-// means no gate. Rows of wwords words, one bit per 16x16-pixel cell of the frame.
+// means no gate. Rows of wwords words, one bit per 16x16-pixel cell of the frame. A candidate needs a
+// set bit in a cell within `margin` pixels (per axis) of its window centre.
 struct GateCells {
     const uint32_t* bits;
     const int* ambiguous;  // frames with more ambiguous cells than amb_limit are scanned in full
-    int amb_limit, wwords, w16, h16;
+    int amb_limit, wwords, w16, h16, margin;
 };
+
+// The cells [lo, hi] of one axis within m pixels of the window-centre pixel coordinate p (p >= 0,
+// truncated); n16 cells on the axis. m = 16 is the centre's cell and one cell on either side.
+__host__ __device__ __forceinline__ int gate_cell_lo(int p, int m) { return (p - m) / 16 > 0 ? (p - m) / 16 : 0; }
+__host__ __device__ __forceinline__ int gate_cell_hi(int p, int m, int n16) { return (p + m) / 16 < n16 - 1 ? (p + m) / 16 : n16 - 1; }
 
 // any set bit of octave row bitmaps `B` in cells [cx0, cx1] x [cy0, cy1]
 __device__ __forceinline__ bool gate_any_bit(const uint32_t* __restrict__ B, int wwords, int cx0, int cx1, int cy0, int cy1) {

@@ -86,7 +86,6 @@ Detector::~Detector() {
     clear();
     if (order_ev_) cudaEventDestroy(order_ev_);
     if (d_lnet_) cudaFree(d_lnet_);
-    if (d_gate_) cudaFree(d_gate_);
     if (d_lg_) cudaFree(d_lg_);
 }
 
@@ -597,8 +596,7 @@ ccnn_status Detector::gate_set(const float* params, int n, float threshold, floa
     }
     cudaSetDevice(device_);
     gate_params_.assign(params, params + n);
-    if (!d_gate_) CCNN_CUDA(cudaMalloc(&d_gate_, sizeof(float) * kGateParams));
-    CCNN_CUDA(cudaMemcpy(d_gate_, params, sizeof(float) * kGateParams, cudaMemcpyHostToDevice));
+    std::copy(params, params + kGateParams, gate_net_.p);
     gate_on_ = true;
     gate_thr_ = threshold;
     gate_amb_frac_ = fallback_fraction;
@@ -608,6 +606,7 @@ ccnn_status Detector::gate_set(const float* params, int n, float threshold, floa
         if (st != CCNN_OK) return st;
         s.exec_plan = nullptr;  // the per-frame graphs are captured again with the gate
     }
+    for (auto& b : batches_) b.exec_plan = nullptr;  // and the batched ones (their streams are the slots')
     return CCNN_OK;
 }
 
@@ -642,6 +641,21 @@ void Detector::get_schedule(int* frame_slots, int* window_ctas_per_sm, int* fron
     if (batch_bpsm) *batch_bpsm = batch_bpsm_;
 }
 
+ccnn_status Detector::gate_set_margin(int pixels) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (pixels < 0 || pixels > 64) {
+        set_error("gate margin: 0-64 pixels");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    gate_margin_ = pixels;
+    for (auto& s : slots_) {
+        if (s.st) cudaStreamSynchronize(s.st);
+        s.exec_plan = nullptr;  // the per-frame graphs are captured again with the new margin
+    }
+    for (auto& b : batches_) b.exec_plan = nullptr;
+    return CCNN_OK;
+}
+
 ccnn_status Detector::gate_disable() {
     std::lock_guard<std::mutex> lk(mu_);
     gate_on_ = false;
@@ -649,6 +663,7 @@ ccnn_status Detector::gate_disable() {
         if (s.st) cudaStreamSynchronize(s.st);
         s.exec_plan = nullptr;
     }
+    for (auto& b : batches_) b.exec_plan = nullptr;
     return CCNN_OK;
 }
 
@@ -761,8 +776,8 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
         e = launch_gray(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st, s.gray_feat);
     CCNN_CUDA(e);
     if (gated) {
-        CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.gray_feat != nullptr, p.levels.data(), p.n_levels, s.gate,
-                              gate_thr_, gate_amb_frac_, s.d_back_on, s.d_front_on, s.st));
+        CCNN_CUDA(launch_gate(gate_net_, s.d_gray, s.gray_pitch, p.gw, p.gh, s.gray_feat != nullptr, p.levels.data(), p.n_levels, s.gate,
+                              gate_thr_, gate_amb_frac_, gate_margin_, s.d_back_on, s.d_front_on, s.st));
     }
     const bool single = single_launch_stage1() && p.n_levels > 0 && p.n_levels <= kMaxBatchLevels;
     if (single) {
@@ -779,7 +794,7 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
         F.counts[0] = s.d_counts;
         F.front_on[0] = gated ? s.d_front_on : nullptr;
         F.back_on[0] = gated ? s.d_back_on : nullptr;
-        F.cells[0] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{};
+        F.cells[0] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_, gate_margin_) : GateCells{};
         if (!p.chunks.empty()) CCNN_CUDA(cudaMemsetAsync(s.d_counts, 0, sizeof(int) * p.chunks.size(), s.st));
         BatchQueue Q;
         build_batch_queue(&Q, 1, p.n_levels, (int)p.chunks.size(), p.k1_tiles, p.k2_tiles, cfg_.thr1);
@@ -801,7 +816,7 @@ ccnn_status Detector::enqueue_kernels(Slot& s, const Plan& p) {
         } else {
             CCNN_CUDA(launch_stage1(w1_, p.levels.data(), p.n_levels, nullptr, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
                                     gated ? s.d_front_on : nullptr, gated ? s.d_back_on : nullptr,
-                                    gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{}, s1_sched_,
+                                    gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_, gate_margin_) : GateCells{}, s1_sched_,
                                     GrayRef{s.d_gray, s.gray_pitch, p.gw, p.gh}));
         }
     }
@@ -1391,8 +1406,8 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
             CCNN_CUDA(launch_gray(s.d_in, (int)p.in_pitch, p.in_w, p.in_h, p.ch, s.d_gray, s.gray_pitch, s.st, feat));
         CCNN_CUDA(cudaEventRecord(ev[1], s.st));
         if (gated) {
-            CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, feat != nullptr, p.levels.data(), p.n_levels, s.gate, gate_thr_,
-                                  gate_amb_frac_, s.d_back_on, s.d_front_on, s.st));
+            CCNN_CUDA(launch_gate(gate_net_, s.d_gray, s.gray_pitch, p.gw, p.gh, feat != nullptr, p.levels.data(), p.n_levels, s.gate, gate_thr_,
+                                  gate_amb_frac_, gate_margin_, s.d_back_on, s.d_front_on, s.st));
         }
         CCNN_CUDA(cudaEventRecord(ev[K + 1], s.st));
         if (legacy_) CCNN_CUDA(launch_pyramid(p.levels.data(), p.n_levels, s.d_gray, s.gray_pitch, p.gw, p.gh, s.d_limg, s.st));
@@ -1407,7 +1422,7 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
             if (ls != CCNN_OK) return ls;
         } else
             CCNN_CUDA(launch_stage1_back(w1_, p.levels.data(), p.n_levels, s.d_s1, s.d_resp, s.st, s.d_counts, cfg_.thr1,
-                                         gated ? s.d_back_on : nullptr, gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{},
+                                         gated ? s.d_back_on : nullptr, gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_, gate_margin_) : GateCells{},
                                          s1_sched_));
         CCNN_CUDA(cudaEventRecord(ev[4], s.st));
         CCNN_CUDA(launch_cand_write(p.d_chunks, (int)p.chunks.size(), p.d_levels, s.d_resp, cfg_.thr1, s.d_counts, s.d_cands, s.d_ncand,
@@ -1446,7 +1461,7 @@ ccnn_status Detector::profile(int iters, float* ms, int n_ms) {
         F.counts[0] = s.d_counts;
         F.front_on[0] = gated ? s.d_front_on : nullptr;
         F.back_on[0] = gated ? s.d_back_on : nullptr;
-        F.cells[0] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{};
+        F.cells[0] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_, gate_margin_) : GateCells{};
         BatchQueue Q;
         build_batch_queue(&Q, 1, p.n_levels, (int)p.chunks.size(), p.k1_tiles, p.k2_tiles, cfg_.thr1);
         const int grid = sm_count_ * stage1_batch_blocks_per_sm(batch_bpsm_);
@@ -1638,7 +1653,7 @@ ccnn_status Detector::enqueue_batch_kernels(BatchCtx& c, const Plan& p, int B) {
         F.counts[f] = s.d_counts;
         F.front_on[f] = gated ? s.d_front_on : nullptr;
         F.back_on[f] = gated ? s.d_back_on : nullptr;
-        F.cells[f] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_) : GateCells{};
+        F.cells[f] = gated ? gate_cells(s.gate, p.gw, p.gh, gate_amb_frac_, gate_margin_) : GateCells{};
         C.cands[f] = s.d_cands;
         C.ncand[f] = s.d_ncand;
         WB.gray[f] = s.d_gray;
@@ -1655,8 +1670,8 @@ ccnn_status Detector::enqueue_batch_kernels(BatchCtx& c, const Plan& p, int B) {
     if (gated)
         for (int f = 0; f < B; ++f) {
             Slot& s = slots_[c.first_slot + f];
-            CCNN_CUDA(launch_gate(d_gate_, s.d_gray, s.gray_pitch, p.gw, p.gh, true, p.levels.data(), p.n_levels, s.gate, gate_thr_,
-                                  gate_amb_frac_, s.d_back_on, s.d_front_on, st));
+            CCNN_CUDA(launch_gate(gate_net_, s.d_gray, s.gray_pitch, p.gw, p.gh, true, p.levels.data(), p.n_levels, s.gate, gate_thr_,
+                                  gate_amb_frac_, gate_margin_, s.d_back_on, s.d_front_on, st));
         }
     CCNN_CUDA(launch_counts_zero_batch(F, (int)p.chunks.size(), B, st));
     BatchQueue Q;

@@ -141,6 +141,7 @@ class Detector {
     // stage-1 tiles the gate let run in the last frame (slot 0), of all, and whether it fell back
     ccnn_status gate_stats(int* front_run, int* front_total, int* back_run, int* back_total, int* fallback);
     ccnn_status gate_probabilities(float* out, int cap, int* n);
+    ccnn_status gate_set_margin(int pixels);
 
     // Non-blocking use of one slot by a single scheduling thread (the serving loop): launch a
     // host frame on slot k, test for completion, fetch the faces. Frames must have the size the
@@ -212,9 +213,10 @@ class Detector {
     ccnn_status launch_batch(BatchCtx& c, const Plan& p, const ccnn_image* imgs, int B, bool device_input);
     ccnn_status collect_batch(BatchCtx& c, int B, ccnn_face* faces, int cap_per, int* n_faces, ccnn_status* worst);
     bool batch_usable(const Plan& p) const;
-    float* d_gate_ = nullptr;        // learned gate parameters (device memory)
+    GateNet gate_net_{};             // learned gate parameters (passed to the inference kernel by value)
     bool gate_on_ = false;
     float gate_thr_ = 0.5f, gate_amb_frac_ = 0.25f;
+    int gate_margin_ = 16;           // pixels around a candidate's window centre the gate searches
     std::vector<float> gate_params_;
     ccnn_status alloc_gate(Slot& s);
     int pat_w_ = kPatW, pat_h_ = kPatH;     // stage-1 window

@@ -264,17 +264,16 @@ namespace {
 constexpr int kIX = 16, kIY = 8;
 constexpr int kFX = kIX + 4, kFY = kIY + 4, kAX = kIX + 2, kAY = kIY + 2;
 
-__global__ void __launch_bounds__(256) gate_infer_kernel(const float* __restrict__ P, const __half* __restrict__ feat, int w8, int h8,
+__global__ void __launch_bounds__(256) gate_infer_kernel(const __grid_constant__ GateNet P, const __half* __restrict__ feat, int w8, int h8,
                                                          float thr, float amb_lo, uint32_t* __restrict__ bits, int wwords,
                                                          float* __restrict__ prob, int* __restrict__ ambiguous) {
-    __shared__ float sp[kGateParams];
+    const float* sp = P.p;  // the parameters travel in the constant bank (warp-uniform reads)
     __shared__ __half sf[kFY][kFX];
     __shared__ __half sa1[kGC][kAY][kAX];
     __shared__ __half sa2[kGC][kIY][kIX];
     __shared__ int samb;
     const int tid = threadIdx.x;
     const int x0 = blockIdx.x * kIX, y0 = blockIdx.y * kIY;
-    for (int i = tid; i < kGateParams; i += blockDim.x) sp[i] = P[i];
     if (tid == 0) samb = 0;
     if (tid < kFX * kFY) {
         const int fx = x0 - 2 + tid % kFX, fy = y0 - 2 + tid / kFX;
@@ -353,17 +352,17 @@ __global__ void __launch_bounds__(256) gate_infer_kernel(const float* __restrict
     if (tid == 0 && samb) atomicAdd(ambiguous, samb);
 }
 
-// cells within one cell of the window centres ((4*o + 11.5) / s, (4*o + 13.5) / s) of the
+// cells within `m` pixels of the window centres ((4*o + 11.5) / s, (4*o + 13.5) / s) of the
 // response pixels o in [ox0, ox1] x [oy0, oy1] of a level
-__device__ __forceinline__ void centre_cells(const LevelDesc& L, int ox0, int ox1, int oy0, int oy1, int w16, int h16, int* r) {
-    r[0] = max(0, (int)((4.f * ox0 + 11.5f) * L.inv_scale) / 16 - 1);
-    r[1] = min(w16 - 1, (int)((4.f * ox1 + 11.5f) * L.inv_scale) / 16 + 1);
-    r[2] = max(0, (int)((4.f * oy0 + 13.5f) * L.inv_scale) / 16 - 1);
-    r[3] = min(h16 - 1, (int)((4.f * oy1 + 13.5f) * L.inv_scale) / 16 + 1);
+__device__ __forceinline__ void centre_cells(const LevelDesc& L, int ox0, int ox1, int oy0, int oy1, int w16, int h16, int m, int* r) {
+    r[0] = gate_cell_lo((int)((4.f * ox0 + 11.5f) * L.inv_scale), m);
+    r[1] = gate_cell_hi((int)((4.f * ox1 + 11.5f) * L.inv_scale), m, w16);
+    r[2] = gate_cell_lo((int)((4.f * oy0 + 13.5f) * L.inv_scale), m);
+    r[3] = gate_cell_hi((int)((4.f * oy1 + 13.5f) * L.inv_scale), m, h16);
 }
 
 // Tile activity for one group of levels: threads [0, nb) decide the back tiles (32x16 response
-// pixels: active when a likely cell of the level's octave lies near their window centres), the
+// pixels: active when a likely cell of the level's octave lies within `margin` pixels of their window centres), the
 // rest the front tiles (active when a back tile that reads their S1 pixels can be: the union of
 // those back tiles' cell ranges is tested). A frame with too many ambiguous cells runs in full.
 // The bitmaps are staged in shared memory first (a query walks up to a few dozen rows, which as
@@ -372,7 +371,7 @@ __device__ __forceinline__ void centre_cells(const LevelDesc& L, int ox0, int ox
 constexpr int kMaskSmemWords = 12288;
 
 __global__ void gate_mask_kernel(const __grid_constant__ LevelTable LT, int nb, const uint32_t* __restrict__ gbits, int n_words, int wwords,
-                                 int w16, int h16, const int* __restrict__ ambiguous, int amb_limit, uint8_t* __restrict__ back_on,
+                                 int w16, int h16, int margin, const int* __restrict__ ambiguous, int amb_limit, uint8_t* __restrict__ back_on,
                                  uint8_t* __restrict__ front_on) {
     extern __shared__ uint32_t sbits[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -394,7 +393,7 @@ __global__ void gate_mask_kernel(const __grid_constant__ LevelTable LT, int nb, 
         const int t = g - L.k2_base;
         const int ox0 = (t % L.k2_tiles_x) * kK2TileX, oy0 = (t / L.k2_tiles_x) * kK2TileY;
         int r[4];
-        centre_cells(L, ox0, min(ox0 + kK2TileX, L.ow) - 1, oy0, min(oy0 + kK2TileY, L.oh) - 1, w16, h16, r);
+        centre_cells(L, ox0, min(ox0 + kK2TileX, L.ow) - 1, oy0, min(oy0 + kK2TileY, L.oh) - 1, w16, h16, margin, r);
         back_on[g] = gate_any_bit(bits + (long long)min(L.octave, kGK - 1) * h16 * wwords, wwords, r[0], r[1], r[2], r[3]) ? 1 : 0;
         return;
     }
@@ -416,15 +415,17 @@ __global__ void gate_mask_kernel(const __grid_constant__ LevelTable LT, int nb, 
         return;
     }
     int r[4];
-    centre_cells(L, bx0 * kK2TileX, min((bx1 + 1) * kK2TileX, L.ow) - 1, by0 * kK2TileY, min((by1 + 1) * kK2TileY, L.oh) - 1, w16, h16, r);
+    centre_cells(L, bx0 * kK2TileX, min((bx1 + 1) * kK2TileX, L.ow) - 1, by0 * kK2TileY, min((by1 + 1) * kK2TileY, L.oh) - 1, w16, h16, margin,
+                 r);
     front_on[g] = gate_any_bit(bits + (long long)min(L.octave, kGK - 1) * h16 * wwords, wwords, r[0], r[1], r[2], r[3]) ? 1 : 0;
 }
 
 }  // namespace
 
-GateCells gate_cells(GateScratch sc, int gw, int gh, float amb_frac) {
+GateCells gate_cells(GateScratch sc, int gw, int gh, float amb_frac, int margin) {
     const int w16 = (gw / 8) / 2, h16 = (gh / 8) / 2;
     GateCells c;
+    c.margin = margin;
     c.bits = sc.bits;
     c.ambiguous = sc.ambiguous;
     c.amb_limit = (int)(amb_frac * (float)(w16 * h16 * kGK));
@@ -439,17 +440,18 @@ int gate_bitmap_words(int gw, int gh) {
     return kGK * h16 * ((w16 + 31) / 32);
 }
 
-cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, int gw, int gh, bool feat_ready, const LevelDesc* levels,
-                        int n_levels, GateScratch sc, float thr, float amb_frac, uint8_t* back_on, uint8_t* front_on, cudaStream_t st) {
+cudaError_t launch_gate(const GateNet& net, const float* gray, int gpitch, int gw, int gh, bool feat_ready, const LevelDesc* levels,
+                        int n_levels, GateScratch sc, float thr, float amb_frac, int margin, uint8_t* back_on, uint8_t* front_on,
+                        cudaStream_t st) {
     const int w8 = gw / 8, h8 = gh / 8, w16 = w8 / 2, h16 = h8 / 2;
     const int wwords = (w16 + 31) / 32;
     // the ambiguous-cell counter and the bitmaps right behind it are one zeroed range
     cudaError_t e = cudaMemsetAsync(sc.ambiguous, 0, sizeof(uint32_t) * ((size_t)gate_bitmap_words(gw, gh) + 1), st);
     if (e != cudaSuccess) return e;
     if (!feat_ready) gate_features_kernel<<<dim3(blocks(w8, 128), h8), 128, 0, st>>>(gray, gpitch, w8, h8, sc.feat);
-    gate_infer_kernel<<<dim3((w8 + kIX - 1) / kIX, (h8 + kIY - 1) / kIY), 256, 0, st>>>(d_params, sc.feat, w8, h8, thr, 0.25f * thr, sc.bits,
+    gate_infer_kernel<<<dim3((w8 + kIX - 1) / kIX, (h8 + kIY - 1) / kIY), 256, 0, st>>>(net, sc.feat, w8, h8, thr, 0.25f * thr, sc.bits,
                                                                                        wwords, sc.prob, sc.ambiguous);
-    const int amb_limit = gate_cells(sc, gw, gh, amb_frac).amb_limit;
+    const int amb_limit = gate_cells(sc, gw, gh, amb_frac, margin).amb_limit;
     const int n_words = gate_bitmap_words(gw, gh);
     for (int g0 = 0; g0 < n_levels; g0 += kParamLevels) {
         LevelTable T;
@@ -461,7 +463,7 @@ cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, in
         const int nf = last.k1_base + last.k1_tiles_x * ((last.p1h + kK1TileY - 1) / kK1TileY) - T.lv[0].k1_base;
         if (nb + nf > 0)
             gate_mask_kernel<<<blocks(nb + nf, 128), 128, n_words <= kMaskSmemWords ? sizeof(uint32_t) * n_words : 0, st>>>(
-                T, nb, sc.bits, n_words, wwords, w16, h16, sc.ambiguous, amb_limit, back_on, front_on);
+                T, nb, sc.bits, n_words, wwords, w16, h16, margin, sc.ambiguous, amb_limit, back_on, front_on);
     }
     return cudaGetLastError();
 }

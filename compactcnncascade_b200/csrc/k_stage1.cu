@@ -338,15 +338,16 @@ __device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, 
     const int x = threadIdx.x & (kK2TileX - 1), y = (threadIdx.x / kK2TileX) * 2;
     if (cells.bits && *cells.ambiguous <= cells.amb_limit) {
         // learned gate, per warp (its 32 x 2 response pixels): when no likely cell of the level's
-        // octave lies within one cell of any of their window centres, every candidate among them
+        // octave lies within the margin of any of their window centres, every candidate among them
         // would be dropped below, so the warp writes the skip marker instead of computing them
         const int gy = oy0 + y;  // warp-uniform
         const int gx1 = min(ox0 + kK2TileX, L.ow) - 1, gy1 = min(gy + 1, L.oh - 1);
-        const int cx0 = (int)((4.f * ox0 + 11.5f) * L.inv_scale) / 16, cx1 = (int)((4.f * gx1 + 11.5f) * L.inv_scale) / 16;
-        const int cy0 = (int)((4.f * gy + 13.5f) * L.inv_scale) / 16, cy1 = (int)((4.f * gy1 + 13.5f) * L.inv_scale) / 16;
+        const int px0 = (int)((4.f * ox0 + 11.5f) * L.inv_scale), px1 = (int)((4.f * gx1 + 11.5f) * L.inv_scale);
+        const int py0 = (int)((4.f * gy + 13.5f) * L.inv_scale), py1 = (int)((4.f * gy1 + 13.5f) * L.inv_scale);
         const uint32_t* B = cells.bits + (long long)min(L.octave, kGK - 1) * cells.h16 * cells.wwords;
-        if (gy >= L.oh || !gate_any_bit(B, cells.wwords, max(0, cx0 - 1), min(cells.w16 - 1, cx1 + 1), max(0, cy0 - 1),
-                                       min(cells.h16 - 1, cy1 + 1))) {
+        const int m = cells.margin;
+        if (gy >= L.oh || !gate_any_bit(B, cells.wwords, gate_cell_lo(px0, m), gate_cell_hi(px1, m, cells.w16), gate_cell_lo(py0, m),
+                                       gate_cell_hi(py1, m, cells.h16))) {
             const int gx = ox0 + x;
             if (gx < L.ow) {
                 if (gy < L.oh) resp[L.resp_off + (long long)gy * L.ow + gx] = -1e30f;
@@ -418,13 +419,14 @@ __device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, 
         float rv[2] = {f2_lo(r), f2_hi(r)};
         if (cells.bits && (rv[0] > thr || rv[1] > thr) && *cells.ambiguous <= cells.amb_limit) {
             // learned gate, per candidate: its window centre ((4x + 11.5) / s, (4y + 13.5) / s) needs a
-            // likely cell of its octave within one cell
+            // likely cell of its octave within the margin
             const uint32_t* B = cells.bits + (long long)min(L.octave, kGK - 1) * cells.h16 * cells.wwords;
-            const int cx = (int)((4.f * gx + 11.5f) * L.inv_scale) / 16;
+            const int px = (int)((4.f * gx + 11.5f) * L.inv_scale), m = cells.margin;
             for (int k = 0; k < 2; ++k) {
                 if (!(rv[k] > thr)) continue;
-                const int cy = (int)((4.f * (gy + k) + 13.5f) * L.inv_scale) / 16;
-                if (!gate_any_bit(B, cells.wwords, max(0, cx - 1), min(cells.w16 - 1, cx + 1), max(0, cy - 1), min(cells.h16 - 1, cy + 1)))
+                const int py = (int)((4.f * (gy + k) + 13.5f) * L.inv_scale);
+                if (!gate_any_bit(B, cells.wwords, gate_cell_lo(px, m), gate_cell_hi(px, m, cells.w16), gate_cell_lo(py, m),
+                                  gate_cell_hi(py, m, cells.h16)))
                     rv[k] = -1e30f;
             }
         }

@@ -73,11 +73,16 @@ struct GateScratch {
 int gate_bitmap_words(int gw, int gh);
 // the gate network on the frame's gray image, then the stage-1 tile activity of every level
 // the cell bitmaps of a gated frame for the stage-1 back kernel
-GateCells gate_cells(GateScratch sc, int gw, int gh, float amb_frac);
+GateCells gate_cells(GateScratch sc, int gw, int gh, float amb_frac, int margin);
 // feat_ready: sc.feat already holds the frame's features (the gray launch wrote them); otherwise they
 // are computed from `gray` first
-cudaError_t launch_gate(const float* d_params, const float* gray, int gpitch, int gw, int gh, bool feat_ready, const LevelDesc* levels,
-                        int n_levels, GateScratch sc, float thr, float amb_frac, uint8_t* back_on, uint8_t* front_on, cudaStream_t st);
+// the gate network's parameters as a kernel parameter (read from the constant bank)
+struct GateNet {
+    float p[kGateParams];
+};
+cudaError_t launch_gate(const GateNet& net, const float* gray, int gpitch, int gw, int gh, bool feat_ready, const LevelDesc* levels,
+                        int n_levels, GateScratch sc, float thr, float amb_frac, int margin, uint8_t* back_on, uint8_t* front_on,
+                        cudaStream_t st);
 cudaError_t launch_gate_labels(const Candidate* cands, const CandResult* res, const int* ncand, int cap, const LevelDesc* d_levels, int gw, int gh,
                                uint8_t* labels, cudaStream_t st);
 
@@ -171,7 +176,7 @@ struct GrayRef {
 // parameters); level tiles resampled from `gray`, or read from limg + img_off when gray.p is null
 // counts (optional, zeroed by the caller): per candidate-scan chunk, responses > thr
 // cells (optional): the gate's cell bitmaps; a response above thr whose window centre has no likely
-// cell within one cell of it (in its level's octave) is written below every threshold
+// cell within cells.margin cells of it (in its level's octave) is written below every threshold
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
                           cudaStream_t st, int* counts = nullptr, float thr = 0.f, const uint8_t* front_on = nullptr,
                           const uint8_t* back_on = nullptr, GateCells cells = GateCells{}, Stage1Sched sched = Stage1Sched{},

@@ -59,6 +59,7 @@ class Server {
     ~Server();
     ccnn_status submit(const ccnn_image& img, long long* ticket);
     ccnn_status set_gate(const float* params, int n, float threshold, float fallback_fraction);
+    ccnn_status set_gate_margin(int pixels);
     ccnn_status take(long long ticket, bool block, ccnn_face* faces, int cap, int* n, double* lat);
     void stats(ccnn_server_stats* out);
 
@@ -73,6 +74,7 @@ class Server {
     ccnn_params params_{};
     std::vector<float> gate_;  // learned-gate parameters for every class (empty: full scan)
     float gate_thr_ = 0.5f, gate_fb_ = 0.25f;
+    int gate_margin_ = 16;
     std::string models_[3];
     bool has_models_ = false;
     size_t budget_ = 0;
@@ -139,6 +141,20 @@ ccnn_status Server::set_gate(const float* params, int n, float threshold, float 
     gate_.assign(params, params + n);
     gate_thr_ = threshold;
     gate_fb_ = fallback_fraction;
+    return CCNN_OK;
+}
+
+ccnn_status Server::set_gate_margin(int pixels) {
+    if (pixels < 0 || pixels > 64) {
+        set_error("gate margin: 0-64 pixels");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> lk(mu_);
+    if (submitted_ > 0) {
+        set_error("the gate margin must be set before the first frame is submitted");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    gate_margin_ = pixels;
     return CCNN_OK;
 }
 
@@ -271,6 +287,7 @@ ccnn_status Server::make_class(const ccnn_image& img, ResClass** out, bool* retr
             c->det.reset(new Detector());
             st = c->det->create(p, models, slots, colour);
             if (st == CCNN_OK && !gate_.empty()) st = c->det->gate_set(gate_.data(), (int)gate_.size(), gate_thr_, gate_fb_);
+            if (st == CCNN_OK && !gate_.empty()) st = c->det->gate_set_margin(gate_margin_);
             if (st != CCNN_ERR_OOM || !evict_one()) break;
         }
         if (st == CCNN_ERR_OOM) {
@@ -439,6 +456,14 @@ extern "C" CCNN_API ccnn_status ccnn_server_create(const ccnn_params* params, co
     if (st != CCNN_OK) return st;
     *out = s.release();
     return CCNN_OK;
+}
+
+extern "C" CCNN_API ccnn_status ccnn_server_set_gate_margin(ccnn_server s, int pixels) {
+    if (!s) {
+        ccnn::set_error("invalid arguments");
+        return CCNN_ERR_INVALID_ARG;
+    }
+    return s->srv.set_gate_margin(pixels);
 }
 
 extern "C" CCNN_API ccnn_status ccnn_server_set_gate(ccnn_server s, const float* params, int n_params, float threshold,

@@ -185,9 +185,9 @@ def box_recall(ref, got, iou=0.5):
 
 
 def evaluate(det, seeds, params, thresholds, fallback_fraction=0.25, width=FRAME_W, height=FRAME_H, n_faces=N_FACES,
-             min_patch=MIN_PATCH, max_patch=MAX_PATCH):
+             min_patch=MIN_PATCH, max_patch=MAX_PATCH, margin=16):
     """Box recall of the gated cascade against the plain one on the seeded frames, and the share
-    of stage-1 tiles that ran, per threshold."""
+    of stage-1 tiles that ran, per threshold (candidate margin `margin` pixels)."""
     import torch
     from . import synth_frame_device
     frame = torch.empty((height, width, 3), dtype=torch.uint8, device="cuda")
@@ -199,6 +199,7 @@ def evaluate(det, seeds, params, thresholds, fallback_fraction=0.25, width=FRAME
     out = []
     for thr in thresholds:
         det.setGate(params, thr, fallback_fraction)
+        det.setGateMargin(margin)
         hit = tot = 0
         fr = ft = br = bt = fb = 0
         frames_full = 0
@@ -210,29 +211,35 @@ def evaluate(det, seeds, params, thresholds, fallback_fraction=0.25, width=FRAME
             a, b, c, d, e = det.gateStats()
             fr, ft, br, bt, fb = fr + a, ft + b, br + c, bt + d, fb + e
             frames_full += int(h == t)
-        out.append({"threshold": thr, "box_recall": hit / max(1, tot), "boxes": tot, "frames_all_boxes": frames_full,
+        out.append({"threshold": thr, "margin": margin, "box_recall": hit / max(1, tot), "boxes": tot, "frames_all_boxes": frames_full,
                     "front_tiles_run": fr / max(1, ft), "back_tiles_run": br / max(1, bt), "fallback_frames": fb})
+    det.setGateMargin(16)
     det.disableGate()
     return out
 
 
 def _operating_point(ev, thresholds):
-    """The highest threshold that kept >= 99.5% of the plain boxes on the held-out frames (half a
-    point of margin over the 99% recall target for frames outside the evaluation set)."""
-    ok = [r["threshold"] for r in ev if r["box_recall"] >= 0.995]
-    return max(ok) if ok else min(thresholds)
+    """(threshold, margin): of the evaluated pairs that kept >= 99.5% of the plain boxes on the
+    held-out frames (half a point over the 99% recall target, for frames outside the evaluation
+    set), the one that runs the fewest stage-1 back tiles (ties: the higher threshold)."""
+    ok = [r for r in ev if r["box_recall"] >= 0.995]
+    if not ok:
+        return min(thresholds), 16
+    best = min(ok, key=lambda r: (r["back_tiles_run"], -r["threshold"]))
+    return best["threshold"], best.get("margin", 16)
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description="train the learned gate on frames labelled by the plain cascade")
     ap.add_argument("--train-frames", type=int, default=20000)
     ap.add_argument("--eval-frames", type=int, default=1000)
-    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--epochs", type=int, default=100)
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--lr", type=float, default=3e-3)
-    ap.add_argument("--pos-weight", type=float, default=40.0)
+    ap.add_argument("--pos-weight", type=float, default=80.0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--thresholds", default="0.02,0.05,0.1,0.2,0.3,0.4,0.5")
+    ap.add_argument("--margins", default="8,16", help="candidate margins (pixels) to evaluate")
     ap.add_argument("--fallback", type=float, default=0.25)
     ap.add_argument("--out", default=WEIGHTS_1080P)
     ap.add_argument("--report", default=None, help="write the evaluation as JSON here")
@@ -244,20 +251,29 @@ def main(argv=None):
     if det.Init(detector_params()) != 0:
         raise RuntimeError(_capi.last_error())
     thr = [float(x) for x in a.thresholds.split(",")]
-    if a.eval_only:
-        params, meta = load(a.out), load_meta(a.out)
-        ev = evaluate(det, range(EVAL_SEED0, EVAL_SEED0 + a.eval_frames), params, thr, a.fallback)
+    margins = [int(x) for x in a.margins.split(",")]
+
+    def evaluate_all(params):
+        ev = []
+        for m in margins:
+            ev += evaluate(det, range(EVAL_SEED0, EVAL_SEED0 + a.eval_frames), params, thr, a.fallback, margin=m)
         for r in ev:
             print(json.dumps(r), flush=True)
+        return ev
+
+    if a.eval_only:
+        params, meta = load(a.out), load_meta(a.out)
+        ev = evaluate_all(params)
+        op_thr, op_margin = _operating_point(ev, thr)
         meta.update(eval=ev, eval_frames=a.eval_frames, eval_seeds=[EVAL_SEED0, EVAL_SEED0 + a.eval_frames],
-                    operating_threshold=_operating_point(ev, thr))
-        print(f"operating threshold {meta['operating_threshold']}", flush=True)
+                    operating_threshold=op_thr, operating_margin=op_margin)
+        print(f"operating threshold {op_thr}, margin {op_margin} px", flush=True)
         save(a.out, params, meta)
         if a.report:
             with open(a.report, "w") as f:
                 json.dump({"weights": os.path.basename(a.out), "eval_frames": a.eval_frames,
                            "eval_seeds": meta["eval_seeds"], "fallback_fraction": a.fallback,
-                           "operating_threshold": meta["operating_threshold"], "eval": ev,
+                           "operating_threshold": op_thr, "operating_margin": op_margin, "eval": ev,
                            "workload": meta.get("workload"), "reference": "plain cascade boxes matched at IoU >= 0.5"}, f, indent=1)
         return 0
     t0 = time.time()
@@ -268,12 +284,10 @@ def main(argv=None):
     t2 = time.time()
     print(f"trained {a.epochs} epochs in {t2 - t1:.1f} s; loss {losses[0]:.4f} -> {losses[-1]:.4f}", flush=True)
     del ds
-    ev = evaluate(det, range(EVAL_SEED0, EVAL_SEED0 + a.eval_frames), params, thr, a.fallback)
-    for r in ev:
-        print(json.dumps(r), flush=True)
-    op = _operating_point(ev, thr)
-    print(f"operating threshold {op}", flush=True)
-    meta = {"operating_threshold": op, "train_frames": a.train_frames, "train_seeds": [TRAIN_SEED0, TRAIN_SEED0 + a.train_frames], "epochs": a.epochs,
+    ev = evaluate_all(params)
+    op, op_margin = _operating_point(ev, thr)
+    print(f"operating threshold {op}, margin {op_margin} px", flush=True)
+    meta = {"operating_threshold": op, "operating_margin": op_margin, "train_frames": a.train_frames, "train_seeds": [TRAIN_SEED0, TRAIN_SEED0 + a.train_frames], "epochs": a.epochs,
             "batch": a.batch, "lr": a.lr, "pos_weight": a.pos_weight, "init_seed": a.seed,
             "loss_first_last": [float(losses[0]), float(losses[-1])],
             "workload": f"{FRAME_W}x{FRAME_H} synthetic, {N_FACES} patches {MIN_PATCH}-{MAX_PATCH} px, min face {MIN_FACE}, "

@@ -38,6 +38,12 @@ CCNN_API ccnn_status ccnn_gate_set(ccnn_handle h, const float* params, int n_par
 /* Back to the full scan. */
 CCNN_API ccnn_status ccnn_gate_disable(ccnn_handle h);
 
+/* How far (in frame pixels along each axis, 0-64, default 16: the centre's cell and one cell on
+ * either side) from a stage-1 candidate's window centre the gate looks for a likely cell of the
+ * candidate's octave; the stage-1 tiles are kept by the same rule. A smaller margin skips more work
+ * and keeps fewer of the plain cascade's boxes. */
+CCNN_API ccnn_status ccnn_gate_set_margin(ccnn_handle h, int pixels);
+
 /* Stage-1 tiles of the handle's last frame: how many of the front (pooled layer-1) and back
  * (response) tiles ran, of how many, and whether the frame fell back to the full scan. With the
  * gate off every tile runs. */

@@ -50,6 +50,9 @@ CCNN_API ccnn_status ccnn_server_destroy(ccnn_server s);
 /* Turns the learned gate (include/ccnn_gate.h, ccnn_gate_set) on for every resolution class the
  * server creates; only before the first frame is submitted (CCNN_ERR_INVALID_ARG after). */
 CCNN_API ccnn_status ccnn_server_set_gate(ccnn_server s, const float* params, int n_params, float threshold, float fallback_fraction);
+/* The gate's candidate margin (ccnn_gate_set_margin, pixels 0-64, default 16) for every class; only
+ * before the first frame is submitted. */
+CCNN_API ccnn_status ccnn_server_set_gate_margin(ccnn_server s, int pixels);
 /* Queues one frame; *ticket identifies its result. CCNN_BUSY when max_queue requests wait. */
 CCNN_API ccnn_status ccnn_server_submit(ccnn_server s, const ccnn_image* img, long long* ticket);
 /* Result of a ticket: CCNN_PENDING while unfinished (poll), or blocks until it is done (wait).

@@ -184,6 +184,30 @@ def test_gate_rejects_bad_arguments():
         d.setGate(np.zeros(10, np.float32))
     with pytest.raises(ccnn.CCNNError):
         d.setGate(np.zeros(700, np.float32), threshold=1.5)
+    with pytest.raises(ccnn.CCNNError):
+        d.setGateMargin(65)
+
+
+def test_wider_margin_keeps_more():
+    """The candidate margin only widens or narrows the search: a wider margin runs a superset of the
+    tiles and keeps at least the boxes of a narrower one; the default (16 px) is the one-cell rule."""
+    params = gate.load() if os.path.exists(gate.WEIGHTS_1080P) else gate.init_params(3)
+    imgs = [ccnn.synth_frame(1920, 1080, 70 + i, 20, 30, 300)[0] for i in range(3)]
+    d0 = _det(1920, 1080)
+    d0.setGate(params, 0.3, 0.25)
+    default = [d0.Detect(im) for im in imgs]
+    d = _det(1920, 1080)
+    d.setGate(params, 0.3, 0.25)
+    runs = {}
+    for m in (0, 8, 16, 64):
+        d.setGateMargin(m)
+        got = [d.Detect(im) for im in imgs]
+        runs[m] = d.gateStats()
+        if m == 16:
+            assert got == default
+    for a, b in ((0, 8), (8, 16), (16, 64)):
+        assert runs[a][0] <= runs[b][0] and runs[a][2] <= runs[b][2]
+    assert runs[0][2] < runs[64][2]
 
 
 def test_batch_path_uses_the_gate():
@@ -214,12 +238,12 @@ def test_trained_gate_keeps_recall_and_skips_work():
     cascade's boxes are found while well under half of the stage-1 tiles run. The untrained
     network at the same threshold does not get both."""
     meta = gate.load_meta()
-    thr = meta.get("operating_threshold", 0.1)
+    thr, margin = meta.get("operating_threshold", 0.1), meta.get("operating_margin", 16)
     d = ccnn.FaceDetector()
     assert d.Init(gate.detector_params()) == 0
     seeds = range(gate.EVAL_SEED0 + 5000, gate.EVAL_SEED0 + 5040)
-    trained = gate.evaluate(d, seeds, gate.load(), [thr])[0]
+    trained = gate.evaluate(d, seeds, gate.load(), [thr], margin=margin)[0]
     assert trained["box_recall"] >= 0.99
     assert trained["back_tiles_run"] <= 0.5
-    untrained = gate.evaluate(d, seeds, gate.init_params(0), [thr])[0]
+    untrained = gate.evaluate(d, seeds, gate.init_params(0), [thr], margin=margin)[0]
     assert untrained["box_recall"] < 0.99 or untrained["back_tiles_run"] > 0.5
