@@ -188,8 +188,11 @@ def run_batched_pyramid(dev, args):
             return gms.value
 
         res = {}
-        for form, sched in (("per_frame", {"frame_slots": B, "batch_frames": 0}),
-                            ("batched", {"frame_slots": 2 * B, "batch_frames": B})):
+        # the autotuner's schedule for this workload where it has one (its other knobs also for the
+        # batched form)
+        tuned = autotune.lookup(p) or {}
+        for form, sched in (("per_frame", dict(tuned, frame_slots=tuned.get("frame_slots", B), batch_frames=0)),
+                            ("batched", dict(tuned, frame_slots=2 * B, batch_frames=B))):
             autotune.set_schedule(det, sched)
             for _ in range(max(3, args.warmup)):
                 step()
@@ -204,7 +207,8 @@ def run_batched_pyramid(dev, args):
                 res["_pf_faces"] = ref_faces
             n_levels = len(det.levels())
             res[form] = {"frames_per_s": round(steps * B / (ms / 1e3), 1), "steps": steps,
-                         "launches_per_8_frames": launches_per_frames(8, n_levels, sched["batch_frames"])}
+                         "launches_per_8_frames": launches_per_frames(8, n_levels, sched["batch_frames"]),
+                         "schedule": autotune.get_schedule(det)}
         res.pop("_pf_faces", None)
         autotune.set_schedule(det, {"frame_slots": B, "batch_frames": 0})
         lat = []
@@ -219,8 +223,8 @@ def run_batched_pyramid(dev, args):
         det.Clear()
     out["note"] = ("seeded frames with 60 face patches 20-600 px, scale 1.05, min face 20, no max face; device-resident frames, "
                    "device time from CUDA events. per_frame: every frame's chain one CUDA graph (stage 1, whose front kernel "
-                   "resamples the pyramid levels, in level tables of at most 32 levels a launch), 8 frames in flight. batched: 8 "
-                   "frames one graph, the pyramid and stage 1 "
+                   "resamples the pyramid levels, in level tables of at most 32 levels a launch), the autotuned frames in flight. "
+                   "batched: 8 frames one graph, the pyramid and stage 1 "
                    "of all levels of all 8 frames in one persistent launch fed by a device work queue, two 8-frame groups in flight")
     return out
 
