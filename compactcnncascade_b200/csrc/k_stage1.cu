@@ -122,14 +122,40 @@ __device__ __forceinline__ void resample_front_tile(FrontSmem& S, const GrayRef&
     }
 }
 
+// The learned gate inside a running stage-1 tile: whether any response pixel of [rx0, rx1] x [ry0, ry1]
+// (clamped to the level's response map) has a likely cell of the level's octave within the margin of
+// its window centre ((4x + 11.5) / s, (4y + 13.5) / s). The centre moves monotonically with x and y, so
+// the rectangle's cells are those of its corners (the same rule as the gate's tile decisions). Only
+// live response pixels can become candidates; everything else a gated tile computes is skipped.
+__device__ __forceinline__ bool gate_gating(const GateCells& cells) { return cells.bits && *cells.ambiguous <= cells.amb_limit; }
+
+__device__ __forceinline__ bool gate_live(const GateCells& cells, const LevelDesc& L, int rx0, int rx1, int ry0, int ry1) {
+    rx0 = max(rx0, 0);
+    ry0 = max(ry0, 0);
+    rx1 = min(rx1, L.ow - 1);
+    ry1 = min(ry1, L.oh - 1);
+    if (rx0 > rx1 || ry0 > ry1) return false;
+    const int px0 = (int)((4.f * rx0 + 11.5f) * L.inv_scale), px1 = (int)((4.f * rx1 + 11.5f) * L.inv_scale);
+    const int py0 = (int)((4.f * ry0 + 13.5f) * L.inv_scale), py1 = (int)((4.f * ry1 + 13.5f) * L.inv_scale);
+    const uint32_t* B = cells.bits + (long long)min(L.octave, kGK - 1) * cells.h16 * cells.wwords;
+    const int m = cells.margin;
+    return gate_any_bit(B, cells.wwords, gate_cell_lo(px0, m), gate_cell_hi(px1, m, cells.w16), gate_cell_lo(py0, m),
+                        gate_cell_hi(py1, m, cells.h16));
+}
+
 // Front tile t of level L: its (67 x 35) level-image tile staged in S.T (resampled from the gray
 // frame G when kFromGray, else read from the stored level images limg), then the 4x4 conv + folded
 // BN/LReLU + 2x2 max of the 4 L1 maps for 32 x 16 pooled pixels (two vertically adjacent pixels a
 // thread) and the 4 neighbour-map sums written to the S1 arena. kCoherent: a stored level image was
 // written earlier in the same launch (read through L2, not the read-only path).
+// cells (the learned gate, optional): a warp whose S1 strip (2 rows x 32 columns) feeds no live
+// response pixel writes nothing. S1 row y feeds pooled-L2 rows ceil((y - 3) / 2) .. y / 2 (a 3x3
+// conv at the 2x2 pool positions), and L2 row Y feeds response rows Y - 4 .. Y (the 4-wide, 5-tall L3
+// kernel); columns alike with the 4-wide kernel. The back kernel computes exactly the live pixels'
+// inputs, so a skipped strip is never read for a value that is kept.
 template <bool kFromGray, bool kCoherent>
 __device__ __forceinline__ void front_tile(const Stage1W& W, FrontSmem& S, const LevelDesc& L, int t, const float* __restrict__ limg,
-                                           const GrayRef& G, float* __restrict__ s1) {
+                                           const GrayRef& G, float* __restrict__ s1, const GateCells& cells) {
     const int px0 = (t % L.k1_tiles_x) * kK1TileX;
     const int py0 = (t / L.k1_tiles_x) * kK1TileY;
     const int ix0 = 2 * px0, iy0 = 2 * py0;
@@ -143,6 +169,10 @@ __device__ __forceinline__ void front_tile(const Stage1W& W, FrontSmem& S, const
 
     const int qx = threadIdx.x & (kK1TileX - 1);
     const int qy = (threadIdx.x >> 5) * 2;
+    if (gate_gating(cells)) {
+        const int ya = py0 + qy, yb = ya + 1, xa = px0, xb = px0 + kK1TileX - 1;  // warp-uniform strip
+        if (!gate_live(cells, L, ((xa - 3 + 1) >> 1) - 3, xb >> 1, ((ya - 3 + 1) >> 1) - 4, yb >> 1)) return;
+    }
     const f2_t nz = f2_ld(W.negzero);
     // pr[r][c] = (input row 2qy+r, row 2qy+r+2) at column 2qx+c: the windows of both pixels
     f2_t pr[5][5];
@@ -189,12 +219,12 @@ __device__ __forceinline__ void front_tile(const Stage1W& W, FrontSmem& S, const
 template <bool kFromGray, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) stage1_front_kernel(const __grid_constant__ Stage1W W, const __grid_constant__ LevelTable LT,
                                                               const float* __restrict__ limg, const GrayRef G, float* __restrict__ s1,
-                                                              const uint8_t* __restrict__ front_on) {
+                                                              const uint8_t* __restrict__ front_on, const GateCells cells) {
     __shared__ FrontSmem S;
     const int g = LT.first + blockIdx.x;
     if (front_on && !front_on[g]) return;  // gated off: no back tile reads this one
     const LevelDesc& L = LT.lv[find_level<&LevelDesc::k1_base>(LT, g)];
-    front_tile<kFromGray, false>(W, S, L, g - L.k1_base, limg, G, s1);
+    front_tile<kFromGray, false>(W, S, L, g - L.k1_base, limg, G, s1, cells);
 }
 
 constexpr int kP2TW = kK2TileX + 3;   // 35 pooled L2 columns (halo 3)
@@ -275,6 +305,11 @@ __device__ __forceinline__ f2_t pool_l2_pair(const BackSmem& S, const Stage1W& W
 //      the pair: the 16 L3 maps (4w x 5h), the 52 hidden neurons and the output neuron.
 // Back tile t of level L as above; g is its global back-tile index (the gate's tile index).
 // kCoherent: the S1 arena was written earlier in the same launch (read through L2).
+// With the learned gate (cells), a warp (32 x 2 response pixels) without a live pixel writes the skip
+// marker instead of computing, the L2 phase computes only the rows live warps read (warp w reads L2
+// rows 2w .. 2w + 5), and every pixel that is not live is written as the skip marker: only live
+// pixels can become candidates, and their inputs are exactly what runs (the front kernel skips the
+// rest of S1).
 template <bool kCoherent>
 __device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, BackSmem& S, const LevelDesc& L, int t, int g,
                                           const float* __restrict__ s1, float* __restrict__ resp, int* __restrict__ counts, float thr,
@@ -290,18 +325,35 @@ __device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, 
     }
     const int sx0 = 2 * ox0, sy0 = 2 * oy0;
     const f2_t nz = f2_ld(W.negzero);
+    const bool gating = gate_gating(cells);
+    __shared__ int s_live[kK2TileY / 2];  // per warp: any live response pixel
+    if (gating && (threadIdx.x & 31) == 0) {
+        const int ry = oy0 + 2 * (threadIdx.x >> 5);
+        s_live[threadIdx.x >> 5] = gate_live(cells, L, ox0, ox0 + kK2TileX - 1, ry, ry + 1) ? 1 : 0;
+    }
 
     // first half: pooled L2 maps 0-3, sums 0-2; (P2 + P3) and P3 of each pixel carried over
     float carry23[kP2Passes], carry3[kP2Passes];
     load_back_half<kCoherent>(S, s1, L, sx0, sy0, 0);
     __syncthreads();
+    uint32_t live = 0xffu;  // live warps
+    if (gating) {
+        live = 0u;
+#pragma unroll
+        for (int w = 0; w < kK2TileY / 2; ++w) live |= (s_live[w] ? 1u : 0u) << w;
+    }
+    // L2 row y is read by warps ceil((y - 5) / 2) .. y / 2
+    auto need_row = [&](int y) {
+        const int wlo = max(0, (y - 5 + 1) >> 1), whi = min(kK2TileY / 2 - 1, y >> 1);
+        return wlo <= whi && ((live >> wlo) & ((1u << (whi - wlo + 1)) - 1u)) != 0u;
+    };
 #pragma unroll
     for (int k = 0; k < kP2Passes; ++k) {
         const int p = threadIdx.x + 256 * k;
         carry23[k] = carry3[k] = 0.f;
-        if (p < kP2Px) {
-            int x, y;
-            p2_pixel(p, &x, &y);
+        int x = 0, y = 0;
+        if (p < kP2Px) p2_pixel(p, &x, &y);
+        if (p < kP2Px && need_row(y)) {
             const f2_t a = pool_l2_pair(S, W, 0, 0, x, y, nz), b = pool_l2_pair(S, W, 1, 1, x, y, nz);
             const float P0 = f2_lo(a), P1 = f2_hi(a), P2 = f2_lo(b), P3 = f2_hi(b);
             const float s01 = fadd(P0, P1);
@@ -319,9 +371,9 @@ __device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, 
 #pragma unroll
     for (int k = 0; k < kP2Passes; ++k) {
         const int p = threadIdx.x + 256 * k;
-        if (p < kP2Px) {
-            int x, y;
-            p2_pixel(p, &x, &y);
+        int x = 0, y = 0;
+        if (p < kP2Px) p2_pixel(p, &x, &y);
+        if (p < kP2Px && need_row(y)) {
             const f2_t a = pool_l2_pair(S, W, 2, 0, x, y, nz), b = pool_l2_pair(S, W, 3, 1, x, y, nz);
             const float P4 = f2_lo(a), P5 = f2_hi(a), P6 = f2_lo(b), P7 = f2_hi(b);
             S.s2[3][y][x] = fadd(carry23[k], P4);
@@ -336,25 +388,14 @@ __device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, 
 
     // C: pixels (x, y) and (x, y + 1)
     const int x = threadIdx.x & (kK2TileX - 1), y = (threadIdx.x / kK2TileX) * 2;
-    if (cells.bits && *cells.ambiguous <= cells.amb_limit) {
-        // learned gate, per warp (its 32 x 2 response pixels): when no likely cell of the level's
-        // octave lies within the margin of any of their window centres, every candidate among them
-        // would be dropped below, so the warp writes the skip marker instead of computing them
-        const int gy = oy0 + y;  // warp-uniform
-        const int gx1 = min(ox0 + kK2TileX, L.ow) - 1, gy1 = min(gy + 1, L.oh - 1);
-        const int px0 = (int)((4.f * ox0 + 11.5f) * L.inv_scale), px1 = (int)((4.f * gx1 + 11.5f) * L.inv_scale);
-        const int py0 = (int)((4.f * gy + 13.5f) * L.inv_scale), py1 = (int)((4.f * gy1 + 13.5f) * L.inv_scale);
-        const uint32_t* B = cells.bits + (long long)min(L.octave, kGK - 1) * cells.h16 * cells.wwords;
-        const int m = cells.margin;
-        if (gy >= L.oh || !gate_any_bit(B, cells.wwords, gate_cell_lo(px0, m), gate_cell_hi(px1, m, cells.w16), gate_cell_lo(py0, m),
-                                       gate_cell_hi(py1, m, cells.h16))) {
-            const int gx = ox0 + x;
-            if (gx < L.ow) {
-                if (gy < L.oh) resp[L.resp_off + (long long)gy * L.ow + gx] = -1e30f;
-                if (gy + 1 < L.oh) resp[L.resp_off + (long long)(gy + 1) * L.ow + gx] = -1e30f;
-            }
-            return;
+    if (!((live >> (threadIdx.x >> 5)) & 1u)) {
+        // no live pixel in the warp: the skip marker instead of the responses
+        const int gx = ox0 + x, gy = oy0 + y;
+        if (gx < L.ow) {
+            if (gy < L.oh) resp[L.resp_off + (long long)gy * L.ow + gx] = -1e30f;
+            if (gy + 1 < L.oh) resp[L.resp_off + (long long)(gy + 1) * L.ow + gx] = -1e30f;
         }
+        return;
     }
     // L3 maps (2k, 2k+1) of the pixel pair, both from neighbour-sum map k; conv_5x4 keeps one
     // partial sum per kernel row, added in row order
@@ -417,18 +458,11 @@ __device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, 
     const int gx = ox0 + x, gy = oy0 + y;
     if (gx < L.ow) {
         float rv[2] = {f2_lo(r), f2_hi(r)};
-        if (cells.bits && (rv[0] > thr || rv[1] > thr) && *cells.ambiguous <= cells.amb_limit) {
-            // learned gate, per candidate: its window centre ((4x + 11.5) / s, (4y + 13.5) / s) needs a
-            // likely cell of its octave within the margin
-            const uint32_t* B = cells.bits + (long long)min(L.octave, kGK - 1) * cells.h16 * cells.wwords;
-            const int px = (int)((4.f * gx + 11.5f) * L.inv_scale), m = cells.margin;
-            for (int k = 0; k < 2; ++k) {
-                if (!(rv[k] > thr)) continue;
-                const int py = (int)((4.f * (gy + k) + 13.5f) * L.inv_scale);
-                if (!gate_any_bit(B, cells.wwords, gate_cell_lo(px, m), gate_cell_hi(px, m, cells.w16), gate_cell_lo(py, m),
-                                  gate_cell_hi(py, m, cells.h16)))
-                    rv[k] = -1e30f;
-            }
+        if (gating) {
+            // only live pixels keep their response (a candidate needs a likely cell of its octave within
+            // the margin of its window centre); the others may have read skipped inputs
+            for (int k = 0; k < 2; ++k)
+                if (!gate_live(cells, L, gx, gx, gy + k, gy + k)) rv[k] = -1e30f;
         }
         // candidates (response > treshold_1) are counted per scan chunk for the compaction
         if (gy < L.oh) {
@@ -511,15 +545,17 @@ static cudaError_t launch_grouped(const LevelDesc* levels, int n_levels, int Lev
 }
 
 cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st,
-                                const uint8_t* front_on, Stage1Sched sched, GrayRef gray) {
+                                const uint8_t* front_on, Stage1Sched sched, GrayRef gray, GateCells cells) {
     return launch_grouped(
         levels, n_levels, &LevelDesc::k1_base, [](const LevelDesc& L) { return L.k1_tiles_x * ((L.p1h + kK1TileY - 1) / kK1TileY); },
         [&](const LevelTable& T, int blocks) {
             const bool four = sched.front_blocks_per_sm >= 4;
             if (gray.p)
-                (four ? stage1_front_kernel<true, 4> : stage1_front_kernel<true, 3>)<<<blocks, 256, 0, st>>>(W, T, limg, gray, s1, front_on);
+                (four ? stage1_front_kernel<true, 4> : stage1_front_kernel<true, 3>)<<<blocks, 256, 0, st>>>(W, T, limg, gray, s1, front_on,
+                                                                                                              cells);
             else
-                (four ? stage1_front_kernel<false, 4> : stage1_front_kernel<false, 3>)<<<blocks, 256, 0, st>>>(W, T, limg, gray, s1, front_on);
+                (four ? stage1_front_kernel<false, 4> : stage1_front_kernel<false, 3>)<<<blocks, 256, 0, st>>>(W, T, limg, gray, s1, front_on,
+                                                                                                                cells);
         });
 }
 
@@ -539,7 +575,7 @@ cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_
 cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, float* resp,
                           cudaStream_t st, int* counts, float thr, const uint8_t* front_on, const uint8_t* back_on, GateCells cells,
                           Stage1Sched sched, GrayRef gray) {
-    cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st, front_on, sched, gray);
+    cudaError_t e = launch_stage1_front(W, levels, n_levels, limg, s1, st, front_on, sched, gray, cells);
     if (e != cudaSuccess) return e;
     return launch_stage1_back(W, levels, n_levels, s1, resp, st, counts, thr, back_on, cells, sched);
 }
@@ -644,7 +680,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) stage1_batch_kernel(const __g
         if (stage == 0) {
             if (!F.front_on[f] || F.front_on[f][g])
                 front_tile<true, false>(W, *reinterpret_cast<FrontSmem*>(smem_raw), L, g - L.k1_base, nullptr,
-                                  GrayRef{F.gray[f], F.gpitch, F.gw, F.gh}, F.s1[f]);
+                                        GrayRef{F.gray[f], F.gpitch, F.gw, F.gh}, F.s1[f], F.cells[f]);
         } else {
             back_tile<true>(W, D, *reinterpret_cast<BackSmem*>(smem_raw), L, g - L.k2_base, g, F.s1[f], F.resp[f], F.counts[f], Q.thr,
                             F.back_on[f], F.cells[f]);

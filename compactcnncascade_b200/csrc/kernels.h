@@ -184,7 +184,8 @@ cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_level
 // front_on / back_on (optional): per-tile activity from the gate; inactive back tiles write
 // responses below every threshold
 cudaError_t launch_stage1_front(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* limg, float* s1, cudaStream_t st,
-                                const uint8_t* front_on = nullptr, Stage1Sched sched = Stage1Sched{}, GrayRef gray = GrayRef{});
+                                const uint8_t* front_on = nullptr, Stage1Sched sched = Stage1Sched{}, GrayRef gray = GrayRef{},
+                                GateCells cells = GateCells{});
 // dynamic shared memory of the stage-1 back kernel (set once per device before any launch)
 cudaError_t stage1_setup();
 cudaError_t launch_stage1_back(const Stage1W& W, const LevelDesc* levels, int n_levels, const float* s1, float* resp, cudaStream_t st,
