@@ -445,7 +445,7 @@ def main():
                       for r in rates]
             print(json.dumps({"metric": "serving loop p50/p99 ms and fps, mixed 640x480/1280x720/1920x1080/3840x2160 at 30/30/30/10 %",
                               "unit": "ms", "data": "synthetic (seeded generator)", "frames_per_rate": args.serve_frames_sweep,
-                              "sweep": sweep, "gated_threshold": gthr, "sweep_gated": gsweep}), flush=True)
+                              "sweep": sweep, "gated_threshold": gthr, "gated_margin_px": gmargin, "sweep_gated": gsweep}), flush=True)
         return
 
     from compactcnncascade_b200.replicas import rank_seeds
