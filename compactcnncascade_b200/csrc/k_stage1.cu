@@ -105,7 +105,9 @@ __device__ __forceinline__ float resample_px(const GrayRef& G, const LevelDesc& 
     return fadd(fmul(top, sy.c), fmul(bot, sy.f));
 }
 
-__device__ __forceinline__ void resample_front_tile(FrontSmem& S, const GrayRef& G, const LevelDesc& L, int ix0, int iy0) {
+// rows: bit r set = tile row r is read by a warp that computes (the others are left as they are)
+__device__ __forceinline__ void resample_front_tile(FrontSmem& S, const GrayRef& G, const LevelDesc& L, int ix0, int iy0,
+                                                    unsigned long long rows) {
     static_assert(kInW == 67 && kInH == 35, "64 + 3 columns, 35 rows in 4 row groups");
     {
         const int c = threadIdx.x & 63, g = threadIdx.x >> 6;
@@ -113,12 +115,12 @@ __device__ __forceinline__ void resample_front_tile(FrontSmem& S, const GrayRef&
 #pragma unroll
         for (int k = 0; k < (kInH + 3) / 4; ++k) {
             const int r = g + 4 * k;
-            if (r < kInH) S.T.put(r, c, resample_px(G, L, sx, ix0 + c, iy0 + r));
+            if (r < kInH && ((rows >> r) & 1ull)) S.T.put(r, c, resample_px(G, L, sx, ix0 + c, iy0 + r));
         }
     }
     if (threadIdx.x < 3 * kInH) {
         const int c = 64 + threadIdx.x % 3, r = threadIdx.x / 3;
-        S.T.put(r, c, resample_px(G, L, sample_col(ix0 + c, L.sclx, G.w), ix0 + c, iy0 + r));
+        if ((rows >> r) & 1ull) S.T.put(r, c, resample_px(G, L, sample_col(ix0 + c, L.sclx, G.w), ix0 + c, iy0 + r));
     }
 }
 
@@ -160,8 +162,28 @@ __device__ __forceinline__ void front_tile(const Stage1W& W, FrontSmem& S, const
     const int py0 = (t / L.k1_tiles_x) * kK1TileY;
     const int ix0 = 2 * px0, iy0 = 2 * py0;
 
+    // with the gate: which warps have a live pixel downstream (warp w computes pooled rows 2w, 2w + 1 from
+    // tile rows 4w .. 4w + 6, so only those rows of live warps are resampled)
+    uint32_t live = 0xffu;
+    unsigned long long rows = ~0ull;
+    if (gate_gating(cells)) {
+        __shared__ int s_flive[kK1TileY / 2];
+        if ((threadIdx.x & 31) == 0) {
+            const int ya = py0 + 2 * (threadIdx.x >> 5), yb = ya + 1, xa = px0, xb = px0 + kK1TileX - 1;
+            s_flive[threadIdx.x >> 5] = gate_live(cells, L, ((xa - 3 + 1) >> 1) - 3, xb >> 1, ((ya - 3 + 1) >> 1) - 4, yb >> 1) ? 1 : 0;
+        }
+        __syncthreads();
+        live = 0u;
+        rows = 0ull;
+#pragma unroll
+        for (int w = 0; w < kK1TileY / 2; ++w)
+            if (s_flive[w]) {
+                live |= 1u << w;
+                rows |= 0x7full << (4 * w);
+            }
+    }
     if constexpr (kFromGray)
-        resample_front_tile(S, G, L, ix0, iy0);
+        resample_front_tile(S, G, L, ix0, iy0, rows);
     else
         load_front_tile<kCoherent>(S.T, limg + L.img_off, L, ix0, iy0);
     __syncthreads();
@@ -169,10 +191,7 @@ __device__ __forceinline__ void front_tile(const Stage1W& W, FrontSmem& S, const
 
     const int qx = threadIdx.x & (kK1TileX - 1);
     const int qy = (threadIdx.x >> 5) * 2;
-    if (gate_gating(cells)) {
-        const int ya = py0 + qy, yb = ya + 1, xa = px0, xb = px0 + kK1TileX - 1;  // warp-uniform strip
-        if (!gate_live(cells, L, ((xa - 3 + 1) >> 1) - 3, xb >> 1, ((ya - 3 + 1) >> 1) - 4, yb >> 1)) return;
-    }
+    if (!((live >> (threadIdx.x >> 5)) & 1u)) return;  // no live response pixel downstream of this warp
     const f2_t nz = f2_ld(W.negzero);
     // pr[r][c] = (input row 2qy+r, row 2qy+r+2) at column 2qx+c: the windows of both pixels
     f2_t pr[5][5];
