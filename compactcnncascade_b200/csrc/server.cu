@@ -73,6 +73,7 @@ class Server {
 
     ccnn_params params_{};
     std::vector<float> gate_;  // learned-gate parameters for every class (empty: full scan)
+    std::vector<ccnn_face> fetch_buf_;  // results of a finished slot (scheduler thread only)
     float gate_thr_ = 0.5f, gate_fb_ = 0.25f;
     int gate_margin_ = 16;
     std::string models_[3];
@@ -319,10 +320,12 @@ bool Server::collect_finished() {
         for (int k = 0; k < (int)c->slot_req.size(); ++k) {
             std::shared_ptr<Request>& r = c->slot_req[k];
             if (!r || !c->det->slot_done(k)) continue;
-            std::vector<ccnn_face> faces(kResultCap);
+            // fetched into one reusable buffer; the request keeps only its own faces
+            if (fetch_buf_.size() < (size_t)kResultCap) fetch_buf_.resize(kResultCap);
             int n = 0;
-            const ccnn_status st = c->det->fetch(k, faces.data(), kResultCap, &n);
+            const ccnn_status st = c->det->fetch(k, fetch_buf_.data(), kResultCap, &n);
             const std::string err = st < 0 ? std::string(ccnn_last_error()) : std::string();
+            std::vector<ccnn_face> faces(fetch_buf_.begin(), fetch_buf_.begin() + (st < 0 ? 0 : std::min(std::max(n, 0), kResultCap)));
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 r->faces.swap(faces);
