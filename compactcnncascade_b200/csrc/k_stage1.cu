@@ -608,9 +608,10 @@ cudaError_t launch_stage1(const Stage1W& W, const LevelDesc* levels, int n_level
 // loads by one thread, a bounded number of times); the diagonal queue order puts about one frame's
 // worth of other items between a frame's front tiles and its back tiles, so the polls almost never
 // wait. An item only waits on items queued before it, and a block holds at most the item it works on
-// and the one it claimed after it, so every wait ends whatever the number of resident blocks. The
-// level images come from the batched pyramid launch before; the S1 planes are written earlier in the
-// same launch and are read through L2 (ld.global.cg), never the read-only path.
+// and the one it claimed after it, so every wait ends whatever the number of resident blocks. Front
+// items resample their level tiles from the gray frames (written by the gray launch before); the S1
+// planes are written earlier in the same launch and are read through L2 (ld.global.cg), never the
+// read-only path.
 
 void build_batch_queue(BatchQueue* q, int n_frames, int n_levels, int n_chunks, int front_items, int back_items, float thr) {
     q->n_frames = n_frames;

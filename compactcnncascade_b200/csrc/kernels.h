@@ -86,8 +86,9 @@ cudaError_t launch_gate(const GateNet& net, const float* gray, int gpitch, int g
 cudaError_t launch_gate_labels(const Candidate* cands, const CandResult* res, const int* ncand, int cap, const LevelDesc* d_levels, int gw, int gh,
                                uint8_t* labels, cudaStream_t st);
 
-// every level image of a frame into the level arena (img_off / img_pitch of each descriptor);
-// blocks of kPyrCols columns x kPyrRows rows (pyr_wq column blocks per level row band)
+// every level image of a frame into the level arena (img_off / img_pitch of each descriptor), for the
+// legacy family (the CNTK stage-1 front kernel resamples its tiles itself); blocks of kPyrCols columns x
+// kPyrRows rows (pyr_wq column blocks per level row band)
 constexpr int kPyrCols = 256, kPyrRows = 8;
 cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* gray, int gpitch, int gw, int gh, float* limg,
                            cudaStream_t st,
