@@ -181,15 +181,14 @@ cudaError_t launch_gray_u8_resized(const uint8_t* src, int spitch, int sw, int s
 // weights for all its rows, and a warp's loads and stores walk consecutive columns. Columns between
 // the level width and the row pitch are written as zeros.
 __global__ void __launch_bounds__(kPyrCols) pyramid_kernel(const __grid_constant__ LevelTable LT, const float* __restrict__ gray,
-                                                           int gpitch, int gw, int gh, float* __restrict__ limg,
-                                                           const uint8_t* __restrict__ front_on) {
+                                                           int gpitch, int gw, int gh, float* __restrict__ limg) {
     const int g = LT.first + blockIdx.x;
     const LevelDesc& L = LT.lv[find_level<&LevelDesc::pyr_base>(LT, g)];
-    pyramid_block(L, g - L.pyr_base, gray, gpitch, gw, gh, limg, front_on);
+    pyramid_block(L, g - L.pyr_base, gray, gpitch, gw, gh, limg);
 }
 
 cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* gray, int gpitch, int gw, int gh, float* limg,
-                           cudaStream_t st, const uint8_t* front_on) {
+                           cudaStream_t st) {
     for (int g0 = 0; g0 < n_levels; g0 += kParamLevels) {
         LevelTable T;
         T.n = n_levels - g0 < kParamLevels ? n_levels - g0 : kParamLevels;
@@ -197,7 +196,7 @@ cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* g
         T.first = T.lv[0].pyr_base;
         const LevelDesc& last = T.lv[T.n - 1];
         const int blocks = last.pyr_base + last.pyr_wq * ((last.h + kPyrRows - 1) / kPyrRows) - T.first;
-        if (blocks > 0) pyramid_kernel<<<blocks, kPyrCols, 0, st>>>(T, gray, gpitch, gw, gh, limg, front_on);
+        if (blocks > 0) pyramid_kernel<<<blocks, kPyrCols, 0, st>>>(T, gray, gpitch, gw, gh, limg);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

@@ -22,7 +22,6 @@
 // search over the level descriptors (kernel parameters), so a frame is two launches per group of
 // up to kParamLevels levels.
 #include "kernels.h"
-#include "pyramid.cuh"
 #include "resample.cuh"
 
 namespace ccnn {

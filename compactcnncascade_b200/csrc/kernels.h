@@ -91,8 +91,7 @@ cudaError_t launch_gate_labels(const Candidate* cands, const CandResult* res, co
 // kPyrRows rows (pyr_wq column blocks per level row band)
 constexpr int kPyrCols = 256, kPyrRows = 8;
 cudaError_t launch_pyramid(const LevelDesc* levels, int n_levels, const float* gray, int gpitch, int gw, int gh, float* limg,
-                           cudaStream_t st,
-                           const uint8_t* front_on = nullptr);
+                           cudaStream_t st);
 // ---- batched form: one persistent launch runs the pyramid and stage 1 of B frames ----
 constexpr int kMaxBatch = 16;
 // per-frame buffers of the frames of one batch (frame f = entry f); the gray frames share one size

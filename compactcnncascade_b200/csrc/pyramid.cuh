@@ -2,7 +2,7 @@
 // ImageResizer::FastImageResize, image_resize.cpp:564-584): block `local` of level L covers kPyrCols
 // columns (one a thread) of kPyrRows rows of the level image, computed from the gray frame and
 // written to the level arena at L.img_off (columns past the level width up to its pitch get zeros).
-// front_on (optional, the learned gate): a block that no running stage-1 front tile reads is left out.
+// Only the legacy family stores level images (the CNTK stage-1 front kernel resamples its own tiles).
 #pragma once
 
 #include "kernels.h"
@@ -11,26 +11,9 @@
 namespace ccnn {
 
 __device__ __forceinline__ void pyramid_block(const LevelDesc& L, int local, const float* __restrict__ gray, int gpitch, int gw, int gh,
-                                              float* __restrict__ limg, const uint8_t* __restrict__ front_on) {
+                                              float* __restrict__ limg) {
     const int rb = local / L.pyr_wq;
     const int cb = local - rb * L.pyr_wq;
-    if (front_on) {
-        // with the learned gate only the stage-1 front tiles that run read the level image: a block
-        // that none of them reads is left out (front tile (tx, ty) reads rows [32 ty, 32 ty + 35)
-        // and columns [64 tx, 64 tx + 68))
-        const int ty0 = max(0, (kPyrRows * rb - (2 * kK1TileY + 3) + 2 * kK1TileY) / (2 * kK1TileY));
-        const int ty1 = min((L.p1h + kK1TileY - 1) / kK1TileY - 1, (kPyrRows * rb + kPyrRows - 1) / (2 * kK1TileY));
-        const int tx0 = max(0, (kPyrCols * cb - (2 * kK1TileX + 4) + 2 * kK1TileX) / (2 * kK1TileX));
-        const int tx1 = min(L.k1_tiles_x - 1, (kPyrCols * cb + kPyrCols - 1) / (2 * kK1TileX));
-        bool need = false;
-        for (int ty = ty0; ty <= ty1 && !need; ++ty)
-            for (int tx = tx0; tx <= tx1; ++tx)
-                if (front_on[L.k1_base + ty * L.k1_tiles_x + tx]) {
-                    need = true;
-                    break;
-                }
-        if (!need) return;
-    }
     const int x = cb * kPyrCols + threadIdx.x;
     if (x >= L.img_pitch) return;
     float* out = limg + L.img_off + x;
