@@ -615,6 +615,12 @@ def main():
                       "frac": round(value / world * fb_frame / (hbm_peak * 1e9), 5),
                       "note": "whole-frame algorithmic bytes (BGR read, gray write, gray samples of every level pixel, S1 planes and response maps written and read) "
                               "x frames/s"},
+        "frame_fp32": {"ops_per_frame": work["stage1_front"][0] + work["stage1_back"][0],
+                       "achieved": round(value / world * (work["stage1_front"][0] + work["stage1_back"][0]) / 1e12, 3),
+                       "unit": "T lane ops/s",
+                       "frac": round(value / world * (work["stage1_front"][0] + work["stage1_back"][0]) / 1e12 / fp32_peak, 4),
+                       "note": "the pipeline's stage-1 fp32 lane operations (front + back, per the formula in algorithmic_work) x "
+                               "frames/s per GPU against the same measured ceiling: the whole frame stream, not one launch"},
         "single_launch_stage1": ({"ms": round(single_launch_ms, 4),
                                   "achieved": round((work["stage1_front"][0] + work["stage1_back"][0]) / (single_launch_ms * 1e-3) / 1e12, 3),
                                   "frac": round((work["stage1_front"][0] + work["stage1_back"][0]) / (single_launch_ms * 1e-3) / 1e12 / fp32_peak, 4),
