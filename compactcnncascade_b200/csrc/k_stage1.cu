@@ -249,11 +249,10 @@ constexpr int kP2TW = kK2TileX + 3;   // 35 pooled L2 columns (halo 3)
 constexpr int kP2TH = kK2TileY + 4;   // 20 pooled L2 rows (halo 4)
 constexpr int kS1TW = 2 * kP2TW + 2;  // 72
 constexpr int kS1TH = 2 * kP2TH + 2;  // 42
-constexpr int kS1TWh = kS1TW / 2;     // 36 columns of each parity
 constexpr int kS2P = kP2TW + 1;       // 36: ts2 row pitch
 
 struct BackSmem {
-    float s1[2][kS1TH][kS1TW];    // half of the S1 tile (maps 2h, 2h+1); column c at (c & 1) * kS1TWh + (c >> 1)
+    float s1[2][kS1TH][kS1TW];    // two S1 maps of the tile, row-major: map k in s1[k & 1] (double buffer)
     float s2[8][kP2TH][kS2P];     // the 8 neighbour sums of the pooled L2 maps
 };
 constexpr int kBackSmemBytes = (int)sizeof(BackSmem);  // 47,232 B: four blocks fit a SM
@@ -273,34 +272,43 @@ __device__ __forceinline__ void p2_pixel(int p, int* x, int* y) {
     }
 }
 
-// S1 half h of a back tile (maps 2h and 2h+1) into S.s1 with 16-byte loads; columns past the plane
-// pitch and rows past p1h read as 0 (no valid response pixel depends on them)
-template <bool kCoherent>
-__device__ __forceinline__ void load_back_half(BackSmem& S, const float* __restrict__ s1, const LevelDesc& L, int sx0, int sy0, int h) {
-    const float* base = s1 + L.s1_off + (long long)(2 * h) * L.s1_plane;
+// S1 map k of a back tile into S.s1[k & 1] by asynchronous 16-byte copies (cp.async through L2, one
+// commit group); columns past the plane pitch and rows past p1h are zero-filled (no valid response
+// pixel depends on them). The copies land while the block computes on the other buffer.
+__device__ __forceinline__ void load_back_map_async(BackSmem& S, const float* __restrict__ s1, const LevelDesc& L, int sx0, int sy0, int k) {
+    const float* base = s1 + L.s1_off + (long long)k * L.s1_plane;
     constexpr int kV = kS1TW / 4;
-    for (int i = threadIdx.x; i < 2 * kS1TH * kV; i += blockDim.x) {
-        const int row = i / kV, c4 = i - row * kV;
-        const int m = row / kS1TH, rr = row - m * kS1TH;
+    float* buf = &S.s1[k & 1][0][0];
+    for (int i = threadIdx.x; i < kS1TH * kV; i += blockDim.x) {
+        const int rr = i / kV, c4 = i - rr * kV;
         const int x = sx0 + 4 * c4, y = sy0 + rr;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (y < L.p1h && x < L.s1_pitch) {
-            const float4* src = reinterpret_cast<const float4*>(base + m * L.s1_plane + (long long)y * L.s1_pitch + x);
-            v = kCoherent ? __ldcg(src) : __ldg(src);
-        }
-        *reinterpret_cast<float2*>(&S.s1[m][rr][2 * c4]) = make_float2(v.x, v.z);
-        *reinterpret_cast<float2*>(&S.s1[m][rr][kS1TWh + 2 * c4]) = make_float2(v.y, v.w);
+        const bool in = y < L.p1h && x < L.s1_pitch;  // x and the pitch are multiples of 4: the whole vector is in the row
+        const float* src = in ? base + (long long)y * L.s1_pitch + x : base;
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(buf + rr * kS1TW + 4 * c4);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(in ? 16 : 0) : "memory");
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
-// The pooled L2 maps (2i, 2i+1) at tile pixel (x, y), both from S1 map i (held as S.s1[i - 2h]):
-// 3x3 conv + BN/LReLU at the four positions of the 2x2 window, then their max
-__device__ __forceinline__ f2_t pool_l2_pair(const BackSmem& S, const Stage1W& W, int i, int il, int x, int y, f2_t nz) {
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// The pooled L2 maps (2i, 2i+1) at tile pixel (x, y), both from S1 map i (the buffer T): 3x3 conv +
+// BN/LReLU at the four positions of the 2x2 window, then their max. A warp reads 32 consecutive
+// column pairs of a row (8-byte loads, no bank conflicts).
+__device__ __forceinline__ f2_t pool_l2_pair(const float (*T)[kS1TW], const Stage1W& W, int i, int x, int y, f2_t nz) {
     f2_t q[4][4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) q[r][c] = f2_dup(S.s1[il][2 * y + r][(c & 1) * kS1TWh + x + (c >> 1)]);
+    for (int r = 0; r < 4; ++r) {
+        const float2 u = *reinterpret_cast<const float2*>(&T[2 * y + r][2 * x]);
+        const float2 v = *reinterpret_cast<const float2*>(&T[2 * y + r][2 * x + 2]);
+        q[r][0] = f2_dup(u.x);
+        q[r][1] = f2_dup(u.y);
+        q[r][2] = f2_dup(v.x);
+        q[r][3] = f2_dup(v.y);
+    }
     f2_t cv[4];
 #pragma unroll
     for (int d = 0; d < 4; ++d) {
@@ -314,11 +322,11 @@ __device__ __forceinline__ f2_t pool_l2_pair(const BackSmem& S, const Stage1W& W
 }
 
 // back: one CTA per 32 x 16 tile of response pixels.
-//   A/B in two halves: the S1 maps 0-1 of the tile (2 x 42 x 72) are staged in shared memory with
-//      16-byte loads, the pooled L2 maps 0-3 computed on the 35 x 20 halo tile (maps 2i and 2i+1
-//      read the same S1 map i: one packed pair) and the neighbour sums 0-2 written; the two sums
-//      that also need maps 4-5 stay in registers while S1 maps 2-3 replace 0-1 and the second half
-//      finishes sums 3-7. Half the S1 tile in shared memory is what lets four blocks share a SM.
+//   A/B map by map: the four S1 maps of the tile (42 x 72 each) pass through two shared-memory
+//      buffers, map k + 1 copied asynchronously while the pooled L2 maps (2k, 2k+1) are computed from
+//      map k on the 35 x 20 halo tile (one packed pair); the neighbour sums are written as soon as
+//      their three maps are known, the two partial sums a pixel still needs kept in registers. Two
+//      S1 maps in shared memory is what lets four blocks share a SM.
 //   C: every thread finishes two vertically adjacent response pixels, every operation packed over
 //      the pair: the 16 L3 maps (4w x 5h), the 52 hidden neurons and the output neuron.
 // Back tile t of level L as above; g is its global back-tile index (the gate's tile index).
@@ -350,56 +358,52 @@ __device__ __forceinline__ void back_tile(const Stage1W& W, const Stage1Dup& D, 
         s_live[threadIdx.x >> 5] = gate_live(cells, L, ox0, ox0 + kK2TileX - 1, ry, ry + 1) ? 1 : 0;
     }
 
-    // first half: pooled L2 maps 0-3, sums 0-2; (P2 + P3) and P3 of each pixel carried over
-    float carry23[kP2Passes], carry3[kP2Passes];
-    load_back_half<kCoherent>(S, s1, L, sx0, sy0, 0);
-    __syncthreads();
+    load_back_map_async(S, s1, L, sx0, sy0, 0);
+    load_back_map_async(S, s1, L, sx0, sy0, 1);
     uint32_t live = 0xffu;  // live warps
-    if (gating) {
-        live = 0u;
-#pragma unroll
-        for (int w = 0; w < kK2TileY / 2; ++w) live |= (s_live[w] ? 1u : 0u) << w;
-    }
     // L2 row y is read by warps ceil((y - 5) / 2) .. y / 2
     auto need_row = [&](int y) {
         const int wlo = max(0, (y - 5 + 1) >> 1), whi = min(kK2TileY / 2 - 1, y >> 1);
         return wlo <= whi && ((live >> wlo) & ((1u << (whi - wlo + 1)) - 1u)) != 0u;
     };
+    // pooled L2 maps (2k, 2k+1) = (A, B) from S1 map k; the sums in the reference's order:
+    // s0 = P0 + P1, s1 = s0 + P2, s(2j) = (P(2j-1) + P(2j)) + P(2j+1), s(2j+1) = (P(2j) + P(2j+1)) + P(2j+2),
+    // s7 = P6 + P7; ca and cb carry (P(2k) + P(2k+1)) and P(2k+1) to the next map
+    float ca[kP2Passes], cb[kP2Passes];
 #pragma unroll
-    for (int k = 0; k < kP2Passes; ++k) {
-        const int p = threadIdx.x + 256 * k;
-        carry23[k] = carry3[k] = 0.f;
-        int x = 0, y = 0;
-        if (p < kP2Px) p2_pixel(p, &x, &y);
-        if (p < kP2Px && need_row(y)) {
-            const f2_t a = pool_l2_pair(S, W, 0, 0, x, y, nz), b = pool_l2_pair(S, W, 1, 1, x, y, nz);
-            const float P0 = f2_lo(a), P1 = f2_hi(a), P2 = f2_lo(b), P3 = f2_hi(b);
-            const float s01 = fadd(P0, P1);
-            S.s2[0][y][x] = s01;
-            S.s2[1][y][x] = fadd(s01, P2);
-            S.s2[2][y][x] = fadd(fadd(P1, P2), P3);
-            carry23[k] = fadd(P2, P3);
-            carry3[k] = P3;
+    for (int k = 0; k < 4; ++k) {
+        if (k == 0)
+            cp_async_wait<1>();
+        else
+            cp_async_wait<0>();
+        __syncthreads();  // map k is in shared memory for every thread, and map k - 1's buffer is free
+        if (k == 0 && gating) {
+            live = 0u;
+#pragma unroll
+            for (int w = 0; w < kK2TileY / 2; ++w) live |= (s_live[w] ? 1u : 0u) << w;
         }
-    }
-    __syncthreads();
-    // second half: pooled L2 maps 4-7, sums 3-7
-    load_back_half<kCoherent>(S, s1, L, sx0, sy0, 1);
-    __syncthreads();
+        if (k == 1 || k == 2) load_back_map_async(S, s1, L, sx0, sy0, k + 1);
+        const float(*T)[kS1TW] = S.s1[k & 1];
 #pragma unroll
-    for (int k = 0; k < kP2Passes; ++k) {
-        const int p = threadIdx.x + 256 * k;
-        int x = 0, y = 0;
-        if (p < kP2Px) p2_pixel(p, &x, &y);
-        if (p < kP2Px && need_row(y)) {
-            const f2_t a = pool_l2_pair(S, W, 2, 0, x, y, nz), b = pool_l2_pair(S, W, 3, 1, x, y, nz);
-            const float P4 = f2_lo(a), P5 = f2_hi(a), P6 = f2_lo(b), P7 = f2_hi(b);
-            S.s2[3][y][x] = fadd(carry23[k], P4);
-            S.s2[4][y][x] = fadd(fadd(carry3[k], P4), P5);
-            S.s2[5][y][x] = fadd(fadd(P4, P5), P6);
-            const float s67 = fadd(P6, P7);
-            S.s2[6][y][x] = fadd(fadd(P5, P6), P7);
-            S.s2[7][y][x] = s67;
+        for (int kk = 0; kk < kP2Passes; ++kk) {
+            const int p = threadIdx.x + 256 * kk;
+            int x = 0, y = 0;
+            if (p < kP2Px) p2_pixel(p, &x, &y);
+            if (p < kP2Px && need_row(y)) {
+                const f2_t a = pool_l2_pair(T, W, k, x, y, nz);
+                const float A = f2_lo(a), B = f2_hi(a);
+                if (k == 0) {
+                    const float s01 = fadd(A, B);
+                    S.s2[0][y][x] = s01;
+                    ca[kk] = s01;
+                } else {
+                    S.s2[2 * k - 1][y][x] = fadd(ca[kk], A);
+                    S.s2[2 * k][y][x] = fadd(fadd(cb[kk], A), B);
+                    if (k < 3) ca[kk] = fadd(A, B);
+                    else S.s2[7][y][x] = fadd(A, B);
+                }
+                cb[kk] = B;
+            }
         }
     }
     __syncthreads();
