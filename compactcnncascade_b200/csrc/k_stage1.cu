@@ -10,8 +10,9 @@
 //        a stored image is read instead where the caller gives one), runs the 4x4 conv + folded
 //        BN/LReLU + 2x2 max for the 4 L1 maps and writes the 4 neighbour-map sums that L2 consumes
 //        (S1 arena).
-// back:  one CTA per 32x16 tile of response pixels. It stages the S1 tile (4 x 42 x 72, two maps at
-//        a time) in shared memory, computes the 8 pooled L2 maps and their sums on the 35 x 20 halo
+// back:  one CTA per 32x16 tile of response pixels. It stages the S1 tile (4 x 42 x 72) one map at a
+//        time through two shared-memory buffers (asynchronous copies of the next map overlap the
+//        current one's compute), computes the 8 pooled L2 maps and their sums on the 35 x 20 halo
 //        tile, then every thread finishes two vertically adjacent response pixels: the 16 L3 maps
 //        (4w x 5h), the 52 hidden neurons and the output neuron.
 // Both kernels come in two register budgets (3 or 4 resident 256-thread blocks per SM), chosen per
