@@ -6,8 +6,9 @@
 // mulCN_add_tanhW (:646-672), mulC/mulC1_add (:952-984), tanhW (:673-690).
 //
 // front: one CTA per 32x16 tile of pooled L1 pixels of one level. The CTA resamples its (67 x 35)
-//        input tile of the level image straight from the gray frame (the pyramid is never stored;
-//        a stored image is read instead where the caller gives one), runs the 4x4 conv + folded
+//        input tile straight from the gray frame (the pyramid is never stored; a stored image is read
+//        instead where the caller gives one; with the learned gate each warp resamples only the 7
+//        rows of its own two pooled rows and runs on its own), runs the 4x4 conv + folded
 //        BN/LReLU + 2x2 max for the 4 L1 maps and writes the 4 neighbour-map sums that L2 consumes
 //        (S1 arena).
 // back:  one CTA per 32x16 tile of response pixels. It stages the S1 tile (4 x 42 x 72) one map at a
@@ -79,16 +80,23 @@ __device__ __forceinline__ void load_front_tile(FrontTile& T, const float* __res
     }
 }
 
-// The front tile straight from the gray frame: every level pixel of the (67 x 35) tile resampled the
-// way the pyramid kernel writes it (copy, nearest neighbour, or bilinear on the 12-bit fixed-point
-// steps; RunCPUDetect, cnn_detector_v3.cpp:2090-2104, with ImageResizer, image_resize.cpp:46-122,
-// 393-541), so the level image is never stored. Thread (g, c) takes tile column c < 64 (its column
-// sample in registers) and rows g, g + 4, ... of it, so a warp reads 32 neighbouring columns of the
-// same gray rows; columns 64-66 follow, one sample a thread. Pixels outside the level read as 0, like
-// the zero columns past a stored level image's width. The gray frame was written by an earlier
-// launch (read-only path).
+// The input rows of one warp of a gated front tile: warp w computes pooled rows 2w and 2w + 1 from
+// tile rows 4w .. 4w + 6, held here as local rows 0..6, row r next to row r + 2 (columns split by
+// parity, as in FrontTile). Rows 4w + 4 .. 4w + 6 are also the next warp's first three; each warp
+// resamples its own copy, so no block barrier separates resampling and compute.
+struct FrontWarpRows {
+    float2 p[5][2][kInWh];
+    __device__ __forceinline__ void put(int r, int c, float v) {
+        if (r <= 4) p[r][c & 1][c >> 1].x = v;
+        if (r >= 2) p[r - 2][c & 1][c >> 1].y = v;
+    }
+};
+
 struct FrontSmem {
-    FrontTile T;
+    union {
+        FrontTile T;                    // the block's whole input tile (full scan, or a stored level image)
+        FrontWarpRows w[kK1TileY / 2];  // each warp's own input rows (gated scan from the gray frame)
+    };
 };
 
 // level pixel (x, y) = tile (c, r) from its column sample sx
@@ -105,9 +113,17 @@ __device__ __forceinline__ float resample_px(const GrayRef& G, const LevelDesc& 
     return fadd(fmul(top, sy.c), fmul(bot, sy.f));
 }
 
-// rows: bit r set = tile row r is read by a warp that computes (the others are left as they are)
-__device__ __forceinline__ void resample_front_tile(FrontSmem& S, const GrayRef& G, const LevelDesc& L, int ix0, int iy0,
-                                                    unsigned long long rows) {
+// Front-tile input straight from the gray frame: every level pixel resampled the way the pyramid
+// kernel writes it (copy, nearest neighbour, or bilinear on the 12-bit fixed-point steps;
+// RunCPUDetect, cnn_detector_v3.cpp:2090-2104, with ImageResizer, image_resize.cpp:46-122, 393-541),
+// so the level image is never stored. Pixels outside the level read as 0, like the zero columns past
+// a stored level image's width. The gray frame was written by an earlier launch (read-only path).
+//
+// The whole (67 x 35) tile by the block (the full scan: every warp computes, so no row is resampled
+// twice): thread (g, c) takes tile column c < 64 (its column sample in registers) and rows g, g + 4,
+// ... of it, so a warp reads 32 neighbouring columns of the same gray rows; columns 64-66 follow, one
+// sample a thread.
+__device__ __forceinline__ void resample_front_tile(FrontTile& T, const GrayRef& G, const LevelDesc& L, int ix0, int iy0) {
     static_assert(kInW == 67 && kInH == 35, "64 + 3 columns, 35 rows in 4 row groups");
     {
         const int c = threadIdx.x & 63, g = threadIdx.x >> 6;
@@ -115,12 +131,30 @@ __device__ __forceinline__ void resample_front_tile(FrontSmem& S, const GrayRef&
 #pragma unroll
         for (int k = 0; k < (kInH + 3) / 4; ++k) {
             const int r = g + 4 * k;
-            if (r < kInH && ((rows >> r) & 1ull)) S.T.put(r, c, resample_px(G, L, sx, ix0 + c, iy0 + r));
+            if (r < kInH) T.put(r, c, resample_px(G, L, sx, ix0 + c, iy0 + r));
         }
     }
     if (threadIdx.x < 3 * kInH) {
         const int c = 64 + threadIdx.x % 3, r = threadIdx.x / 3;
-        if ((rows >> r) & 1ull) S.T.put(r, c, resample_px(G, L, sample_col(ix0 + c, L.sclx, G.w), ix0 + c, iy0 + r));
+        T.put(r, c, resample_px(G, L, sample_col(ix0 + c, L.sclx, G.w), ix0 + c, iy0 + r));
+    }
+}
+
+// One warp's 7 input rows from tile row y0 on (the gated scan, where warps run on their own): lane l
+// takes tile columns l and l + 32 (their column samples in registers); columns 64-66 of the rows
+// follow, one sample a lane.
+__device__ __forceinline__ void resample_warp_rows(FrontWarpRows& R, const GrayRef& G, const LevelDesc& L, int ix0, int y0, int lane) {
+    const AxisSample sa = sample_col(ix0 + lane, L.sclx, G.w), sb = sample_col(ix0 + lane + 32, L.sclx, G.w);
+#pragma unroll
+    for (int r = 0; r < 7; ++r) {
+        const float va = resample_px(G, L, sa, ix0 + lane, y0 + r);
+        const float vb = resample_px(G, L, sb, ix0 + lane + 32, y0 + r);
+        R.put(r, lane, va);
+        R.put(r, lane + 32, vb);
+    }
+    if (lane < 21) {
+        const int c = 64 + lane % 3, r = lane / 3;
+        R.put(r, c, resample_px(G, L, sample_col(ix0 + c, L.sclx, G.w), ix0 + c, y0 + r));
     }
 }
 
@@ -145,8 +179,9 @@ __device__ __forceinline__ bool gate_live(const GateCells& cells, const LevelDes
                         gate_cell_hi(py1, m, cells.h16));
 }
 
-// Front tile t of level L: its (67 x 35) level-image tile staged in S.T (resampled from the gray
-// frame G when kFromGray, else read from the stored level images limg), then the 4x4 conv + folded
+// Front tile t of level L: its (67 x 35) level-image tile in shared memory (resampled from the gray
+// frame G when kFromGray, by the block, or with the gate by each warp for its own 7 rows; else read
+// from the stored level images limg by the block), then the 4x4 conv + folded
 // BN/LReLU + 2x2 max of the 4 L1 maps for 32 x 16 pooled pixels (two vertically adjacent pixels a
 // thread) and the 4 neighbour-map sums written to the S1 arena. kCoherent: a stored level image was
 // written earlier in the same launch (read through L2, not the read-only path).
@@ -162,43 +197,53 @@ __device__ __forceinline__ void front_tile(const Stage1W& W, FrontSmem& S, const
     const int py0 = (t / L.k1_tiles_x) * kK1TileY;
     const int ix0 = 2 * px0, iy0 = 2 * py0;
 
-    // with the gate: which warps have a live pixel downstream (warp w computes pooled rows 2w, 2w + 1 from
-    // tile rows 4w .. 4w + 6, so only those rows of live warps are resampled)
-    uint32_t live = 0xffu;
-    unsigned long long rows = ~0ull;
-    if (gate_gating(cells)) {
-        __shared__ int s_flive[kK1TileY / 2];
-        if ((threadIdx.x & 31) == 0) {
-            const int ya = py0 + 2 * (threadIdx.x >> 5), yb = ya + 1, xa = px0, xb = px0 + kK1TileX - 1;
-            s_flive[threadIdx.x >> 5] = gate_live(cells, L, ((xa - 3 + 1) >> 1) - 3, xb >> 1, ((ya - 3 + 1) >> 1) - 4, yb >> 1) ? 1 : 0;
-        }
-        __syncthreads();
-        live = 0u;
-        rows = 0ull;
-#pragma unroll
-        for (int w = 0; w < kK1TileY / 2; ++w)
-            if (s_flive[w]) {
-                live |= 1u << w;
-                rows |= 0x7full << (4 * w);
-            }
-    }
-    if constexpr (kFromGray)
-        resample_front_tile(S, G, L, ix0, iy0, rows);
-    else
-        load_front_tile<kCoherent>(S.T, limg + L.img_off, L, ix0, iy0);
-    __syncthreads();
-    const FrontTile& T = S.T;
-
     const int qx = threadIdx.x & (kK1TileX - 1);
     const int qy = (threadIdx.x >> 5) * 2;
-    if (!((live >> (threadIdx.x >> 5)) & 1u)) return;  // no live response pixel downstream of this warp
+    // with the gate: whether the warp has a live pixel downstream (warp w computes pooled rows 2w, 2w + 1)
+    auto warp_live = [&]() {
+        const int ya = py0 + qy, yb = ya + 1, xa = px0, xb = px0 + kK1TileX - 1;
+        return gate_live(cells, L, ((xa - 3 + 1) >> 1) - 3, xb >> 1, ((ya - 3 + 1) >> 1) - 4, yb >> 1);
+    };
+    const float2(*In)[2][kInWh];  // In[r] = (input row 2qy + r, row 2qy + r + 2), r = 0..4
+    if (kFromGray && gate_gating(cells)) {
+        // with the gate every warp runs on its own: its liveness, its 7 input rows, its two pooled rows
+        // (the rows a live warp shares with a dead neighbour are not resampled twice over the tile, and
+        // no warp waits for the block)
+        int lv = 0;
+        if ((threadIdx.x & 31) == 0) lv = warp_live() ? 1 : 0;
+        if (!__shfl_sync(0xffffffffu, lv, 0)) return;  // no live response pixel downstream of this warp
+        FrontWarpRows& R = S.w[threadIdx.x >> 5];
+        resample_warp_rows(R, G, L, ix0, iy0 + 2 * qy, threadIdx.x & 31);
+        __syncwarp();
+        In = R.p;
+    } else if (kFromGray) {
+        // the full scan: the block resamples the tile once
+        resample_front_tile(S.T, G, L, ix0, iy0);
+        __syncthreads();
+        In = &S.T.p[2 * qy];
+    } else {
+        uint32_t live = 0xffu;
+        if (gate_gating(cells)) {
+            __shared__ int s_flive[kK1TileY / 2];
+            if ((threadIdx.x & 31) == 0) s_flive[threadIdx.x >> 5] = warp_live() ? 1 : 0;
+            __syncthreads();
+            live = 0u;
+#pragma unroll
+            for (int w = 0; w < kK1TileY / 2; ++w)
+                if (s_flive[w]) live |= 1u << w;
+        }
+        load_front_tile<kCoherent>(S.T, limg + L.img_off, L, ix0, iy0);
+        __syncthreads();
+        if (!((live >> (threadIdx.x >> 5)) & 1u)) return;  // no live response pixel downstream of this warp
+        In = &S.T.p[2 * qy];
+    }
     const f2_t nz = f2_ld(W.negzero);
     // pr[r][c] = (input row 2qy+r, row 2qy+r+2) at column 2qx+c: the windows of both pixels
     f2_t pr[5][5];
 #pragma unroll
     for (int r = 0; r < 5; ++r)
 #pragma unroll
-        for (int c = 0; c < 5; ++c) pr[r][c] = *reinterpret_cast<const f2_t*>(&T.p[2 * qy + r][c & 1][qx + (c >> 1)]);
+        for (int c = 0; c < 5; ++c) pr[r][c] = *reinterpret_cast<const f2_t*>(&In[r][c & 1][qx + (c >> 1)]);
 
     // packed over the two pixels (lo = row qy, hi = row qy + 1)
     f2_t P[4];
