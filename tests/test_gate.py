@@ -75,3 +75,34 @@ def test_shipped_weights_load():
     assert p.shape == (700,) and np.all(np.isfinite(p))
     meta = gate.load_meta()
     assert meta["train_frames"] >= 1000 and meta["eval_frames"] >= 100
+
+
+def test_operating_point_rule():
+    """Of the evaluated (threshold, margin) pairs with >= 99.5 % box recall, the one that runs the fewest
+    back tiles (ties: the higher threshold); none reaching it: the lowest threshold, one cell of margin."""
+    ev = [{"threshold": 0.1, "margin": 8, "box_recall": 0.999, "back_tiles_run": 0.30},
+          {"threshold": 0.3, "margin": 8, "box_recall": 0.996, "back_tiles_run": 0.26},
+          {"threshold": 0.5, "margin": 8, "box_recall": 0.990, "back_tiles_run": 0.22},
+          {"threshold": 0.4, "margin": 16, "box_recall": 0.997, "back_tiles_run": 0.26}]
+    assert gate._operating_point(ev, [0.1, 0.3, 0.4, 0.5]) == (0.4, 16)
+    assert gate._operating_point(ev[:3], [0.1, 0.3, 0.5]) == (0.3, 8)
+    assert gate._operating_point([dict(r, box_recall=0.98) for r in ev], [0.1, 0.3, 0.4, 0.5]) == (0.1, 16)
+
+
+def test_shipped_operating_point_follows_its_evaluation():
+    """The operating point recorded with the shipped weights is the rule's choice on the committed
+    1,000-frame held-out evaluation, and it keeps at least 99.5 % of the plain cascade's boxes there."""
+    import json
+    import os
+    rec = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "profiles", "gate_heldout_eval_1080p.json")
+    if not os.path.exists(gate.WEIGHTS_1080P) or not os.path.exists(rec):
+        pytest.skip("no trained weights or evaluation record")
+    with open(rec) as fh:
+        r = json.load(fh)
+    thr = sorted({e["threshold"] for e in r["eval"]})
+    op = gate._operating_point(r["eval"], thr)
+    assert op == (r["operating_threshold"], r["operating_margin"])
+    meta = gate.load_meta()
+    assert (meta["operating_threshold"], meta["operating_margin"]) == op
+    chosen = [e for e in r["eval"] if (e["threshold"], e["margin"]) == op]
+    assert len(chosen) == 1 and chosen[0]["box_recall"] >= 0.995 and r["eval_frames"] >= 1000
