@@ -29,7 +29,7 @@ import sys
 from . import _capi
 
 TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "schedules.json")
-KNOBS = (("frame_slots", (4, 8, 12, 16)), ("window_ctas_per_sm", (2, 3, 4, 5, 6)), ("front_blocks_per_sm", (3, 4)),
+KNOBS = (("frame_slots", (4, 8, 12, 16, 24, 32)), ("window_ctas_per_sm", (2, 3, 4, 5, 6)), ("front_blocks_per_sm", (3, 4)),
          ("back_blocks_per_sm", (3, 4)), ("batch_frames", (0, 1, 2, 4, 8)), ("batch_blocks_per_sm", (1, 2, 3, 4)))
 DEFAULTS = {"frame_slots": 8, "window_ctas_per_sm": 4, "front_blocks_per_sm": 3, "back_blocks_per_sm": 4, "batch_frames": 0,
             "batch_blocks_per_sm": 3}
